@@ -1,0 +1,255 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+The oracle restates the reference's Newton-step linear solve in plain C
+(``maspcg_oracle.c``).  It is the parity checker for the CUDA path and the
+timed CPU baseline; nothing in ``agipc_learning_b200`` imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+PRECOND_DIAG3 = 0
+PRECOND_MAS32 = 2
+PRECOND_NONE = -1
+GATE_RZ = 0
+GATE_EUCLID = 1
+STATUS_NAMES = {1: "converged", 2: "iteration_cap", 3: "nonpositive_curvature", 4: "nonfinite", 5: "invalid_rz"}
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "liboracle.so")
+
+
+class _PcgOpts(ctypes.Structure):
+    _fields_ = [("precond", ctypes.c_int), ("gate", ctypes.c_int), ("tol", ctypes.c_double),
+                ("max_iter", ctypes.c_int), ("nb", ctypes.c_int), ("fem_offset", ctypes.c_int),
+                ("fem_count", ctypes.c_int), ("abd_bodies", ctypes.c_int), ("replay_checks", ctypes.c_int)]
+
+
+class _PcgResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("status", ctypes.c_int), ("rz0", ctypes.c_double),
+                ("rz_last", ctypes.c_double), ("rel_res_recursive", ctypes.c_double),
+                ("rel_res_true", ctypes.c_double)]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P, I, D, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+        sig = {
+            "orc_convert_triplets": (I, [I, P, P, P, P, P, P]),
+            "orc_sym_spmv": (None, [D, P, P, P, I, I, P, D, P]),
+            "orc_upper_to_full_bcsr": (I, [I, I, P, P, P, P, P, P]),
+            "orc_bcsr_spmv": (None, [I, P, P, P, P, P]),
+            "orc_mas_create": (P, [I, I, P, P, P, I, P, I, P]),
+            "orc_mas_free": (None, [P]),
+            "orc_compute_num_levels": (I, [I]),
+            "orc_mas_levelnum": (I, [P]),
+            "orc_hierarchy_capacity": (LL, [LL, LL, LL, LL]),
+            "orc_mas_going_next_capacity": (LL, [P]),
+            "orc_mas_reorder": (I, [P, P, I]),
+            "orc_mas_get_hierarchy": (None, [P, P, P, P, P, P, P]),
+            "orc_mas_total_clusters": (I, [P]),
+            "orc_mas_prepare_hessian": (None, [P, P, P, P, P, I, I]),
+            "orc_mas_get_domains": (None, [P, P, P]),
+            "orc_mas_precondition": (None, [P, P, P]),
+            "orc_local_checks": (None, [I, P, P, P]),
+            "orc_diag3_inverse": (None, [I, I, P, P, P, P]),
+            "orc_abd_inverse": (I, [I, I, P, P, P, P]),
+            "orc_pcg": (I, [ctypes.POINTER(_PcgOpts), P, P, P, I, P, P, P, ctypes.POINTER(_PcgResult)]),
+            "orc_num_threads": (I, []),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def convert_triplets(rows, cols, vals):
+    n = len(rows)
+    r, c, v = _c(rows, np.int32), _c(cols, np.int32), _c(vals, np.float64).reshape(n, 9)
+    orow, ocol, oval = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros((n, 9))
+    u = lib().orc_convert_triplets(n, _p(r), _p(c), _p(v), _p(orow), _p(ocol), _p(oval))
+    return orow[:u].copy(), ocol[:u].copy(), oval[:u].copy()
+
+
+def sym_spmv(a, vals, rows, cols, x, b=0.0, y=None):
+    x = _c(x, np.float64)
+    y = np.zeros_like(x) if y is None else _c(y, np.float64).copy()
+    v = _c(vals, np.float64)
+    lib().orc_sym_spmv(float(a), _p(v), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)), len(rows), len(x), _p(x),
+                       float(b), _p(y))
+    return y
+
+
+def upper_to_full_bcsr(nb, rows, cols, vals):
+    n = len(rows)
+    rowptr = np.zeros(nb + 1, np.int32)
+    col = np.zeros(2 * n + 1, np.int32)
+    fv = np.zeros((2 * n + 1, 9))
+    t = lib().orc_upper_to_full_bcsr(nb, n, _p(_c(rows, np.int32)), _p(_c(cols, np.int32)),
+                                     _p(_c(vals, np.float64)), _p(rowptr), _p(col), _p(fv))
+    return rowptr, col[:t].copy(), fv[:t].copy()
+
+
+def bcsr_spmv(rowptr, col, vals, x):
+    x = _c(x, np.float64)
+    y = np.zeros_like(x)
+    lib().orc_bcsr_spmv(len(rowptr) - 1, _p(_c(rowptr, np.int32)), _p(_c(col, np.int32)), _p(_c(vals, np.float64)),
+                        _p(x), _p(y))
+    return y
+
+
+def compute_num_levels(n):
+    return lib().orc_compute_num_levels(int(n))
+
+
+def hierarchy_capacity(vertices, mapped, levels, bank):
+    return lib().orc_hierarchy_capacity(vertices, mapped, levels, bank)
+
+
+class Mas32:
+    """TraditionalMAS32Preconditioner restated on the CPU."""
+
+    def __init__(self, vert_num, node_offset, neighbor_start, neighbor_num, neighbor_list, part_map_real,
+                 real_map_part):
+        self._keep = [_c(neighbor_start, np.uint32), _c(neighbor_num, np.uint32),
+                      _c(neighbor_list if len(neighbor_list) else np.zeros(1), np.uint32),
+                      _c(part_map_real, np.int32), _c(real_map_part, np.int32)]
+        s, n, l, pm, rm = self._keep
+        self.h = lib().orc_mas_create(int(vert_num), int(node_offset), _p(s), _p(n), _p(l), int(len(neighbor_list)),
+                                      _p(pm), int(len(pm)), _p(rm))
+        if not self.h:
+            raise ValueError("invalid MAS32 inputs")
+        self.nv = int(vert_num)
+        self.c0 = len(pm)
+        self.levelnum = lib().orc_mas_levelnum(self.h)
+        self.total_clusters = 0
+
+    @classmethod
+    def from_system(cls, s):
+        return cls(s.fem_count, s.node_offset, s.neighbor_start, s.neighbor_num, s.neighbor_list, s.part_map_real,
+                   s.real_map_part)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_mas_free(self.h)
+            self.h = None
+
+    def reorder(self, pairs=None):
+        p = None if pairs is None or len(pairs) == 0 else _c(pairs, np.int32).reshape(-1, 4)
+        self.total_clusters = lib().orc_mas_reorder(self.h, _p(p), 0 if p is None else len(p))
+        return self.total_clusters
+
+    def hierarchy(self):
+        L = self.levelnum
+        cap = lib().orc_mas_going_next_capacity(self.h)
+        fm = np.zeros(self.nv, np.uint32)
+        cst = np.zeros(self.nv * L, np.int32)
+        gn = np.zeros(cap, np.int32)
+        ls = np.zeros(2 * (L + 1), np.int32)
+        ct = np.zeros(self.nv * 6, np.int32)
+        po = np.zeros(self.c0 // 32, np.int32)
+        lib().orc_mas_get_hierarchy(self.h, _p(fm), _p(cst), _p(gn), _p(ls), _p(ct), _p(po))
+        return {"fine_mask": fm, "coarse_space_tables": cst.reshape(L, self.nv), "going_next": gn,
+                "level_size": ls.reshape(L + 1, 2), "coarse_table": ct.reshape(self.nv, 6),
+                "prefix_original": po, "total_clusters": self.total_clusters, "levelnum": L}
+
+    def prepare_hessian(self, vals, rows, cols, indices=None, offset=0):
+        n = len(rows) if indices is None else len(indices)
+        self._mat = (_c(vals, np.float64), _c(rows, np.int32), _c(cols, np.int32))
+        ind = None if indices is None else _c(indices, np.uint32)
+        lib().orc_mas_prepare_hessian(self.h, _p(self._mat[0]), _p(self._mat[1]), _p(self._mat[2]), _p(ind),
+                                      int(offset), int(n))
+
+    def domains(self):
+        nd = self.total_clusters // 32
+        p64 = np.zeros((nd, 528, 9))
+        i32 = np.zeros((nd, 528, 9), np.float32)
+        lib().orc_mas_get_domains(self.h, _p(p64), _p(i32))
+        return p64, i32
+
+    def precondition(self, R):
+        R = _c(R, np.float64)
+        Z = np.zeros_like(R)
+        lib().orc_mas_precondition(self.h, _p(R), _p(Z))
+        return Z
+
+
+def local_checks(packed64, inverse32):
+    packed64 = _c(packed64, np.float64)
+    inverse32 = _c(inverse32, np.float32)
+    n = packed64.shape[0]
+    out = np.zeros((n, 7))
+    lib().orc_local_checks(n, _p(packed64), _p(inverse32), _p(out))
+    keys = ["local_finite", "inverse_finite", "local_spd", "inverse_spd", "minimum_local_diagonal",
+            "minimum_inverse_diagonal", "inverse_residual"]
+    return [dict(zip(keys, row)) for row in out]
+
+
+def diag3_inverse(nb, rows, cols, vals):
+    out = np.zeros((nb, 9))
+    lib().orc_diag3_inverse(nb, len(rows), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)), _p(_c(vals, np.float64)),
+                            _p(out))
+    return out
+
+
+def abd_inverse(bodies, rows, cols, vals):
+    out = np.zeros((bodies, 12, 12))
+    ok = lib().orc_abd_inverse(bodies, len(rows), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)),
+                               _p(_c(vals, np.float64)), _p(out))
+    return out, bool(ok)
+
+
+def pcg(vals, rows, cols, nb, b, *, precond=PRECOND_MAS32, gate=GATE_RZ, tol=1e-4, max_iter=0, fem_offset=0,
+        fem_count=0, abd_bodies=0, mas: Mas32 | None = None, replay_checks=False):
+    """PCGSolver::pcg restated; returns (x, result dict)."""
+    o = _PcgOpts(precond, gate, tol, max_iter, nb, fem_offset, fem_count, abd_bodies, 1 if replay_checks else 0)
+    res = _PcgResult()
+    b = _c(b, np.float64)
+    x = np.zeros_like(b)
+    lib().orc_pcg(ctypes.byref(o), _p(_c(vals, np.float64)), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)),
+                  len(rows), None if mas is None else mas.h, _p(b), _p(x), ctypes.byref(res))
+    return x, {"iterations": res.iterations, "status": STATUS_NAMES.get(res.status, res.status), "rz0": res.rz0,
+               "rz_last": res.rz_last, "rel_res_recursive": res.rel_res_recursive, "rel_res_true": res.rel_res_true}
+
+
+def solve_system(s, *, precond=PRECOND_MAS32, gate=GATE_RZ, tol=1e-4, max_iter=0, replay_checks=False):
+    """Full reference pipeline on a synth.System: MAS build then PCG."""
+    mas = None
+    if precond == PRECOND_MAS32 and s.fem_count > 0:
+        mas = Mas32.from_system(s)
+        mas.reorder(s.pairs)
+        sel = np.nonzero((s.rows >= s.fem_offset) & (s.rows < s.fem_offset + s.fem_count) &
+                         (s.cols >= s.fem_offset) & (s.cols < s.fem_offset + s.fem_count))[0].astype(np.uint32)
+        mas.prepare_hessian(s.vals, s.rows, s.cols, sel, s.fem_offset)
+    x, r = pcg(s.vals, s.rows, s.cols, s.nb, s.b, precond=precond, gate=gate, tol=tol, max_iter=max_iter,
+               fem_offset=s.fem_offset, fem_count=s.fem_count, abd_bodies=s.abd_bodies, mas=mas,
+               replay_checks=replay_checks)
+    return x, r, mas
+
+
+def num_threads():
+    return lib().orc_num_threads()
