@@ -1,0 +1,546 @@
+// capi.cu -- the extern "C" boundary declared in include/maspcg.h.
+//
+// Every entry point validates its arguments, turns exceptions into a
+// maspcg_status and keeps the message for maspcg_last_error; nothing aborts.
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "maspcg_internal.cuh"
+
+using maspcg::DBuf;
+using maspcg::Error;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+bool is_device_ptr(const void* p)
+{
+  if (!p) return false;
+  cudaPointerAttributes at{};
+  const cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// A device view of a caller array: the caller's pointer when it is device
+// memory, else a staged copy.
+template <typename T>
+const T* device_in(maspcg_handle* h, const T* user, size_t count, DBuf<T>& stage)
+{
+  if (count == 0) return nullptr;
+  MREQ(user != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null array argument");
+  if (is_device_ptr(user)) return user;
+  stage.resize(count);
+  MCK(cudaMemcpyAsync(stage.get(), user, count * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+  return stage.get();
+}
+
+template <typename T>
+std::vector<T> host_copy(maspcg_handle* h, const T* user, size_t count)
+{
+  std::vector<T> v(count);
+  if (!count) return v;
+  MREQ(user != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null array argument");
+  if (is_device_ptr(user)) {
+    MCK(cudaMemcpyAsync(v.data(), user, count * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+  } else {
+    std::copy(user, user + count, v.begin());
+  }
+  return v;
+}
+
+template <typename F>
+maspcg_status guard(maspcg_handle* h, F&& f)
+{
+  if (!h) return MASPCG_ERR_NULL_HANDLE;
+  try {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev != h->device) MCK(cudaSetDevice(h->device));
+    f();
+    h->last_error.clear();
+    return MASPCG_OK;
+  } catch (const Error& e) {
+    h->last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    h->last_error = "host allocation failed";
+    return MASPCG_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    h->last_error = e.what();
+    return MASPCG_ERR_CUDA;
+  }
+}
+
+int compute_num_levels(int vert_num)
+{
+  // computeNumLevels (TraditionalMAS32Preconditioner.cu:2142-2161)
+  int n_level = 1;
+  int level_sz = (vert_num + 31) / 32 * 32;
+  while (level_sz > 32) {
+    level_sz /= 32;
+    n_level++;
+    level_sz = (level_sz + 31) / 32 * 32;
+  }
+  n_level += 1;
+  return n_level > 6 ? 6 : n_level;
+}
+
+long long hierarchy_capacity(long long vertices, long long mapped, long long levels, long long bank)
+{
+  // gipc::hierarchy_capacity (gipc/hierarchy_capacity.h:10-22)
+  const long long base = std::max(vertices, mapped);
+  if (!base || !levels) return 0;
+  const long long maximum = (long long)(((unsigned long long)-1 >> 1) / sizeof(unsigned int));
+  MREQ(bank && base <= maximum && bank - 1 <= maximum - base, MASPCG_ERR_CAPACITY, "MAS hierarchy alignment overflow");
+  const long long padded = (base + bank - 1) / bank * bank;
+  MREQ(padded <= maximum / levels, MASPCG_ERR_CAPACITY, "MAS hierarchy capacity overflow");
+  MREQ(padded * levels <= 0x7fffffffLL, MASPCG_ERR_CAPACITY, "MAS hierarchy exceeds 32-bit indices");
+  return padded * levels;
+}
+
+void alloc_vectors(maspcg_handle* h)
+{
+  const size_t n = 3 * (size_t)h->nb_int;
+  const size_t es = maspcg::vec_elem_size(h);
+  for (auto* b : {&h->vx, &h->vr, &h->vz, &h->vp, &h->vap}) b->resize(n * es);
+  h->b64.resize(n);
+  h->x64.resize(n);
+  h->r64.resize(n);
+  const size_t io = 3 * (size_t)std::max(h->nb, h->nb_int);
+  h->io_a.resize(io);
+  h->io_b.resize(io);
+  const int parts = 16 * h->sm_count + 64;
+  h->partial.resize(parts);
+  h->partial_rz.resize(parts);
+}
+
+}  // namespace
+
+extern "C" {
+
+MASPCG_API void maspcg_config_default(maspcg_config* c)
+{
+  if (!c) return;
+  c->tolerance = 1e-4;
+  c->max_iter_ratio = 0.3;
+  c->max_iterations = 0;
+  c->gate = MASPCG_GATE_RZ;
+  c->precision = MASPCG_PREC_REFERENCE;
+  c->inverse_storage = MASPCG_INV_FP32;
+  c->preconditioner = MASPCG_PRECOND_MAS32;
+  c->refinement_period = 16;
+  c->bank_size = 32;
+  c->iterations_per_launch = 8;
+}
+
+MASPCG_API const char* maspcg_status_string(int s)
+{
+  switch (s) {
+    case MASPCG_OK: return "ok";
+    case MASPCG_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case MASPCG_ERR_NULL_HANDLE: return "null handle";
+    case MASPCG_ERR_CUDA: return "CUDA error";
+    case MASPCG_ERR_OUT_OF_MEMORY: return "out of memory";
+    case MASPCG_ERR_NOT_READY: return "not ready (call order)";
+    case MASPCG_ERR_CAPACITY: return "capacity exceeded";
+    case MASPCG_ERR_NO_DEVICE: return "no CUDA device";
+    case MASPCG_ERR_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown status";
+  }
+}
+
+MASPCG_API const char* maspcg_last_error(const maspcg_handle* h)
+{
+  return h ? h->last_error.c_str() : g_create_error.c_str();
+}
+
+MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle** out)
+{
+  g_create_error.clear();
+  if (!out) {
+    g_create_error = "out is null";
+    return MASPCG_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  maspcg_config c;
+  maspcg_config_default(&c);
+  if (cfg) c = *cfg;
+  if (c.bank_size != 32) {
+    g_create_error = "only the 32-vertex MAS bank is supported";
+    return MASPCG_ERR_UNSUPPORTED;
+  }
+  if (!(c.tolerance > 0) || c.precision < 0 || c.precision > 2 || c.gate < 0 || c.gate > 1 ||
+      c.inverse_storage < 0 || c.inverse_storage > 2 ||
+      !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
+        c.preconditioner == MASPCG_PRECOND_NONE) ||
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0)) {
+    g_create_error = "invalid configuration";
+    return MASPCG_ERR_INVALID_ARGUMENT;
+  }
+  if (c.refinement_period <= 0) c.refinement_period = 16;
+  if (c.iterations_per_launch <= 0) c.iterations_per_launch = 8;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    g_create_error = "no CUDA device";
+    return MASPCG_ERR_NO_DEVICE;
+  }
+  maspcg_handle* h = nullptr;
+  try {
+    h = new maspcg_handle();
+    h->cfg = c;
+    MCK(cudaGetDevice(&h->device));
+    MCK(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device));
+    MCK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    MCK(cudaEventCreate(&h->ev0));
+    MCK(cudaEventCreate(&h->ev1));
+    MCK(cudaMallocHost(reinterpret_cast<void**>(&h->h_scal), sizeof(maspcg::PcgScalars)));
+    h->scal.resize(1);
+    h->grid_stream = 4 * h->sm_count;
+    h->failed.resize(4);
+    MCK(cudaMemset(h->failed.get(), 0, 4 * sizeof(int)));
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    if (h) maspcg_destroy(h);
+    return MASPCG_ERR_CUDA;
+  }
+  *out = h;
+  return MASPCG_OK;
+}
+
+MASPCG_API maspcg_status maspcg_destroy(maspcg_handle* h)
+{
+  if (!h) return MASPCG_ERR_NULL_HANDLE;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->h_scal) cudaFreeHost(h->h_scal);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return MASPCG_OK;
+}
+
+MASPCG_API maspcg_status maspcg_set_stream(maspcg_handle* h, void* stream)
+{
+  return guard(h, [&] {
+    MCK(cudaStreamSynchronize(h->stream));
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int collision_node_offset,
+                                          const uint32_t* neighbor_start, const uint32_t* neighbor_num,
+                                          const uint32_t* neighbor_list, int neighbor_list_size,
+                                          const int* part_map_real, int part_map_size, const int* real_map_part)
+{
+  return guard(h, [&] {
+    MREQ(vert_num >= 1, MASPCG_ERR_INVALID_ARGUMENT, "vert_num must be >= 1");
+    MREQ(part_map_size >= vert_num && part_map_size % 32 == 0, MASPCG_ERR_INVALID_ARGUMENT,
+         "part_map_size must be a multiple of 32 and >= vert_num");
+    MREQ(neighbor_list_size >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative neighbor_list_size");
+    const auto st = host_copy(h, neighbor_start, vert_num);
+    const auto nn = host_copy(h, neighbor_num, vert_num);
+    const auto nl = host_copy(h, neighbor_list, (size_t)neighbor_list_size);
+    const auto pmr = host_copy(h, part_map_real, part_map_size);
+    const auto rmp = host_copy(h, real_map_part, vert_num);
+    for (int v = 0; v < vert_num; ++v) {
+      MREQ((long long)st[v] + nn[v] <= neighbor_list_size, MASPCG_ERR_INVALID_ARGUMENT,
+           "neighbour range exceeds the list");
+      MREQ(rmp[v] >= 0 && rmp[v] < part_map_size, MASPCG_ERR_INVALID_ARGUMENT, "real_map_part out of range");
+      MREQ(pmr[rmp[v]] == v, MASPCG_ERR_INVALID_ARGUMENT, "part_map_real / real_map_part disagree");
+    }
+    for (int i = 0; i < neighbor_list_size; ++i)
+      MREQ(nl[i] < (uint32_t)vert_num, MASPCG_ERR_INVALID_ARGUMENT, "neighbour index out of range");
+    int mapped = 0;
+    for (int s = 0; s < part_map_size; ++s) {
+      MREQ(pmr[s] >= -1 && pmr[s] < vert_num, MASPCG_ERR_INVALID_ARGUMENT, "part_map_real out of range");
+      mapped += pmr[s] >= 0;
+    }
+    MREQ(mapped == vert_num, MASPCG_ERR_INVALID_ARGUMENT, "part_map_real must map every vertex once");
+    for (int b = 0; b < part_map_size / 32; ++b)
+      MREQ(pmr[32 * b] >= 0, MASPCG_ERR_INVALID_ARGUMENT, "lane 0 of every 32-slot bank must hold a vertex");
+
+    h->nv = vert_num;
+    h->c0 = part_map_size;
+    h->node_offset = collision_node_offset;
+    h->nlist_size = neighbor_list_size;
+    h->levelnum = compute_num_levels(std::max(part_map_size, vert_num));
+    h->gn_cap = hierarchy_capacity(vert_num, part_map_size, h->levelnum, 32);
+    cudaStream_t s = h->stream;
+    auto up = [&](auto& buf, const auto& vec) {
+      buf.resize(std::max<size_t>(vec.size(), 1));
+      if (!vec.empty())
+        MCK(cudaMemcpyAsync(buf.get(), vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, s));
+    };
+    up(h->nstart, st);
+    up(h->nnum_init, nn);
+    up(h->nlist_init, nl);
+    h->nnum.resize(vert_num);
+    h->nlist.resize(std::max(neighbor_list_size, 1));
+    up(h->pmr, pmr);
+    up(h->rmp, rmp);
+    h->h_pmr = pmr;
+    h->h_rmp = rmp;
+    const int L = h->levelnum;
+    h->fine_mask.resize(vert_num);
+    h->next_mask.resize(vert_num);
+    h->next_prefix.resize(vert_num / 32 + 2);
+    h->next_prefix_sum.resize(vert_num / 32 + 2);
+    h->prefix_orig.resize(part_map_size / 32 + 1);
+    h->prefix_sum_orig.resize(part_map_size / 32 + 1);
+    h->cst.resize((size_t)vert_num * L);
+    h->going_next.resize((size_t)h->gn_cap);
+    MCK(cudaMemsetAsync(h->going_next.get(), 0xff, (size_t)h->gn_cap * 4, s));
+    h->coarse_table.resize((size_t)vert_num * 6);
+    h->level_size.resize(2 * (L + 1));
+    MCK(cudaStreamSynchronize(s));
+    h->has_graph = true;
+    h->has_matrix = h->has_precond = false;
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_set_contacts(maspcg_handle* h, const int* pairs4, int n_pairs)
+{
+  return guard(h, [&] {
+    MREQ(h->has_graph, MASPCG_ERR_NOT_READY, "set_graph first");
+    MREQ(n_pairs >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative pair count");
+    const auto p = host_copy(h, pairs4, 4 * (size_t)n_pairs);
+    for (int i = 0; i < n_pairs; ++i) {
+      int x = p[4 * i], y = p[4 * i + 1], z = p[4 * i + 2], w = p[4 * i + 3];
+      int v[4], cnt;
+      // decoding of _buildCollisionConnection_new (:1550-1962)
+      if (x >= 0) {
+        if (w < 0) w = -w - 1;
+        cnt = 4;
+      } else {
+        x = -x - 1;
+        if (z < 0) {
+          if (y < 0) { y = -y - 1; z = -z - 1; w = -w - 1; cnt = 4; }
+          else cnt = 2;
+        } else if (w < 0) {
+          if (y < 0) { y = -y - 1; w = -w - 1; cnt = 4; }
+          else cnt = 3;
+        } else cnt = 4;
+      }
+      v[0] = x; v[1] = y; v[2] = z; v[3] = w;
+      for (int q = 0; q < cnt; ++q)
+        MREQ(v[q] - h->node_offset < h->nv, MASPCG_ERR_INVALID_ARGUMENT, "contact vertex beyond the FEM range");
+    }
+    h->pairs.resize(std::max<size_t>(4 * (size_t)n_pairs, 4));
+    if (n_pairs)
+      MCK(cudaMemcpyAsync(h->pairs.get(), p.data(), p.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    h->n_pairs = n_pairs;
+    h->has_precond = false;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* values9, const int* rows,
+                                                const int* cols, int n_blocks, int block_rows, int fem_offset_blocks,
+                                                int abd_body_count)
+{
+  return guard(h, [&] {
+    MREQ(n_blocks >= 1 && block_rows >= 1, MASPCG_ERR_INVALID_ARGUMENT, "empty matrix");
+    MREQ(fem_offset_blocks >= 0 && abd_body_count >= 0 && 4LL * abd_body_count <= block_rows,
+         MASPCG_ERR_INVALID_ARGUMENT, "invalid offsets");
+    MREQ(n_blocks <= (1 << 29), MASPCG_ERR_CAPACITY, "too many blocks");
+    if (h->cfg.preconditioner == MASPCG_PRECOND_MAS32) {
+      MREQ(h->has_graph, MASPCG_ERR_NOT_READY, "MAS32 needs set_graph before set_matrix_bcoo");
+      MREQ(4LL * abd_body_count <= fem_offset_blocks, MASPCG_ERR_INVALID_ARGUMENT, "ABD rows overlap the FEM range");
+      MREQ((long long)fem_offset_blocks + h->nv <= block_rows, MASPCG_ERR_INVALID_ARGUMENT,
+           "FEM range exceeds block_rows");
+    }
+    h->nb = block_rows;
+    h->fem_off = fem_offset_blocks;
+    h->abd_bodies = abd_body_count;
+    h->n_in = n_blocks;
+    const double* v = device_in(h, values9, (size_t)9 * n_blocks, h->in_vals);
+    const int* r = device_in(h, rows, (size_t)n_blocks, h->in_rows);
+    const int* c = device_in(h, cols, (size_t)n_blocks, h->in_cols);
+    maspcg::build_internal_matrix(h, v, r, c, n_blocks);
+    alloc_vectors(h);
+    MCK(cudaStreamSynchronize(h->stream));
+    h->has_matrix = true;
+    h->has_precond = false;
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_build_preconditioner(maspcg_handle* h)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    if (h->mas_layout) {
+      maspcg::build_hierarchy(h);
+      maspcg::build_mas_domains(h, nullptr);
+    }
+    maspcg::build_block_jacobi(h);
+    MCK(cudaStreamSynchronize(h->stream));
+    h->has_precond = true;
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_solve(maspcg_handle* h, const double* b, double* x, maspcg_result* out)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond, MASPCG_ERR_NOT_READY, "build_preconditioner first");
+    MREQ(b && x, MASPCG_ERR_INVALID_ARGUMENT, "null vector");
+    const size_t n = 3 * (size_t)h->nb;
+    const double* bd = device_in(h, b, n, h->io_a);
+    maspcg::permute_in(h, bd, h->b64.get());
+    maspcg::solve(h, h->b64.get(), h->io_b.get(), out);
+    if (is_device_ptr(x)) {
+      maspcg::permute_out(h, h->io_b.get(), x);
+    } else {
+      maspcg::permute_out(h, h->io_b.get(), h->io_a.get());
+      MCK(cudaMemcpyAsync(x, h->io_a.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_apply_preconditioner(maspcg_handle* h, const double* r, double* z)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond, MASPCG_ERR_NOT_READY, "build_preconditioner first");
+    MREQ(r && z, MASPCG_ERR_INVALID_ARGUMENT, "null vector");
+    const size_t n = 3 * (size_t)h->nb;
+    const double* rd = device_in(h, r, n, h->io_a);
+    maspcg::permute_in(h, rd, h->io_b.get());
+    maspcg::apply_preconditioner64(h, h->io_b.get(), h->r64.get());
+    if (is_device_ptr(z)) {
+      maspcg::permute_out(h, h->r64.get(), z);
+    } else {
+      maspcg::permute_out(h, h->r64.get(), h->io_a.get());
+      MCK(cudaMemcpyAsync(z, h->io_a.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_spmv(maspcg_handle* h, double a, const double* x, double b, double* y)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    MREQ(x && y, MASPCG_ERR_INVALID_ARGUMENT, "null vector");
+    const size_t n = 3 * (size_t)h->nb;
+    const double* xd = device_in(h, x, n, h->io_a);
+    maspcg::permute_in(h, xd, h->io_b.get());
+    if (b != 0.0) {
+      const double* yd = device_in(h, (const double*)y, n, h->io_a);
+      maspcg::permute_in(h, yd, h->r64.get());
+    }
+    maspcg::launch_spmv64(h, h->io_b.get(), h->r64.get(), a, b);
+    if (is_device_ptr(y)) {
+      maspcg::permute_out(h, h->r64.get(), y);
+    } else {
+      maspcg::permute_out(h, h->r64.get(), h->io_a.get());
+      MCK(cudaMemcpyAsync(y, h->io_a.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_get_info(maspcg_handle* h, maspcg_info* info)
+{
+  return guard(h, [&] {
+    MREQ(info, MASPCG_ERR_INVALID_ARGUMENT, "null info");
+    maspcg_info i{};
+    i.levelnum = h->levelnum;
+    i.total_clusters = h->lv.total_clusters;
+    i.domains = h->lv.domains;
+    i.vert_num = h->nv;
+    i.part_map_size = h->c0;
+    i.going_next_capacity = h->gn_cap;
+    i.internal_block_rows = h->nb_int;
+    i.bcsr_blocks = h->nnzb;
+    i.failed_domains = h->failed_domains;
+    i.kernel_launches = h->kernel_launches;
+    *info = i;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_get_hierarchy(maspcg_handle* h, uint32_t* fine_mask, int* cst, int* going_next,
+                                              int* level_size, int* coarse_table, int* prefix_original)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS32 preconditioner first");
+    cudaStream_t s = h->stream;
+    const size_t nv = h->nv;
+    if (fine_mask) MCK(cudaMemcpyAsync(fine_mask, h->fine_mask.get(), nv * 4, cudaMemcpyDeviceToHost, s));
+    if (cst) MCK(cudaMemcpyAsync(cst, h->cst.get(), nv * h->levelnum * 4, cudaMemcpyDeviceToHost, s));
+    if (going_next)
+      MCK(cudaMemcpyAsync(going_next, h->going_next.get(), (size_t)h->gn_cap * 4, cudaMemcpyDeviceToHost, s));
+    if (level_size)
+      MCK(cudaMemcpyAsync(level_size, h->level_size.get(), sizeof(int) * 2 * (h->levelnum + 1), cudaMemcpyDeviceToHost,
+                          s));
+    if (coarse_table) MCK(cudaMemcpyAsync(coarse_table, h->coarse_table.get(), nv * 6 * 4, cudaMemcpyDeviceToHost, s));
+    if (prefix_original)
+      MCK(cudaMemcpyAsync(prefix_original, h->prefix_orig.get(), (size_t)(h->c0 / 32) * 4, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_get_bcsr(maspcg_handle* h, int* rowptr, int* colidx, double* values, int* internal_of_row)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    cudaStream_t s = h->stream;
+    if (rowptr) MCK(cudaMemcpyAsync(rowptr, h->rowptr.get(), sizeof(int) * (h->nb_int + 1), cudaMemcpyDeviceToHost, s));
+    if (colidx) MCK(cudaMemcpyAsync(colidx, h->colidx.get(), sizeof(int) * h->nnzb, cudaMemcpyDeviceToHost, s));
+    if (values)
+      MCK(cudaMemcpyAsync(values, h->val64.get(), sizeof(double) * 9 * (size_t)h->nnzb, cudaMemcpyDeviceToHost, s));
+    if (internal_of_row)
+      MCK(cudaMemcpyAsync(internal_of_row, h->int_of_row.get(), sizeof(int) * h->nb, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS32 preconditioner first");
+    MREQ(out, MASPCG_ERR_INVALID_ARGUMENT, "null output");
+    maspcg::decode_inverses(h, out);
+  });
+}
+
+MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* out)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS32 preconditioner first");
+    MREQ(out, MASPCG_ERR_INVALID_ARGUMENT, "null output");
+    const size_t n = (size_t)h->lv.domains * maspcg::kPacked * 9;
+    DBuf<double> tmp;
+    tmp.resize(n);
+    MCK(cudaMemsetAsync(tmp.get(), 0, n * sizeof(double), h->stream));
+    maspcg::build_mas_domains(h, tmp.get());
+    MCK(cudaMemcpyAsync(out, tmp.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond, MASPCG_ERR_NOT_READY, "build_preconditioner first");
+    MREQ(mean_ms && repeats >= 1, MASPCG_ERR_INVALID_ARGUMENT, "bad arguments");
+    *mean_ms = maspcg::time_stage(h, stage, repeats);
+    h->graph_dirty = true;
+  });
+}
+
+}  // extern "C"

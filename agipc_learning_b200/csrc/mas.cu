@@ -1,0 +1,674 @@
+// mas.cu -- MAS32 domain matrices, inverses and the preconditioner apply.
+//
+// Build (once per Newton step, after the hierarchy):
+//   * member lists: for every coarse level a stable radix sort of the fine
+//     slots by their level node, so each coarse node owns a contiguous,
+//     fixed-order list of fine rows;
+//   * one CTA per domain (all levels in one launch): warp a owns destination
+//     block-row a; it walks the fine rows of its node and every block whose
+//     column node lies in the same bank is added by the lane that owns that
+//     column -- the Galerkin sum P^T A P of prepare_hessian_bcoo_kernel and
+//     prepare_hessian_bcoo_sum_kernel (TraditionalMAS32Preconditioner.cu:
+//     2234-2464) without atomics and in a fixed order;
+//   * the 96x96 FP64 matrix stays in registers (thread (a,b) holds block
+//     (a,b)); zero diagonals become 1 (expand_symmetric_mas32 :1062-1096) and
+//     it is inverted in place by Gauss-Jordan elimination without pivoting,
+//     as __inverse6_P96x96 (:1099-1146) does, with the pivot (= the squared
+//     Cholesky diagonal) checked > 0;
+//   * the inverse is stored as 17 wrapped diagonals x 9 elements x 32 lanes,
+//     in FP32 or scaled BF16/FP16.
+// Apply (every PCG iteration): restriction by in-warp segmented sums, one warp
+// per domain for the symmetric 96x96 matvec (each stored block is used for
+// both triangles through a shuffle), prolongation by the goingNext chain.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+
+#include "maspcg_internal.cuh"
+#include "pcg_device.cuh"
+
+namespace maspcg {
+namespace {
+
+constexpr int kTpb = 256;
+
+template <typename T>
+__device__ __forceinline__ float to_f(T v);
+template <>
+__device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <>
+__device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+
+template <typename T>
+__device__ __forceinline__ T from_d(double v);
+template <>
+__device__ __forceinline__ float from_d<float>(double v) { return (float)v; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) { return __float2bfloat16_rn((float)v); }
+template <>
+__device__ __forceinline__ __half from_d<__half>(double v) { return __float2half_rn((float)v); }
+
+template <typename T>
+__device__ __forceinline__ float ld_vec(const T* p);
+template <>
+__device__ __forceinline__ float ld_vec<float>(const float* p) { return *p; }
+template <>
+__device__ __forceinline__ float ld_vec<double>(const double* p) { return (float)*p; }
+
+
+// ------------------------------------------------------------------ build --
+
+__global__ void k_member_keys(const int* __restrict__ cmap, int c0, int count, unsigned* keys, int* vals)
+{
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= c0) return;
+  const int c = cmap[s];
+  keys[s] = c >= 0 ? (unsigned)c : (unsigned)count;
+  vals[s] = s;
+}
+
+__global__ void k_member_offsets(const unsigned* __restrict__ keys, int nreal, int count, int* off)
+{
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nreal) return;
+  const unsigned k = keys[p];
+  if (p == 0 || keys[p - 1] != k) off[k] = p;
+  if (p == nreal - 1) off[count] = nreal;
+}
+
+__device__ __forceinline__ int pk(int a, int b) { return kBank * a - a * (a + 1) / 2 + b; }
+
+template <typename TI, bool kAssembled>
+__global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a)
+{
+  __shared__ double prow[2][96];
+  __shared__ double stage[32][16 * 9];
+  __shared__ int sdest[32][16];
+  __shared__ float sscale[96];
+  __shared__ int fail;
+
+  const int g = blockIdx.x;
+  int L = 0;
+  while (L + 1 < a.lv.levelnum && g >= a.lv.dom_begin[L + 1]) ++L;
+  const int kdom = g - a.lv.dom_begin[L];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) fail = 0;
+
+  // ---- Galerkin assembly of destination block-row w
+  double acc[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+  const int node = kBank * kdom + w;
+  int mb = 0, me = 0;
+  if (L == 0) {
+    if (a.pmr[node] >= 0) me = 1;
+  } else if (node < a.lv.count[L]) {
+    mb = a.off[L][node];
+    me = a.off[L][node + 1];
+  }
+  const int* cmap = (L == 0) ? nullptr : a.cmap[L];
+  const int* members = (L == 0) ? nullptr : a.perm[L];
+  for (int mi = mb; mi < me; ++mi) {
+    const int v = (L == 0) ? node : members[mi];
+    const int row = a.fem_off + v;
+    const int rs = a.rowptr[row], re = a.rowptr[row + 1];
+    for (int t0 = rs; t0 < re; t0 += 16) {
+      const int nblk = min(16, re - t0);
+      if (lane < nblk) {
+        int dest = -1;
+        const int u = a.colidx[t0 + lane] - a.fem_off;
+        if (u >= 0 && u < a.c0) {
+          const int B = (L == 0) ? u : cmap[u];
+          if (B >= 0 && (B >> 5) == kdom) dest = B & 31;
+        }
+        sdest[w][lane] = dest;
+      }
+      const double* src = a.val64 + 9 * (size_t)t0;
+      for (int q = lane; q < nblk * 9; q += 32) stage[w][q] = src[q];
+      __syncwarp();
+      for (int j = 0; j < nblk; ++j) {
+        if (sdest[w][j] == lane) {
+#pragma unroll
+          for (int e = 0; e < 9; ++e) acc[e] += stage[w][9 * j + e];
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (kAssembled && lane >= w) {
+    double* o = a.assembled + ((size_t)g * kPacked + pk(w, lane)) * 9;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) o[i + 3 * j] = acc[3 * i + j];
+  }
+  if (lane == w) {
+    if (acc[0] == 0.0) acc[0] = 1.0;
+    if (acc[4] == 0.0) acc[4] = 1.0;
+    if (acc[8] == 0.0) acc[8] = 1.0;
+  }
+
+  // ---- in-place Gauss-Jordan inversion, thread (w,lane) holds block (w,lane)
+  for (int q = 0; q < kBank; ++q) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int j = 3 * q + c;
+      double* pr = prow[j & 1];
+      if (w == q) {
+        pr[3 * lane + 0] = acc[3 * c + 0];
+        pr[3 * lane + 1] = acc[3 * c + 1];
+        pr[3 * lane + 2] = acc[3 * c + 2];
+      }
+      const double m0 = __shfl_sync(kFull, acc[c], q);
+      const double m1 = __shfl_sync(kFull, acc[3 + c], q);
+      const double m2 = __shfl_sync(kFull, acc[6 + c], q);
+      __syncthreads();
+      double piv = pr[j];
+      if (!(piv > 0.0) || !isfinite(piv)) {
+        if (threadIdx.x == 0) fail = 1;
+        piv = 1.0;
+      }
+      const double inv = 1.0 / piv;
+      const double p[3] = {pr[3 * lane], pr[3 * lane + 1], pr[3 * lane + 2]};
+      const double mm[3] = {m0, m1, m2};
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const bool rowj = (w == q) && (i == c);
+        const double f = mm[i] * inv;
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+          const bool colj = (lane == q) && (jj == c);
+          double& x = acc[3 * i + jj];
+          if (rowj && colj)
+            x = inv;
+          else if (rowj)
+            x = p[jj] * inv;
+          else if (colj)
+            x = -f;
+          else
+            x = fma(-f, p[jj], x);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
+
+  // ---- store: block (w,lane) at diagonal d = (lane - w) mod 32
+  const int d = (lane - w) & 31;
+  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * kInvElems;
+  constexpr bool kScaled = !std::is_same<TI, float>::value;
+  if (kScaled) {
+    if (lane == w) {
+      sscale[3 * w + 0] = (float)sqrt(fmax(acc[0], 1e-300));
+      sscale[3 * w + 1] = (float)sqrt(fmax(acc[4], 1e-300));
+      sscale[3 * w + 2] = (float)sqrt(fmax(acc[8], 1e-300));
+    }
+    __syncthreads();
+    if (threadIdx.x < 96) a.scale[(size_t)g * 96 + threadIdx.x] = sscale[threadIdx.x];
+  }
+  if (d <= 16) {
+    const bool zero = (d == 16) && (w >= 16);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double v = zero ? 0.0 : acc[3 * i + j];
+        if (kScaled) v = v / ((double)sscale[3 * w + i] * (double)sscale[3 * lane + j]);
+        out[(d * 9 + 3 * i + j) * kBank + w] = from_d<TI>(v);
+      }
+  }
+}
+
+// ------------------------------------------------------------------ apply --
+
+// z_l = (A^-1 x)_l for one domain held by one warp; x, y: the lane's 3 rows.
+template <typename TI>
+__device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const float* __restrict__ scale, int lane,
+                                             const float x[3], float y[3])
+{
+  float s[3] = {1.f, 1.f, 1.f};
+  if (scale) {
+    s[0] = scale[3 * lane];
+    s[1] = scale[3 * lane + 1];
+    s[2] = scale[3 * lane + 2];
+  }
+  const float x0 = x[0] * s[0], x1 = x[1] * s[1], x2 = x[2] * s[2];
+  float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+#pragma unroll
+  for (int d = 0; d < kDiags; ++d) {
+    const int c = (lane + d) & 31;
+    const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
+    float B[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) B[e] = to_f<TI>(inv[(d * 9 + e) * kBank + lane]);
+    y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
+    y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
+    y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
+    if (d != 0) {
+      const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
+      const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
+      const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
+      const int src = (lane - d) & 31;
+      y0 += __shfl_sync(kFull, t0, src);
+      y1 += __shfl_sync(kFull, t1, src);
+      y2 += __shfl_sync(kFull, t2, src);
+    }
+  }
+  y[0] = y0 * s[0];
+  y[1] = y1 * s[1];
+  y[2] = y2 * s[2];
+}
+
+// Leader of each key group gets the group sum in ascending lane order.
+__device__ __forceinline__ void group_sum(int key, const float v[3], float out[3], bool& leader)
+{
+  const unsigned grp = __match_any_sync(kFull, key);
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+  for (int src = 0; src < 32; ++src) {
+    const float a0 = __shfl_sync(kFull, v[0], src), a1 = __shfl_sync(kFull, v[1], src),
+                a2 = __shfl_sync(kFull, v[2], src);
+    if ((grp >> src) & 1u) {
+      s0 += a0;
+      s1 += a1;
+      s2 += a2;
+    }
+  }
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+  leader = (__ffs(grp) - 1) == (int)(threadIdx.x & 31);
+}
+
+struct ApplyArgs {
+  const int* cmap1;
+  const int* going_next;
+  float* coarse_r;
+  float* coarse_z;
+  float* zacc1;
+  const void* inv;
+  const float* scale;
+  int fem_off, c0;
+  LevelInfo lv;
+};
+
+template <typename Tv>
+__global__ void k_restrict0(ApplyArgs a, const Tv* __restrict__ r, const PcgScalars* s)
+{
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int bank = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (bank >= a.c0 / kBank) return;
+  const int slot = bank * kBank + lane;
+  const int key = a.cmap1[slot];
+  const Tv* rp = r + 3 * (size_t)(a.fem_off + slot);
+  const float v[3] = {ld_vec(rp), ld_vec(rp + 1), ld_vec(rp + 2)};
+  float o[3];
+  bool leader;
+  group_sum(key >= 0 ? key : -1 - lane, v, o, leader);
+  if (leader && key >= 0) {
+    float* d = a.coarse_r + 3 * (size_t)key;
+    d[0] = o[0];
+    d[1] = o[1];
+    d[2] = o[2];
+  }
+}
+
+__global__ void k_restrictL(ApplyArgs a, int level_prev, const PcgScalars* s)
+{
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int bank = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int count = a.lv.count[level_prev];
+  if (bank >= (count + kBank - 1) / kBank) return;
+  const int node = bank * kBank + lane;
+  const bool valid = node < count;
+  const int sg = a.lv.begin[level_prev] + node;
+  float v[3] = {0.f, 0.f, 0.f};
+  int key = -1 - lane;
+  if (valid) {
+    const float* src = a.coarse_r + 3 * (size_t)(sg - a.c0);
+    v[0] = src[0];
+    v[1] = src[1];
+    v[2] = src[2];
+    key = a.going_next[sg];
+  }
+  float o[3];
+  bool leader;
+  group_sum(key, v, o, leader);
+  if (leader && valid) {
+    float* d = a.coarse_r + 3 * (size_t)(key - a.c0);
+    d[0] = o[0];
+    d[1] = o[1];
+    d[2] = o[2];
+  }
+}
+
+template <typename TI>
+__global__ void k_coarse_apply(ApplyArgs a, const PcgScalars* s)
+{
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int lane = threadIdx.x & 31;
+  const int g = a.lv.dom_begin[1] + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (g >= a.lv.domains) return;
+  const size_t base = (size_t)(kBank * g + lane - a.c0) * 3;
+  const float x[3] = {a.coarse_r[base], a.coarse_r[base + 1], a.coarse_r[base + 2]};
+  float y[3];
+  domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * kInvElems,
+                   a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
+  a.coarse_z[base] = y[0];
+  a.coarse_z[base + 1] = y[1];
+  a.coarse_z[base + 2] = y[2];
+}
+
+__global__ void k_prolong1(ApplyArgs a, const PcgScalars* s)
+{
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= a.lv.count[1]) return;
+  const float* z = a.coarse_z;
+  float z0 = z[3 * (size_t)A], z1 = z[3 * (size_t)A + 1], z2 = z[3 * (size_t)A + 2];
+  int cur = a.c0 + A;
+  for (int l = 2; l < a.lv.levelnum; ++l) {
+    cur = a.going_next[cur];
+    const float* q = z + 3 * (size_t)(cur - a.c0);
+    z0 += q[0];
+    z1 += q[1];
+    z2 += q[2];
+  }
+  a.zacc1[3 * (size_t)A] = z0;
+  a.zacc1[3 * (size_t)A + 1] = z1;
+  a.zacc1[3 * (size_t)A + 2] = z2;
+}
+
+}  // namespace
+
+// Level-0 apply + prolongation + r.z; with `partial` set, the last block
+// completes the r.z reduction over [0, total_parts) and, for mode > 0,
+// updates the PCG scalars (rz0 / beta / k).
+template <typename TI, typename Tv, typename Tacc>
+__global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
+                                                      int part_base, int total_parts, int mode, PcgScalars* s)
+{
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int lane = threadIdx.x & 31;
+  const int warps_total = gridDim.x * (blockDim.x >> 5);
+  Tacc dot = 0;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < a.lv.dom_begin[1]; g += warps_total) {
+    const int slot = kBank * g + lane;
+    const size_t row3 = 3 * (size_t)(a.fem_off + slot);
+    const Tv r0 = r[row3], r1 = r[row3 + 1], r2 = r[row3 + 2];
+    const float x[3] = {(float)r0, (float)r1, (float)r2};
+    float y[3];
+    domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * kInvElems,
+                     a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
+    const int c1 = a.cmap1[slot];
+    if (c1 >= 0) {
+      y[0] += a.zacc1[3 * (size_t)c1];
+      y[1] += a.zacc1[3 * (size_t)c1 + 1];
+      y[2] += a.zacc1[3 * (size_t)c1 + 2];
+    } else {
+      y[0] = y[1] = y[2] = 0.f;
+    }
+    z[row3] = (Tv)y[0];
+    z[row3 + 1] = (Tv)y[1];
+    z[row3 + 2] = (Tv)y[2];
+    dot += (Tacc)r0 * (Tacc)(Tv)y[0] + (Tacc)r1 * (Tacc)(Tv)y[1] + (Tacc)r2 * (Tacc)(Tv)y[2];
+  }
+  if (partial) {
+    Tacc total = 0;
+    if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
+                          total) &&
+        threadIdx.x == 0 && mode > 0)
+      rz_update(s, (double)total, mode);
+  }
+}
+
+void launch_factor(maspcg_handle* h, double* assembled_out);
+
+void build_mas_domains(maspcg_handle* h, double* assembled_out)
+{
+  cudaStream_t st = h->stream;
+  const LevelInfo& lv = h->lv;
+  const int c0 = h->c0;
+  // member lists per coarse level
+  h->sort_keys.resize(c0);
+  h->sort_keys_out.resize(c0);
+  h->sort_vals.resize(c0);
+  size_t need = 0;
+  MCK(cub::DeviceRadixSort::SortPairs(nullptr, need, (const unsigned*)nullptr, (unsigned*)nullptr, (const int*)nullptr,
+                                      (int*)nullptr, c0, 0, 32));
+  h->cub_tmp.resize(std::max(need, h->cub_tmp.n));
+  for (int l = 1; l < lv.levelnum; ++l) {
+    const int count = lv.count[l];
+    int bits = 1;
+    while ((1ll << bits) <= count) ++bits;
+    k_member_keys<<<ceil_div(c0, kTpb), kTpb, 0, st>>>(h->cmap[l].get(), c0, count,
+                                                      reinterpret_cast<unsigned*>(h->sort_keys.get()),
+                                                      h->sort_vals.get()); MLAUNCHED(h);
+    h->perm[l].resize(c0);
+    h->off[l].resize(count + 1);
+    size_t tb = h->cub_tmp.cap;
+    MCK(cub::DeviceRadixSort::SortPairs(h->cub_tmp.get(), tb, reinterpret_cast<const unsigned*>(h->sort_keys.get()),
+                                        reinterpret_cast<unsigned*>(h->sort_keys_out.get()), h->sort_vals.get(),
+                                        h->perm[l].get(), c0, 0, bits, st));
+    k_member_offsets<<<ceil_div(h->nv, kTpb), kTpb, 0, st>>>(
+        reinterpret_cast<const unsigned*>(h->sort_keys_out.get()), h->nv, count, h->off[l].get()); MLAUNCHED(h);
+  }
+  // storage
+  const int storage = h->cfg.inverse_storage;
+  const size_t esize = storage == MASPCG_INV_FP32 ? 4 : 2;
+  h->inv.resize((size_t)lv.domains * kInvElems * esize, 16);
+  if (storage != MASPCG_INV_FP32) h->inv_scale.resize((size_t)lv.domains * 96);
+  MCK(cudaMemsetAsync(h->failed.get() + 3, 0, sizeof(int), st));
+  launch_factor(h, assembled_out);
+  // coarse work vectors (padding entries stay zero)
+  const size_t coarse = (size_t)(lv.total_clusters - c0) * 3;
+  h->coarse_r.resize(coarse > 0 ? coarse : 3);
+  h->coarse_z.resize(coarse > 0 ? coarse : 3);
+  h->zacc1.resize((size_t)std::max(lv.count[1], 1) * 3);
+  MCK(cudaMemsetAsync(h->coarse_r.get(), 0, h->coarse_r.bytes(), st));
+  MCK(cudaMemsetAsync(h->coarse_z.get(), 0, h->coarse_z.bytes(), st));
+  int f = 0;
+  MCK(cudaMemcpyAsync(&f, h->failed.get() + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaStreamSynchronize(st));
+  h->failed_domains = f;
+}
+
+void launch_factor(maspcg_handle* h, double* assembled_out)
+{
+  cudaStream_t st = h->stream;
+  const LevelInfo& lv = h->lv;
+  const int c0 = h->c0;
+  const int storage = h->cfg.inverse_storage;
+  FactorArgs fa{};
+  fa.lv = lv;
+  for (int l = 1; l < lv.levelnum; ++l) {
+    fa.cmap[l] = h->cmap[l].get();
+    fa.perm[l] = h->perm[l].get();
+    fa.off[l] = h->off[l].get();
+  }
+  fa.pmr = h->pmr.get();
+  fa.rowptr = h->rowptr.get();
+  fa.colidx = h->colidx.get();
+  fa.val64 = h->val64.get();
+  fa.fem_off = h->fem_off;
+  fa.c0 = c0;
+  fa.inv = h->inv.get();
+  fa.scale = storage == MASPCG_INV_FP32 ? nullptr : h->inv_scale.get();
+  fa.failed = h->failed.get() + 3;
+  fa.assembled = assembled_out;
+  const int grid = lv.domains;
+  if (assembled_out) {
+    if (storage == MASPCG_INV_FP32)
+      k_domain_factor<float, true><<<grid, 1024, 0, st>>>(fa);
+    else if (storage == MASPCG_INV_BF16)
+      k_domain_factor<__nv_bfloat16, true><<<grid, 1024, 0, st>>>(fa);
+    else
+      k_domain_factor<__half, true><<<grid, 1024, 0, st>>>(fa);
+  } else {
+    if (storage == MASPCG_INV_FP32)
+      k_domain_factor<float, false><<<grid, 1024, 0, st>>>(fa);
+    else if (storage == MASPCG_INV_BF16)
+      k_domain_factor<__nv_bfloat16, false><<<grid, 1024, 0, st>>>(fa);
+    else
+      k_domain_factor<__half, false><<<grid, 1024, 0, st>>>(fa);
+  }
+  MLAUNCHED(h);
+  MCK(cudaGetLastError());
+}
+
+namespace {
+ApplyArgs make_apply_args(maspcg_handle* h)
+{
+  ApplyArgs a{};
+  a.cmap1 = h->cmap[1].get();
+  a.going_next = h->going_next.get();
+  a.coarse_r = h->coarse_r.get();
+  a.coarse_z = h->coarse_z.get();
+  a.zacc1 = h->zacc1.get();
+  a.inv = h->inv.get();
+  a.scale = h->cfg.inverse_storage == MASPCG_INV_FP32 ? nullptr : h->inv_scale.get();
+  a.fem_off = h->fem_off;
+  a.c0 = h->c0;
+  a.lv = h->lv;
+  return a;
+}
+
+template <typename TI, typename Tv, typename Tacc>
+void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
+                 int grid0, PcgScalars* s)
+{
+  cudaStream_t st = h->stream;
+  ApplyArgs a = make_apply_args(h);
+  const LevelInfo& lv = h->lv;
+  const int banks0 = h->c0 / kBank;
+  k_restrict0<Tv><<<ceil_div((long long)banks0 * 32, kTpb), kTpb, 0, st>>>(a, r, s); MLAUNCHED(h);
+  for (int l = 2; l < lv.levelnum; ++l) {
+    const int banks = ceil_div(lv.count[l - 1], kBank);
+    k_restrictL<<<ceil_div((long long)banks * 32, kTpb), kTpb, 0, st>>>(a, l - 1, s); MLAUNCHED(h);
+  }
+  const int coarse_domains = lv.domains - lv.dom_begin[1];
+  if (coarse_domains > 0) {
+    k_coarse_apply<TI><<<ceil_div((long long)coarse_domains * 32, kTpb), kTpb, 0, st>>>(a, s);
+    MLAUNCHED(h);
+  }
+  k_prolong1<<<ceil_div(lv.count[1], kTpb), kTpb, 0, st>>>(a, s); MLAUNCHED(h);
+  k_level0_apply<TI, Tv, Tacc><<<grid0, kTpb, 0, st>>>(a, r, z, partial, part_base, total_parts, mode, s); MLAUNCHED(h);
+}
+}  // namespace
+
+// Explicit launcher used by pcg.cu.
+template <typename Tv, typename Tacc>
+void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
+               int grid0, PcgScalars* s)
+{
+  switch (h->cfg.inverse_storage) {
+    case MASPCG_INV_BF16:
+      mas_apply_t<__nv_bfloat16, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s);
+      break;
+    case MASPCG_INV_FP16:
+      mas_apply_t<__half, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s);
+      break;
+    default: mas_apply_t<float, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s); break;
+  }
+  MCK(cudaGetLastError());
+}
+
+// Stage timing helpers: the level-0 domain apply alone, and the domain
+// assembly + inversion alone (member lists from the last build).
+template <typename Tv, typename Tacc>
+void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s)
+{
+  ApplyArgs a = make_apply_args(h);
+  switch (h->cfg.inverse_storage) {
+    case MASPCG_INV_BF16:
+      k_level0_apply<__nv_bfloat16, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s);
+      break;
+    case MASPCG_INV_FP16:
+      k_level0_apply<__half, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s);
+      break;
+    default: k_level0_apply<float, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s); break;
+  }
+  MLAUNCHED(h);
+  MCK(cudaGetLastError());
+}
+template void mas_level0_only<float, float>(maspcg_handle*, const float*, float*, float*, int, PcgScalars*);
+template void mas_level0_only<float, double>(maspcg_handle*, const float*, float*, double*, int, PcgScalars*);
+template void mas_level0_only<double, double>(maspcg_handle*, const double*, double*, double*, int, PcgScalars*);
+
+template void mas_apply<float, float>(maspcg_handle*, const float*, float*, float*, int, int, int, int, PcgScalars*);
+template void mas_apply<float, double>(maspcg_handle*, const float*, float*, double*, int, int, int, int,
+                                       PcgScalars*);
+template void mas_apply<double, double>(maspcg_handle*, const double*, double*, double*, int, int, int, int,
+                                        PcgScalars*);
+
+int mas_level0_grid(maspcg_handle* h)
+{
+  const int warps = h->lv.dom_begin[1];
+  return std::max(1, std::min(ceil_div((long long)warps * 32, kTpb), 8 * h->sm_count));
+}
+
+// Decode the stored inverses into the reference's packed FP32 layout.
+void decode_inverses(maspcg_handle* h, float* out)
+{
+  const int D = h->lv.domains;
+  const int storage = h->cfg.inverse_storage;
+  const size_t esize = storage == MASPCG_INV_FP32 ? 4 : 2;
+  std::vector<unsigned char> raw((size_t)D * kInvElems * esize);
+  std::vector<float> sc;
+  MCK(cudaMemcpyAsync(raw.data(), h->inv.get(), raw.size(), cudaMemcpyDeviceToHost, h->stream));
+  if (storage != MASPCG_INV_FP32) {
+    sc.resize((size_t)D * 96);
+    MCK(cudaMemcpyAsync(sc.data(), h->inv_scale.get(), sc.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+  }
+  MCK(cudaStreamSynchronize(h->stream));
+  auto elem = [&](size_t idx) -> float {
+    if (storage == MASPCG_INV_FP32) {
+      float f;
+      std::memcpy(&f, raw.data() + idx * 4, 4);
+      return f;
+    }
+    uint16_t u;
+    std::memcpy(&u, raw.data() + idx * 2, 2);
+    if (storage == MASPCG_INV_BF16) {
+      uint32_t w = (uint32_t)u << 16;
+      float f;
+      std::memcpy(&f, &w, 4);
+      return f;
+    }
+    // IEEE half -> float
+    const uint32_t sign = (u >> 15) & 1, ex = (u >> 10) & 0x1f, man = u & 0x3ff;
+    float f;
+    if (ex == 0)
+      f = std::ldexp((float)man, -24);
+    else if (ex == 31)
+      f = man ? NAN : INFINITY;
+    else
+      f = std::ldexp((float)(man | 0x400), (int)ex - 25);
+    return sign ? -f : f;
+  };
+  for (int g = 0; g < D; ++g)
+    for (int a = 0; a < kBank; ++a)
+      for (int b = a; b < kBank; ++b) {
+        // block (a,b) lives at lane a, diagonal d=b-a when d <= 16, else it is the
+        // transpose of (b,a) at lane b, diagonal 32-(b-a).
+        const int d = b - a;
+        const bool direct = d <= 16 && !(d == 16 && a >= 16);
+        const int lane = direct ? a : b, dd = direct ? d : (32 - d) & 31;
+        float* o = out + ((size_t)g * kPacked + (kBank * a - a * (a + 1) / 2 + b)) * 9;
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            const int ei = direct ? 3 * i + j : 3 * j + i;
+            float v = elem((size_t)g * kInvElems + (size_t)(dd * 9 + ei) * kBank + lane);
+            if (storage != MASPCG_INV_FP32) v *= sc[(size_t)g * 96 + 3 * a + i] * sc[(size_t)g * 96 + 3 * b + j];
+            o[i + 3 * j] = v;  // column-major
+          }
+      }
+}
+
+}  // namespace maspcg

@@ -1,0 +1,263 @@
+// maspcg_internal.cuh -- shared definitions of the B200 MAS-PCG library.
+//
+// Data layout (HBM):
+//   * Internal block-row order: [rows before the FEM range][the part_map_size
+//     MAS slots of the FEM range, in partition order, padding slots empty]
+//     [rows after the FEM range].  A level-0 MAS domain is 32 consecutive
+//     internal rows, so restriction and prolongation at level 0 are the
+//     identity and a domain's residual is 96 contiguous floats.
+//   * Matrix: full block-CSR (both triangles) over internal rows, 3x3 blocks
+//     row-major; FP64 copy (reference precision, true residual) and FP32 copy
+//     (inner iterations).
+//   * Domain inverses: 17 "diagonals" x 9 elements x 32 lanes per domain;
+//     element (i,j) of block (l, (l+d) mod 32) at [d][3i+j][l]; diagonal 16 is
+//     stored for l < 16 only (zeros above).  16-bit storage is symmetrically
+//     scaled: S^-1 A^-1 S^-1 with S = diag(sqrt(diag A^-1)), scales in FP32.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "maspcg.h"
+
+namespace maspcg {
+
+constexpr int kBank = 32;
+constexpr int kPacked = kBank * (kBank + 1) / 2;  // 528
+constexpr int kDiags = 17;
+constexpr int kInvElems = kDiags * 9 * kBank;      // 4896 stored elements per domain
+constexpr int kMaxLevels = 6;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct Error : std::runtime_error {
+  maspcg_status status;
+  Error(maspcg_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define MCK(expr)                                                                                  \
+  do {                                                                                             \
+    cudaError_t e_ = (expr);                                                                       \
+    if (e_ != cudaSuccess) {                                                                       \
+      throw ::maspcg::Error(e_ == cudaErrorMemoryAllocation ? MASPCG_ERR_OUT_OF_MEMORY : MASPCG_ERR_CUDA, \
+                            std::string(#expr) + ": " + cudaGetErrorString(e_));                  \
+    }                                                                                              \
+  } while (0)
+
+#define MREQ(cond, status, msg)                         \
+  do {                                                  \
+    if (!(cond)) throw ::maspcg::Error((status), (msg)); \
+  } while (0)
+
+// Grow-only device buffer.
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = n = 0;
+  }
+  // `pad` extra elements keep 16-byte vector loads of the tail in bounds.
+  void resize(size_t count, size_t pad = 0)
+  {
+    const size_t need = count + pad;
+    if (need > cap) {
+      if (p) cudaFree(p);
+      p = nullptr;
+      cap = 0;
+      if (need) {
+        MCK(cudaMalloc(reinterpret_cast<void**>(&p), need * sizeof(T)));
+        cap = need;
+      }
+    }
+    n = count;
+  }
+  T* get() const { return p; }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// Device-resident PCG state; every iteration kernel reads it, only the last
+// block of a reduction writes it.
+struct PcgScalars {
+  double rz, rz0, rz_new, pap, alpha, beta, rr, bb, rr_true;
+  int k;          // current iteration (1-based, PCGSolver::pcg's k)
+  int status;     // maspcg_solve_status, plus kNeedTrue
+  int max_iter;   // PCGSolver: loop while k < max_iter
+  int refinements;
+  int iterations; // reported iteration count once stopped
+  int gate;
+  double tol;
+  unsigned tickets[8];
+};
+
+constexpr int kNeedTrue = 16;  // MIXED: recursive gate met or period end; true residual pending
+constexpr int kCapPending = 32;
+
+enum Ticket { kTicketSpmv = 0, kTicketXr = 1, kTicketRz = 2, kTicketTrue = 3, kTicketAux = 4 };
+
+struct LevelInfo {
+  int levelnum;
+  int count[kMaxLevels + 1];      // nodes per level (level 0: part_map_size slots)
+  int begin[kMaxLevels + 1];      // first global cluster slot of the level
+  int dom_begin[kMaxLevels + 1];  // first domain of the level
+  int total_clusters;
+  int domains;
+};
+
+// Pointers used by the domain factorisation kernel, one entry per level.
+struct FactorArgs {
+  LevelInfo lv;
+  const int* cmap[kMaxLevels];   // fine slot -> level-L local node (-1 padding); level 0 unused
+  const int* perm[kMaxLevels];   // level-L member lists (fine slots), level >= 1
+  const int* off[kMaxLevels];    // level-L member offsets [count+1], level >= 1
+  const int* pmr;                // part_map_real
+  const int* rowptr;
+  const int* colidx;
+  const double* val64;           // row-major blocks
+  int fem_off;
+  int c0;
+  void* inv;                     // kInvElems per domain, type per storage
+  float* scale;                  // 96 per domain (16-bit storage)
+  int* failed;                   // count of domains with a pivot <= 0
+  double* assembled;             // optional: packed FP64 domain matrices (reference layout)
+};
+
+}  // namespace maspcg
+
+// ---------------------------------------------------------------- handle ---
+struct maspcg_handle {
+  maspcg_config cfg{};
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int device = 0;
+  int sm_count = 148;
+  std::string last_error;
+
+  // ---- graph (set_graph)
+  bool has_graph = false;
+  int nv = 0, c0 = 0, levelnum = 0, node_offset = 0, nlist_size = 0;
+  long long gn_cap = 0;
+  maspcg::DBuf<uint32_t> nstart, nnum_init, nlist_init, nnum, nlist;
+  maspcg::DBuf<int> pmr, rmp;
+  std::vector<int> h_pmr, h_rmp;
+  maspcg::DBuf<int> pairs;
+  int n_pairs = 0;
+
+  // ---- hierarchy (build)
+  maspcg::DBuf<uint32_t> fine_mask, next_mask, next_prefix, next_prefix_sum;
+  maspcg::DBuf<int> prefix_orig, prefix_sum_orig, cst, going_next, coarse_table, level_size;
+  maspcg::LevelInfo lv{};
+  maspcg::DBuf<int> cmap[maspcg::kMaxLevels], perm[maspcg::kMaxLevels], off[maspcg::kMaxLevels];
+  maspcg::DBuf<int> sort_keys, sort_vals, sort_keys_out;
+  maspcg::DBuf<unsigned char> cub_tmp;
+  maspcg::DBuf<int> scan_tmp;
+
+  // ---- matrix (set_matrix_bcoo)
+  bool has_matrix = false;
+  int nb = 0, fem_off = 0, abd_bodies = 0, nb_int = 0, n_in = 0, nnzb = 0;
+  bool mas_layout = false;  // internal order uses the MAS partition
+  maspcg::DBuf<int> int_of_row, row_of_int;
+  maspcg::DBuf<int> rowptr, colidx;
+  maspcg::DBuf<double> val64;
+  maspcg::DBuf<float> val32;
+  maspcg::DBuf<unsigned long long> keys, keys_sorted;
+  maspcg::DBuf<int> kv, kv_sorted, seg_head, seg_start, row_count;
+  maspcg::DBuf<double> in_vals;
+  maspcg::DBuf<int> in_rows, in_cols;
+
+  // ---- preconditioner (build)
+  bool has_precond = false;
+  maspcg::DBuf<unsigned char> inv;  // domain inverses
+  maspcg::DBuf<float> inv_scale;
+  maspcg::DBuf<int> failed;
+  int failed_domains = 0;
+  maspcg::DBuf<float> coarse_r, coarse_z, zacc1;
+  maspcg::DBuf<double> abd_inv64;
+  maspcg::DBuf<float> abd_inv32;
+  maspcg::DBuf<double> diag_inv64;
+  maspcg::DBuf<float> diag_inv32;
+
+  // ---- PCG
+  maspcg::DBuf<unsigned char> vx, vr, vz, vp, vap;  // vectors in the working precision
+  maspcg::DBuf<double> b64, x64, r64;               // FP64: rhs, x (hi), residual scratch
+  maspcg::DBuf<double> partial, partial_rz;
+  maspcg::DBuf<maspcg::PcgScalars> scal;
+  maspcg::PcgScalars* h_scal = nullptr;  // pinned mirror
+  maspcg::DBuf<double> io_a, io_b;       // staging for host pointers / permutations
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_batch = 0;
+  bool graph_dirty = true;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int grid_stream = 0;  // CTAs for grid-stride kernels
+  long long kernel_launches = 0;  // this library's kernels launched on the handle
+  long long graph_kernels = 0;    // kernel nodes of the captured batch graph
+};
+
+namespace maspcg {
+
+// hierarchy.cu
+void build_hierarchy(maspcg_handle* h);
+
+// matrix.cu
+void build_internal_matrix(maspcg_handle* h, const double* vals_dev, const int* rows_dev, const int* cols_dev, int n);
+void launch_spmv64(maspcg_handle* h, const double* x, double* y, double a, double b);  // internal order
+void permute_in(maspcg_handle* h, const double* src_orig, double* dst_int);
+void permute_out(maspcg_handle* h, const double* src_int, double* dst_orig);
+void build_block_jacobi(maspcg_handle* h);
+
+// mas.cu
+void build_mas_domains(maspcg_handle* h, double* assembled_out);
+void mas_apply_launch(maspcg_handle* h, const void* r, void* z, bool finalize_rz);
+void decode_inverses(maspcg_handle* h, float* out_host);
+
+// Count one launch of this library (graph captures are corrected afterwards).
+#define MLAUNCHED(h) (++(h)->kernel_launches)
+
+// pcg.cu
+double time_stage(maspcg_handle* h, int stage, int repeats);
+void solve(maspcg_handle* h, const double* b_dev, double* x_dev, maspcg_result* res);
+void apply_preconditioner64(maspcg_handle* h, const double* r_int, double* z_int);
+size_t vec_elem_size(const maspcg_handle* h);
+
+// common device helpers
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+template <typename T, int NT>
+__device__ __forceinline__ T block_sum(T v, T* smem /* NT/32 */)
+{
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) smem[w] = v;
+  __syncthreads();
+  T s = 0;
+  if (w == 0) {
+    s = (l < NT / 32) ? smem[l] : T(0);
+    s = warp_sum(s);
+  }
+  __syncthreads();
+  return s;  // valid in warp 0
+}
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace maspcg

@@ -1,0 +1,78 @@
+// pcg_device.cuh -- grid reductions with a last-block epilogue and the
+// device-side PCG scalar updates shared by the iteration kernels.
+#pragma once
+#include "maspcg_internal.cuh"
+
+namespace maspcg {
+
+constexpr int kRedTpb = 256;
+
+// Block-sum v, store it in partial[slot]; the last block to arrive (counted
+// on *ticket against `expected` blocks) sums partial[0..total_parts) in a
+// fixed order.  Returns true in every thread of that last block; the sum is
+// valid in thread 0.
+template <typename Tacc>
+__device__ __forceinline__ bool grid_finish(Tacc v, Tacc* partial, int slot, int total_parts, unsigned* ticket,
+                                            unsigned expected, Tacc& total)
+{
+  __shared__ Tacc red[kRedTpb / 32];
+  __shared__ int last;
+  const Tacc b = block_sum<Tacc, kRedTpb>(v, red);
+  if (threadIdx.x == 0) {
+    partial[slot] = b;
+    __threadfence();
+    const unsigned t = atomicAdd(ticket, 1u);
+    last = (t == expected - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  Tacc s = 0;
+  for (int i = threadIdx.x; i < total_parts; i += blockDim.x) s += __ldcg(partial + i);
+  s = block_sum<Tacc, kRedTpb>(s, red);
+  if (threadIdx.x == 0) {
+    total = s;
+    *ticket = 0u;
+  }
+  return true;
+}
+
+// End of the preconditioner apply: r^T z of this iteration.
+// mode 1: initial apply (rz0); mode 2: inside the loop (beta, k++).
+__device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode)
+{
+  s->rz_new = rz_new;
+  if (mode == 1 && rz_new == 0.0 && s->bb == 0.0) {  // b = 0: x = 0 is exact
+    s->rz = s->rz0 = 0.0;
+    s->k = 0;
+    s->status = MASPCG_SOLVE_CONVERGED;
+    s->iterations = 0;
+    return;
+  }
+  if (!isfinite(rz_new)) {
+    s->status = MASPCG_SOLVE_NONFINITE;
+    s->iterations = s->k;
+    return;
+  }
+  if (!(rz_new > 0.0)) {
+    s->status = MASPCG_SOLVE_INVALID_RZ;
+    s->iterations = s->k;
+    return;
+  }
+  if (mode == 1) {
+    s->rz = rz_new;
+    s->rz0 = rz_new;
+    s->k = 1;
+    s->beta = 0.0;
+  } else {
+    s->beta = rz_new / s->rz;
+    s->rz = rz_new;
+    s->k += 1;
+  }
+  if (s->k >= s->max_iter) {
+    s->status = MASPCG_SOLVE_ITERATION_CAP;
+    s->iterations = s->max_iter;
+  }
+}
+
+}  // namespace maspcg

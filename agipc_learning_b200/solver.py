@@ -1,0 +1,308 @@
+"""Host-side mirror of StiffGIPC's linear-solve interface over the C ABI.
+
+``MasPcg`` owns one ``maspcg_handle``.  ``PCGSolverConfig``, ``PCGSolver`` and
+``TraditionalMAS32Preconditioner`` keep the reference's names, argument
+meaning and call order (``linear_system/solver/pcg_solver.h:7-50``,
+``TraditionalMAS32Preconditioner.cuh:35-129``, caller ``gl_main.cu:1502-1536``)
+so code written against the reference maps one to one.  Arrays may be numpy
+arrays (host) or CUDA torch tensors (device); every call goes through
+``libmaspcg.so``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+_PREC = {"reference": N.PREC_REFERENCE, "fp32": N.PREC_FP32, "mixed": N.PREC_MIXED}
+_GATE = {"rz": N.GATE_RZ, "euclid": N.GATE_EUCLID}
+_INV = {"fp32": N.INV_FP32, "bf16": N.INV_BF16, "fp16": N.INV_FP16}
+_PC = {"mas32": N.PRECOND_MAS32, "block_jacobi": N.PRECOND_BLOCK_JACOBI, "none": N.PRECOND_NONE}
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+class _Arg:
+    """Pointer to a contiguous numpy array or CUDA tensor of a given dtype."""
+
+    def __init__(self, a, np_dtype, writable=False):
+        self.keep = None
+        if a is None:
+            self.ptr = None
+            return
+        if _is_torch(a):
+            import torch
+            want = {np.float64: torch.float64, np.int32: torch.int32, np.uint32: torch.int32}[np_dtype]
+            if a.dtype != want or not a.is_contiguous():
+                if writable:
+                    raise ValueError("output tensor must be contiguous with the right dtype")
+                a = a.to(want).contiguous()
+            self.keep = a
+            self.ptr = ctypes.c_void_p(a.data_ptr())
+        else:
+            arr = np.asarray(a)
+            if arr.dtype != np_dtype or not arr.flags["C_CONTIGUOUS"]:
+                if writable:
+                    raise ValueError("output array must be C-contiguous with the right dtype")
+                arr = np.ascontiguousarray(arr, dtype=np_dtype)
+            self.keep = arr
+            self.ptr = arr.ctypes.data_as(ctypes.c_void_p)
+
+
+class MasPcg:
+    """One linear system on one GPU: graph -> contacts -> matrix -> build -> solve."""
+
+    def __init__(self, *, tolerance=1e-4, max_iter_ratio=0.3, max_iterations=0, gate="rz", precision="reference",
+                 inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8):
+        lib = N.load()
+        cfg = N.Config()
+        lib.maspcg_config_default(ctypes.byref(cfg))
+        cfg.tolerance = tolerance
+        cfg.max_iter_ratio = max_iter_ratio
+        cfg.max_iterations = max_iterations
+        cfg.gate = _GATE[gate]
+        cfg.precision = _PREC[precision]
+        cfg.inverse_storage = _INV[inverse]
+        cfg.preconditioner = _PC[preconditioner]
+        cfg.refinement_period = refinement_period
+        cfg.iterations_per_launch = iterations_per_launch
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        N.check(lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)), None)
+        self.h = h
+        self.lib = lib
+        self.nb = 0
+        self.nv = 0
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.maspcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, status):
+        N.check(status, self.h)
+
+    # -- inputs
+    def set_stream(self, stream_ptr: int | None):
+        self._ck(self.lib.maspcg_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def set_graph(self, vert_num, node_offset, neighbor_start, neighbor_num, neighbor_list, part_map_real,
+                  real_map_part):
+        a = [_Arg(neighbor_start, np.uint32), _Arg(neighbor_num, np.uint32),
+             _Arg(neighbor_list if len(neighbor_list) else np.zeros(1, np.uint32), np.uint32),
+             _Arg(part_map_real, np.int32), _Arg(real_map_part, np.int32)]
+        self._ck(self.lib.maspcg_set_graph(self.h, int(vert_num), int(node_offset), a[0].ptr, a[1].ptr, a[2].ptr,
+                                           int(len(neighbor_list)), a[3].ptr, int(len(part_map_real)), a[4].ptr))
+        self.nv = int(vert_num)
+
+    def set_contacts(self, pairs):
+        p = np.zeros((0, 4), np.int32) if pairs is None else pairs
+        n = len(p)
+        arg = _Arg(p if n else np.zeros(4, np.int32), np.int32)
+        self._ck(self.lib.maspcg_set_contacts(self.h, arg.ptr, int(n)))
+
+    def set_matrix(self, vals, rows, cols, block_rows, fem_offset=0, abd_bodies=0):
+        v, r, c = _Arg(vals, np.float64), _Arg(rows, np.int32), _Arg(cols, np.int32)
+        self._ck(self.lib.maspcg_set_matrix_bcoo(self.h, v.ptr, r.ptr, c.ptr, int(len(rows)), int(block_rows),
+                                                 int(fem_offset), int(abd_bodies)))
+        self.nb = int(block_rows)
+
+    def build(self):
+        self._ck(self.lib.maspcg_build_preconditioner(self.h))
+
+    @classmethod
+    def from_system(cls, s, **cfg):
+        """Set up graph, contacts and matrix of a synth.System and build."""
+        m = cls(**cfg)
+        if m.cfg.preconditioner == N.PRECOND_MAS32 and s.fem_count > 0:
+            m.set_graph(s.fem_count, s.node_offset, s.neighbor_start, s.neighbor_num, s.neighbor_list,
+                        s.part_map_real, s.real_map_part)
+            m.set_contacts(s.pairs)
+        m.set_matrix(s.vals, s.rows, s.cols, s.nb, s.fem_offset, s.abd_bodies)
+        m.build()
+        return m
+
+    # -- operations
+    def _out(self, out, n):
+        if out is None:
+            out = np.zeros(n, np.float64)
+        return out, _Arg(out, np.float64, writable=True)
+
+    def solve(self, b, x=None):
+        bx = _Arg(b, np.float64)
+        x, xa = self._out(x, 3 * self.nb)
+        res = N.Result()
+        self._ck(self.lib.maspcg_solve(self.h, bx.ptr, xa.ptr, ctypes.byref(res)))
+        return x, res.as_dict()
+
+    def apply_preconditioner(self, r, z=None):
+        ra = _Arg(r, np.float64)
+        z, za = self._out(z, 3 * self.nb)
+        self._ck(self.lib.maspcg_apply_preconditioner(self.h, ra.ptr, za.ptr))
+        return z
+
+    def spmv(self, x, a=1.0, b=0.0, y=None):
+        xa = _Arg(x, np.float64)
+        if y is None:
+            y = np.zeros(3 * self.nb, np.float64)
+        ya = _Arg(y, np.float64, writable=True)
+        self._ck(self.lib.maspcg_spmv(self.h, float(a), xa.ptr, float(b), ya.ptr))
+        return y
+
+    # -- introspection
+    def info(self):
+        i = N.Info()
+        self._ck(self.lib.maspcg_get_info(self.h, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in i._fields_}
+
+    def hierarchy(self):
+        i = self.info()
+        L, nv = i["levelnum"], i["vert_num"]
+        fm = np.zeros(nv, np.uint32)
+        cst = np.zeros(L * nv, np.int32)
+        gn = np.zeros(i["going_next_capacity"], np.int32)
+        ls = np.zeros(2 * (L + 1), np.int32)
+        ct = np.zeros(6 * nv, np.int32)
+        po = np.zeros(i["part_map_size"] // 32, np.int32)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self._ck(self.lib.maspcg_get_hierarchy(self.h, p(fm), p(cst), p(gn), p(ls), p(ct), p(po)))
+        return {"fine_mask": fm, "coarse_space_tables": cst.reshape(L, nv), "going_next": gn,
+                "level_size": ls.reshape(L + 1, 2), "coarse_table": ct.reshape(nv, 6), "prefix_original": po,
+                "total_clusters": i["total_clusters"], "levelnum": L}
+
+    def bcsr(self):
+        i = self.info()
+        rp = np.zeros(i["internal_block_rows"] + 1, np.int32)
+        ci = np.zeros(i["bcsr_blocks"], np.int32)
+        vals = np.zeros((i["bcsr_blocks"], 9), np.float64)
+        iof = np.zeros(self.nb, np.int32)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self._ck(self.lib.maspcg_get_bcsr(self.h, p(rp), p(ci), p(vals), p(iof)))
+        return rp, ci, vals, iof
+
+    def domain_inverses(self):
+        d = self.info()["domains"]
+        out = np.zeros((d, 528, 9), np.float32)
+        self._ck(self.lib.maspcg_get_domain_inverses(self.h, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def time_stage(self, stage: int, repeats: int = 20) -> float:
+        """Mean device ms of one stage (0 SpMV, 1 preconditioner, 2 MAS level-0
+        apply, 3 domain assembly + inversion) over `repeats` back-to-back runs."""
+        ms = ctypes.c_double()
+        self._ck(self.lib.maspcg_time_stage(self.h, int(stage), int(repeats), ctypes.byref(ms)))
+        return ms.value
+
+    def domain_matrices(self):
+        d = self.info()["domains"]
+        out = np.zeros((d, 528, 9), np.float64)
+        self._ck(self.lib.maspcg_get_domain_matrices(self.h, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+
+# ------------------------------------------------------------ reference names
+
+
+@dataclass
+class PCGSolverConfig:
+    """gipc::PCGSolverConfig (linear_system/solver/pcg_solver.h:7-17)."""
+
+    max_iter_ratio: float = 0.3
+    global_tol_rate: float = 1e-4
+    use_bsr: bool = True
+
+
+class PCGSolver:
+    """gipc::PCGSolver over an assembled system: solve(x, b) -> iterations.
+
+    ``system`` is anything with ``vals, rows, cols, nb, fem_offset, fem_count,
+    abd_bodies`` and the MAS32 graph fields (``synth.System``)."""
+
+    def __init__(self, cfg: PCGSolverConfig | None = None, *, preconditioner="mas32", **engine_cfg):
+        self.cfg = cfg or PCGSolverConfig()
+        self.preconditioner = preconditioner
+        self.engine_cfg = engine_cfg
+        self.engine: MasPcg | None = None
+        self.last_result = None
+
+    def bind(self, system):
+        self.engine = MasPcg.from_system(system, tolerance=self.cfg.global_tol_rate,
+                                         max_iter_ratio=self.cfg.max_iter_ratio, preconditioner=self.preconditioner,
+                                         **self.engine_cfg)
+        return self
+
+    def solve(self, x, b) -> int:
+        if self.engine is None:
+            raise RuntimeError("bind(system) first")
+        _, res = self.engine.solve(b, x)
+        self.last_result = res
+        return res["iterations"]
+
+
+class TraditionalMAS32Preconditioner:
+    """gpu_mas32::TraditionalMAS32Preconditioner (TraditionalMAS32Preconditioner.cuh:35-129).
+
+    The caller sequence of gl_main.cu:1502-1536 works unchanged:
+    initPreconditioner_Neighbor, fill the public arrays, initPreconditioner_Matrix,
+    then per Newton step setPreconditioner_bcoo and preconditioning."""
+
+    def __init__(self, **engine_cfg):
+        self.engine_cfg = engine_cfg
+        self.neighborListSize = 0
+        self.d_neighborListInit = None
+        self.d_neighborStart = None
+        self.d_neighborNumInit = None
+        self.d_partId_map_real = None
+        self.d_real_map_partId = None
+        self._engine: MasPcg | None = None
+
+    def initPreconditioner_Neighbor(self, vertNum, mCollision_node_offset, totalNeighborNum, m_collisonPairs,
+                                    partMapSize):
+        self.totalNodes = int(vertNum)
+        self.collision_node_Offset = int(mCollision_node_offset)
+        self.totalNeighborNum = int(totalNeighborNum)
+        self._collisonPairs = m_collisonPairs
+        self.totalMapNodes = int(partMapSize)
+
+    def initPreconditioner_Matrix(self):
+        e = MasPcg(preconditioner="mas32", **self.engine_cfg)
+        lst = np.asarray(self.d_neighborListInit)[: self.neighborListSize]
+        e.set_graph(self.totalNodes, self.collision_node_Offset, self.d_neighborStart, self.d_neighborNumInit, lst,
+                    np.asarray(self.d_partId_map_real)[: self.totalMapNodes], self.d_real_map_partId)
+        self._engine = e
+
+    def setPreconditioner_bcoo(self, triplet_values, row_ids, col_ids, indices, offset, triplet_num, cpNum):
+        idx = np.asarray(indices)[:triplet_num]
+        vals = np.asarray(triplet_values).reshape(-1, 9)[idx]
+        rows = np.asarray(row_ids)[idx] - offset
+        cols = np.asarray(col_ids)[idx] - offset
+        pairs = None if self._collisonPairs is None else np.asarray(self._collisonPairs).reshape(-1, 4)[:cpNum]
+        self._engine.set_contacts(pairs)
+        self._engine.set_matrix(vals, rows, cols, self.totalNodes, 0, 0)
+        self._engine.build()
+
+    def preconditioning(self, R, Z=None):
+        return self._engine.apply_preconditioner(R, Z)
+
+    def FreeMAS(self):
+        if self._engine is not None:
+            self._engine.close()
+            self._engine = None

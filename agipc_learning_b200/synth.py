@@ -6,8 +6,12 @@ workloads below rebuild systems of the same structure from the same formulas
 element Hessians (``femEnergy.cu:432-459``), lumped mass (``gl_main.cu:611-614``),
 IPC barrier Hessians for point-triangle / edge-edge pairs, and affine bodies
 with ``J^T H`` coupling blocks (``setup_abd_system_gradient_and_hessian.cu:348-405``).
-Scaling follows the reference: ``A = M + dt^2 K + kappa * barrier``
-(``GIPC.cu:10183-10199``).
+Scaling: ``A = M + dt^2 (K + kappa * barrier)``, the incremental potential
+of IPC.  The reference enters mass unscaled and elasticity with dt^2
+(``GIPC.cu:10183-10199``, ``femEnergy.cu:1719-1856``) and passes an adaptive
+kappa that absorbs dt^2 to the barrier (``GIPC.cu:9935-9943``); the workloads
+fix kappa, so dt^2 is applied explicitly.  Unscaled, kappa=1e7 makes contact
+blocks ~1e7 times the elastic ones and FP32 products of A lose positivity.
 
 Every system is returned as the unique upper BCOO that
 ``GlobalLinearSystem::convert_new`` hands to the solver
@@ -192,7 +196,7 @@ def cube_system(n: int, *, E: float = 1e5, nu: float = 0.45, rho: float = 1000.0
             r = np.zeros(10 * pt_pairs, np.int32)
             c = np.zeros(10 * pt_pairs, np.int32)
             v = np.zeros((10 * pt_pairs, 9), np.float64)
-            k = lib.syn_contacts_pt(nx, ny, nz, h, _p(X), ntri, _p(tris), pt_pairs, dhat, kappa, seed + 101, 0, 0,
+            k = lib.syn_contacts_pt(nx, ny, nz, h, _p(X), ntri, _p(tris), pt_pairs, dhat, kappa * dt * dt, seed + 101, 0, 0,
                                     _p(p4), _p(r), _p(c), _p(v))
             pairs.append(p4[:k]); R.append(r[:10 * k]); C.append(c[:10 * k]); V.append(v[:10 * k])
         if ee_pairs:
@@ -203,7 +207,7 @@ def cube_system(n: int, *, E: float = 1e5, nu: float = 0.45, rho: float = 1000.0
             r = np.zeros(10 * ee_pairs, np.int32)
             c = np.zeros(10 * ee_pairs, np.int32)
             v = np.zeros((10 * ee_pairs, 9), np.float64)
-            k = lib.syn_contacts_ee(nx, ny, nz, h, _p(X), ne, _p(edges), ee_pairs, dhat, kappa, seed + 202, 0, 0,
+            k = lib.syn_contacts_ee(nx, ny, nz, h, _p(X), ne, _p(edges), ee_pairs, dhat, kappa * dt * dt, seed + 202, 0, 0,
                                     _p(p4), _p(r), _p(c), _p(v))
             pairs.append(p4[:k]); R.append(r[:10 * k]); C.append(c[:10 * k]); V.append(v[:10 * k])
     rows, cols, vals = assemble(np.concatenate(R), np.concatenate(C), np.concatenate(V))
@@ -244,7 +248,7 @@ def hybrid_system(bodies: int = 2000, slab=(100, 100, 10), *, E: float = 1e8, nu
     cr = np.zeros(28 * pairs, np.int32)
     cc = np.zeros(28 * pairs, np.int32)
     cv = np.zeros((28 * pairs, 9), np.float64)
-    w = lib.syn_abd_contacts(bodies, body_size, len(top), _p(top), _p(X), pairs, dhat, kappa, h, seed + 303, off,
+    w = lib.syn_abd_contacts(bodies, body_size, len(top), _p(top), _p(X), pairs, dhat, kappa * dt * dt, h, seed + 303, off,
                              _p(p4), _p(cr), _p(cc), _p(cv))
     R.append(cr[:w]); C.append(cc[:w]); V.append(cv[:w])
     rows, cols, vals = assemble(np.concatenate(R), np.concatenate(C), np.concatenate(V))

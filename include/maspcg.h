@@ -1,0 +1,241 @@
+/*
+ * maspcg.h -- C ABI of the B200 MAS-preconditioned PCG for StiffGIPC's
+ * Newton-step linear solve.
+ *
+ * One handle owns one linear system on one GPU: the neighbour graph and
+ * partition of the FEM vertices (MAS32 hierarchy input), the contact pairs of
+ * the current Newton step, the assembled block-sparse Hessian, the
+ * preconditioner built from it, and the PCG work space.  All entry points
+ * return a maspcg_status; none aborts or exits.  A handle is thread-compatible
+ * (one host thread at a time), not thread-safe.  All device work is issued on
+ * the handle's stream.
+ *
+ * Pointers: every array argument may be a host pointer or a device pointer
+ * (detected with cudaPointerGetAttributes); host arrays are copied in/out
+ * inside the call.
+ *
+ * Layouts restated from the reference (KLBSTL/AGIPC_LEARNING):
+ *   - 3x3 block: 9 doubles, Eigen::Matrix3d column-major, element (r,c) at
+ *     r + 3c (StiffGIPC/linear_system/linear_system/global_matrix.h:18-25);
+ *   - matrix: upper BCOO, row <= col, block (r,c) holds A_rc and implies
+ *     A_cr = A_rc^T (StiffGIPC/linear_system/utils/spmv.cu:28-53);
+ *   - vectors: double, 3 per block row (double3 in the reference);
+ *   - contact pairs: int4 with IPC's sign encoding
+ *     (StiffGIPC/TraditionalMAS32Preconditioner.cu:1550-1962).
+ */
+#ifndef MASPCG_H
+#define MASPCG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MASPCG_API __attribute__((visibility("default")))
+#else
+#define MASPCG_API
+#endif
+
+typedef struct maspcg_handle maspcg_handle;
+
+typedef enum {
+  MASPCG_OK = 0,
+  MASPCG_ERR_INVALID_ARGUMENT = 1,
+  MASPCG_ERR_NULL_HANDLE = 2,
+  MASPCG_ERR_CUDA = 3,
+  MASPCG_ERR_OUT_OF_MEMORY = 4,
+  MASPCG_ERR_NOT_READY = 5, /* call order: graph -> matrix -> build -> solve */
+  MASPCG_ERR_CAPACITY = 6,  /* hierarchy / size overflow (gipc::hierarchy_capacity) */
+  MASPCG_ERR_NO_DEVICE = 7,
+  MASPCG_ERR_UNSUPPORTED = 8
+} maspcg_status;
+
+/* Preconditioner ids follow the reference's P_type (gl_main.cu:1248-1250). */
+typedef enum {
+  MASPCG_PRECOND_BLOCK_JACOBI = 0, /* DiagPreconditioner: 3x3 block inverse */
+  MASPCG_PRECOND_MAS32 = 2,        /* TraditionalMAS32 on the FEM range + ABD 12x12 */
+  MASPCG_PRECOND_NONE = 3
+} maspcg_preconditioner;
+
+typedef enum {
+  /* FP64 matrix, vectors and dots; FP32 MAS apply: the reference's arithmetic */
+  MASPCG_PREC_REFERENCE = 0,
+  /* everything FP32 (matrix, vectors, dots, FP32 domain inverses) */
+  MASPCG_PREC_FP32 = 1,
+  /* FP32 matrix and vectors, 16-bit domain inverses with FP32 accumulation,
+   * FP64 dots, FP64 true residual every refinement_period iterations with
+   * residual replacement (reliable updates); stops on the FP64 true residual */
+  MASPCG_PREC_MIXED = 2
+} maspcg_precision;
+
+typedef enum {
+  MASPCG_GATE_RZ = 0,    /* PCGSolver::pcg: |r^T z| <= tol * r0^T z0, tested after the update */
+  MASPCG_GATE_EUCLID = 1 /* ||r|| <= tol * ||b|| */
+} maspcg_gate;
+
+typedef enum { MASPCG_INV_FP32 = 0, MASPCG_INV_BF16 = 1, MASPCG_INV_FP16 = 2 } maspcg_inverse_storage;
+
+typedef struct {
+  double tolerance;      /* PCGSolverConfig::global_tol_rate (1e-4) */
+  double max_iter_ratio; /* PCGSolverConfig::max_iter_ratio (0.3): max_iter = ratio * dof */
+  int max_iterations;    /* > 0 overrides max_iter_ratio */
+  int gate;              /* maspcg_gate */
+  int precision;         /* maspcg_precision */
+  int inverse_storage;   /* maspcg_inverse_storage (FP32 unless MIXED) */
+  int preconditioner;    /* maspcg_preconditioner */
+  int refinement_period; /* MIXED: iterations between FP64 true residuals (default 16) */
+  int bank_size;         /* MAS bank; 32 (GPU_MAS_BANKSIZE) is the only supported value */
+  int iterations_per_launch; /* PCG iterations per CUDA-graph launch (default 8) */
+} maspcg_config;
+
+typedef struct {
+  int iterations;           /* PCGSolver::pcg return value semantics */
+  int status;               /* maspcg_solve_status */
+  int refinements;          /* FP64 true-residual replacements (MIXED) */
+  int launches;             /* CUDA-graph launches */
+  double rz0;               /* r0^T z0 */
+  double rz_final;          /* last r^T z used by the gate */
+  double rel_res_recursive; /* ||r_k|| / ||b|| of the recursive residual */
+  double rel_res_true;      /* ||b - A x|| / ||b|| in FP64 with the FP64 input matrix */
+  double solve_ms;          /* device time of maspcg_solve (events) */
+} maspcg_result;
+
+typedef enum {
+  MASPCG_SOLVE_RUNNING = 0,
+  MASPCG_SOLVE_CONVERGED = 1,
+  MASPCG_SOLVE_ITERATION_CAP = 2,
+  MASPCG_SOLVE_NONPOSITIVE_CURVATURE = 3, /* p^T A p <= 0 */
+  MASPCG_SOLVE_NONFINITE = 4,
+  MASPCG_SOLVE_INVALID_RZ = 5 /* r^T z <= 0 or non-finite: preconditioner not SPD */
+} maspcg_solve_status;
+
+/* Defaults of PCGSolverConfig (pcg_solver.h:7-17) and the app
+ * (Assets/scene/parameterSetting.txt:14): tol 1e-4, ratio 0.3, rz gate,
+ * reference precision, MAS32. */
+MASPCG_API void maspcg_config_default(maspcg_config* cfg);
+
+MASPCG_API const char* maspcg_status_string(int status);
+/* Message of the last failing call on this handle ("" if none); NULL handle:
+ * the last failure of maspcg_create on this thread. */
+MASPCG_API const char* maspcg_last_error(const maspcg_handle* h);
+
+/* Replaces GlobalLinearSystem::create<PCGSolver>(PCGSolverConfig) and the
+ * preconditioner factory (StiffGIPC/gipc/gipc.cu:67-100,
+ * linear_system/solver/pcg_solver.h:7-24).  Uses the current CUDA device. */
+MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle** out);
+MASPCG_API maspcg_status maspcg_destroy(maspcg_handle* h);
+/* cudaStream_t; NULL selects the handle's own stream. */
+MASPCG_API maspcg_status maspcg_set_stream(maspcg_handle* h, void* stream);
+
+/* Replaces TraditionalMAS32Preconditioner::initPreconditioner_Neighbor +
+ * the caller's cudaMemcpy of d_neighborListInit / d_neighborStart /
+ * d_neighborNumInit / d_partId_map_real / d_real_map_partId +
+ * initPreconditioner_Matrix (TraditionalMAS32Preconditioner.cuh:78-101,
+ * TraditionalMAS32Preconditioner.cu:2889-2977, caller gl_main.cu:1502-1536).
+ *   vert_num              FEM vertices (totalNodes)
+ *   collision_node_offset vertex-number offset of the FEM range in contact pairs
+ *   neighbor_*            vertex neighbour CSR (u32), list of neighbor_list_size
+ *   part_map_real         part_map_size slots (multiple of 32): slot -> vertex or -1
+ *   real_map_part         vert_num entries: vertex -> slot
+ * Lane 0 of every 32-slot bank must hold a vertex (the reference leaves the
+ * bank's component count undefined otherwise). */
+MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int collision_node_offset,
+                                          const uint32_t* neighbor_start, const uint32_t* neighbor_num,
+                                          const uint32_t* neighbor_list, int neighbor_list_size,
+                                          const int* part_map_real, int part_map_size, const int* real_map_part);
+
+/* Contact pairs of the current Newton step: the _collisonPairs / cpNum pair of
+ * TraditionalMAS32Preconditioner::setPreconditioner_bcoo
+ * (TraditionalMAS32Preconditioner.cu:2643-2682).  pairs4 holds 4*n_pairs ints. */
+MASPCG_API maspcg_status maspcg_set_contacts(maspcg_handle* h, const int* pairs4, int n_pairs);
+
+/* The assembled system: GIPCTripletMatrix after Converter::convert
+ * (global_matrix.h:18-203, converter.cu:137-284).  Upper BCOO (row <= col; a
+ * lower entry is taken as its transposed upper block), any order; duplicate
+ * (row,col) blocks are summed.
+ *   block_rows         total block rows of the system
+ *   fem_offset_blocks  first block row of the FEM vertices (MAS range)
+ *   abd_body_count     affine bodies occupying block rows [0, 4*abd_body_count) */
+MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* values9_colmajor, const int* rows,
+                                                const int* cols, int n_blocks, int block_rows, int fem_offset_blocks,
+                                                int abd_body_count);
+
+/* Replaces LocalPreconditioner::assemble of TraditionalMAS32_Preconditioner /
+ * ABDPreconditioner / DiagPreconditioner
+ * (traditional_mas32_preconditioner.cu:20-32, abd_preconditioner.cu:33-36,
+ * diag_preconditioner.cu:74-80): hierarchy for the current contacts,
+ * domain matrices, inverses. */
+MASPCG_API maspcg_status maspcg_build_preconditioner(maspcg_handle* h);
+
+/* Replaces IterativeSolver::solve(x, b) -> iterations
+ * (i_linear_system_solver.h:43-44, pcg_solver.cu:160-326).  b, x: 3*block_rows
+ * doubles.  out may be NULL. */
+MASPCG_API maspcg_status maspcg_solve(maspcg_handle* h, const double* b, double* x, maspcg_result* out);
+
+/* Replaces GlobalLinearSystem::apply_preconditioner(z, r)
+ * (global_linear_system.cu:293-306): z = M^-1 r over the whole system. */
+MASPCG_API maspcg_status maspcg_apply_preconditioner(maspcg_handle* h, const double* r, double* z);
+
+/* Replaces GlobalLinearSystem::spmv(a, x, b, y) (global_linear_system.cu:323-364):
+ * y = a*A*x + b*y in FP64. */
+MASPCG_API maspcg_status maspcg_spmv(maspcg_handle* h, double a, const double* x, double b, double* y);
+
+/* ---- introspection (parity tests, diagnostics) ---- */
+
+typedef struct {
+  int levelnum;          /* computeNumLevels */
+  int total_clusters;    /* totalNumberClusters */
+  int domains;           /* total_clusters / 32 */
+  int vert_num;          /* totalNodes */
+  int part_map_size;     /* totalMapNodes */
+  long long going_next_capacity;
+  int internal_block_rows;
+  int bcsr_blocks;       /* stored blocks of the full BCSR */
+  int failed_domains;    /* domains whose elimination met a pivot <= 0 */
+  long long kernel_launches; /* kernels of this library launched on the handle so far
+                                (graph launches count every kernel node) */
+} maspcg_info;
+
+MASPCG_API maspcg_status maspcg_get_info(maspcg_handle* h, maspcg_info* info);
+
+/* Integer hierarchy after the last build, reference layouts
+ * (TraditionalMAS32Preconditioner.cuh:35-64); any pointer may be NULL; host
+ * pointers.  fine_mask[vert_num], coarse_space_tables[levelnum*vert_num],
+ * going_next[going_next_capacity], level_size[2*(levelnum+1)],
+ * coarse_table[6*vert_num], prefix_original[part_map_size/32]. */
+MASPCG_API maspcg_status maspcg_get_hierarchy(maspcg_handle* h, uint32_t* fine_mask, int* coarse_space_tables,
+                                              int* going_next, int* level_size, int* coarse_table,
+                                              int* prefix_original);
+
+/* Full BCSR (both triangles) in the internal block-row order.  rowptr
+ * [internal_block_rows+1], colidx [bcsr_blocks], values [9*bcsr_blocks]
+ * row-major FP64 (may be NULL), internal_of_row [block_rows] (may be NULL). */
+MASPCG_API maspcg_status maspcg_get_bcsr(maspcg_handle* h, int* rowptr, int* colidx, double* values_rowmajor,
+                                         int* internal_of_row);
+
+/* Domain inverses in the reference's packed layout (GPUMas32MatrixSymf):
+ * 528 upper 3x3 blocks per domain, block (a,b) at 32a - a(a+1)/2 + b, 9 floats
+ * column-major; decoded from whatever precision is stored.  out: domains*528*9. */
+MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out);
+
+/* Assembled FP64 domain matrices (GPUMas32MatrixSymT layout) of the last
+ * build, before the zero-diagonal rule: recomputed on demand. out: domains*528*9. */
+MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* out);
+
+/* Benchmark introspection (no counterpart in the reference): run one stage
+ * `repeats` times between two CUDA events on the handle's stream and return
+ * the mean device milliseconds per run.  Stages:
+ *   0  PCG SpMV with the p.Ap reduction, working precision
+ *   1  full preconditioner apply z = M^-1 r, working precision
+ *   2  MAS level-0 domain apply alone (restriction/coarse levels excluded)
+ *   3  MAS domain assembly + inversion (build)
+ *   4  one full PCG iteration (the captured batch divided by its length)
+ * Vector contents are left unspecified afterwards. */
+MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MASPCG_H */

@@ -1,0 +1,216 @@
+"""CUDA path vs the CPU oracle, through the C ABI (needs a B200).
+
+Integer work is compared bit-exactly (hierarchy, BCSR structure); FP64
+assembly to 1e-12 relative; FP32 inverses and the FP32 MAS apply to 2e-4
+relative; PCG in the reference precision to the same iteration count (+-1)
+and solution within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from agipc_learning_b200 import synth
+from agipc_learning_b200.solver import MasPcg
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cfg0():
+    return synth.config_system(0)
+
+
+@pytest.fixture(scope="module")
+def cfg1_small():
+    return synth.config_system(1, scale=24)
+
+
+def _oracle_mas(s):
+    m = oracle.Mas32.from_system(s)
+    m.reorder(s.pairs)
+    sel = np.nonzero((s.rows >= s.fem_offset) & (s.rows < s.fem_offset + s.fem_count) &
+                     (s.cols >= s.fem_offset) & (s.cols < s.fem_offset + s.fem_count))[0].astype(np.uint32)
+    m.prepare_hessian(s.vals, s.rows, s.cols, sel, s.fem_offset)
+    return m
+
+
+def _compare_hierarchy(g, o):
+    L = o["levelnum"]
+    assert g["levelnum"] == L
+    assert np.array_equal(g["fine_mask"], o["fine_mask"])
+    assert np.array_equal(g["coarse_space_tables"], o["coarse_space_tables"])
+    assert np.array_equal(g["going_next"], o["going_next"])
+    assert np.array_equal(g["level_size"][1:], o["level_size"][1:])
+    assert np.array_equal(g["coarse_table"][:, :L - 1], o["coarse_table"][:, :L - 1])
+    assert np.array_equal(g["prefix_original"], o["prefix_original"])
+    assert g["total_clusters"] == o["total_clusters"]
+
+
+def test_spmv_kat_through_abi():
+    vals, rows, cols, x, y0, a, b = H.spmv_kat_system()
+    ref = H.spmv_kat_expected(vals, rows, cols, x, y0, a, b)
+    with MasPcg(preconditioner="none") as m:
+        m.set_matrix(vals, rows, cols, 20)
+        y = m.spmv(x, a, b, y0.copy())
+    assert np.max(np.abs(y - ref)) <= 1e-10
+
+
+def test_hierarchy_kat_through_abi():
+    valid, start, num, lst, pmr, rmp = H.hierarchy_kat_inputs()
+    exp = H.hierarchy_kat_expected()
+    eye9 = np.eye(3).T.reshape(9)
+    with MasPcg() as m:
+        m.set_graph(valid, 0, start, num, lst, pmr, rmp)
+        m.set_contacts(None)
+        m.set_matrix(np.tile(eye9, (valid, 1)), np.arange(valid, dtype=np.int32), np.arange(valid, dtype=np.int32),
+                     valid)
+        m.build()
+        g = m.hierarchy()
+    assert np.array_equal(g["fine_mask"], exp["fine_mask"])
+    assert np.array_equal(g["coarse_space_tables"][0], exp["coarse"])
+    assert np.array_equal(g["going_next"][:valid], exp["going_next"])
+    assert list(g["prefix_original"]) == exp["prefix"]
+    assert tuple(g["level_size"][1]) == exp["level_size1"]
+
+
+@pytest.mark.parametrize("which", ["cfg0", "cfg1_small"])
+def test_hierarchy_bit_exact(which, request):
+    s = request.getfixturevalue(which)
+    o = _oracle_mas(s)
+    with MasPcg.from_system(s) as m:
+        _compare_hierarchy(m.hierarchy(), o.hierarchy())
+
+
+def test_bcsr_structure_bit_exact(cfg1_small):
+    s = cfg1_small
+    with MasPcg.from_system(s) as m:
+        rp, ci, vals, iof = m.bcsr()
+        nb_int = m.info()["internal_block_rows"]
+    orp, oci, ov = oracle.upper_to_full_bcsr(s.nb, s.rows, s.cols, s.vals)
+    prp, pci, pv = H.permute_full_bcsr(nb_int, iof, orp, oci, ov)
+    assert np.array_equal(rp, prp)
+    assert np.array_equal(ci, pci)
+    assert np.array_equal(vals, pv)
+
+
+@pytest.mark.parametrize("which", ["cfg0", "cfg1_small"])
+def test_domain_matrices_and_inverses(which, request):
+    s = request.getfixturevalue(which)
+    o = _oracle_mas(s)
+    p64, i32 = o.domains()
+    # per-entry bound: the same Galerkin sums over |A| (coarse entries cancel)
+    oa = oracle.Mas32.from_system(s)
+    oa.reorder(s.pairs)
+    oa.prepare_hessian(np.abs(s.vals), s.rows, s.cols, None, s.fem_offset)
+    bound, _ = oa.domains()
+    with MasPcg.from_system(s) as m:
+        assert m.info()["failed_domains"] == 0
+        g64 = m.domain_matrices()
+        gi = m.domain_inverses()
+    assert np.all(np.abs(g64 - p64) <= 1e-13 * bound + 1e-300)
+    # inverses: level-0 domains elementwise, all domains by the reference's
+    # local diagnostic (check_local_matrices :76-147)
+    d0 = s.fem_count // 32
+    iscale = np.abs(i32[:d0]).reshape(d0, -1).max(axis=1)[:, None, None]
+    assert np.max(np.abs(gi[:d0] - i32[:d0]) / iscale) <= 2e-4
+    cg, co = oracle.local_checks(p64, gi), oracle.local_checks(p64, i32)
+    assert all(c["local_spd"] and c["inverse_spd"] for c in cg)
+    assert max(c["inverse_residual"] for c in cg) <= max(1e-3, 10 * max(c["inverse_residual"] for c in co))
+
+
+@pytest.mark.parametrize("which", ["cfg0", "cfg1_small"])
+def test_mas_apply(which, request):
+    s = request.getfixturevalue(which)
+    o = _oracle_mas(s)
+    r = s.b
+    z_ref = o.precondition(r)
+    with MasPcg.from_system(s) as m:
+        z = m.apply_preconditioner(r)
+    assert np.linalg.norm(z - z_ref) / np.linalg.norm(z_ref) <= 2e-4
+
+
+@pytest.mark.parametrize("gate", ["rz", "euclid"])
+def test_pcg_reference_precision_matches_oracle(cfg1_small, gate):
+    s = cfg1_small
+    og = oracle.GATE_RZ if gate == "rz" else oracle.GATE_EUCLID
+    xo, ro, _ = oracle.solve_system(s, gate=og)
+    with MasPcg.from_system(s, gate=gate, precision="reference") as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged"
+    assert abs(res["iterations"] - ro["iterations"]) <= max(1, int(0.1 * ro["iterations"]))
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-4
+    assert res["rel_res_true"] == pytest.approx(ro["rel_res_true"], rel=0.05)
+
+
+def test_kat257_through_abi():
+    k = H.kat257_padded()
+    pub = k["published"]["mas32"]
+    with MasPcg(gate="euclid", tolerance=1e-3, max_iterations=k["limit"] + 1) as m:
+        m.set_graph(k["padded"], 0, k["start"], k["num"], k["lst"], k["ident"], k["ident"])
+        m.set_contacts(None)
+        m.set_matrix(k["vals"], k["rows"], k["cols"], k["padded"])
+        m.build()
+        assert m.info()["domains"] == pub["domains"]
+        x, res = m.solve(k["rhs"])
+    assert res["iterations"] == pub["iterations"]
+    assert res["rel_res_true"] == pytest.approx(pub["true_relative_residual"], abs=5e-7)
+    d = np.linalg.norm(x - k["ref"]) / np.linalg.norm(k["ref"])
+    assert d == pytest.approx(pub["relative_direction_difference"], abs=5e-5)
+
+
+@pytest.mark.parametrize("precision,inverse", [("fp32", "fp32"), ("mixed", "bf16"), ("mixed", "fp16")])
+def test_lower_precision_forms_reach_tolerance(cfg0, precision, inverse):
+    s = cfg0
+    with MasPcg.from_system(s, gate="euclid", precision=precision, inverse=inverse) as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged", res
+    # FP64-verified residual: MIXED stops on it, FP32 is reported against it
+    limit = 1e-4 if precision == "mixed" else 5e-4
+    assert res["rel_res_true"] <= limit, res
+    Ax = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
+    assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) == pytest.approx(res["rel_res_true"], rel=1e-6)
+
+
+def test_block_jacobi_matches_oracle(cfg0):
+    s = cfg0
+    xo, ro, _ = oracle.solve_system(s, precond=oracle.PRECOND_DIAG3, gate=oracle.GATE_EUCLID)
+    with MasPcg.from_system(s, preconditioner="block_jacobi", gate="euclid") as m:
+        x, res = m.solve(s.b)
+    assert abs(res["iterations"] - ro["iterations"]) <= max(1, int(0.02 * ro["iterations"]))
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-5
+
+
+def test_hybrid_abd_fem_matches_oracle():
+    s = synth.config_system(2, scale=16)
+    xo, ro, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID)
+    with MasPcg.from_system(s, gate="euclid") as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged"
+    assert abs(res["iterations"] - ro["iterations"]) <= max(1, int(0.1 * ro["iterations"]))
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-4
+
+
+def test_nonfinite_rhs_reports_status_without_fault(cfg0):
+    s = cfg0
+    b = s.b.copy()
+    b[5] = np.nan
+    with MasPcg.from_system(s) as m:
+        _, res = m.solve(b)
+        assert res["status_name"] in ("nonfinite", "invalid_rz")
+        # the handle stays usable
+        x, res2 = m.solve(s.b)
+        assert res2["status_name"] == "converged"
+
+
+def test_device_pointer_inputs(cfg0):
+    import torch
+    s = cfg0
+    with MasPcg.from_system(s, gate="euclid") as m:
+        xh, rh = m.solve(s.b)
+        bd = torch.from_numpy(s.b).cuda()
+        xd = torch.zeros_like(bd)
+        _, rd = m.solve(bd, xd)
+        torch.cuda.synchronize()
+    assert rh["iterations"] == rd["iterations"]
+    assert np.array_equal(xh, xd.cpu().numpy())
