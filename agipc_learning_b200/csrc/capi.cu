@@ -205,8 +205,8 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     MCK(cudaMallocHost(reinterpret_cast<void**>(&h->h_scal), sizeof(maspcg::PcgScalars)));
     h->scal.resize(1);
     h->grid_stream = 4 * h->sm_count;
-    h->failed.resize(4);
-    MCK(cudaMemset(h->failed.get(), 0, 4 * sizeof(int)));
+    h->failed.resize(8);
+    MCK(cudaMemset(h->failed.get(), 0, 8 * sizeof(int)));
   } catch (const std::exception& e) {
     g_create_error = e.what();
     if (h) maspcg_destroy(h);

@@ -28,6 +28,7 @@
 
 #include "maspcg_internal.cuh"
 #include "pcg_device.cuh"
+#include "spmv_tma.cuh"
 
 namespace maspcg {
 namespace {
@@ -82,62 +83,143 @@ __global__ void k_member_offsets(const unsigned* __restrict__ keys, int nreal, i
 
 __device__ __forceinline__ int pk(int a, int b) { return kBank * a - a * (a + 1) / 2 + b; }
 
-template <typename TI, bool kAssembled>
-__global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a)
+// Accumulate the fine row `row` into the owner lanes: every block whose
+// column's level node `B` lies in bank `bank` is added by lane B % 32.
+// Staging: 16 blocks per chunk through the warp's shared-memory slots, so
+// the 9 doubles of a block are read coalesced and summed in block order.
+__device__ __forceinline__ void gather_row(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                           const double* __restrict__ val64, const int* __restrict__ cmap, int row,
+                                           int fem_off, int c0, int bank, int lane, double* stage, int* sdest,
+                                           double acc[9])
 {
-  __shared__ double prow[2][96];
-  __shared__ double stage[32][16 * 9];
-  __shared__ int sdest[32][16];
-  __shared__ float sscale[96];
-  __shared__ int fail;
+  const int rs = rowptr[row], re = rowptr[row + 1];
+  for (int t0 = rs; t0 < re; t0 += 16) {
+    const int nblk = min(16, re - t0);
+    if (lane < nblk) {
+      int dest = -1;
+      const int u = colidx[t0 + lane] - fem_off;
+      if (u >= 0 && u < c0) {
+        const int B = cmap ? cmap[u] : u;
+        if (B >= 0 && (B >> 5) == bank) dest = B & 31;
+      }
+      sdest[lane] = dest;
+    }
+    const double* src = val64 + 9 * (size_t)t0;
+    for (int q = lane; q < nblk * 9; q += 32) stage[q] = src[q];
+    __syncwarp();
+    for (int j = 0; j < nblk; ++j) {
+      if (sdest[j] == lane) {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) acc[e] += stage[9 * j + e];
+      }
+    }
+    __syncwarp();
+  }
+}
 
-  const int g = blockIdx.x;
-  int L = 0;
-  while (L + 1 < a.lv.levelnum && g >= a.lv.dom_begin[L + 1]) ++L;
-  const int kdom = g - a.lv.dom_begin[L];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) fail = 0;
+struct CoarseArgs {
+  const int* perm[kMaxLevels];
+  const int* cmap[kMaxLevels];
+  int slice_base[kMaxLevels + 1];  // first warp item of each level (levels >= 1)
+  int dom_begin[kMaxLevels + 1];
+  int levelnum;
+  int slice_rows;
+  int nv;
+  const int* rowptr;
+  const int* colidx;
+  const double* val64;
+  int fem_off, c0;
+  double* coarse64;  // (domains - dom_begin[1]) x 32 x 32 blocks, row-major 3x3
+};
 
-  // ---- Galerkin assembly of destination block-row w
+// Coarse-level Galerkin sums: one warp per slice of a level's member list
+// (fine rows grouped by node); the slice's partial block-row is reduced in
+// registers and added to the FP64 coarse domain matrix once per node.
+__global__ void __launch_bounds__(256) k_coarse_assemble(CoarseArgs a)
+{
+  __shared__ double stage_s[8][16 * 9];
+  __shared__ int sdest_s[8][16];
+  const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, lw = threadIdx.x >> 5;
+  int L = 1;
+  while (L + 1 < a.levelnum && item >= a.slice_base[L + 1]) ++L;
+  if (item >= a.slice_base[a.levelnum]) return;
+  const int sl = item - a.slice_base[L];
+  const int p0 = sl * a.slice_rows, p1 = min(p0 + a.slice_rows, a.nv);
+  const int* perm = a.perm[L];
+  const int* cmap = a.cmap[L];
   double acc[9];
 #pragma unroll
   for (int e = 0; e < 9; ++e) acc[e] = 0.0;
-  const int node = kBank * kdom + w;
-  int mb = 0, me = 0;
-  if (L == 0) {
-    if (a.pmr[node] >= 0) me = 1;
-  } else if (node < a.lv.count[L]) {
-    mb = a.off[L][node];
-    me = a.off[L][node + 1];
-  }
-  const int* cmap = (L == 0) ? nullptr : a.cmap[L];
-  const int* members = (L == 0) ? nullptr : a.perm[L];
-  for (int mi = mb; mi < me; ++mi) {
-    const int v = (L == 0) ? node : members[mi];
-    const int row = a.fem_off + v;
-    const int rs = a.rowptr[row], re = a.rowptr[row + 1];
-    for (int t0 = rs; t0 < re; t0 += 16) {
-      const int nblk = min(16, re - t0);
-      if (lane < nblk) {
-        int dest = -1;
-        const int u = a.colidx[t0 + lane] - a.fem_off;
-        if (u >= 0 && u < a.c0) {
-          const int B = (L == 0) ? u : cmap[u];
-          if (B >= 0 && (B >> 5) == kdom) dest = B & 31;
-        }
-        sdest[w][lane] = dest;
-      }
-      const double* src = a.val64 + 9 * (size_t)t0;
-      for (int q = lane; q < nblk * 9; q += 32) stage[w][q] = src[q];
-      __syncwarp();
-      for (int j = 0; j < nblk; ++j) {
-        if (sdest[w][j] == lane) {
+  int node = -1;
+  auto flush = [&](int A) {
+    const int local = a.dom_begin[L] + (A >> 5) - a.dom_begin[1];
+    double* dst = a.coarse64 + (((size_t)local * 32 + (A & 31)) * 32 + lane) * 9;
 #pragma unroll
-          for (int e = 0; e < 9; ++e) acc[e] += stage[w][9 * j + e];
-        }
-      }
-      __syncwarp();
+    for (int e = 0; e < 9; ++e)
+      if (acc[e] != 0.0) atomicAdd(dst + e, acc[e]);
+  };
+  for (int pos = p0; pos < p1; ++pos) {
+    const int v = perm[pos];
+    const int A = cmap[v];
+    if (A != node) {
+      if (node >= 0) flush(node);
+#pragma unroll
+      for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+      node = A;
     }
+    gather_row(a.rowptr, a.colidx, a.val64, cmap, a.fem_off + v, a.fem_off, a.c0, A >> 5, lane, stage_s[lw],
+               sdest_s[lw], acc);
+  }
+  if (node >= 0) flush(node);
+}
+
+// Location of the lower block (a,b), a >= b, in the 17-diagonal layout.
+__device__ __forceinline__ void lower_slot(int a, int b, int& l, int& d)
+{
+  if (a - b <= 16) {
+    l = b;
+    d = a - b;
+  } else {
+    l = a;
+    d = 32 - (a - b);
+  }
+}
+
+// One CTA per domain; thread (w,lane) owns block (w,lane) of the 96x96 FP64
+// matrix.  FP32 storage: in-place Gauss-Jordan inverse, symmetric layout.
+// 16-bit storage: Cholesky A = L L^T, W = L^-1, stored W S^-1 with column
+// scales S, so the applied operator S (W S^-1)^T (W S^-1) S stays SPD whatever
+// the rounding.
+template <typename TI, bool kAssembled>
+__global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom_offset)
+{
+  __shared__ double buf[2][96];
+  __shared__ double stage[32][16 * 9];
+  __shared__ int sdest[32][16];
+  __shared__ float sscale[96];
+  __shared__ unsigned smax[96];
+  __shared__ double spiv[2][2];  // per step: 1/pivot (GJ) or {sqrt(pivot), 1/sqrt(pivot)} (Cholesky)
+  __shared__ int fail;
+
+  const int g = blockIdx.x + dom_offset;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) fail = 0;
+  if (threadIdx.x < 96) smax[threadIdx.x] = 0u;
+
+  double acc[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+  const int d0 = a.lv.dom_begin[1];
+  if (g < d0) {
+    const int slot = kBank * g + w;
+    if (a.pmr[slot] >= 0)
+      gather_row(a.rowptr, a.colidx, a.val64, nullptr, a.fem_off + slot, a.fem_off, a.c0, g, lane, stage[w],
+                 sdest[w], acc);
+  } else {
+    const double* src = a.coarse64 + (((size_t)(g - d0) * 32 + w) * 32 + lane) * 9;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = src[e];
   }
   if (kAssembled && lane >= w) {
     double* o = a.assembled + ((size_t)g * kPacked + pk(w, lane)) * 9;
@@ -151,117 +233,271 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a)
     if (acc[4] == 0.0) acc[4] = 1.0;
     if (acc[8] == 0.0) acc[8] = 1.0;
   }
+  constexpr bool kFactored = !std::is_same<TI, float>::value;
+  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * kInvElems;
 
-  // ---- in-place Gauss-Jordan inversion, thread (w,lane) holds block (w,lane)
+  if (!kFactored) {
+    // ---- in-place Gauss-Jordan inversion (the elimination of __inverse6_P96x96)
+    for (int q = 0; q < kBank; ++q) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int j = 3 * q + c;
+        double* pr = buf[j & 1];
+        if (w == q) {
+          pr[3 * lane + 0] = acc[3 * c + 0];
+          pr[3 * lane + 1] = acc[3 * c + 1];
+          pr[3 * lane + 2] = acc[3 * c + 2];
+          if (lane == q) {  // the pivot's owner inverts it once for the CTA
+            double pv = acc[4 * c];
+            if (!(pv > 0.0) || !isfinite(pv)) {
+              fail = 1;
+              pv = 1.0;
+            }
+            spiv[j & 1][0] = 1.0 / pv;
+          }
+        }
+        const double m0 = __shfl_sync(kFull, acc[c], q);
+        const double m1 = __shfl_sync(kFull, acc[3 + c], q);
+        const double m2 = __shfl_sync(kFull, acc[6 + c], q);
+        __syncthreads();
+        const double inv = spiv[j & 1][0];
+        const double p[3] = {pr[3 * lane], pr[3 * lane + 1], pr[3 * lane + 2]};
+        const double mm[3] = {m0, m1, m2};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const bool rowj = (w == q) && (i == c);
+          const double f = mm[i] * inv;
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) {
+            const bool colj = (lane == q) && (jj == c);
+            double& x = acc[3 * i + jj];
+            if (rowj && colj)
+              x = inv;
+            else if (rowj)
+              x = p[jj] * inv;
+            else if (colj)
+              x = -f;
+            else
+              x = fma(-f, p[jj], x);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
+    const int d = (lane - w) & 31;
+    if (d <= 16) {
+      const bool zero = (d == 16) && (w >= 16);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) out[(d * 9 + 3 * i + j) * kBank + w] = from_d<TI>(zero ? 0.0 : acc[3 * i + j]);
+    }
+    return;
+  }
+
+  // ---- Cholesky, right-looking, lower blocks (w >= lane) hold L afterwards
   for (int q = 0; q < kBank; ++q) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int j = 3 * q + c;
-      double* pr = prow[j & 1];
+      const int k = 3 * q + c;
+      double* col = buf[k & 1];
+      if (lane == q) {
+        col[3 * w + 0] = acc[c];
+        col[3 * w + 1] = acc[3 + c];
+        col[3 * w + 2] = acc[6 + c];
+        if (w == q) {  // the pivot's owner takes its square root once
+          double pv = acc[4 * c];
+          if (!(pv > 0.0) || !isfinite(pv)) {
+            fail = 1;
+            pv = 1.0;
+          }
+          const double r = sqrt(pv);
+          spiv[k & 1][0] = r;
+          spiv[k & 1][1] = 1.0 / r;
+        }
+      }
+      __syncthreads();
+      const double dk = spiv[k & 1][0], invd = spiv[k & 1][1];
+      const double lr[3] = {col[3 * w] * invd, col[3 * w + 1] * invd, col[3 * w + 2] * invd};
+      const double ls[3] = {col[3 * lane] * invd, col[3 * lane + 1] * invd, col[3 * lane + 2] * invd};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+          const int r = 3 * w + i, sc = 3 * lane + jj;
+          double& x = acc[3 * i + jj];
+          if (sc == k && r >= k)
+            x = (r == k) ? dk : lr[i];
+          else if (r > k && sc > k && sc <= r)
+            x = fma(-lr[i], ls[jj], x);
+        }
+    }
+  }
+  __syncthreads();
+  // ---- W = L^-1 by right-looking elimination on the identity
+  double xr[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) xr[e] = (w == lane && (e % 4) == 0) ? 1.0 : 0.0;
+  for (int q = 0; q < kBank; ++q) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int k = 3 * q + c;
+      double* row = buf[k & 1];
+      const double lkk = __shfl_sync(kFull, acc[4 * c], q);  // L[k][k] (warp q, lane q)
       if (w == q) {
-        pr[3 * lane + 0] = acc[3 * c + 0];
-        pr[3 * lane + 1] = acc[3 * c + 1];
-        pr[3 * lane + 2] = acc[3 * c + 2];
+        const double inv = 1.0 / lkk;
+        xr[3 * c + 0] *= inv;
+        xr[3 * c + 1] *= inv;
+        xr[3 * c + 2] *= inv;
+        row[3 * lane + 0] = xr[3 * c + 0];
+        row[3 * lane + 1] = xr[3 * c + 1];
+        row[3 * lane + 2] = xr[3 * c + 2];
       }
       const double m0 = __shfl_sync(kFull, acc[c], q);
       const double m1 = __shfl_sync(kFull, acc[3 + c], q);
       const double m2 = __shfl_sync(kFull, acc[6 + c], q);
       __syncthreads();
-      double piv = pr[j];
-      if (!(piv > 0.0) || !isfinite(piv)) {
-        if (threadIdx.x == 0) fail = 1;
-        piv = 1.0;
-      }
-      const double inv = 1.0 / piv;
-      const double p[3] = {pr[3 * lane], pr[3 * lane + 1], pr[3 * lane + 2]};
+      const double xk[3] = {row[3 * lane], row[3 * lane + 1], row[3 * lane + 2]};
       const double mm[3] = {m0, m1, m2};
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const bool rowj = (w == q) && (i == c);
-        const double f = mm[i] * inv;
+      for (int i = 0; i < 3; ++i)
+        if (3 * w + i > k) {
 #pragma unroll
-        for (int jj = 0; jj < 3; ++jj) {
-          const bool colj = (lane == q) && (jj == c);
-          double& x = acc[3 * i + jj];
-          if (rowj && colj)
-            x = inv;
-          else if (rowj)
-            x = p[jj] * inv;
-          else if (colj)
-            x = -f;
-          else
-            x = fma(-f, p[jj], x);
+          for (int jj = 0; jj < 3; ++jj) xr[3 * i + jj] = fma(-mm[i], xk[jj], xr[3 * i + jj]);
         }
-      }
+    }
+  }
+  // ---- column scales and factored store (lower blocks only)
+  if (w >= lane) {
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) {
+      const float m = (float)fmax(fmax(fabs(xr[jj]), fabs(xr[3 + jj])), fabs(xr[6 + jj]));
+      atomicMax(smax + 3 * lane + jj, __float_as_uint(m));
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
-
-  // ---- store: block (w,lane) at diagonal d = (lane - w) mod 32
-  const int d = (lane - w) & 31;
-  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * kInvElems;
-  constexpr bool kScaled = !std::is_same<TI, float>::value;
-  if (kScaled) {
-    if (lane == w) {
-      sscale[3 * w + 0] = (float)sqrt(fmax(acc[0], 1e-300));
-      sscale[3 * w + 1] = (float)sqrt(fmax(acc[4], 1e-300));
-      sscale[3 * w + 2] = (float)sqrt(fmax(acc[8], 1e-300));
-    }
-    __syncthreads();
-    if (threadIdx.x < 96) a.scale[(size_t)g * 96 + threadIdx.x] = sscale[threadIdx.x];
+  if (threadIdx.x < 96) {
+    float sv = __uint_as_float(smax[threadIdx.x]);
+    if (!(sv > 0.f) || !isfinite(sv)) sv = 1.f;
+    sscale[threadIdx.x] = sv;
+    a.scale[(size_t)g * 96 + threadIdx.x] = sv;
   }
-  if (d <= 16) {
-    const bool zero = (d == 16) && (w >= 16);
+  __syncthreads();
+  if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
+  if (w >= lane) {
+    int l, d;
+    lower_slot(w, lane, l, d);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        double v = zero ? 0.0 : acc[3 * i + j];
-        if (kScaled) v = v / ((double)sscale[3 * w + i] * (double)sscale[3 * lane + j]);
-        out[(d * 9 + 3 * i + j) * kBank + w] = from_d<TI>(v);
+      for (int jj = 0; jj < 3; ++jj) {
+        const double v = (w == lane && jj > i) ? 0.0 : xr[3 * i + jj] / (double)sscale[3 * lane + jj];
+        out[(d * 9 + 3 * i + jj) * kBank + l] = from_d<TI>(v);
+        if (w - lane == 16) out[(16 * 9 + 3 * i + jj) * kBank + w] = from_d<TI>(0.0);
       }
   }
 }
 
 // ------------------------------------------------------------------ apply --
 
-// z_l = (A^-1 x)_l for one domain held by one warp; x, y: the lane's 3 rows.
+// z_l = (M x)_l for one domain held by one warp; x, y: the lane's 3 rows.
+// FP32 storage holds the symmetric inverse (each stored block serves both
+// triangles through a shuffle).  16-bit storage holds the scaled factor
+// V = W S^-1 of M = W^T W (W lower); two passes t = V (S x), y = S V^T t.
 template <typename TI>
 __device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const float* __restrict__ scale, int lane,
                                              const float x[3], float y[3])
 {
-  float s[3] = {1.f, 1.f, 1.f};
-  if (scale) {
-    s[0] = scale[3 * lane];
-    s[1] = scale[3 * lane + 1];
-    s[2] = scale[3 * lane + 2];
-  }
-  const float x0 = x[0] * s[0], x1 = x[1] * s[1], x2 = x[2] * s[2];
-  float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+  if constexpr (std::is_same<TI, float>::value) {
+    const float x0 = x[0], x1 = x[1], x2 = x[2];
+    float y0 = 0.f, y1 = 0.f, y2 = 0.f;
 #pragma unroll
-  for (int d = 0; d < kDiags; ++d) {
-    const int c = (lane + d) & 31;
-    const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
-    float B[9];
+    for (int d = 0; d < kDiags; ++d) {
+      const int c = (lane + d) & 31;
+      const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
+      float B[9];
 #pragma unroll
-    for (int e = 0; e < 9; ++e) B[e] = to_f<TI>(inv[(d * 9 + e) * kBank + lane]);
-    y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
-    y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
-    y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
-    if (d != 0) {
-      const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
-      const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
-      const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
-      const int src = (lane - d) & 31;
-      y0 += __shfl_sync(kFull, t0, src);
-      y1 += __shfl_sync(kFull, t1, src);
-      y2 += __shfl_sync(kFull, t2, src);
+      for (int e = 0; e < 9; ++e) B[e] = inv[(d * 9 + e) * kBank + lane];
+      y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
+      y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
+      y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
+      if (d != 0) {
+        const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
+        const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
+        const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
+        const int src = (lane - d) & 31;
+        y0 += __shfl_sync(kFull, t0, src);
+        y1 += __shfl_sync(kFull, t1, src);
+        y2 += __shfl_sync(kFull, t2, src);
+      }
     }
+    y[0] = y0;
+    y[1] = y1;
+    y[2] = y2;
+  } else {
+    const float s0 = scale[3 * lane], s1 = scale[3 * lane + 1], s2 = scale[3 * lane + 2];
+    const float x0 = x[0] * s0, x1 = x[1] * s1, x2 = x[2] * s2;
+    // pass 1: t = V xs
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+#pragma unroll 4
+    for (int d = 0; d < kDiags; ++d) {
+      float B[9];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) B[e] = to_f<TI>(inv[(d * 9 + e) * kBank + lane]);
+      if (d == 0) {
+        t0 += B[0] * x0 + B[1] * x1 + B[2] * x2;
+        t1 += B[3] * x0 + B[4] * x1 + B[5] * x2;
+        t2 += B[6] * x0 + B[7] * x1 + B[8] * x2;
+      } else {
+        const int c = (lane + d) & 31;
+        const bool below = lane + d >= 32;  // stored block is V_{lane,c}, c < lane
+        const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
+        const float u0 = below ? c0 : x0, u1 = below ? c1 : x1, u2 = below ? c2 : x2;
+        const float p0 = B[0] * u0 + B[1] * u1 + B[2] * u2;
+        const float p1 = B[3] * u0 + B[4] * u1 + B[5] * u2;
+        const float p2 = B[6] * u0 + B[7] * u1 + B[8] * u2;
+        const int src = (lane - d) & 31;
+        const float r0 = __shfl_sync(kFull, below ? 0.f : p0, src);
+        const float r1 = __shfl_sync(kFull, below ? 0.f : p1, src);
+        const float r2 = __shfl_sync(kFull, below ? 0.f : p2, src);
+        t0 += (below ? p0 : 0.f) + r0;
+        t1 += (below ? p1 : 0.f) + r1;
+        t2 += (below ? p2 : 0.f) + r2;
+      }
+    }
+    // pass 2: z = V^T t
+    float z0 = 0.f, z1 = 0.f, z2 = 0.f;
+#pragma unroll 4
+    for (int d = 0; d < kDiags; ++d) {
+      float B[9];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) B[e] = to_f<TI>(inv[(d * 9 + e) * kBank + lane]);
+      if (d == 0) {
+        z0 += B[0] * t0 + B[3] * t1 + B[6] * t2;
+        z1 += B[1] * t0 + B[4] * t1 + B[7] * t2;
+        z2 += B[2] * t0 + B[5] * t1 + B[8] * t2;
+      } else {
+        const int c = (lane + d) & 31;
+        const bool below = lane + d >= 32;
+        const float c0 = __shfl_sync(kFull, t0, c), c1 = __shfl_sync(kFull, t1, c), c2 = __shfl_sync(kFull, t2, c);
+        const float u0 = below ? t0 : c0, u1 = below ? t1 : c1, u2 = below ? t2 : c2;
+        const float p0 = B[0] * u0 + B[3] * u1 + B[6] * u2;
+        const float p1 = B[1] * u0 + B[4] * u1 + B[7] * u2;
+        const float p2 = B[2] * u0 + B[5] * u1 + B[8] * u2;
+        const int src = (lane - d) & 31;
+        const float r0 = __shfl_sync(kFull, below ? p0 : 0.f, src);
+        const float r1 = __shfl_sync(kFull, below ? p1 : 0.f, src);
+        const float r2 = __shfl_sync(kFull, below ? p2 : 0.f, src);
+        z0 += (below ? 0.f : p0) + r0;
+        z1 += (below ? 0.f : p1) + r1;
+        z2 += (below ? 0.f : p2) + r2;
+      }
+    }
+    y[0] = z0 * s0;
+    y[1] = z1 * s1;
+    y[2] = z2 * s2;
   }
-  y[0] = y0 * s[0];
-  y[1] = y1 * s[1];
-  y[2] = y2 * s[2];
 }
 
 // Leader of each key group gets the group sum in ascending lane order.
@@ -428,6 +664,125 @@ __global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __r
   }
 }
 
+// Domain apply with the inverse staged by TMA: each warp streams its
+// domains' stored blocks (one contiguous bulk copy per domain) into a
+// double-buffered shared-memory slot and applies them from there, so the
+// two passes of the factored form read global memory once.  Level 0 reads
+// r / writes z (plus the coarse correction and r.z); coarse levels read and
+// write the coarse R/Z arrays.
+constexpr int kApplyWarps = 4;
+
+template <typename TI, typename Tv, typename Tacc, bool kLevel0>
+__global__ void __launch_bounds__(kApplyWarps * 32, 2)
+    k_apply_tma(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
+                PcgScalars* s, int g_begin, int g_end, int* err)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[kApplyWarps][2];
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  constexpr unsigned kBytes = kInvElems * sizeof(TI);
+  const int lw = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warps_total = gridDim.x * kApplyWarps;
+  const int gw = blockIdx.x * kApplyWarps + lw;
+  unsigned char* buf0 = smem + (size_t)lw * 2 * kBytes;
+  unsigned char* buf1 = buf0 + kBytes;
+  const TI* inv = reinterpret_cast<const TI*>(a.inv);
+  if (lane == 0) {
+    mbar_init(&bar[lw][0], 1);
+    mbar_init(&bar[lw][1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const int g0 = g_begin + gw, g1 = g0 + warps_total;
+    if (g0 < g_end) {
+      mbar_expect_tx(&bar[lw][0], kBytes);
+      tma_bulk_g2s(buf0, inv + (size_t)g0 * kInvElems, kBytes, &bar[lw][0]);
+    }
+    if (g1 < g_end) {
+      mbar_expect_tx(&bar[lw][1], kBytes);
+      tma_bulk_g2s(buf1, inv + (size_t)g1 * kInvElems, kBytes, &bar[lw][1]);
+    }
+  }
+  __syncwarp();
+  unsigned ph0 = 0, ph1 = 0;
+  Tacc dot = 0;
+  int i = 0;
+  bool ok = true;
+  for (int g = g_begin + gw; g < g_end; g += warps_total, ++i) {
+    const int st = i & 1;
+    const bool w = mbar_wait(&bar[lw][st], st ? ph1 : ph0);
+    if (w) {
+      if (st)
+        ph1 ^= 1u;
+      else
+        ph0 ^= 1u;
+    }
+    if (!__all_sync(kFull, w)) {
+      ok = false;
+      break;
+    }
+    const TI* blk = reinterpret_cast<const TI*>(st ? buf1 : buf0);
+    const float* sc = a.scale + (size_t)g * 96;
+    float x[3], y[3];
+    size_t base;
+    if (kLevel0) {
+      base = 3 * (size_t)(a.fem_off + kBank * g + lane);
+      x[0] = (float)r[base];
+      x[1] = (float)r[base + 1];
+      x[2] = (float)r[base + 2];
+    } else {
+      base = (size_t)(kBank * g + lane - a.c0) * 3;
+      x[0] = a.coarse_r[base];
+      x[1] = a.coarse_r[base + 1];
+      x[2] = a.coarse_r[base + 2];
+    }
+    domain_apply<TI>(blk, sc, lane, x, y);
+    __syncwarp();
+    if (lane == 0 && g + 2 * warps_total < g_end) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&bar[lw][st], kBytes);
+      tma_bulk_g2s(st ? buf1 : buf0, inv + (size_t)(g + 2 * warps_total) * kInvElems, kBytes, &bar[lw][st]);
+    }
+    if (kLevel0) {
+      const int slot = kBank * g + lane;
+      const int c1 = a.cmap1[slot];
+      if (c1 >= 0) {
+        y[0] += a.zacc1[3 * (size_t)c1];
+        y[1] += a.zacc1[3 * (size_t)c1 + 1];
+        y[2] += a.zacc1[3 * (size_t)c1 + 2];
+      } else {
+        y[0] = y[1] = y[2] = 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const Tv zv = (Tv)y[q];
+        z[base + q] = zv;
+        dot += (Tacc)r[base + q] * (Tacc)zv;
+      }
+    } else {
+      a.coarse_z[base] = y[0];
+      a.coarse_z[base + 1] = y[1];
+      a.coarse_z[base + 2] = y[2];
+    }
+  }
+  if (!ok) {
+    if (lane == 0) {
+      atomicExch(err, 1);
+      for (int j = 0; j < 2; ++j) {
+        const int gj = g_begin + gw + (i + j) * warps_total;
+        if (gj < g_end) mbar_wait(&bar[lw][(i + j) & 1], ((i + j) & 1) ? ph1 : ph0);
+      }
+      if (s) s->status = MASPCG_SOLVE_NONFINITE;
+    }
+    return;
+  }
+  if (kLevel0 && partial) {
+    Tacc total = 0;
+    if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
+                          total) &&
+        threadIdx.x == 0 && mode > 0)
+      rz_update(s, (double)total, mode);
+  }
+}
+
 void launch_factor(maspcg_handle* h, double* assembled_out);
 
 void build_mas_domains(maspcg_handle* h, double* assembled_out)
@@ -485,6 +840,34 @@ void launch_factor(maspcg_handle* h, double* assembled_out)
   const LevelInfo& lv = h->lv;
   const int c0 = h->c0;
   const int storage = h->cfg.inverse_storage;
+  const int d0 = lv.dom_begin[1];
+  const int coarse_domains = lv.domains - d0;
+  // coarse-level Galerkin sums
+  h->coarse64.resize((size_t)std::max(coarse_domains, 1) * 1024 * 9);
+  MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * 1024 * 9 * sizeof(double), st));
+  CoarseArgs ca{};
+  ca.levelnum = lv.levelnum;
+  ca.slice_rows = 64;
+  ca.nv = h->nv;
+  int items = 0;
+  for (int l = 1; l < lv.levelnum; ++l) {
+    ca.perm[l] = h->perm[l].get();
+    ca.cmap[l] = h->cmap[l].get();
+    ca.slice_base[l] = items;
+    items += ceil_div(h->nv, ca.slice_rows);
+  }
+  ca.slice_base[lv.levelnum] = items;
+  for (int l = 0; l <= lv.levelnum; ++l) ca.dom_begin[l] = lv.dom_begin[l];
+  ca.rowptr = h->rowptr.get();
+  ca.colidx = h->colidx.get();
+  ca.val64 = h->val64.get();
+  ca.fem_off = h->fem_off;
+  ca.c0 = c0;
+  ca.coarse64 = h->coarse64.get();
+  if (items > 0) {
+    k_coarse_assemble<<<ceil_div((long long)items * 32, 256), 256, 0, st>>>(ca);
+    MLAUNCHED(h);
+  }
   FactorArgs fa{};
   fa.lv = lv;
   for (int l = 1; l < lv.levelnum; ++l) {
@@ -502,22 +885,25 @@ void launch_factor(maspcg_handle* h, double* assembled_out)
   fa.scale = storage == MASPCG_INV_FP32 ? nullptr : h->inv_scale.get();
   fa.failed = h->failed.get() + 3;
   fa.assembled = assembled_out;
+  fa.coarse64 = h->coarse64.get();
   const int grid = lv.domains;
+#define MAS_FACTOR(TI, ASM) k_domain_factor<TI, ASM><<<grid, 1024, 0, st>>>(fa, 0)
   if (assembled_out) {
     if (storage == MASPCG_INV_FP32)
-      k_domain_factor<float, true><<<grid, 1024, 0, st>>>(fa);
+      MAS_FACTOR(float, true);
     else if (storage == MASPCG_INV_BF16)
-      k_domain_factor<__nv_bfloat16, true><<<grid, 1024, 0, st>>>(fa);
+      MAS_FACTOR(__nv_bfloat16, true);
     else
-      k_domain_factor<__half, true><<<grid, 1024, 0, st>>>(fa);
+      MAS_FACTOR(__half, true);
   } else {
     if (storage == MASPCG_INV_FP32)
-      k_domain_factor<float, false><<<grid, 1024, 0, st>>>(fa);
+      MAS_FACTOR(float, false);
     else if (storage == MASPCG_INV_BF16)
-      k_domain_factor<__nv_bfloat16, false><<<grid, 1024, 0, st>>>(fa);
+      MAS_FACTOR(__nv_bfloat16, false);
     else
-      k_domain_factor<__half, false><<<grid, 1024, 0, st>>>(fa);
+      MAS_FACTOR(__half, false);
   }
+#undef MAS_FACTOR
   MLAUNCHED(h);
   MCK(cudaGetLastError());
 }
@@ -539,6 +925,21 @@ ApplyArgs make_apply_args(maspcg_handle* h)
   return a;
 }
 
+template <typename TI, typename Tv, typename Tacc, bool kLevel0>
+void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, Tacc* partial, int part_base,
+                      int total_parts, int mode, PcgScalars* s, int g_begin, int g_end, int grid)
+{
+  constexpr int bytes = kApplyWarps * 2 * kInvElems * (int)sizeof(TI);
+  static bool configured = false;
+  if (!configured) {
+    MCK(cudaFuncSetAttribute(k_apply_tma<TI, Tv, Tacc, kLevel0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    configured = true;
+  }
+  k_apply_tma<TI, Tv, Tacc, kLevel0><<<grid, kApplyWarps * 32, bytes, h->stream>>>(
+      a, r, z, partial, part_base, total_parts, mode, s, g_begin, g_end, h->failed.get() + 4);
+  MLAUNCHED(h);
+}
+
 template <typename TI, typename Tv, typename Tacc>
 void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                  int grid0, PcgScalars* s)
@@ -547,18 +948,34 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
   const int banks0 = h->c0 / kBank;
-  k_restrict0<Tv><<<ceil_div((long long)banks0 * 32, kTpb), kTpb, 0, st>>>(a, r, s); MLAUNCHED(h);
+  constexpr bool kStaged = !std::is_same<TI, float>::value;
+  k_restrict0<Tv><<<ceil_div((long long)banks0 * 32, kTpb), kTpb, 0, st>>>(a, r, s);
+  MLAUNCHED(h);
   for (int l = 2; l < lv.levelnum; ++l) {
     const int banks = ceil_div(lv.count[l - 1], kBank);
-    k_restrictL<<<ceil_div((long long)banks * 32, kTpb), kTpb, 0, st>>>(a, l - 1, s); MLAUNCHED(h);
-  }
-  const int coarse_domains = lv.domains - lv.dom_begin[1];
-  if (coarse_domains > 0) {
-    k_coarse_apply<TI><<<ceil_div((long long)coarse_domains * 32, kTpb), kTpb, 0, st>>>(a, s);
+    k_restrictL<<<ceil_div((long long)banks * 32, kTpb), kTpb, 0, st>>>(a, l - 1, s);
     MLAUNCHED(h);
   }
-  k_prolong1<<<ceil_div(lv.count[1], kTpb), kTpb, 0, st>>>(a, s); MLAUNCHED(h);
-  k_level0_apply<TI, Tv, Tacc><<<grid0, kTpb, 0, st>>>(a, r, z, partial, part_base, total_parts, mode, s); MLAUNCHED(h);
+  const int d0 = lv.dom_begin[1];
+  const int coarse_domains = lv.domains - d0;
+  if (coarse_domains > 0) {
+    if (kStaged) {
+      launch_apply_tma<TI, Tv, Tacc, false>(h, a, r, z, nullptr, 0, 0, 0, s, d0, lv.domains,
+                                            ceil_div(coarse_domains, kApplyWarps));
+    } else {
+      k_coarse_apply<TI><<<ceil_div((long long)coarse_domains * 32, kTpb), kTpb, 0, st>>>(a, s);
+      MLAUNCHED(h);
+    }
+  }
+  k_prolong1<<<ceil_div(lv.count[1], kTpb), kTpb, 0, st>>>(a, s);
+  MLAUNCHED(h);
+  if (kStaged) {
+    const int grid = std::max(1, std::min(ceil_div(d0, kApplyWarps), 2 * h->sm_count));
+    launch_apply_tma<TI, Tv, Tacc, true>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid);
+  } else {
+    k_level0_apply<TI, Tv, Tacc><<<grid0, kTpb, 0, st>>>(a, r, z, partial, part_base, total_parts, mode, s);
+    MLAUNCHED(h);
+  }
 }
 }  // namespace
 
@@ -585,16 +1002,19 @@ template <typename Tv, typename Tacc>
 void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s)
 {
   ApplyArgs a = make_apply_args(h);
+  const int d0 = h->lv.dom_begin[1];
   switch (h->cfg.inverse_storage) {
     case MASPCG_INV_BF16:
-      k_level0_apply<__nv_bfloat16, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s);
+      launch_apply_tma<__nv_bfloat16, Tv, Tacc, true>(h, a, r, z, partial, 0, grid0, 0, s, 0, d0, grid0);
       break;
     case MASPCG_INV_FP16:
-      k_level0_apply<__half, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s);
+      launch_apply_tma<__half, Tv, Tacc, true>(h, a, r, z, partial, 0, grid0, 0, s, 0, d0, grid0);
       break;
-    default: k_level0_apply<float, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s); break;
+    default:
+      k_level0_apply<float, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s);
+      MLAUNCHED(h);
+      break;
   }
-  MLAUNCHED(h);
   MCK(cudaGetLastError());
 }
 template void mas_level0_only<float, float>(maspcg_handle*, const float*, float*, float*, int, PcgScalars*);
@@ -610,6 +1030,8 @@ template void mas_apply<double, double>(maspcg_handle*, const double*, double*, 
 int mas_level0_grid(maspcg_handle* h)
 {
   const int warps = h->lv.dom_begin[1];
+  if (h->cfg.inverse_storage != MASPCG_INV_FP32)  // TMA-staged apply (launch_apply_tma)
+    return std::max(1, std::min(ceil_div(warps, kApplyWarps), 2 * h->sm_count));
   return std::max(1, std::min(ceil_div((long long)warps * 32, kTpb), 8 * h->sm_count));
 }
 
@@ -652,23 +1074,53 @@ void decode_inverses(maspcg_handle* h, float* out)
       f = std::ldexp((float)(man | 0x400), (int)ex - 25);
     return sign ? -f : f;
   };
-  for (int g = 0; g < D; ++g)
+  if (storage == MASPCG_INV_FP32) {
+    for (int g = 0; g < D; ++g)
+      for (int a = 0; a < kBank; ++a)
+        for (int b = a; b < kBank; ++b) {
+          // block (a,b) lives at lane a, diagonal b-a when that is <= 16, else it
+          // is the transpose of (b,a) at lane b, diagonal 32-(b-a).
+          const int d = b - a;
+          const bool direct = d <= 16;
+          const int lane = direct ? a : b, dd = direct ? d : 32 - d;
+          float* o = out + ((size_t)g * kPacked + (kBank * a - a * (a + 1) / 2 + b)) * 9;
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+              const int ei = direct ? 3 * i + j : 3 * j + i;
+              o[i + 3 * j] = elem((size_t)g * kInvElems + (size_t)(dd * 9 + ei) * kBank + lane);
+            }
+        }
+    return;
+  }
+  // factored storage: rebuild W (lower, column-scaled) and form W^T W
+  std::vector<double> W(96 * 96), M(96 * 96);
+  for (int g = 0; g < D; ++g) {
+    std::fill(W.begin(), W.end(), 0.0);
+    const float* scg = sc.data() + (size_t)g * 96;
+    for (int d = 0; d < kDiags; ++d)
+      for (int l = 0; l < kBank; ++l) {
+        if (d == 16 && l >= 16) continue;
+        const int c = (l + d) & 31;
+        const int ra = (d == 0 || l + d >= 32) ? l : c;  // block row (the larger index)
+        const int cb = (d == 0 || l + d >= 32) ? c : l;
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            W[(3 * ra + i) * 96 + 3 * cb + j] =
+                (double)elem((size_t)g * kInvElems + (size_t)(d * 9 + 3 * i + j) * kBank + l) * scg[3 * cb + j];
+      }
+    for (int r = 0; r < 96; ++r)
+      for (int q = r; q < 96; ++q) {
+        double acc = 0;
+        for (int k = std::max(r, q); k < 96; ++k) acc += W[k * 96 + r] * W[k * 96 + q];
+        M[r * 96 + q] = M[q * 96 + r] = acc;
+      }
     for (int a = 0; a < kBank; ++a)
       for (int b = a; b < kBank; ++b) {
-        // block (a,b) lives at lane a, diagonal d=b-a when d <= 16, else it is the
-        // transpose of (b,a) at lane b, diagonal 32-(b-a).
-        const int d = b - a;
-        const bool direct = d <= 16 && !(d == 16 && a >= 16);
-        const int lane = direct ? a : b, dd = direct ? d : (32 - d) & 31;
         float* o = out + ((size_t)g * kPacked + (kBank * a - a * (a + 1) / 2 + b)) * 9;
         for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j) {
-            const int ei = direct ? 3 * i + j : 3 * j + i;
-            float v = elem((size_t)g * kInvElems + (size_t)(dd * 9 + ei) * kBank + lane);
-            if (storage != MASPCG_INV_FP32) v *= sc[(size_t)g * 96 + 3 * a + i] * sc[(size_t)g * 96 + 3 * b + j];
-            o[i + 3 * j] = v;  // column-major
-          }
+          for (int j = 0; j < 3; ++j) o[i + 3 * j] = (float)M[(3 * a + i) * 96 + 3 * b + j];
       }
+  }
 }
 
 }  // namespace maspcg

@@ -134,6 +134,7 @@ struct FactorArgs {
   float* scale;                  // 96 per domain (16-bit storage)
   int* failed;                   // count of domains with a pivot <= 0
   double* assembled;             // optional: packed FP64 domain matrices (reference layout)
+  const double* coarse64;        // coarse-level domain matrices (32x32 blocks, row-major 3x3)
 };
 
 }  // namespace maspcg
@@ -186,6 +187,7 @@ struct maspcg_handle {
   maspcg::DBuf<int> failed;
   int failed_domains = 0;
   maspcg::DBuf<float> coarse_r, coarse_z, zacc1;
+  maspcg::DBuf<double> coarse64;
   maspcg::DBuf<double> abd_inv64;
   maspcg::DBuf<float> abd_inv32;
   maspcg::DBuf<double> diag_inv64;

@@ -282,8 +282,8 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   h->kv_sorted.resize(m);
   h->seg_head.resize(m);
   h->seg_start.resize(m + 1);
-  h->failed.resize(4);
-  MCK(cudaMemsetAsync(h->failed.get(), 0, sizeof(int) * 4, st));
+  h->failed.resize(8);
+  MCK(cudaMemsetAsync(h->failed.get(), 0, sizeof(int) * 8, st));
   k_make_keys<<<ceil_div(n, kTpb), kTpb, 0, st>>>(rows, cols, n, nb, h->int_of_row.get(), bits, h->keys.get(),
                                                  h->kv.get(), h->failed.get()); MLAUNCHED(h);
   // keys use 2*bits bits; the all-ones sentinel still sorts last on 2*bits+1
@@ -309,7 +309,7 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   const int nnzb = tail[0] + tail[1];
   const int m_valid = m - flags[2];  // sentinels (one per diagonal input block) sort last
   h->nnzb = nnzb;
-  h->colidx.resize(nnzb);
+  h->colidx.resize(nnzb, 4);  // 16-byte tail for TMA bulk copies
   h->val64.resize((size_t)9 * nnzb, 2);
   h->val32.resize((size_t)9 * nnzb, 4);
   h->row_count.resize(nb_int + 1);

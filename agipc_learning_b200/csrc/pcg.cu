@@ -20,6 +20,7 @@
 #include "maspcg_internal.cuh"
 #include "pcg_device.cuh"
 #include "spmv_row.cuh"
+#include "spmv_tma.cuh"
 
 namespace maspcg {
 
@@ -89,6 +90,140 @@ __global__ void __launch_bounds__(kTpb) k_spmv_dot(const int* __restrict__ rowpt
       ap[3 * (size_t)row + sub] = y;
       dot += (Tacc)p[3 * (size_t)row + sub] * (Tacc)y;
     }
+  }
+  Tacc total = 0;
+  if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
+      threadIdx.x == 0) {
+    const double pap = (double)total;
+    s->pap = pap;
+    if (!isfinite(pap)) {
+      s->status = MASPCG_SOLVE_NONFINITE;
+      s->iterations = s->k;
+    } else if (!(pap > 0.0)) {
+      s->status = MASPCG_SOLVE_NONPOSITIVE_CURVATURE;
+      s->iterations = s->k;
+    } else {
+      s->alpha = s->rz / pap;
+    }
+  }
+}
+
+// Ap = A p with the block stream staged by TMA (spmv_tma.cuh) and p.Ap;
+// last block: alpha.  `err` records an expired mbarrier wait.
+template <typename Tm, typename Tv, typename Tacc>
+__global__ void __launch_bounds__(kTmaThreads, 2)
+    k_spmv_tma(const int* __restrict__ rowptr, const int* __restrict__ colidx, const Tm* __restrict__ val,
+               const Tv* __restrict__ p, Tv* ap, int nrows, Tacc* partial, PcgScalars* s, int* err)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  if (!running(s)) return;
+  using St = TmaStage<Tm>;
+  unsigned char* sval0 = smem;
+  unsigned char* sval1 = smem + St::kValBytes;
+  unsigned char* scol0 = smem + 2 * St::kValBytes;
+  unsigned char* scol1 = smem + 2 * St::kValBytes + St::kColBytes;
+  const int nchunks = (nrows + kTmaRows - 1) / kTmaRows;
+  const int tid = threadIdx.x, grp = tid >> 4, sub = tid & 15;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto staged = [&](int chunk) {
+    const int r0 = chunk * kTmaRows, r1 = min(r0 + kTmaRows, nrows);
+    const int nb = rowptr[r1] - rowptr[r0];
+    return nb > 0 && nb <= St::kCap;
+  };
+  if (tid == 0) {
+    const int c0 = blockIdx.x, c1 = blockIdx.x + gridDim.x;
+    if (c0 < nchunks) chunk_issue<Tm>(c0, nrows, rowptr, val, colidx, sval0, scol0, &bar[0]);
+    if (c1 < nchunks) chunk_issue<Tm>(c1, nrows, rowptr, val, colidx, sval1, scol1, &bar[1]);
+  }
+  unsigned phase0 = 0, phase1 = 0;
+  Tacc dot = 0;
+  int i = 0;
+  bool ok = true;
+  for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x, ++i) {
+    const int st = i & 1;
+    const int r0 = chunk * kTmaRows, r1 = min(r0 + kTmaRows, nrows);
+    const int b0 = rowptr[r0];
+    const bool stg = staged(chunk);
+    if (stg) {
+      const bool w = mbar_wait(st ? &bar[1] : &bar[0], st ? phase1 : phase0);
+      if (w) {
+        if (st)
+          phase1 ^= 1u;
+        else
+          phase0 ^= 1u;
+      }
+      if (!__syncthreads_and(w)) {
+        ok = false;
+        break;
+      }
+    }
+    const int row = r0 + grp;
+    const bool has = row < r1;
+    const int rs = has ? rowptr[row] : 0, re = has ? rowptr[row + 1] : 0;
+    typename AccOf<Tm>::type acc[3];
+    if (stg) {
+      using A = typename AccOf<Tm>::type;
+      const unsigned char* sv = st ? sval1 : sval0;
+      const unsigned char* sc = st ? scol1 : scol0;
+      const Tm* vb = reinterpret_cast<const Tm*>(sv + (((size_t)b0 * 9 * sizeof(Tm)) & 15));
+      const int* cb = reinterpret_cast<const int*>(sc + (((size_t)b0 * 4) & 15));
+      A a0 = 0, a1 = 0, a2 = 0;
+      for (int t = rs + sub; t < re; t += 16) {
+        const int lt = t - b0;
+        const int c = cb[lt];
+        const Tm* B = vb + 9 * lt;
+        const A x0 = (A)ldv(p + 3 * (size_t)c), x1 = (A)ldv(p + 3 * (size_t)c + 1), x2 = (A)ldv(p + 3 * (size_t)c + 2);
+        a0 += (A)B[0] * x0 + (A)B[1] * x1 + (A)B[2] * x2;
+        a1 += (A)B[3] * x0 + (A)B[4] * x1 + (A)B[5] * x2;
+        a2 += (A)B[6] * x0 + (A)B[7] * x1 + (A)B[8] * x2;
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(kFull, a0, o, 16);
+        a1 += __shfl_xor_sync(kFull, a1, o, 16);
+        a2 += __shfl_xor_sync(kFull, a2, o, 16);
+      }
+      acc[0] = a0;
+      acc[1] = a1;
+      acc[2] = a2;
+    } else {
+      row_product<Tm, Tv, 16>(rs, re, colidx, val, p, sub, acc);
+    }
+    if (has && sub < 3) {
+      const Tv y = (Tv)acc[sub];
+      ap[3 * (size_t)row + sub] = y;
+      dot += (Tacc)p[3 * (size_t)row + sub] * (Tacc)y;
+    }
+    __syncthreads();  // the stage is free again
+    if (tid == 0) {
+      const int nxt = chunk + 2 * gridDim.x;
+      if (nxt < nchunks) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        chunk_issue<Tm>(nxt, nrows, rowptr, val, colidx, st ? sval1 : sval0, st ? scol1 : scol0,
+                        st ? &bar[1] : &bar[0]);
+      }
+    }
+  }
+  if (!ok) {
+    // drain the copies this CTA still has in flight (bounded), report, leave
+    if (tid == 0) {
+      atomicExch(err, 1);
+      for (int j = 0; j < 2; ++j) {
+        const int chunk = blockIdx.x + (i + j) * gridDim.x;
+        if (chunk < nchunks && staged(chunk)) {
+          const int stj = (i + j) & 1;
+          mbar_wait(stj ? &bar[1] : &bar[0], stj ? phase1 : phase0);
+        }
+      }
+      s->status = MASPCG_SOLVE_NONFINITE;
+    }
+    return;
   }
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
@@ -336,13 +471,28 @@ struct Engine {
   {
     cudaStream_t st = h->stream;
     k_update_p<Tv><<<gstream, kTpb, 0, st>>>(V(h->vz), V(h->vp), n, s); MLAUNCHED(h);
-    k_spmv_dot<Tm, Tv, Tacc, 16><<<gspmv, kTpb, 0, st>>>(h->rowptr.get(), h->colidx.get(), matrix(), V(h->vp),
-                                                        V(h->vap), h->nb_int, partial(), s); MLAUNCHED(h);
+    spmv_tma(s);
     k_update_xr<Tv, Tacc><<<gstream, kTpb, 0, st>>>(V(h->vx), V(h->vr), V(h->vp), V(h->vap), n, mixed ? 1 : 0,
                                                    partial(), s); MLAUNCHED(h);
   }
 
   const Tm* matrix();
+
+  void spmv_tma(PcgScalars* s)
+  {
+    using St = TmaStage<Tm>;
+    constexpr int bytes = 2 * (St::kValBytes + St::kColBytes);
+    static bool configured = false;
+    if (!configured) {
+      MCK(cudaFuncSetAttribute(k_spmv_tma<Tm, Tv, Tacc>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      configured = true;
+    }
+    const int grid = std::max(1, std::min(2 * h->sm_count, ceil_div(h->nb_int, kTmaRows)));
+    k_spmv_tma<Tm, Tv, Tacc><<<grid, kTmaThreads, bytes, h->stream>>>(h->rowptr.get(), h->colidx.get(), matrix(),
+                                                                      V(h->vp), V(h->vap), h->nb_int, partial(), s,
+                                                                      h->failed.get() + 4);
+    MLAUNCHED(h);
+  }
 
   void true_residual(PcgScalars* s)
   {
@@ -380,7 +530,8 @@ struct Engine {
     MREQ(stage != 2 || mas, MASPCG_ERR_NOT_READY, "stage 2 needs a MAS32 preconditioner");
     auto once = [&]() {
       switch (stage) {
-        case 0:
+        case 0: spmv_tma(s); break;
+        case 4:
           k_spmv_dot<Tm, Tv, Tacc, 16><<<gspmv, kTpb, 0, st>>>(h->rowptr.get(), h->colidx.get(), matrix(), V(h->vp),
                                                               V(h->vap), h->nb_int, partial(), s);
           MLAUNCHED(h);
@@ -417,6 +568,7 @@ struct Engine {
     init.gate = mixed ? MASPCG_GATE_EUCLID : h->cfg.gate;
     init.tol = h->cfg.tolerance;
     MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    MCK(cudaMemsetAsync(h->failed.get() + 4, 0, sizeof(int), st));
     MCK(cudaEventRecord(h->ev0, st));
     k_init<Tv><<<gstream, kTpb, 0, st>>>(b_int, V(h->vx), V(h->vr), mixed ? h->x64.get() : nullptr, n,
                                          h->partial_rz.get(), s); MLAUNCHED(h);
@@ -456,6 +608,11 @@ struct Engine {
       ++launches;
       MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
       MCK(cudaStreamSynchronize(st));
+    }
+    {
+      int terr = 0;
+      MCK(cudaMemcpy(&terr, h->failed.get() + 4, sizeof(int), cudaMemcpyDeviceToHost));
+      MREQ(terr == 0, MASPCG_ERR_CUDA, "a TMA mbarrier wait expired in the SpMV");
     }
     // final FP64 iterate
     if (mixed) {

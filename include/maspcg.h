@@ -231,7 +231,7 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
  *   1  full preconditioner apply z = M^-1 r, working precision
  *   2  MAS level-0 domain apply alone (restriction/coarse levels excluded)
  *   3  MAS domain assembly + inversion (build)
- *   4  one full PCG iteration (the captured batch divided by its length)
+ *   4  PCG SpMV without the TMA staging (direct loads), for comparison
  * Vector contents are left unspecified afterwards. */
 MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);
 
