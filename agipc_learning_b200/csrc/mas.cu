@@ -535,6 +535,7 @@ struct ApplyArgs {
 template <typename Tv>
 __global__ void k_restrict0(ApplyArgs a, const Tv* __restrict__ r, const PcgScalars* s)
 {
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int bank = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -556,6 +557,7 @@ __global__ void k_restrict0(ApplyArgs a, const Tv* __restrict__ r, const PcgScal
 
 __global__ void k_restrictL(ApplyArgs a, int level_prev, const PcgScalars* s)
 {
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int bank = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -587,6 +589,7 @@ __global__ void k_restrictL(ApplyArgs a, int level_prev, const PcgScalars* s)
 template <typename TI>
 __global__ void k_coarse_apply(ApplyArgs a, const PcgScalars* s)
 {
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int lane = threadIdx.x & 31;
   const int g = a.lv.dom_begin[1] + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -603,6 +606,7 @@ __global__ void k_coarse_apply(ApplyArgs a, const PcgScalars* s)
 
 __global__ void k_prolong1(ApplyArgs a, const PcgScalars* s)
 {
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int A = blockIdx.x * blockDim.x + threadIdx.x;
   if (A >= a.lv.count[1]) return;
@@ -630,6 +634,7 @@ template <typename TI, typename Tv, typename Tacc>
 __global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
                                                       int part_base, int total_parts, int mode, PcgScalars* s)
 {
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int lane = threadIdx.x & 31;
   const int warps_total = gridDim.x * (blockDim.x >> 5);
@@ -679,6 +684,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 2)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kApplyWarps][2];
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   constexpr unsigned kBytes = kInvElems * sizeof(TI);
   const int lw = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -763,21 +769,20 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 2)
       a.coarse_z[base + 2] = y[2];
     }
   }
-  if (!ok) {
-    if (lane == 0) {
-      atomicExch(err, 1);
-      for (int j = 0; j < 2; ++j) {
-        const int gj = g_begin + gw + (i + j) * warps_total;
-        if (gj < g_end) mbar_wait(&bar[lw][(i + j) & 1], ((i + j) & 1) ? ph1 : ph0);
-      }
-      if (s) s->status = MASPCG_SOLVE_NONFINITE;
+  if (!ok && lane == 0) {
+    // drain this warp's copies still in flight (bounded), report
+    atomicExch(err, 1);
+    for (int j = 0; j < 2; ++j) {
+      const int gj = g_begin + gw + (i + j) * warps_total;
+      if (gj < g_end) mbar_wait(&bar[lw][(i + j) & 1], ((i + j) & 1) ? ph1 : ph0);
     }
-    return;
+    if (s) s->status = MASPCG_SOLVE_NONFINITE;
   }
+  if (__syncthreads_or(!ok)) return;  // the whole CTA leaves together
   if (kLevel0 && partial) {
     Tacc total = 0;
-    if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
-                          total) &&
+    if (grid_finish<Tacc, kApplyWarps * 32>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz],
+                                            gridDim.x, total) &&
         threadIdx.x == 0 && mode > 0)
       rz_update(s, (double)total, mode);
   }
@@ -935,7 +940,7 @@ void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, 
     MCK(cudaFuncSetAttribute(k_apply_tma<TI, Tv, Tacc, kLevel0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     configured = true;
   }
-  k_apply_tma<TI, Tv, Tacc, kLevel0><<<grid, kApplyWarps * 32, bytes, h->stream>>>(
+  launch_pdl(h, k_apply_tma<TI, Tv, Tacc, kLevel0>, dim3(grid), dim3(kApplyWarps * 32), bytes, 
       a, r, z, partial, part_base, total_parts, mode, s, g_begin, g_end, h->failed.get() + 4);
   MLAUNCHED(h);
 }
@@ -944,16 +949,15 @@ template <typename TI, typename Tv, typename Tacc>
 void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                  int grid0, PcgScalars* s)
 {
-  cudaStream_t st = h->stream;
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
   const int banks0 = h->c0 / kBank;
   constexpr bool kStaged = !std::is_same<TI, float>::value;
-  k_restrict0<Tv><<<ceil_div((long long)banks0 * 32, kTpb), kTpb, 0, st>>>(a, r, s);
+  launch_pdl(h, k_restrict0<Tv>, dim3(ceil_div((long long)banks0 * 32, kTpb)), dim3(kTpb), 0, a, r, s);
   MLAUNCHED(h);
   for (int l = 2; l < lv.levelnum; ++l) {
     const int banks = ceil_div(lv.count[l - 1], kBank);
-    k_restrictL<<<ceil_div((long long)banks * 32, kTpb), kTpb, 0, st>>>(a, l - 1, s);
+    launch_pdl(h, k_restrictL, dim3(ceil_div((long long)banks * 32, kTpb)), dim3(kTpb), 0, a, l - 1, s);
     MLAUNCHED(h);
   }
   const int d0 = lv.dom_begin[1];
@@ -963,17 +967,17 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
       launch_apply_tma<TI, Tv, Tacc, false>(h, a, r, z, nullptr, 0, 0, 0, s, d0, lv.domains,
                                             ceil_div(coarse_domains, kApplyWarps));
     } else {
-      k_coarse_apply<TI><<<ceil_div((long long)coarse_domains * 32, kTpb), kTpb, 0, st>>>(a, s);
+      launch_pdl(h, k_coarse_apply<TI>, dim3(ceil_div((long long)coarse_domains * 32, kTpb)), dim3(kTpb), 0, a, s);
       MLAUNCHED(h);
     }
   }
-  k_prolong1<<<ceil_div(lv.count[1], kTpb), kTpb, 0, st>>>(a, s);
+  launch_pdl(h, k_prolong1, dim3(ceil_div(lv.count[1], kTpb)), dim3(kTpb), 0, a, s);
   MLAUNCHED(h);
   if (kStaged) {
     const int grid = std::max(1, std::min(ceil_div(d0, kApplyWarps), 2 * h->sm_count));
     launch_apply_tma<TI, Tv, Tacc, true>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid);
   } else {
-    k_level0_apply<TI, Tv, Tacc><<<grid0, kTpb, 0, st>>>(a, r, z, partial, part_base, total_parts, mode, s);
+    launch_pdl(h, k_level0_apply<TI, Tv, Tacc>, dim3(grid0), dim3(kTpb), 0, a, r, z, partial, part_base, total_parts, mode, s);
     MLAUNCHED(h);
   }
 }

@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include <cstring>
+#include <utility>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -207,6 +208,7 @@ struct maspcg_handle {
   int grid_stream = 0;  // CTAs for grid-stride kernels
   long long kernel_launches = 0;  // this library's kernels launched on the handle
   long long graph_kernels = 0;    // kernel nodes of the captured batch graph
+  bool use_pdl = true;            // programmatic dependent launch for the iteration kernels
 };
 
 namespace maspcg {
@@ -261,5 +263,32 @@ __device__ __forceinline__ T block_sum(T v, T* smem /* NT/32 */)
 }
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Programmatic dependent launch: an iteration kernel lets its successor be
+// scheduled at once and then waits for its predecessor's completion (and
+// memory) before touching anything it produced.  Without the launch
+// attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter()
+{
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(maspcg_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args)
+{
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = h->use_pdl ? 1 : 0;
+  MCK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+  ++h->kernel_launches;
+}
 
 }  // namespace maspcg

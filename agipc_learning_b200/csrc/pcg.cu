@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(kTpb) k_init(const double* __restrict__ b, Tv*
 template <typename Tv>
 __global__ void __launch_bounds__(kTpb) k_update_p(const Tv* __restrict__ z, Tv* p, int n, const PcgScalars* s)
 {
+  pdl_enter();
   if (!running(s)) return;
   const bool first = s->k == 1;
   const Tv beta = (Tv)s->beta;
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
+  pdl_enter();
   if (!running(s)) return;
   using St = TmaStage<Tm>;
   unsigned char* sval0 = smem;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
     return;
   }
   Tacc total = 0;
-  if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
+  if (grid_finish<Tacc, kTmaThreads>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0) {
     const double pap = (double)total;
     s->pap = pap;
@@ -249,6 +251,7 @@ template <typename Tv, typename Tacc>
 __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p, const Tv* __restrict__ ap,
                                                      int n, int mixed, Tacc* partial, PcgScalars* s)
 {
+  pdl_enter();
   if (!running(s)) return;
   const Tv alpha = (Tv)s->alpha;
   Tacc acc = 0;
@@ -283,6 +286,7 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
 // MIXED: fold the FP32 correction into the FP64 iterate.
 __global__ void __launch_bounds__(kTpb) k_fold_x(double* xhi, float* xlo, int n, int force, const PcgScalars* s)
 {
+  pdl_enter();
   if (!force && !(s->status == MASPCG_SOLVE_RUNNING || s->status == kNeedTrue)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     xhi[i] += (double)xlo[i];
@@ -298,6 +302,7 @@ __global__ void __launch_bounds__(kTpb) k_true_residual(const int* __restrict__ 
                                                          const double* __restrict__ b, float* r32, int nrows,
                                                          double* partial, PcgScalars* s)
 {
+  pdl_enter();
   if (!(s->status == MASPCG_SOLVE_RUNNING || s->status == kNeedTrue)) return;
   const int groups_per_block = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
@@ -342,6 +347,7 @@ __global__ void __launch_bounds__(kTpb) k_other_apply(const Tv* __restrict__ r, 
                                                        const Tinv* __restrict__ diag_inv, Tacc* partial, int part_base,
                                                        int total_parts, int finalize, int mode, PcgScalars* s)
 {
+  pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   Tacc dot = 0;
   const int stride = gridDim.x * blockDim.x;
@@ -447,18 +453,17 @@ struct Engine {
 
   void precondition(const Tv* r, Tv* z, int mode, PcgScalars* s)
   {
-    cudaStream_t st = h->stream;
     const bool ref = h->cfg.precision == MASPCG_PREC_REFERENCE;
     if (gother) {
       const bool bj = h->cfg.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI;
       const int mas_lo = mas ? h->fem_off : 0, mas_hi = mas ? h->fem_off + h->c0 : 0;
       const int bodies = (h->cfg.preconditioner == MASPCG_PRECOND_NONE) ? 0 : h->abd_bodies;
       if (ref)
-        k_other_apply<Tv, Tacc, double><<<gother, kTpb, 0, st>>>(
+        launch_pdl(h, k_other_apply<Tv, Tacc, double>, dim3(gother), dim3(kTpb), 0, 
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv64.get(), bj ? h->diag_inv64.get() : nullptr,
             s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
       else
-        k_other_apply<Tv, Tacc, float><<<gother, kTpb, 0, st>>>(
+        launch_pdl(h, k_other_apply<Tv, Tacc, float>, dim3(gother), dim3(kTpb), 0, 
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv32.get(), bj ? h->diag_inv32.get() : nullptr,
             s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
       MLAUNCHED(h);
@@ -469,11 +474,10 @@ struct Engine {
 
   void iteration_head(PcgScalars* s)
   {
-    cudaStream_t st = h->stream;
-    k_update_p<Tv><<<gstream, kTpb, 0, st>>>(V(h->vz), V(h->vp), n, s); MLAUNCHED(h);
+    launch_pdl(h, k_update_p<Tv>, dim3(gstream), dim3(kTpb), 0, V(h->vz), V(h->vp), n, s);
     spmv_tma(s);
-    k_update_xr<Tv, Tacc><<<gstream, kTpb, 0, st>>>(V(h->vx), V(h->vr), V(h->vp), V(h->vap), n, mixed ? 1 : 0,
-                                                   partial(), s); MLAUNCHED(h);
+    launch_pdl(h, k_update_xr<Tv, Tacc>, dim3(gstream), dim3(kTpb), 0, V(h->vx), V(h->vr), V(h->vp), V(h->vap), n, mixed ? 1 : 0,
+                                                   partial(), s);
   }
 
   const Tm* matrix();
@@ -488,7 +492,7 @@ struct Engine {
       configured = true;
     }
     const int grid = std::max(1, std::min(2 * h->sm_count, ceil_div(h->nb_int, kTmaRows)));
-    k_spmv_tma<Tm, Tv, Tacc><<<grid, kTmaThreads, bytes, h->stream>>>(h->rowptr.get(), h->colidx.get(), matrix(),
+    launch_pdl(h, k_spmv_tma<Tm, Tv, Tacc>, dim3(grid), dim3(kTmaThreads), bytes, h->rowptr.get(), h->colidx.get(), matrix(),
                                                                       V(h->vp), V(h->vap), h->nb_int, partial(), s,
                                                                       h->failed.get() + 4);
     MLAUNCHED(h);
@@ -496,11 +500,10 @@ struct Engine {
 
   void true_residual(PcgScalars* s)
   {
-    cudaStream_t st = h->stream;
-    k_fold_x<<<gstream, kTpb, 0, st>>>(h->x64.get(), reinterpret_cast<float*>(h->vx.get()), n, 0, s); MLAUNCHED(h);
-    k_true_residual<16><<<gspmv, kTpb, 0, st>>>(h->rowptr.get(), h->colidx.get(), h->val64.get(), h->x64.get(),
+    launch_pdl(h, k_fold_x, dim3(gstream), dim3(kTpb), 0, h->x64.get(), reinterpret_cast<float*>(h->vx.get()), n, 0, s);
+    launch_pdl(h, k_true_residual<16>, dim3(gspmv), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(), h->x64.get(),
                                                h->b64.get(), reinterpret_cast<float*>(h->vr.get()), h->nb_int,
-                                               h->partial.get(), s); MLAUNCHED(h);
+                                               h->partial.get(), s);
   }
 
   // One graph = `batch` iterations.
@@ -616,7 +619,7 @@ struct Engine {
     }
     // final FP64 iterate
     if (mixed) {
-      k_fold_x<<<gstream, kTpb, 0, st>>>(h->x64.get(), reinterpret_cast<float*>(h->vx.get()), n, 1, s); MLAUNCHED(h);
+      launch_pdl(h, k_fold_x, dim3(gstream), dim3(kTpb), 0, h->x64.get(), reinterpret_cast<float*>(h->vx.get()), n, 1, s);
     } else {
       k_to_f64<Tv><<<ceil_div(n, kTpb), kTpb, 0, st>>>(V(h->vx), h->x64.get(), n); MLAUNCHED(h);
     }

@@ -10,14 +10,16 @@ constexpr int kRedTpb = 256;
 // Block-sum v, store it in partial[slot]; the last block to arrive (counted
 // on *ticket against `expected` blocks) sums partial[0..total_parts) in a
 // fixed order.  Returns true in every thread of that last block; the sum is
-// valid in thread 0.
-template <typename Tacc>
+// valid in thread 0.  NT must equal blockDim.x (the block reduction sizes
+// its shared array and its final warp from it).
+template <typename Tacc, int NT = kRedTpb>
 __device__ __forceinline__ bool grid_finish(Tacc v, Tacc* partial, int slot, int total_parts, unsigned* ticket,
                                             unsigned expected, Tacc& total)
 {
-  __shared__ Tacc red[kRedTpb / 32];
+  static_assert(NT % 32 == 0 && NT >= 32 && NT <= 1024, "block size");
+  __shared__ Tacc red[NT / 32];
   __shared__ int last;
-  const Tacc b = block_sum<Tacc, kRedTpb>(v, red);
+  const Tacc b = block_sum<Tacc, NT>(v, red);
   if (threadIdx.x == 0) {
     partial[slot] = b;
     __threadfence();
@@ -29,7 +31,7 @@ __device__ __forceinline__ bool grid_finish(Tacc v, Tacc* partial, int slot, int
   __threadfence();
   Tacc s = 0;
   for (int i = threadIdx.x; i < total_parts; i += blockDim.x) s += __ldcg(partial + i);
-  s = block_sum<Tacc, kRedTpb>(s, red);
+  s = block_sum<Tacc, NT>(s, red);
   if (threadIdx.x == 0) {
     total = s;
     *ticket = 0u;

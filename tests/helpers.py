@@ -127,3 +127,52 @@ def permute_full_bcsr(nb_int, iof, rowptr, col, vals):
             cs.append(c)
             vs.append(v.reshape(3, 3).T.reshape(9))  # column-major -> row-major
     return rp, np.array(cs, np.int64), np.array(vs).reshape(-1, 9) if vs else np.zeros((0, 9))
+
+
+def unpack_domain(packed):
+    """96x96 symmetric matrix from a domain's 528 packed upper 3x3 blocks
+    (block (a, b), a <= b, at 32a - a(a+1)/2 + b; column-major blocks)."""
+    p = np.asarray(packed, np.float64).reshape(528, 9)
+    A = np.zeros((96, 96))
+    for a in range(32):
+        for b in range(a, 32):
+            blk = p[32 * a - a * (a + 1) // 2 + b].reshape(3, 3).T
+            A[3 * a:3 * a + 3, 3 * b:3 * b + 3] = blk
+            A[3 * b:3 * b + 3, 3 * a:3 * a + 3] = blk.T
+    return A
+
+
+def expand_unused(A):
+    """A with every zero diagonal entry set to 1 (unused domain slots)."""
+    A = A.copy()
+    d = np.diag(A).copy()
+    d[d == 0] = 1.0
+    np.fill_diagonal(A, d)
+    return A
+
+
+def _round_bf16(v):
+    f = np.asarray(v, np.float32)
+    bits = f.view(np.uint32).astype(np.uint64)
+    bits = (bits + 0x7FFF + ((bits >> 16) & 1)) & 0xFFFF0000
+    return bits.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def factored_inverse_16(A, kind):
+    """A^-1 = W^T W with W = L^-1 (A = L L^T), W stored column-scaled in a
+    16-bit type: W = V S, S_j = max_i |W_ij|, V rounded; returns S V^T V S.
+    Zero diagonal entries (unused slots) are set to 1 first, as the kernel does."""
+    L = np.linalg.cholesky(expand_unused(A))
+    W = np.linalg.inv(L)
+    S = np.abs(W).max(axis=0)
+    S[S == 0] = 1.0
+    V = W / S
+    V = _round_bf16(V) if kind == "bf16" else V.astype(np.float16).astype(np.float64)
+    Wr = V * S
+    return Wr.T @ Wr
+
+
+def inverse_residual(A, M):
+    """Root-mean-square entry of A M - I (the oracle's local check)."""
+    R = A @ M - np.eye(A.shape[0])
+    return float(np.sqrt((R * R).sum() / A.shape[0]))

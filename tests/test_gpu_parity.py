@@ -3,7 +3,7 @@
 Integer work is compared bit-exactly (hierarchy, BCSR structure); FP64
 assembly to 1e-12 relative; FP32 inverses and the FP32 MAS apply to 2e-4
 relative; PCG in the reference precision to the same iteration count (+-1)
-and solution within 1e-4 relative.
+and solution within 1e-4 relative (the solver's stopping tolerance).
 """
 import numpy as np
 import pytest
@@ -163,10 +163,13 @@ def test_kat257_through_abi():
     assert d == pytest.approx(pub["relative_direction_difference"], abs=5e-5)
 
 
-@pytest.mark.parametrize("inverse,limit", [("bf16", 2e-2), ("fp16", 3e-3)])
-def test_factored_16bit_inverses(cfg1_small, inverse, limit):
+@pytest.mark.parametrize("inverse", ["bf16", "fp16"])
+def test_factored_16bit_inverses(cfg1_small, inverse):
     """16-bit storage keeps the Cholesky factor W of A^-1 = W^T W: the decoded
-    operator must be SPD and a close inverse of every domain matrix."""
+    operator must be SPD, and no further from the inverse of each domain
+    matrix than the same factorisation done in FP64 and rounded to the 16-bit
+    type on the host (the rounding error grows with the domain's condition
+    number, so this is the meaningful bound)."""
     s = cfg1_small
     o = _oracle_mas(s)
     p64, _ = o.domains()
@@ -175,8 +178,14 @@ def test_factored_16bit_inverses(cfg1_small, inverse, limit):
         gi = m.domain_inverses()
     chk = oracle.local_checks(p64, gi)
     assert all(c["inverse_spd"] and c["inverse_finite"] for c in chk)
-    d0 = s.fem_count // 32
-    assert max(c["inverse_residual"] for c in chk[:d0]) <= limit
+    rng = np.random.default_rng(7)
+    picks = rng.choice(len(p64), size=min(64, len(p64)), replace=False)
+    for d in picks:
+        A = H.expand_unused(H.unpack_domain(p64[d]))
+        M_host = H.factored_inverse_16(A, inverse)
+        r_host = H.inverse_residual(A, M_host)
+        r_gpu = H.inverse_residual(A, H.unpack_domain(gi[d]))
+        assert r_gpu <= 2.0 * r_host + 1e-6, (d, r_gpu, r_host)
 
 
 @pytest.mark.parametrize("which", ["cfg0", "cfg1_small"])
