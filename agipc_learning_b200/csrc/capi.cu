@@ -543,4 +543,19 @@ MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repe
   });
 }
 
+MASPCG_API maspcg_status maspcg_residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b,
+                                                       double* residual_norms, double* rhs_norms)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    MREQ(count >= 1 && count <= MASPCG_RESIDUAL_MAX_VECTORS, MASPCG_ERR_CAPACITY,
+         "count must be 1.." + std::to_string(MASPCG_RESIDUAL_MAX_VECTORS) +
+             ": the fixed scratch holds partial sums for that many vectors");
+    MREQ(x && b && residual_norms, MASPCG_ERR_INVALID_ARGUMENT, "null argument");
+    MREQ(is_device_ptr(x) && is_device_ptr(b), MASPCG_ERR_INVALID_ARGUMENT,
+         "x and b must be device pointers: this entry point stages nothing");
+    maspcg::residual_norms_noalloc(h, count, x, b, residual_norms, rhs_norms);
+  });
+}
+
 }  // extern "C"

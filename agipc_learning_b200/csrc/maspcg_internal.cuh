@@ -234,6 +234,10 @@ void decode_inverses(maspcg_handle* h, float* out_host);
 // pcg.cu
 double time_stage(maspcg_handle* h, int stage, int repeats);
 void solve(maspcg_handle* h, const double* b_dev, double* x_dev, maspcg_result* res);
+
+// residual_noalloc.cu
+void residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b, double* residual_norms,
+                            double* rhs_norms);
 void apply_preconditioner64(maspcg_handle* h, const double* r_int, double* z_int);
 size_t vec_elem_size(const maspcg_handle* h);
 

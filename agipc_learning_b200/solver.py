@@ -167,6 +167,28 @@ class MasPcg:
         self._ck(self.lib.maspcg_spmv(self.h, float(a), xa.ptr, float(b), ya.ptr))
         return y
 
+    def residual_norms_noalloc(self, x, b):
+        """FP64 ||b_j - A x_j|| and ||b_j|| for the rows of two CUDA float64
+        tensors of shape (count, 3*nb) (or (3*nb,)), through the
+        allocation-free entry point: nothing is staged or allocated."""
+        if not (_is_torch(x) and _is_torch(b) and x.is_cuda and b.is_cuda):
+            raise ValueError("x and b must be CUDA tensors")
+        import torch
+        for t in (x, b):
+            if t.dtype != torch.float64 or not t.is_contiguous():
+                raise ValueError("x and b must be contiguous float64")
+        x2, b2 = x.reshape(-1, 3 * self.nb), b.reshape(-1, 3 * self.nb)
+        if x2.shape != b2.shape:
+            raise ValueError("x and b differ in shape")
+        count = x2.shape[0]
+        res = np.zeros(max(count, 1), np.float64)
+        rhs = np.zeros(max(count, 1), np.float64)
+        self._ck(self.lib.maspcg_residual_norms_noalloc(self.h, int(count), ctypes.c_void_p(x2.data_ptr()),
+                                                        ctypes.c_void_p(b2.data_ptr()),
+                                                        res.ctypes.data_as(ctypes.c_void_p),
+                                                        rhs.ctypes.data_as(ctypes.c_void_p)))
+        return res[:count], rhs[:count]
+
     # -- introspection
     def info(self):
         i = N.Info()

@@ -235,6 +235,27 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
  * Vector contents are left unspecified afterwards. */
 MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);
 
+/* Most vectors one maspcg_residual_norms_noalloc call accepts. */
+#define MASPCG_RESIDUAL_MAX_VECTORS 8
+
+/* Allocation-free residual check (no counterpart in the reference): for
+ * j < count, residual_norms[j] = ||b_j - A x_j||_2 and, when rhs_norms is not
+ * NULL, rhs_norms[j] = ||b_j||_2, in FP64, with A the matrix of the last
+ * maspcg_set_matrix_bcoo.  x and b are DEVICE pointers to `count` vectors of
+ * 3*block_rows doubles stored one after another, in the caller's row order;
+ * the norms go to host memory.  count outside 1..MASPCG_RESIDUAL_MAX_VECTORS
+ * returns MASPCG_ERR_CAPACITY; host x or b return MASPCG_ERR_INVALID_ARGUMENT.
+ *
+ * The call allocates no memory: its scratch (per-block partial sums, results
+ * and a completion ticket) is one fixed 65,696-byte device array per device
+ * inside the library, its address looked up once per device.  That set-up
+ * runs on the first call for a device: make that first call before any stream
+ * capture is active.  Calls for one device are serialised by a lock held until
+ * the call's stream has finished; the call synchronises the handle's stream
+ * before it returns. */
+MASPCG_API maspcg_status maspcg_residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b,
+                                                       double* residual_norms, double* rhs_norms);
+
 #ifdef __cplusplus
 }
 #endif
