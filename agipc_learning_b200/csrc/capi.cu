@@ -109,14 +109,15 @@ void alloc_vectors(maspcg_handle* h)
 {
   const size_t n = 3 * (size_t)h->nb_int;
   const size_t es = maspcg::vec_elem_size(h);
-  for (auto* b : {&h->vx, &h->vr, &h->vz, &h->vp, &h->vap}) b->resize(n * es);
+  for (auto* b : {&h->vx, &h->vr, &h->vz, &h->vap}) b->resize(n * es);
+  h->vp4.resize(4 * (size_t)h->nb_int * es, 32);
   h->b64.resize(n);
   h->x64.resize(n);
   h->r64.resize(n);
   const size_t io = 3 * (size_t)std::max(h->nb, h->nb_int);
   h->io_a.resize(io);
   h->io_b.resize(io);
-  const int parts = 16 * h->sm_count + 64;
+  const int parts = 32 * h->sm_count + 64;
   h->partial.resize(parts);
   h->partial_rz.resize(parts);
 }
@@ -540,6 +541,38 @@ MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repe
     MREQ(mean_ms && repeats >= 1, MASPCG_ERR_INVALID_ARGUMENT, "bad arguments");
     *mean_ms = maspcg::time_stage(h, stage, repeats);
     h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n_blocks,
+                                              const double* lam, const double* x, double* grad9)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    MREQ(n_blocks >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative block count");
+    if (n_blocks == 0) return;
+    MREQ(rows && cols && lam && x && grad9, MASPCG_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t n = 3 * (size_t)h->nb;
+    const int* r = device_in(h, rows, (size_t)n_blocks, h->adj_rows);
+    const int* c = device_in(h, cols, (size_t)n_blocks, h->adj_cols);
+    // block indices must address the system (checked on the host copy)
+    {
+      const std::vector<int> hr = host_copy(h, rows, (size_t)n_blocks), hc = host_copy(h, cols, (size_t)n_blocks);
+      for (int t = 0; t < n_blocks; ++t)
+        MREQ(hr[t] >= 0 && hr[t] < h->nb && hc[t] >= 0 && hc[t] < h->nb, MASPCG_ERR_INVALID_ARGUMENT,
+             "block index outside the system");
+    }
+    const double* l = device_in(h, lam, n, h->adj_lam);
+    const double* xv = device_in(h, x, n, h->adj_x);
+    if (is_device_ptr(grad9)) {
+      maspcg::bcoo_gradient(h, r, c, n_blocks, l, xv, grad9);
+    } else {
+      h->adj_grad.resize((size_t)9 * n_blocks);
+      maspcg::bcoo_gradient(h, r, c, n_blocks, l, xv, h->adj_grad.get());
+      MCK(cudaMemcpyAsync(grad9, h->adj_grad.get(), sizeof(double) * 9 * (size_t)n_blocks, cudaMemcpyDeviceToHost,
+                          h->stream));
+    }
+    MCK(cudaStreamSynchronize(h->stream));
   });
 }
 

@@ -28,21 +28,12 @@
 
 #include "maspcg_internal.cuh"
 #include "pcg_device.cuh"
-#include "spmv_tma.cuh"
+#include "tma.cuh"
 
 namespace maspcg {
 namespace {
 
 constexpr int kTpb = 256;
-
-template <typename T>
-__device__ __forceinline__ float to_f(T v);
-template <>
-__device__ __forceinline__ float to_f<float>(float v) { return v; }
-template <>
-__device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
-template <>
-__device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
 
 template <typename T>
 __device__ __forceinline__ T from_d(double v);
@@ -52,13 +43,6 @@ template <>
 __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) { return __float2bfloat16_rn((float)v); }
 template <>
 __device__ __forceinline__ __half from_d<__half>(double v) { return __float2half_rn((float)v); }
-
-template <typename T>
-__device__ __forceinline__ float ld_vec(const T* p);
-template <>
-__device__ __forceinline__ float ld_vec<float>(const float* p) { return *p; }
-template <>
-__device__ __forceinline__ float ld_vec<double>(const double* p) { return (float)*p; }
 
 
 // ------------------------------------------------------------------ build --
@@ -234,7 +218,7 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
     if (acc[8] == 0.0) acc[8] = 1.0;
   }
   constexpr bool kFactored = !std::is_same<TI, float>::value;
-  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * kInvElems;
+  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * inv_elems<TI>();
 
   if (!kFactored) {
     // ---- in-place Gauss-Jordan inversion (the elimination of __inverse6_P96x96)
@@ -393,19 +377,49 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
 #pragma unroll
       for (int jj = 0; jj < 3; ++jj) {
         const double v = (w == lane && jj > i) ? 0.0 : xr[3 * i + jj] / (double)sscale[3 * lane + jj];
-        out[(d * 9 + 3 * i + jj) * kBank + l] = from_d<TI>(v);
-        if (w - lane == 16) out[(16 * 9 + 3 * i + jj) * kBank + w] = from_d<TI>(0.0);
+        out[inv16_pos(d * 9 + 3 * i + jj, l)] = from_d<TI>(v);
+        if (w - lane == 16) out[inv16_pos(16 * 9 + 3 * i + jj, w)] = from_d<TI>(0.0);
       }
+    if (w == lane) out[inv16_pos(kDiags * 9, lane)] = from_d<TI>(0.0);  // pad half of the last word
   }
 }
 
 // ------------------------------------------------------------------ apply --
 
+// 16-bit halves of a packed word (element 2k low, 2k+1 high).
+template <typename TI>
+__device__ __forceinline__ float lo16(uint32_t w);
+template <typename TI>
+__device__ __forceinline__ float hi16(uint32_t w);
+template <>
+__device__ __forceinline__ float lo16<__nv_bfloat16>(uint32_t w)
+{
+  return __uint_as_float(w << 16);
+}
+template <>
+__device__ __forceinline__ float hi16<__nv_bfloat16>(uint32_t w)
+{
+  return __uint_as_float(w & 0xffff0000u);
+}
+template <>
+__device__ __forceinline__ float lo16<__half>(uint32_t w)
+{
+  return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+}
+template <>
+__device__ __forceinline__ float hi16<__half>(uint32_t w)
+{
+  return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+}
+
 // z_l = (M x)_l for one domain held by one warp; x, y: the lane's 3 rows.
 // FP32 storage holds the symmetric inverse (each stored block serves both
 // triangles through a shuffle).  16-bit storage holds the scaled factor
-// V = W S^-1 of M = W^T W (W lower); two passes t = V (S x), y = S V^T t.
-template <typename TI>
+// V = W S^-1 of M = W^T W (W lower); the warp loads the domain's 77 words
+// per lane once (coalesced, streaming) into registers and runs the two
+// passes t = V (S x), y = S V^T t from there.  kShared: `inv` points to a
+// shared-memory copy of the domain record.
+template <typename TI, bool kShared = false>
 __device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const float* __restrict__ scale, int lane,
                                              const float x[3], float y[3])
 {
@@ -436,15 +450,39 @@ __device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const f
     y[1] = y1;
     y[2] = y2;
   } else {
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(inv) + lane;
+    // Global records are loaded once into registers (77 words per lane) and
+    // serve both passes; shared-memory records are read per diagonal in each
+    // pass (volatile: the compiler must not keep them live across passes).
+    uint32_t Wd[kShared ? 1 : kInvWords16];
+    if constexpr (!kShared) {
+#pragma unroll
+      for (int k = 0; k < kInvWords16; ++k) Wd[k] = __ldcs(wp + k * kBank);
+    }
+    auto diag = [&](int d, float B[9]) {
+      const int k0 = 9 * d, w0 = k0 >> 1;
+      uint32_t wv[5];
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        if constexpr (kShared)
+          wv[i] = (w0 + i < kInvWords16) ? reinterpret_cast<const volatile uint32_t*>(wp)[(w0 + i) * kBank] : 0u;
+        else
+          wv[i] = (w0 + i < kInvWords16) ? Wd[w0 + i] : 0u;
+      }
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        const int k = k0 + e;
+        B[e] = (k & 1) ? hi16<TI>(wv[(k >> 1) - w0]) : lo16<TI>(wv[(k >> 1) - w0]);
+      }
+    };
     const float s0 = scale[3 * lane], s1 = scale[3 * lane + 1], s2 = scale[3 * lane + 2];
     const float x0 = x[0] * s0, x1 = x[1] * s1, x2 = x[2] * s2;
     // pass 1: t = V xs
     float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-#pragma unroll 4
+#pragma unroll
     for (int d = 0; d < kDiags; ++d) {
       float B[9];
-#pragma unroll
-      for (int e = 0; e < 9; ++e) B[e] = to_f<TI>(inv[(d * 9 + e) * kBank + lane]);
+      diag(d, B);
       if (d == 0) {
         t0 += B[0] * x0 + B[1] * x1 + B[2] * x2;
         t1 += B[3] * x0 + B[4] * x1 + B[5] * x2;
@@ -466,13 +504,17 @@ __device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const f
         t2 += (below ? p2 : 0.f) + r2;
       }
     }
-    // pass 2: z = V^T t
+    // pass 2: z = V^T t.  The empty asm keeps the packed words (77 registers)
+    // live instead of the 153 unpacked floats of pass 1.
+    if constexpr (!kShared) {
+#pragma unroll
+      for (int k = 0; k < kInvWords16; ++k) asm volatile("" : "+r"(Wd[k]));
+    }
     float z0 = 0.f, z1 = 0.f, z2 = 0.f;
-#pragma unroll 4
+#pragma unroll
     for (int d = 0; d < kDiags; ++d) {
       float B[9];
-#pragma unroll
-      for (int e = 0; e < 9; ++e) B[e] = to_f<TI>(inv[(d * 9 + e) * kBank + lane]);
+      diag(d, B);
       if (d == 0) {
         z0 += B[0] * t0 + B[3] * t1 + B[6] * t2;
         z1 += B[1] * t0 + B[4] * t1 + B[7] * t2;
@@ -522,107 +564,220 @@ __device__ __forceinline__ void group_sum(int key, const float v[3], float out[3
 
 struct ApplyArgs {
   const int* cmap1;
+  const int* cmap[kMaxLevels];  // fine slot -> level-l local node (-1 padding), l >= 1
+  const int* pmr;               // part_map_real: -1 marks a padding slot
   const int* going_next;
   float* coarse_r;
   float* coarse_z;
-  float* zacc1;
   const void* inv;
   const float* scale;
+  int* chain_count;             // per coarse domain: arrivals so far (zero between launches)
+  const int* chain_target;      // per coarse domain: arrivals that complete it
+  int* err;
   int fem_off, c0;
   LevelInfo lv;
 };
 
-template <typename Tv>
-__global__ void k_restrict0(ApplyArgs a, const Tv* __restrict__ r, const PcgScalars* s)
+// Coarse correction of a level-0 slot: the sum over the coarse levels of the
+// level's z at the slot's ancestor (the prolongation, CollectFinalZ).  Returns
+// false for a padding slot, whose z is zero.
+__device__ __forceinline__ bool coarse_correction(const ApplyArgs& a, int slot, float c[3])
 {
+  c[0] = c[1] = c[2] = 0.f;
+  if (a.pmr[slot] < 0) return false;
+  for (int l = 1; l < a.lv.levelnum; ++l) {
+    const float* q = a.coarse_z + 3 * (size_t)(a.lv.begin[l] - a.c0 + a.cmap[l][slot]);
+    c[0] += q[0];
+    c[1] += q[1];
+    c[2] += q[2];
+  }
+  return true;
+}
+
+// Domain-apply kernels: 4 warps per CTA; 16-bit storage keeps a domain's 77
+// packed words per lane in registers, so those instances get up to 168.
+constexpr int kApplyTpb = 128;
+#define MAS_APPLY_BOUNDS(TI) __launch_bounds__(kApplyTpb, sizeof(TI) == 4 ? 4 : 3)
+
+// ---- coarse levels in one kernel (restriction + coarse domain applies) ----
+//
+// BuildMultiLevelR and the coarse part of _schwarzLocalXSym6 as a dataflow
+// over the hierarchy.  CTA c restricts level-0 banks [8c, 8c + 8) (one warp
+// each) into level-1 nodes.  A coarse domain (32 consecutive nodes of level
+// l >= 1) is complete once every unit that writes one of its nodes has
+// finished; each unit counts itself into the domains its parents fall in,
+// and the unit that completes a domain processes it in the same CTA:
+// restricts its nodes into level l + 1 (which may complete further domains)
+// and applies the domain's inverse.  Sums run in a fixed order (group sums
+// in lane order), so the result does not depend on which CTA finishes last;
+// nothing waits.  Counters return to zero as they complete.
+constexpr int kChainWarps = 8;
+constexpr int kChainQueue = 64;
+
+// One thread counts a finished unit, whose parents span global slots
+// [lo, hi], into the parent domains; domains it completes are appended to
+// the CTA's queue (the thread's `tail`).  Release before the counts, acquire
+// after a completion.
+__device__ __forceinline__ void chain_arrive(const ApplyArgs& a, int lo, int hi, int* queue, int& tail)
+{
+  const int d1 = a.lv.dom_begin[1];
+  __threadfence();
+  for (int g = lo / kBank; g <= hi / kBank; ++g) {
+    const int old = atomicAdd(a.chain_count + (g - d1), 1);
+    if (old + 1 == a.chain_target[g - d1]) {
+      a.chain_count[g - d1] = 0;
+      if (tail < kChainQueue)
+        queue[tail++] = g;
+      else
+        atomicExch(a.err, 2);
+    }
+  }
+  __threadfence();
+}
+
+// Level of a coarse domain g.
+__device__ __forceinline__ int domain_level(const LevelInfo& lv, int g)
+{
+  int l = 1;
+  while (l + 1 < lv.levelnum && g >= lv.dom_begin[l + 1]) ++l;
+  return l;
+}
+
+template <typename TI, typename Tv>
+__global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, const Tv* __restrict__ r,
+                                                                  const PcgScalars* s)
+{
+  __shared__ int queue[kChainQueue];
+  __shared__ int tail_s, lo_s, hi_s;
   pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  const int bank = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (bank >= a.c0 / kBank) return;
-  const int slot = bank * kBank + lane;
-  const int key = a.cmap1[slot];
-  const Tv* rp = r + 3 * (size_t)(a.fem_off + slot);
-  const float v[3] = {ld_vec(rp), ld_vec(rp + 1), ld_vec(rp + 2)};
-  float o[3];
-  bool leader;
-  group_sum(key >= 0 ? key : -1 - lane, v, o, leader);
-  if (leader && key >= 0) {
-    float* d = a.coarse_r + 3 * (size_t)key;
-    d[0] = o[0];
-    d[1] = o[1];
-    d[2] = o[2];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    tail_s = 0;
+    lo_s = INT_MAX;
+    hi_s = -1;
+  }
+  __syncthreads();
+  // level 0 -> level 1 (RestrictR of the fine residual)
+  const int bank = blockIdx.x * kChainWarps + w;
+  if (bank < a.c0 / kBank) {
+    const int slot = bank * kBank + lane;
+    const int key = a.cmap1[slot];
+    const Tv* rp = r + 3 * (size_t)(a.fem_off + slot);
+    const float v[3] = {(float)rp[0], (float)rp[1], (float)rp[2]};
+    float o[3];
+    bool leader;
+    group_sum(key >= 0 ? key : -1 - lane, v, o, leader);
+    if (leader && key >= 0) {
+      float* d = a.coarse_r + 3 * (size_t)key;
+      d[0] = o[0];
+      d[1] = o[1];
+      d[2] = o[2];
+    }
+    const int lo = (int)__reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0x7fffffffu);
+    const int hi = (int)__reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
+    const bool any = __any_sync(kFull, key >= 0);  // every lane votes
+    if (lane == 0 && any) {
+      atomicMin(&lo_s, a.c0 + lo);
+      atomicMax(&hi_s, a.c0 + hi);
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0 && hi_s >= 0) {
+    int t = 0;
+    chain_arrive(a, lo_s, hi_s, queue, t);
+    tail_s = t;
+  }
+  __syncthreads();
+  const int tail0 = tail_s;
+  if (tail0 == 0) return;
+  // warp 0: walk up the levels, restricting every completed domain.  Lane 0
+  // owns the queue tail; the loop bound is broadcast from it every step so
+  // the warp never diverges on it.
+  if (w == 0) {
+    int t = tail0;  // meaningful in lane 0
+    for (int i = 0; i < __shfl_sync(kFull, t, 0); ++i) {
+      const int g = queue[i];
+      const int l = domain_level(a.lv, g);
+      if (l + 1 >= a.lv.levelnum) continue;  // top level: nothing above
+      const int sg = g * kBank + lane;         // global slot of the node
+      const bool valid = sg - a.lv.begin[l] < a.lv.count[l];
+      float v[3] = {0.f, 0.f, 0.f};
+      int key = -1 - lane;
+      if (valid) {
+        const float* src = a.coarse_r + 3 * (size_t)(sg - a.c0);
+        v[0] = __ldcg(src);
+        v[1] = __ldcg(src + 1);
+        v[2] = __ldcg(src + 2);
+        key = a.going_next[sg];
+      }
+      float o[3];
+      bool leader;
+      group_sum(key, v, o, leader);
+      if (leader && valid) {
+        float* d = a.coarse_r + 3 * (size_t)(key - a.c0);
+        d[0] = o[0];
+        d[1] = o[1];
+        d[2] = o[2];
+      }
+      const int lo = (int)__reduce_min_sync(kFull, valid ? (unsigned)key : 0x7fffffffu);
+      const int hi = (int)__reduce_max_sync(kFull, valid ? (unsigned)key : 0u);
+      if (lane == 0 && lo <= hi) chain_arrive(a, lo, hi, queue, t);
+      __syncwarp();
+    }
+    if (lane == 0) tail_s = t;
+  }
+  __syncthreads();
+  // all warps: apply the completed domains' inverses
+  const int n = tail_s;
+  for (int i = w; i < n; i += kChainWarps) {
+    const int g = queue[i];
+    const size_t base = (size_t)(kBank * g + lane - a.c0) * 3;
+    const float x[3] = {__ldcg(a.coarse_r + base), __ldcg(a.coarse_r + base + 1), __ldcg(a.coarse_r + base + 2)};
+    float y[3];
+    domain_apply<TI, true>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>(),
+                           a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
+    a.coarse_z[base] = y[0];
+    a.coarse_z[base + 1] = y[1];
+    a.coarse_z[base + 2] = y[2];
   }
 }
 
-__global__ void k_restrictL(ApplyArgs a, int level_prev, const PcgScalars* s)
+// Expected arrivals per coarse domain: the same unit/parent-range rule as
+// k_coarse_chain, counted once per build.
+__global__ void k_chain_targets(ApplyArgs a, int* target)
 {
-  pdl_enter();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  const int bank = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  const int count = a.lv.count[level_prev];
-  if (bank >= (count + kBank - 1) / kBank) return;
-  const int node = bank * kBank + lane;
-  const bool valid = node < count;
-  const int sg = a.lv.begin[level_prev] + node;
-  float v[3] = {0.f, 0.f, 0.f};
-  int key = -1 - lane;
-  if (valid) {
-    const float* src = a.coarse_r + 3 * (size_t)(sg - a.c0);
-    v[0] = src[0];
-    v[1] = src[1];
-    v[2] = src[2];
-    key = a.going_next[sg];
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int d1 = a.lv.dom_begin[1];
+  const int units0 = (a.c0 / kBank + kChainWarps - 1) / kChainWarps;
+  int lo = 0x7fffffff, hi = -1;
+  if (gw < units0) {
+    for (int b = gw * kChainWarps; b < min((gw + 1) * kChainWarps, a.c0 / kBank); ++b) {
+      const int key = a.cmap1[b * kBank + lane];
+      const int l2 = (int)__reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0x7fffffffu);
+      const int h2 = (int)__reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
+      const bool any = __any_sync(kFull, key >= 0);
+      if (any) {
+        lo = min(lo, a.c0 + l2);
+        hi = max(hi, a.c0 + h2);
+      }
+    }
+  } else {
+    const int g = d1 + (gw - units0);  // a coarse domain as a unit
+    if (g >= a.lv.domains) return;
+    const int l = domain_level(a.lv, g);
+    if (l + 1 >= a.lv.levelnum) return;
+    const int sg = g * kBank + lane;
+    const bool valid = sg - a.lv.begin[l] < a.lv.count[l];
+    const int key = valid ? a.going_next[sg] : 0;
+    lo = (int)__reduce_min_sync(kFull, valid ? (unsigned)key : 0x7fffffffu);
+    hi = (int)__reduce_max_sync(kFull, valid ? (unsigned)key : 0u);
+    if (!__any_sync(kFull, valid)) return;
   }
-  float o[3];
-  bool leader;
-  group_sum(key, v, o, leader);
-  if (leader && valid) {
-    float* d = a.coarse_r + 3 * (size_t)(key - a.c0);
-    d[0] = o[0];
-    d[1] = o[1];
-    d[2] = o[2];
-  }
-}
-
-template <typename TI>
-__global__ void k_coarse_apply(ApplyArgs a, const PcgScalars* s)
-{
-  pdl_enter();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  const int lane = threadIdx.x & 31;
-  const int g = a.lv.dom_begin[1] + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (g >= a.lv.domains) return;
-  const size_t base = (size_t)(kBank * g + lane - a.c0) * 3;
-  const float x[3] = {a.coarse_r[base], a.coarse_r[base + 1], a.coarse_r[base + 2]};
-  float y[3];
-  domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * kInvElems,
-                   a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
-  a.coarse_z[base] = y[0];
-  a.coarse_z[base + 1] = y[1];
-  a.coarse_z[base + 2] = y[2];
-}
-
-__global__ void k_prolong1(ApplyArgs a, const PcgScalars* s)
-{
-  pdl_enter();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  const int A = blockIdx.x * blockDim.x + threadIdx.x;
-  if (A >= a.lv.count[1]) return;
-  const float* z = a.coarse_z;
-  float z0 = z[3 * (size_t)A], z1 = z[3 * (size_t)A + 1], z2 = z[3 * (size_t)A + 2];
-  int cur = a.c0 + A;
-  for (int l = 2; l < a.lv.levelnum; ++l) {
-    cur = a.going_next[cur];
-    const float* q = z + 3 * (size_t)(cur - a.c0);
-    z0 += q[0];
-    z1 += q[1];
-    z2 += q[2];
-  }
-  a.zacc1[3 * (size_t)A] = z0;
-  a.zacc1[3 * (size_t)A + 1] = z1;
-  a.zacc1[3 * (size_t)A + 2] = z2;
+  if (lane == 0 && hi >= 0)
+    for (int g = lo / kBank; g <= hi / kBank; ++g) atomicAdd(target + (g - d1), 1);
 }
 
 }  // namespace
@@ -631,7 +786,7 @@ __global__ void k_prolong1(ApplyArgs a, const PcgScalars* s)
 // completes the r.z reduction over [0, total_parts) and, for mode > 0,
 // updates the PCG scalars (rz0 / beta / k).
 template <typename TI, typename Tv, typename Tacc>
-__global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
+__global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
                                                       int part_base, int total_parts, int mode, PcgScalars* s)
 {
   pdl_enter();
@@ -645,13 +800,13 @@ __global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __r
     const Tv r0 = r[row3], r1 = r[row3 + 1], r2 = r[row3 + 2];
     const float x[3] = {(float)r0, (float)r1, (float)r2};
     float y[3];
-    domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * kInvElems,
+    domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>(),
                      a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
-    const int c1 = a.cmap1[slot];
-    if (c1 >= 0) {
-      y[0] += a.zacc1[3 * (size_t)c1];
-      y[1] += a.zacc1[3 * (size_t)c1 + 1];
-      y[2] += a.zacc1[3 * (size_t)c1 + 2];
+    float cc[3];
+    if (coarse_correction(a, slot, cc)) {
+      y[0] += cc[0];
+      y[1] += cc[1];
+      y[2] += cc[2];
     } else {
       y[0] = y[1] = y[2] = 0.f;
     }
@@ -662,7 +817,7 @@ __global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __r
   }
   if (partial) {
     Tacc total = 0;
-    if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
+    if (grid_finish<Tacc, kApplyTpb>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
                           total) &&
         threadIdx.x == 0 && mode > 0)
       rz_update(s, (double)total, mode);
@@ -670,62 +825,60 @@ __global__ void __launch_bounds__(256) k_level0_apply(ApplyArgs a, const Tv* __r
 }
 
 // Domain apply with the inverse staged by TMA: each warp streams its
-// domains' stored blocks (one contiguous bulk copy per domain) into a
-// double-buffered shared-memory slot and applies them from there, so the
-// two passes of the factored form read global memory once.  Level 0 reads
-// r / writes z (plus the coarse correction and r.z); coarse levels read and
-// write the coarse R/Z arrays.
+// domains' stored records (one contiguous bulk copy per domain) into kBuf
+// shared-memory slots of its own and applies them from there, so the two
+// passes of the factored form read global memory once.  kBuf = 2 overlaps a
+// warp's next copy with its arithmetic; kBuf = 1 halves the shared memory per
+// warp and fits more warps per SM.  Level 0 reads r / writes z (plus the
+// coarse correction and r.z); coarse levels read and write the coarse R/Z
+// arrays.  Every wait is bounded; on expiry the warp drains its copies,
+// records the error and the whole CTA leaves.
 constexpr int kApplyWarps = 4;
 
-template <typename TI, typename Tv, typename Tacc, bool kLevel0>
-__global__ void __launch_bounds__(kApplyWarps * 32, 2)
+template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf>
+__global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
     k_apply_tma(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                 PcgScalars* s, int g_begin, int g_end, int* err)
 {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[kApplyWarps][2];
+  __shared__ __align__(8) uint64_t bar[kApplyWarps][kBuf];
   pdl_enter();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  constexpr unsigned kBytes = kInvElems * sizeof(TI);
+  constexpr unsigned kBytes = inv_elems<TI>() * sizeof(TI);
   const int lw = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warps_total = gridDim.x * kApplyWarps;
   const int gw = blockIdx.x * kApplyWarps + lw;
-  unsigned char* buf0 = smem + (size_t)lw * 2 * kBytes;
-  unsigned char* buf1 = buf0 + kBytes;
+  unsigned char* buf = smem + (size_t)lw * kBuf * kBytes;
   const TI* inv = reinterpret_cast<const TI*>(a.inv);
   if (lane == 0) {
-    mbar_init(&bar[lw][0], 1);
-    mbar_init(&bar[lw][1], 1);
+#pragma unroll
+    for (int j = 0; j < kBuf; ++j) mbar_init(&bar[lw][j], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    const int g0 = g_begin + gw, g1 = g0 + warps_total;
-    if (g0 < g_end) {
-      mbar_expect_tx(&bar[lw][0], kBytes);
-      tma_bulk_g2s(buf0, inv + (size_t)g0 * kInvElems, kBytes, &bar[lw][0]);
-    }
-    if (g1 < g_end) {
-      mbar_expect_tx(&bar[lw][1], kBytes);
-      tma_bulk_g2s(buf1, inv + (size_t)g1 * kInvElems, kBytes, &bar[lw][1]);
+#pragma unroll
+    for (int j = 0; j < kBuf; ++j) {
+      const int gj = g_begin + gw + j * warps_total;
+      if (gj < g_end) {
+        mbar_expect_tx(&bar[lw][j], kBytes);
+        tma_bulk_g2s(buf + j * kBytes, inv + (size_t)gj * inv_elems<TI>(), kBytes, &bar[lw][j]);
+      }
     }
   }
   __syncwarp();
-  unsigned ph0 = 0, ph1 = 0;
+  unsigned ph[kBuf];
+#pragma unroll
+  for (int j = 0; j < kBuf; ++j) ph[j] = 0;
   Tacc dot = 0;
   int i = 0;
   bool ok = true;
   for (int g = g_begin + gw; g < g_end; g += warps_total, ++i) {
-    const int st = i & 1;
-    const bool w = mbar_wait(&bar[lw][st], st ? ph1 : ph0);
-    if (w) {
-      if (st)
-        ph1 ^= 1u;
-      else
-        ph0 ^= 1u;
-    }
+    const int st = kBuf == 1 ? 0 : (i & 1);
+    const bool w = mbar_wait(&bar[lw][st], ph[st]);
+    if (w) ph[st] ^= 1u;
     if (!__all_sync(kFull, w)) {
       ok = false;
       break;
     }
-    const TI* blk = reinterpret_cast<const TI*>(st ? buf1 : buf0);
+    const TI* blk = reinterpret_cast<const TI*>(buf + st * kBytes);
     const float* sc = a.scale + (size_t)g * 96;
     float x[3], y[3];
     size_t base;
@@ -740,20 +893,21 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 2)
       x[1] = a.coarse_r[base + 1];
       x[2] = a.coarse_r[base + 2];
     }
-    domain_apply<TI>(blk, sc, lane, x, y);
+    domain_apply<TI, true>(blk, sc, lane, x, y);
     __syncwarp();
-    if (lane == 0 && g + 2 * warps_total < g_end) {
+    const int gn = g + kBuf * warps_total;
+    if (lane == 0 && gn < g_end) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&bar[lw][st], kBytes);
-      tma_bulk_g2s(st ? buf1 : buf0, inv + (size_t)(g + 2 * warps_total) * kInvElems, kBytes, &bar[lw][st]);
+      tma_bulk_g2s(buf + st * kBytes, inv + (size_t)gn * inv_elems<TI>(), kBytes, &bar[lw][st]);
     }
     if (kLevel0) {
       const int slot = kBank * g + lane;
-      const int c1 = a.cmap1[slot];
-      if (c1 >= 0) {
-        y[0] += a.zacc1[3 * (size_t)c1];
-        y[1] += a.zacc1[3 * (size_t)c1 + 1];
-        y[2] += a.zacc1[3 * (size_t)c1 + 2];
+      float cc[3];
+      if (coarse_correction(a, slot, cc)) {
+        y[0] += cc[0];
+        y[1] += cc[1];
+        y[2] += cc[2];
       } else {
         y[0] = y[1] = y[2] = 0.f;
       }
@@ -772,9 +926,11 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 2)
   if (!ok && lane == 0) {
     // drain this warp's copies still in flight (bounded), report
     atomicExch(err, 1);
-    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+    for (int j = 0; j < kBuf; ++j) {
       const int gj = g_begin + gw + (i + j) * warps_total;
-      if (gj < g_end) mbar_wait(&bar[lw][(i + j) & 1], ((i + j) & 1) ? ph1 : ph0);
+      const int sj = kBuf == 1 ? 0 : ((i + j) & 1);
+      if (gj < g_end) mbar_wait(&bar[lw][sj], ph[sj]);
     }
     if (s) s->status = MASPCG_SOLVE_NONFINITE;
   }
@@ -789,6 +945,9 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 2)
 }
 
 void launch_factor(maspcg_handle* h, double* assembled_out);
+namespace {
+ApplyArgs make_apply_args(maspcg_handle* h);
+}
 
 void build_mas_domains(maspcg_handle* h, double* assembled_out)
 {
@@ -822,7 +981,7 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   // storage
   const int storage = h->cfg.inverse_storage;
   const size_t esize = storage == MASPCG_INV_FP32 ? 4 : 2;
-  h->inv.resize((size_t)lv.domains * kInvElems * esize, 16);
+  h->inv.resize((size_t)lv.domains * inv_elems_for(storage) * esize, 16);
   if (storage != MASPCG_INV_FP32) h->inv_scale.resize((size_t)lv.domains * 96);
   MCK(cudaMemsetAsync(h->failed.get() + 3, 0, sizeof(int), st));
   launch_factor(h, assembled_out);
@@ -830,7 +989,17 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   const size_t coarse = (size_t)(lv.total_clusters - c0) * 3;
   h->coarse_r.resize(coarse > 0 ? coarse : 3);
   h->coarse_z.resize(coarse > 0 ? coarse : 3);
-  h->zacc1.resize((size_t)std::max(lv.count[1], 1) * 3);
+  const int coarse_domains = lv.domains - lv.dom_begin[1];
+  h->chain_count.resize((size_t)std::max(coarse_domains, 1));
+  h->chain_target.resize((size_t)std::max(coarse_domains, 1));
+  MCK(cudaMemsetAsync(h->chain_count.get(), 0, h->chain_count.bytes(), st));
+  MCK(cudaMemsetAsync(h->chain_target.get(), 0, h->chain_target.bytes(), st));
+  if (lv.levelnum > 1) {
+    const ApplyArgs aa = make_apply_args(h);
+    const long long units = (c0 / kBank + kChainWarps - 1) / kChainWarps + coarse_domains;
+    k_chain_targets<<<ceil_div(units * 32, kTpb), kTpb, 0, st>>>(aa, h->chain_target.get());
+    MLAUNCHED(h);
+  }
   MCK(cudaMemsetAsync(h->coarse_r.get(), 0, h->coarse_r.bytes(), st));
   MCK(cudaMemsetAsync(h->coarse_z.get(), 0, h->coarse_z.bytes(), st));
   int f = 0;
@@ -921,7 +1090,11 @@ ApplyArgs make_apply_args(maspcg_handle* h)
   a.going_next = h->going_next.get();
   a.coarse_r = h->coarse_r.get();
   a.coarse_z = h->coarse_z.get();
-  a.zacc1 = h->zacc1.get();
+  for (int l = 1; l < h->lv.levelnum && l < kMaxLevels; ++l) a.cmap[l] = h->cmap[l].get();
+  a.pmr = h->pmr.get();
+  a.chain_count = h->chain_count.get();
+  a.chain_target = h->chain_target.get();
+  a.err = h->failed.get() + 4;
   a.inv = h->inv.get();
   a.scale = h->cfg.inverse_storage == MASPCG_INV_FP32 ? nullptr : h->inv_scale.get();
   a.fem_off = h->fem_off;
@@ -930,19 +1103,63 @@ ApplyArgs make_apply_args(maspcg_handle* h)
   return a;
 }
 
-template <typename TI, typename Tv, typename Tacc, bool kLevel0>
+// Level-0 domain apply variants (the solve uses h->apply_variant).
+enum ApplyVariant { kApplyRegisters = 0, kApplyStaged2 = 1, kApplyStaged1 = 2 };
+
+template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf>
 void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, Tacc* partial, int part_base,
                       int total_parts, int mode, PcgScalars* s, int g_begin, int g_end, int grid)
 {
-  constexpr int bytes = kApplyWarps * 2 * kInvElems * (int)sizeof(TI);
+  constexpr int bytes = kApplyWarps * kBuf * inv_elems<TI>() * (int)sizeof(TI);
   static bool configured = false;
   if (!configured) {
-    MCK(cudaFuncSetAttribute(k_apply_tma<TI, Tv, Tacc, kLevel0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    MCK(cudaFuncSetAttribute(k_apply_tma<TI, Tv, Tacc, kLevel0, kBuf>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes));
     configured = true;
   }
-  launch_pdl(h, k_apply_tma<TI, Tv, Tacc, kLevel0>, dim3(grid), dim3(kApplyWarps * 32), bytes, 
-      a, r, z, partial, part_base, total_parts, mode, s, g_begin, g_end, h->failed.get() + 4);
-  MLAUNCHED(h);
+  launch_pdl(h, k_apply_tma<TI, Tv, Tacc, kLevel0, kBuf>, dim3(grid), dim3(kApplyWarps * 32), bytes, a, r, z, partial,
+             part_base, total_parts, mode, s, g_begin, g_end, h->failed.get() + 4);
+}
+
+// CTAs of a staged apply over `domains` domains: one wave of resident CTAs.
+inline int staged_grid(const maspcg_handle* h, int domains, int kbuf)
+{
+  return std::max(1, std::min(ceil_div(domains, kApplyWarps), (kbuf == 1 ? 5 : 2) * h->sm_count));
+}
+
+// CTAs of the level-0 apply in a variant.  The r.z partial sums occupy one
+// slot per CTA, so the PCG engine sizes its reduction with this same count.
+inline int level0_grid(const maspcg_handle* h, int variant)
+{
+  const int d0 = h->lv.dom_begin[1];
+  if (h->cfg.inverse_storage == MASPCG_INV_FP32) variant = kApplyRegisters;
+  switch (variant) {
+    case kApplyStaged2: return staged_grid(h, d0, 2);
+    case kApplyStaged1: return staged_grid(h, d0, 1);
+    default: return std::max(1, std::min(ceil_div((long long)d0 * 32, kApplyTpb), 16 * h->sm_count));
+  }
+}
+
+// Level-0 apply (with the coarse correction and r.z) in the given variant.
+template <typename TI, typename Tv, typename Tacc>
+void level0_apply(maspcg_handle* h, const ApplyArgs& a, int variant, const Tv* r, Tv* z, Tacc* partial, int part_base,
+                  int total_parts, int mode, PcgScalars* s, int grid0)
+{
+  const int d0 = h->lv.dom_begin[1];
+  if (std::is_same<TI, float>::value) variant = kApplyRegisters;
+  // grid0 == level0_grid(h, variant): every CTA owns one r.z slot
+  switch (variant) {
+    case kApplyStaged2:
+      launch_apply_tma<TI, Tv, Tacc, true, 2>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0);
+      break;
+    case kApplyStaged1:
+      launch_apply_tma<TI, Tv, Tacc, true, 1>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0);
+      break;
+    default:
+      launch_pdl(h, k_level0_apply<TI, Tv, Tacc>, dim3(grid0), dim3(kApplyTpb), 0, a, r, z, partial, part_base,
+                 total_parts, mode, s);
+      break;
+  }
 }
 
 template <typename TI, typename Tv, typename Tacc>
@@ -951,35 +1168,11 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
 {
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
-  const int banks0 = h->c0 / kBank;
-  constexpr bool kStaged = !std::is_same<TI, float>::value;
-  launch_pdl(h, k_restrict0<Tv>, dim3(ceil_div((long long)banks0 * 32, kTpb)), dim3(kTpb), 0, a, r, s);
-  MLAUNCHED(h);
-  for (int l = 2; l < lv.levelnum; ++l) {
-    const int banks = ceil_div(lv.count[l - 1], kBank);
-    launch_pdl(h, k_restrictL, dim3(ceil_div((long long)banks * 32, kTpb)), dim3(kTpb), 0, a, l - 1, s);
-    MLAUNCHED(h);
-  }
-  const int d0 = lv.dom_begin[1];
-  const int coarse_domains = lv.domains - d0;
-  if (coarse_domains > 0) {
-    if (kStaged) {
-      launch_apply_tma<TI, Tv, Tacc, false>(h, a, r, z, nullptr, 0, 0, 0, s, d0, lv.domains,
-                                            ceil_div(coarse_domains, kApplyWarps));
-    } else {
-      launch_pdl(h, k_coarse_apply<TI>, dim3(ceil_div((long long)coarse_domains * 32, kTpb)), dim3(kTpb), 0, a, s);
-      MLAUNCHED(h);
-    }
-  }
-  launch_pdl(h, k_prolong1, dim3(ceil_div(lv.count[1], kTpb)), dim3(kTpb), 0, a, s);
-  MLAUNCHED(h);
-  if (kStaged) {
-    const int grid = std::max(1, std::min(ceil_div(d0, kApplyWarps), 2 * h->sm_count));
-    launch_apply_tma<TI, Tv, Tacc, true>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid);
-  } else {
-    launch_pdl(h, k_level0_apply<TI, Tv, Tacc>, dim3(grid0), dim3(kTpb), 0, a, r, z, partial, part_base, total_parts, mode, s);
-    MLAUNCHED(h);
-  }
+  const int variant = std::is_same<TI, float>::value ? (int)kApplyRegisters : h->apply_variant;
+  if (lv.levelnum > 1)
+    launch_pdl(h, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainWarps)), dim3(kChainWarps * 32), 0, a,
+               r, s);
+  level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0);
 }
 }  // namespace
 
@@ -1003,27 +1196,29 @@ void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_bas
 // Stage timing helpers: the level-0 domain apply alone, and the domain
 // assembly + inversion alone (member lists from the last build).
 template <typename Tv, typename Tacc>
-void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s)
+void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant)
 {
   ApplyArgs a = make_apply_args(h);
-  const int d0 = h->lv.dom_begin[1];
+  if (variant < 0) variant = h->apply_variant;
+  const int grid = level0_grid(h, variant);
+  (void)grid0;
   switch (h->cfg.inverse_storage) {
     case MASPCG_INV_BF16:
-      launch_apply_tma<__nv_bfloat16, Tv, Tacc, true>(h, a, r, z, partial, 0, grid0, 0, s, 0, d0, grid0);
+      level0_apply<__nv_bfloat16, Tv, Tacc>(h, a, variant, r, z, partial, 0, grid, 0, s, grid);
       break;
-    case MASPCG_INV_FP16:
-      launch_apply_tma<__half, Tv, Tacc, true>(h, a, r, z, partial, 0, grid0, 0, s, 0, d0, grid0);
-      break;
+    case MASPCG_INV_FP16: level0_apply<__half, Tv, Tacc>(h, a, variant, r, z, partial, 0, grid, 0, s, grid); break;
     default:
-      k_level0_apply<float, Tv, Tacc><<<grid0, kTpb, 0, h->stream>>>(a, r, z, partial, 0, grid0, 0, s);
-      MLAUNCHED(h);
+      MREQ(variant == kApplyRegisters || variant == h->apply_variant, MASPCG_ERR_UNSUPPORTED,
+           "the staged apply exists for 16-bit inverses only");
+      level0_apply<float, Tv, Tacc>(h, a, kApplyRegisters, r, z, partial, 0, grid, 0, s, grid);
       break;
   }
   MCK(cudaGetLastError());
 }
-template void mas_level0_only<float, float>(maspcg_handle*, const float*, float*, float*, int, PcgScalars*);
-template void mas_level0_only<float, double>(maspcg_handle*, const float*, float*, double*, int, PcgScalars*);
-template void mas_level0_only<double, double>(maspcg_handle*, const double*, double*, double*, int, PcgScalars*);
+template void mas_level0_only<float, float>(maspcg_handle*, const float*, float*, float*, int, PcgScalars*, int);
+template void mas_level0_only<float, double>(maspcg_handle*, const float*, float*, double*, int, PcgScalars*, int);
+template void mas_level0_only<double, double>(maspcg_handle*, const double*, double*, double*, int, PcgScalars*,
+                                              int);
 
 template void mas_apply<float, float>(maspcg_handle*, const float*, float*, float*, int, int, int, int, PcgScalars*);
 template void mas_apply<float, double>(maspcg_handle*, const float*, float*, double*, int, int, int, int,
@@ -1031,13 +1226,7 @@ template void mas_apply<float, double>(maspcg_handle*, const float*, float*, dou
 template void mas_apply<double, double>(maspcg_handle*, const double*, double*, double*, int, int, int, int,
                                         PcgScalars*);
 
-int mas_level0_grid(maspcg_handle* h)
-{
-  const int warps = h->lv.dom_begin[1];
-  if (h->cfg.inverse_storage != MASPCG_INV_FP32)  // TMA-staged apply (launch_apply_tma)
-    return std::max(1, std::min(ceil_div(warps, kApplyWarps), 2 * h->sm_count));
-  return std::max(1, std::min(ceil_div((long long)warps * 32, kTpb), 8 * h->sm_count));
-}
+int mas_level0_grid(maspcg_handle* h) { return level0_grid(h, h->apply_variant); }
 
 // Decode the stored inverses into the reference's packed FP32 layout.
 void decode_inverses(maspcg_handle* h, float* out)
@@ -1045,7 +1234,7 @@ void decode_inverses(maspcg_handle* h, float* out)
   const int D = h->lv.domains;
   const int storage = h->cfg.inverse_storage;
   const size_t esize = storage == MASPCG_INV_FP32 ? 4 : 2;
-  std::vector<unsigned char> raw((size_t)D * kInvElems * esize);
+  std::vector<unsigned char> raw((size_t)D * inv_elems_for(storage) * esize);
   std::vector<float> sc;
   MCK(cudaMemcpyAsync(raw.data(), h->inv.get(), raw.size(), cudaMemcpyDeviceToHost, h->stream));
   if (storage != MASPCG_INV_FP32) {
@@ -1110,7 +1299,7 @@ void decode_inverses(maspcg_handle* h, float* out)
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j)
             W[(3 * ra + i) * 96 + 3 * cb + j] =
-                (double)elem((size_t)g * kInvElems + (size_t)(d * 9 + 3 * i + j) * kBank + l) * scg[3 * cb + j];
+                (double)elem((size_t)g * kInvElems16 + (size_t)inv16_pos(d * 9 + 3 * i + j, l)) * scg[3 * cb + j];
       }
     for (int r = 0; r < 96; ++r)
       for (int q = r; q < 96; ++q) {

@@ -33,7 +33,21 @@ namespace maspcg {
 constexpr int kBank = 32;
 constexpr int kPacked = kBank * (kBank + 1) / 2;  // 528
 constexpr int kDiags = 17;
-constexpr int kInvElems = kDiags * 9 * kBank;      // 4896 stored elements per domain
+constexpr int kInvElems = kDiags * 9 * kBank;      // 4896 stored elements per domain (FP32)
+// 16-bit storage packs each lane's 153 elements (17 diagonals x 9, in order
+// 9d + e) two per 32-bit word, word-major: word w of lane l at [w][l]; the
+// high half of the last word is zero.  A warp reads a domain in 77 coalesced
+// 128-byte loads and keeps it in registers for the two factored passes.
+constexpr int kInvWords16 = (kDiags * 9 + 1) / 2;  // 77
+constexpr int kInvElems16 = 2 * kInvWords16 * kBank;  // 4928 stored 16-bit elements per domain
+
+// Stored elements per domain for an inverse element type.
+template <typename TI>
+constexpr int inv_elems() { return sizeof(TI) == 4 ? kInvElems : kInvElems16; }
+inline int inv_elems_for(int storage) { return storage == MASPCG_INV_FP32 ? kInvElems : kInvElems16; }
+
+// Position of element k (= 9d + e) of lane l in a 16-bit domain record.
+__host__ __device__ __forceinline__ int inv16_pos(int k, int l) { return ((k >> 1) * kBank + l) * 2 + (k & 1); }
 constexpr int kMaxLevels = 6;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -131,7 +145,7 @@ struct FactorArgs {
   const double* val64;           // row-major blocks
   int fem_off;
   int c0;
-  void* inv;                     // kInvElems per domain, type per storage
+  void* inv;                     // inv_elems<TI>() per domain, type per storage
   float* scale;                  // 96 per domain (16-bit storage)
   int* failed;                   // count of domains with a pivot <= 0
   double* assembled;             // optional: packed FP64 domain matrices (reference layout)
@@ -174,8 +188,8 @@ struct maspcg_handle {
   bool mas_layout = false;  // internal order uses the MAS partition
   maspcg::DBuf<int> int_of_row, row_of_int;
   maspcg::DBuf<int> rowptr, colidx;
-  maspcg::DBuf<double> val64;
-  maspcg::DBuf<float> val32;
+  maspcg::DBuf<double> val64;     // row-major 3x3 blocks
+  maspcg::DBuf<float> val32;      // tiles of 32 blocks, element-major: (t/32)*288 + 32e + t%32
   maspcg::DBuf<unsigned long long> keys, keys_sorted;
   maspcg::DBuf<int> kv, kv_sorted, seg_head, seg_start, row_count;
   maspcg::DBuf<double> in_vals;
@@ -187,7 +201,8 @@ struct maspcg_handle {
   maspcg::DBuf<float> inv_scale;
   maspcg::DBuf<int> failed;
   int failed_domains = 0;
-  maspcg::DBuf<float> coarse_r, coarse_z, zacc1;
+  maspcg::DBuf<float> coarse_r, coarse_z;
+  maspcg::DBuf<int> chain_count, chain_target;  // coarse-level dataflow counters (per coarse domain)
   maspcg::DBuf<double> coarse64;
   maspcg::DBuf<double> abd_inv64;
   maspcg::DBuf<float> abd_inv32;
@@ -195,12 +210,16 @@ struct maspcg_handle {
   maspcg::DBuf<float> diag_inv32;
 
   // ---- PCG
-  maspcg::DBuf<unsigned char> vx, vr, vz, vp, vap;  // vectors in the working precision
+  maspcg::DBuf<unsigned char> vx, vr, vz, vap;      // vectors in the working precision, 3 per block row
+  maspcg::DBuf<unsigned char> vp4;                  // search direction, padded to 4 per block row
   maspcg::DBuf<double> b64, x64, r64;               // FP64: rhs, x (hi), residual scratch
   maspcg::DBuf<double> partial, partial_rz;
   maspcg::DBuf<maspcg::PcgScalars> scal;
   maspcg::PcgScalars* h_scal = nullptr;  // pinned mirror
   maspcg::DBuf<double> io_a, io_b;       // staging for host pointers / permutations
+  maspcg::DBuf<unsigned char> l2_flush;  // maspcg_time_stage only: written between timed launches
+  maspcg::DBuf<int> adj_rows, adj_cols;   // maspcg_bcoo_gradient staging for host arguments
+  maspcg::DBuf<double> adj_lam, adj_x, adj_grad;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_batch = 0;
   bool graph_dirty = true;
@@ -209,6 +228,7 @@ struct maspcg_handle {
   long long kernel_launches = 0;  // this library's kernels launched on the handle
   long long graph_kernels = 0;    // kernel nodes of the captured batch graph
   bool use_pdl = true;            // programmatic dependent launch for the iteration kernels
+  int apply_variant = 1;          // 16-bit level-0 apply: 0 registers, 1 TMA-staged x2 buffers, 2 TMA-staged x1
 };
 
 namespace maspcg {
@@ -234,6 +254,10 @@ void decode_inverses(maspcg_handle* h, float* out_host);
 // pcg.cu
 double time_stage(maspcg_handle* h, int stage, int repeats);
 void solve(maspcg_handle* h, const double* b_dev, double* x_dev, maspcg_result* res);
+
+// adjoint.cu (device pointers, caller's row order)
+void bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n, const double* lam, const double* x,
+                   double* grad);
 
 // residual_noalloc.cu
 void residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b, double* residual_norms,

@@ -97,7 +97,7 @@ __global__ void k_fill_values(const unsigned long long* __restrict__ keys, const
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
     val64[9 * (size_t)u + q] = a[q];
-    val32[9 * (size_t)u + q] = (float)a[q];
+    val32[(size_t)(u >> 5) * 288 + 32 * q + (u & 31)] = (float)a[q];  // tiles of 32 blocks, element-major
   }
 }
 
@@ -311,7 +311,7 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   h->nnzb = nnzb;
   h->colidx.resize(nnzb, 4);  // 16-byte tail for TMA bulk copies
   h->val64.resize((size_t)9 * nnzb, 2);
-  h->val32.resize((size_t)9 * nnzb, 4);
+  h->val32.resize((size_t)9 * (((size_t)nnzb + 31) / 32 * 32));
   h->row_count.resize(nb_int + 1);
   h->rowptr.resize(nb_int + 1);
   MCK(cudaMemsetAsync(h->row_count.get(), 0, sizeof(int) * (nb_int + 1), st));
@@ -321,7 +321,8 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   tb = h->cub_tmp.cap;
   MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), tb, h->row_count.get(), h->rowptr.get(), nb_int + 1, st));
   k_fill_values<<<ceil_div(nnzb, kTpb), kTpb, 0, st>>>(h->keys_sorted.get(), h->kv_sorted.get(), h->seg_start.get(),
-                                                      nnzb, m_valid, vals, h->val64.get(), h->val32.get()); MLAUNCHED(h);
+                                                      nnzb, m_valid, vals, h->val64.get(), h->val32.get());
+  MLAUNCHED(h);
   MCK(cudaGetLastError());
 }
 

@@ -16,11 +16,11 @@
 // dots, FP64 residual replacement every period with x accumulated in FP64).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "maspcg_internal.cuh"
 #include "pcg_device.cuh"
 #include "spmv_row.cuh"
-#include "spmv_tma.cuh"
 
 namespace maspcg {
 
@@ -28,7 +28,7 @@ template <typename Tv, typename Tacc>
 void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                int grid0, PcgScalars* s);
 template <typename Tv, typename Tacc>
-void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s);
+void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant);
 void launch_factor(maspcg_handle* h, double* assembled_out);
 int mas_level0_grid(maspcg_handle* h);
 
@@ -57,40 +57,185 @@ __global__ void __launch_bounds__(kTpb) k_init(const double* __restrict__ b, Tv*
     s->bb = total;
 }
 
-// p = z (k == 1) or z + beta p
+// ---- padded search direction: one 16-byte (FP32) / 32-byte (FP64) slot per
+// block row, so the SpMV gathers a column's three entries with one vector load.
+template <typename T>
+struct P4;
+template <>
+struct P4<float> {
+  float x, y, z, w;
+};
+template <>
+struct P4<double> {
+  double x, y, z, w;
+};
+
+__device__ __forceinline__ P4<float> ld_p4(const float* p4, int v)
+{
+  const float4 q = __ldg(reinterpret_cast<const float4*>(p4) + v);
+  return {q.x, q.y, q.z, q.w};
+}
+__device__ __forceinline__ P4<double> ld_p4(const double* p4, int v)
+{
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p4) + 2 * v);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p4) + 2 * v + 1);
+  return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st_p4(float* p4, int v, float x, float y, float z)
+{
+  reinterpret_cast<float4*>(p4)[v] = make_float4(x, y, z, 0.f);
+}
+__device__ __forceinline__ void st_p4(double* p4, int v, double x, double y, double z)
+{
+  reinterpret_cast<double2*>(p4)[2 * v] = make_double2(x, y);
+  reinterpret_cast<double2*>(p4)[2 * v + 1] = make_double2(z, 0.0);
+}
+
+// Four consecutive block rows (12 values) of a 3-per-row vector as 16-byte
+// vector loads/stores; `v0` is a multiple of 4.
+template <typename T>
+__device__ __forceinline__ void ld12(const T* p, int v0, T o[12])
+{
+  if constexpr (sizeof(T) == 4) {
+    const float4* q = reinterpret_cast<const float4*>(p + 3 * (size_t)v0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 w = q[k];
+      o[4 * k] = w.x, o[4 * k + 1] = w.y, o[4 * k + 2] = w.z, o[4 * k + 3] = w.w;
+    }
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(p + 3 * (size_t)v0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double2 w = q[k];
+      o[2 * k] = w.x, o[2 * k + 1] = w.y;
+    }
+  }
+}
+template <typename T>
+__device__ __forceinline__ void st12(T* p, int v0, const T o[12])
+{
+  if constexpr (sizeof(T) == 4) {
+    float4* q = reinterpret_cast<float4*>(p + 3 * (size_t)v0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+  } else {
+    double2* q = reinterpret_cast<double2*>(p + 3 * (size_t)v0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) q[k] = make_double2(o[2 * k], o[2 * k + 1]);
+  }
+}
+
+// p = z (k == 1) or z + beta p, written into the padded layout.  Each thread
+// takes four block rows with 16-byte accesses (a scalar tail for the rest).
 template <typename Tv>
-__global__ void __launch_bounds__(kTpb) k_update_p(const Tv* __restrict__ z, Tv* p, int n, const PcgScalars* s)
+__global__ void __launch_bounds__(kTpb) k_update_p(const Tv* __restrict__ z, Tv* p4, int nrows, const PcgScalars* s)
 {
   pdl_enter();
   if (!running(s)) return;
   const bool first = s->k == 1;
   const Tv beta = (Tv)s->beta;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = first ? z[i] : z[i] + beta * p[i];
+  const int quads = nrows >> 2;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x) {
+    Tv zz[12];
+    ld12(z, 4 * q, zz);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int v = 4 * q + j;
+      if (first) {
+        st_p4(p4, v, zz[3 * j], zz[3 * j + 1], zz[3 * j + 2]);
+      } else {
+        const P4<Tv> o = ld_p4(p4, v);
+        st_p4(p4, v, zz[3 * j] + beta * o.x, zz[3 * j + 1] + beta * o.y, zz[3 * j + 2] + beta * o.z);
+      }
+    }
+  }
+  for (int v = 4 * quads + blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
+    const Tv z0 = z[3 * (size_t)v], z1 = z[3 * (size_t)v + 1], z2 = z[3 * (size_t)v + 2];
+    if (first) {
+      st_p4(p4, v, z0, z1, z2);
+    } else {
+      const P4<Tv> o = ld_p4(p4, v);
+      st_p4(p4, v, z0 + beta * o.x, z1 + beta * o.y, z2 + beta * o.z);
+    }
+  }
 }
 
-// Ap = A p (LPR lanes per block row) and p.Ap; last block: alpha.
-template <typename Tm, typename Tv, typename Tacc, int LPR>
-__global__ void __launch_bounds__(kTpb) k_spmv_dot(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                                    const Tm* __restrict__ val, const Tv* __restrict__ p, Tv* ap,
-                                                    int nrows, Tacc* partial, PcgScalars* s)
+// One 3x3 block of the matrix.  FP32: tiles of 32 blocks stored element-major
+// (element e of block t at (t/32)*288 + 32e + t%32), so a warp's element loads
+// are coalesced and a tile is one contiguous 1152-byte run.  FP64: row-major
+// blocks.
+template <bool kTiled, typename Tm>
+__device__ __forceinline__ void load_block(const Tm* __restrict__ val, int t, Tm m[9])
 {
+  if (kTiled) {
+    const Tm* b = val + (size_t)(t >> 5) * 288 + (t & 31);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = __ldcs(b + 32 * e);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = __ldcs(val + 9 * (size_t)t + e);
+  }
+}
+
+// Ap = A p and p.Ap; last block: alpha.  LPR lanes per block row, each lane
+// takes two blocks per step with every load issued before the arithmetic;
+// the next row's extent is fetched while the current row is processed.
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
+__global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                                const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap,
+                                                int nrows, Tacc* partial, PcgScalars* s)
+{
+  pdl_enter();
   if (!running(s)) return;
-  const int groups_per_block = kTpb / LPR;
+  using A = typename AccOf<Tm>::type;
+  constexpr int kRows = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
+  const int step = gridDim.x * kRows;
   Tacc dot = 0;
-  const int iters = (nrows + gridDim.x * groups_per_block - 1) / (gridDim.x * groups_per_block);
-  for (int it = 0; it < iters; ++it) {
-    const int row = (it * gridDim.x + blockIdx.x) * groups_per_block + threadIdx.x / LPR;
-    const bool ok = row < nrows;
-    const int rs = ok ? rowptr[row] : 0, re = ok ? rowptr[row + 1] : 0;
-    typename AccOf<Tm>::type acc[3];
-    row_product<Tm, Tv, LPR>(rs, re, colidx, val, p, sub, acc);
-    if (ok && sub < 3) {
-      const Tv y = (Tv)acc[sub];
-      ap[3 * (size_t)row + sub] = y;
-      dot += (Tacc)p[3 * (size_t)row + sub] * (Tacc)y;
+  int row = blockIdx.x * kRows + threadIdx.x / LPR;
+  int rs = row < nrows ? __ldg(rowptr + row) : 0, re = row < nrows ? __ldg(rowptr + row + 1) : 0;
+  for (int row0 = blockIdx.x * kRows; row0 < nrows; row0 += step) {
+    const int nrow = row + step;
+    const int nrs = nrow < nrows ? __ldg(rowptr + nrow) : 0, nre = nrow < nrows ? __ldg(rowptr + nrow + 1) : 0;
+    A a0 = 0, a1 = 0, a2 = 0;
+    for (int t = rs + sub; t < re; t += 2 * LPR) {
+      const int u = t + LPR;
+      const bool two = u < re;
+      Tm m[9], q[9];
+      const int c = __ldcs(colidx + t);
+      const int d = two ? __ldcs(colidx + u) : c;
+      load_block<kTiled>(val, t, m);
+      if (two) {
+        load_block<kTiled>(val, u, q);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) q[e] = Tm(0);
+      }
+      const P4<Tv> x = ld_p4(p4, c), y = ld_p4(p4, d);
+      a0 += (A)m[0] * (A)x.x + (A)m[1] * (A)x.y + (A)m[2] * (A)x.z;
+      a1 += (A)m[3] * (A)x.x + (A)m[4] * (A)x.y + (A)m[5] * (A)x.z;
+      a2 += (A)m[6] * (A)x.x + (A)m[7] * (A)x.y + (A)m[8] * (A)x.z;
+      a0 += (A)q[0] * (A)y.x + (A)q[1] * (A)y.y + (A)q[2] * (A)y.z;
+      a1 += (A)q[3] * (A)y.x + (A)q[4] * (A)y.y + (A)q[5] * (A)y.z;
+      a2 += (A)q[6] * (A)y.x + (A)q[7] * (A)y.y + (A)q[8] * (A)y.z;
     }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(kFull, a0, o, LPR);
+      a1 += __shfl_xor_sync(kFull, a1, o, LPR);
+      a2 += __shfl_xor_sync(kFull, a2, o, LPR);
+    }
+    if (row < nrows && sub < 3) {
+      const Tv y = (Tv)(sub == 0 ? a0 : (sub == 1 ? a1 : a2));
+      ap[3 * (size_t)row + sub] = y;
+      const P4<Tv> pr = ld_p4(p4, row);
+      const Tv pv = sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z);
+      dot += (Tacc)pv * (Tacc)y;
+    }
+    row = nrow;
+    rs = nrs;
+    re = nre;
   }
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
@@ -109,157 +254,49 @@ __global__ void __launch_bounds__(kTpb) k_spmv_dot(const int* __restrict__ rowpt
   }
 }
 
-// Ap = A p with the block stream staged by TMA (spmv_tma.cuh) and p.Ap;
-// last block: alpha.  `err` records an expired mbarrier wait.
-template <typename Tm, typename Tv, typename Tacc>
-__global__ void __launch_bounds__(kTmaThreads, 2)
-    k_spmv_tma(const int* __restrict__ rowptr, const int* __restrict__ colidx, const Tm* __restrict__ val,
-               const Tv* __restrict__ p, Tv* ap, int nrows, Tacc* partial, PcgScalars* s, int* err)
-{
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[2];
-  pdl_enter();
-  if (!running(s)) return;
-  using St = TmaStage<Tm>;
-  unsigned char* sval0 = smem;
-  unsigned char* sval1 = smem + St::kValBytes;
-  unsigned char* scol0 = smem + 2 * St::kValBytes;
-  unsigned char* scol1 = smem + 2 * St::kValBytes + St::kColBytes;
-  const int nchunks = (nrows + kTmaRows - 1) / kTmaRows;
-  const int tid = threadIdx.x, grp = tid >> 4, sub = tid & 15;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  auto staged = [&](int chunk) {
-    const int r0 = chunk * kTmaRows, r1 = min(r0 + kTmaRows, nrows);
-    const int nb = rowptr[r1] - rowptr[r0];
-    return nb > 0 && nb <= St::kCap;
-  };
-  if (tid == 0) {
-    const int c0 = blockIdx.x, c1 = blockIdx.x + gridDim.x;
-    if (c0 < nchunks) chunk_issue<Tm>(c0, nrows, rowptr, val, colidx, sval0, scol0, &bar[0]);
-    if (c1 < nchunks) chunk_issue<Tm>(c1, nrows, rowptr, val, colidx, sval1, scol1, &bar[1]);
-  }
-  unsigned phase0 = 0, phase1 = 0;
-  Tacc dot = 0;
-  int i = 0;
-  bool ok = true;
-  for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x, ++i) {
-    const int st = i & 1;
-    const int r0 = chunk * kTmaRows, r1 = min(r0 + kTmaRows, nrows);
-    const int b0 = rowptr[r0];
-    const bool stg = staged(chunk);
-    if (stg) {
-      const bool w = mbar_wait(st ? &bar[1] : &bar[0], st ? phase1 : phase0);
-      if (w) {
-        if (st)
-          phase1 ^= 1u;
-        else
-          phase0 ^= 1u;
-      }
-      if (!__syncthreads_and(w)) {
-        ok = false;
-        break;
-      }
-    }
-    const int row = r0 + grp;
-    const bool has = row < r1;
-    const int rs = has ? rowptr[row] : 0, re = has ? rowptr[row + 1] : 0;
-    typename AccOf<Tm>::type acc[3];
-    if (stg) {
-      using A = typename AccOf<Tm>::type;
-      const unsigned char* sv = st ? sval1 : sval0;
-      const unsigned char* sc = st ? scol1 : scol0;
-      const Tm* vb = reinterpret_cast<const Tm*>(sv + (((size_t)b0 * 9 * sizeof(Tm)) & 15));
-      const int* cb = reinterpret_cast<const int*>(sc + (((size_t)b0 * 4) & 15));
-      A a0 = 0, a1 = 0, a2 = 0;
-      for (int t = rs + sub; t < re; t += 16) {
-        const int lt = t - b0;
-        const int c = cb[lt];
-        const Tm* B = vb + 9 * lt;
-        const A x0 = (A)ldv(p + 3 * (size_t)c), x1 = (A)ldv(p + 3 * (size_t)c + 1), x2 = (A)ldv(p + 3 * (size_t)c + 2);
-        a0 += (A)B[0] * x0 + (A)B[1] * x1 + (A)B[2] * x2;
-        a1 += (A)B[3] * x0 + (A)B[4] * x1 + (A)B[5] * x2;
-        a2 += (A)B[6] * x0 + (A)B[7] * x1 + (A)B[8] * x2;
-      }
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(kFull, a0, o, 16);
-        a1 += __shfl_xor_sync(kFull, a1, o, 16);
-        a2 += __shfl_xor_sync(kFull, a2, o, 16);
-      }
-      acc[0] = a0;
-      acc[1] = a1;
-      acc[2] = a2;
-    } else {
-      row_product<Tm, Tv, 16>(rs, re, colidx, val, p, sub, acc);
-    }
-    if (has && sub < 3) {
-      const Tv y = (Tv)acc[sub];
-      ap[3 * (size_t)row + sub] = y;
-      dot += (Tacc)p[3 * (size_t)row + sub] * (Tacc)y;
-    }
-    __syncthreads();  // the stage is free again
-    if (tid == 0) {
-      const int nxt = chunk + 2 * gridDim.x;
-      if (nxt < nchunks) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        chunk_issue<Tm>(nxt, nrows, rowptr, val, colidx, st ? sval1 : sval0, st ? scol1 : scol0,
-                        st ? &bar[1] : &bar[0]);
-      }
-    }
-  }
-  if (!ok) {
-    // drain the copies this CTA still has in flight (bounded), report, leave
-    if (tid == 0) {
-      atomicExch(err, 1);
-      for (int j = 0; j < 2; ++j) {
-        const int chunk = blockIdx.x + (i + j) * gridDim.x;
-        if (chunk < nchunks && staged(chunk)) {
-          const int stj = (i + j) & 1;
-          mbar_wait(stj ? &bar[1] : &bar[0], stj ? phase1 : phase0);
-        }
-      }
-      s->status = MASPCG_SOLVE_NONFINITE;
-    }
-    return;
-  }
-  Tacc total = 0;
-  if (grid_finish<Tacc, kTmaThreads>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
-      threadIdx.x == 0) {
-    const double pap = (double)total;
-    s->pap = pap;
-    if (!isfinite(pap)) {
-      s->status = MASPCG_SOLVE_NONFINITE;
-      s->iterations = s->k;
-    } else if (!(pap > 0.0)) {
-      s->status = MASPCG_SOLVE_NONPOSITIVE_CURVATURE;
-      s->iterations = s->k;
-    } else {
-      s->alpha = s->rz / pap;
-    }
-  }
-}
-
 // x += alpha p, r -= alpha Ap, r.r; last block: stopping gate.
 // MIXED: x is the FP32 correction since the last replacement and a met gate
-// asks for the FP64 true residual instead of stopping.
+// asks for the FP64 true residual instead of stopping.  Four block rows per
+// thread with 16-byte accesses (a scalar tail for the rest).
 template <typename Tv, typename Tacc>
-__global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p, const Tv* __restrict__ ap,
-                                                     int n, int mixed, Tacc* partial, PcgScalars* s)
+__global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p4, const Tv* __restrict__ ap,
+                                                     int nrows, int mixed, Tacc* partial, PcgScalars* s)
 {
   pdl_enter();
   if (!running(s)) return;
   const Tv alpha = (Tv)s->alpha;
   Tacc acc = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[i] += alpha * p[i];
-    const Tv ri = r[i] - alpha * ap[i];
-    r[i] = ri;
-    acc += (Tacc)ri * (Tacc)ri;
+  const int quads = nrows >> 2;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x) {
+    Tv xx[12], rr[12], ww[12], pp[12];
+    ld12(x, 4 * q, xx);
+    ld12(r, 4 * q, rr);
+    ld12(ap, 4 * q, ww);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const P4<Tv> o = ld_p4(p4, 4 * q + j);
+      pp[3 * j] = o.x, pp[3 * j + 1] = o.y, pp[3 * j + 2] = o.z;
+    }
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      xx[k] = xx[k] + alpha * pp[k];
+      rr[k] = rr[k] - alpha * ww[k];
+      acc += (Tacc)rr[k] * (Tacc)rr[k];
+    }
+    st12(x, 4 * q, xx);
+    st12(r, 4 * q, rr);
+  }
+  for (int v = 4 * quads + blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
+    const size_t i = 3 * (size_t)v;
+    const P4<Tv> o = ld_p4(p4, v);
+    const Tv pv[3] = {o.x, o.y, o.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      x[i + k] = x[i + k] + alpha * pv[k];
+      const Tv rn = r[i + k] - alpha * ap[i + k];
+      r[i + k] = rn;
+      acc += (Tacc)rn * (Tacc)rn;
+    }
   }
   Tacc total = 0;
   if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
@@ -426,12 +463,24 @@ __global__ void k_from_f64(const double* __restrict__ x, Tv* y, int n)
   if (i < n) y[i] = (Tv)x[i];
 }
 
+// Reads `n` 16-byte words through L2 (evicting what was cached) without
+// dirtying any line; writes only if the data is nonzero (never, in use).
+__global__ void __launch_bounds__(kTpb) k_l2_evict(const uint4* __restrict__ p, size_t n, unsigned* sink)
+{
+  unsigned acc = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint4 v = __ldcg(p + i);
+    acc |= v.x | v.y | v.z | v.w;
+  }
+  if (acc == 0xffffffffu) *sink = acc;
+}
+
 // ----------------------------------------------------------------- engine --
 
 template <typename Tm, typename Tv, typename Tacc>
 struct Engine {
   maspcg_handle* h;
-  int n, gstream, gspmv, gl0, gother, parts_other, parts_total;
+  int n, gstream, gspmv, grows, gl0, gother, parts_other, parts_total;
   bool mas, mixed;
 
   explicit Engine(maspcg_handle* hh) : h(hh)
@@ -441,6 +490,7 @@ struct Engine {
     mixed = h->cfg.precision == MASPCG_PREC_MIXED;
     gstream = h->grid_stream;
     gspmv = std::max(1, std::min(ceil_div(h->nb_int, kTpb / 16), 4 * h->sm_count));
+    grows = std::max(1, std::min(ceil_div(std::max(h->nb_int / 4, 1), kTpb), 8 * h->sm_count));
     gl0 = mas ? mas_level0_grid(h) : 0;
     const bool other = !mas || h->abd_bodies > 0 || h->fem_off > 0 || h->nb_int > h->fem_off + h->c0;
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;
@@ -466,7 +516,6 @@ struct Engine {
         launch_pdl(h, k_other_apply<Tv, Tacc, float>, dim3(gother), dim3(kTpb), 0, 
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv32.get(), bj ? h->diag_inv32.get() : nullptr,
             s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
-      MLAUNCHED(h);
     }
     if (mas) mas_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s);
     MCK(cudaGetLastError());
@@ -474,28 +523,30 @@ struct Engine {
 
   void iteration_head(PcgScalars* s)
   {
-    launch_pdl(h, k_update_p<Tv>, dim3(gstream), dim3(kTpb), 0, V(h->vz), V(h->vp), n, s);
-    spmv_tma(s);
-    launch_pdl(h, k_update_xr<Tv, Tacc>, dim3(gstream), dim3(kTpb), 0, V(h->vx), V(h->vr), V(h->vp), V(h->vap), n, mixed ? 1 : 0,
-                                                   partial(), s);
+    launch_pdl(h, k_update_p<Tv>, dim3(grows), dim3(kTpb), 0, V(h->vz), V(h->vp4), h->nb_int, s);
+    spmv(s);
+    launch_pdl(h, k_update_xr<Tv, Tacc>, dim3(grows), dim3(kTpb), 0, V(h->vx), V(h->vr), V(h->vp4), V(h->vap),
+               h->nb_int, mixed ? 1 : 0, partial(), s);
   }
 
   const Tm* matrix();
 
-  void spmv_tma(PcgScalars* s)
+  // SpMV rows per CTA step: kTpb / kSpmvLanes.
+  static constexpr int kSpmvLanes = 8;
+
+  void spmv(PcgScalars* s)
   {
-    using St = TmaStage<Tm>;
-    constexpr int bytes = 2 * (St::kValBytes + St::kColBytes);
-    static bool configured = false;
-    if (!configured) {
-      MCK(cudaFuncSetAttribute(k_spmv_tma<Tm, Tv, Tacc>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-      configured = true;
+    constexpr bool kTiled = std::is_same<Tm, float>::value;
+    constexpr int rows = kTpb / kSpmvLanes;
+    // one wave of resident CTAs; the kernel strides over the rest
+    static int per_sm = 0;
+    if (!per_sm) {
+      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv<Tm, Tv, Tacc, kTiled, kSpmvLanes>, kTpb, 0));
+      per_sm = std::max(per_sm, 1);
     }
-    const int grid = std::max(1, std::min(2 * h->sm_count, ceil_div(h->nb_int, kTmaRows)));
-    launch_pdl(h, k_spmv_tma<Tm, Tv, Tacc>, dim3(grid), dim3(kTmaThreads), bytes, h->rowptr.get(), h->colidx.get(), matrix(),
-                                                                      V(h->vp), V(h->vap), h->nb_int, partial(), s,
-                                                                      h->failed.get() + 4);
-    MLAUNCHED(h);
+    const int grid = std::max(1, std::min(ceil_div(h->nb_int, rows), per_sm * h->sm_count));
+    launch_pdl(h, k_spmv<Tm, Tv, Tacc, kTiled, kSpmvLanes>, dim3(grid), dim3(kTpb), 0, h->rowptr.get(),
+               h->colidx.get(), matrix(), V(h->vp4), V(h->vap), h->nb_int, partial(), s);
   }
 
   void true_residual(PcgScalars* s)
@@ -516,6 +567,12 @@ struct Engine {
     }
   }
 
+  // Mean device time of one stage over `repeats` launches.  Before every
+  // launch a 256 MB zero buffer is read through L2 (clean lines only, so the
+  // timed launch pays no write-back), so each launch starts cold as it does
+  // inside the solve, where the SpMV streams more than L2 between two
+  // applies; each launch is bracketed by its own events.  Programmatic
+  // dependent launch is off while timing.
   double time_stage(int stage, int repeats)
   {
     cudaStream_t st = h->stream;
@@ -528,35 +585,56 @@ struct Engine {
     init.max_iter = 1 << 30;
     init.tol = 0.0;
     init.gate = MASPCG_GATE_EUCLID;
-    MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     MREQ(stage != 3 || mas, MASPCG_ERR_NOT_READY, "stage 3 needs a MAS32 preconditioner");
     MREQ(stage != 2 || mas, MASPCG_ERR_NOT_READY, "stage 2 needs a MAS32 preconditioner");
+    MREQ(stage < 4 || stage > 6 || mas, MASPCG_ERR_NOT_READY, "stages 4-6 need a MAS32 preconditioner");
+    MREQ(stage >= 0 && stage <= 6, MASPCG_ERR_INVALID_ARGUMENT, "unknown stage");
+    constexpr size_t kFlushBytes = 256u << 20;
+    if (h->l2_flush.n < kFlushBytes) {
+      h->l2_flush.resize(kFlushBytes);
+      MCK(cudaMemsetAsync(h->l2_flush.get(), 0, kFlushBytes, st));
+    }
+    MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     auto once = [&]() {
       switch (stage) {
-        case 0: spmv_tma(s); break;
-        case 4:
-          k_spmv_dot<Tm, Tv, Tacc, 16><<<gspmv, kTpb, 0, st>>>(h->rowptr.get(), h->colidx.get(), matrix(), V(h->vp),
-                                                              V(h->vap), h->nb_int, partial(), s);
-          MLAUNCHED(h);
-          break;
+        case 0: spmv(s); break;
         case 1: precondition(V(h->vr), V(h->vz), 0, s); break;
-        case 2: mas_level0_only<Tv, Tacc>(h, V(h->vr), V(h->vz), partial_rz(), gl0, s); break;
+        case 2: mas_level0_only<Tv, Tacc>(h, V(h->vr), V(h->vz), partial_rz(), gl0, s, -1); break;
         case 3: launch_factor(h, nullptr); break;
-        default: throw Error(MASPCG_ERR_INVALID_ARGUMENT, "unknown stage");
+        default: mas_level0_only<Tv, Tacc>(h, V(h->vr), V(h->vz), partial_rz(), gl0, s, stage == 6 ? 0 : stage - 3);
       }
     };
-    once();  // warm
-    MCK(cudaEventRecord(h->ev0, st));
-    for (int i = 0; i < repeats; ++i) once();
-    MCK(cudaEventRecord(h->ev1, st));
+    const bool pdl = h->use_pdl;
+    h->use_pdl = false;
+    double total = 0.0;
+    try {
+      once();  // warm
+      for (int i = 0; i < repeats; ++i) {
+        k_l2_evict<<<4 * h->sm_count, kTpb, 0, st>>>(reinterpret_cast<const uint4*>(h->l2_flush.get()),
+                                                     kFlushBytes / 16, reinterpret_cast<unsigned*>(h->l2_flush.get()));
+        MLAUNCHED(h);
+        MCK(cudaEventRecord(h->ev0, st));
+        once();
+        MCK(cudaEventRecord(h->ev1, st));
+        MCK(cudaEventSynchronize(h->ev1));
+        float ms = 0.f;
+        MCK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        total += ms;
+      }
+    } catch (...) {
+      h->use_pdl = pdl;
+      throw;
+    }
+    h->use_pdl = pdl;
     MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
     MCK(cudaStreamSynchronize(st));
     MCK(cudaGetLastError());
-    MREQ(h->h_scal->status == MASPCG_SOLVE_RUNNING, MASPCG_ERR_NOT_READY,
-         "stage timing needs finite vectors: solve once first");
-    float ms = 0.f;
-    MCK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-    return (double)ms / std::max(1, repeats);
+    if (h->h_scal->status != MASPCG_SOLVE_RUNNING)
+      throw Error(MASPCG_ERR_NOT_READY, "stage " + std::to_string(stage) + " left status " +
+                                            std::to_string(h->h_scal->status) + " (pAp " +
+                                            std::to_string(h->h_scal->pap) + ", rz_new " +
+                                            std::to_string(h->h_scal->rz_new) + "): solve once first");
+    return total / std::max(1, repeats);
   }
 
   void run(const double* b_int, maspcg_result* res)
@@ -615,7 +693,9 @@ struct Engine {
     {
       int terr = 0;
       MCK(cudaMemcpy(&terr, h->failed.get() + 4, sizeof(int), cudaMemcpyDeviceToHost));
-      MREQ(terr == 0, MASPCG_ERR_CUDA, "a TMA mbarrier wait expired in the SpMV");
+      MREQ(terr == 0, MASPCG_ERR_CUDA,
+           terr == 2 ? "coarse-level dataflow queue overflow in the preconditioner apply"
+                     : "a TMA mbarrier wait expired in the preconditioner apply");
     }
     // final FP64 iterate
     if (mixed) {

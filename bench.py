@@ -38,7 +38,7 @@ WORKLOAD = "cube 64^3 (262,144 verts, 786,432 DOF), 50,000 point-triangle contac
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=1)
@@ -174,8 +174,8 @@ def run_ours(args, world, rank, local):
     x_d = torch.zeros_like(b_d)
     stream = torch.cuda.Stream(device=dev)
 
-    def make(precision, inverse):
-        m = MasPcg(gate="euclid", precision=precision, inverse=inverse, tolerance=1e-4)
+    def make(precision, inverse, gate="euclid"):
+        m = MasPcg(gate=gate, precision=precision, inverse=inverse, tolerance=1e-4)
         m.set_stream(stream.cuda_stream)
         m.set_graph(s.fem_count, s.node_offset, s.neighbor_start, s.neighbor_num, s.neighbor_list,
                     s.part_map_real, s.real_map_part)
@@ -214,6 +214,12 @@ def run_ours(args, world, rank, local):
         t_mixed, res_mixed = timed(mixed, step, args.steps)
     launches = mixed.info()["kernel_launches"] - launches0
     t_plain, res_plain = timed(plain, step, args.steps)
+    # the reference's own stopping rule (rz gate) in the reference precision
+    refp = make("reference", "fp32", gate="rz")
+    step(refp)
+    k_ref = max(1, min(args.steps, 3))
+    t_ref, res_ref = timed(refp, step, k_ref)
+    refp.close()
 
     # end to end through the C ABI with host (pinned) buffers
     vals_h = torch.from_numpy(s.vals).pin_memory().numpy()
@@ -233,10 +239,20 @@ def run_ours(args, world, rank, local):
 
     # roofline of the dominant kernel (SpMV + p.Ap) and the other stages
     info = mixed.info()
-    ms_spmv = mixed.time_stage(0, 20)
-    ms_prec = mixed.time_stage(1, 20)
-    ms_l0 = mixed.time_stage(2, 20)
-    ms_factor = mixed.time_stage(3, 3)
+    stage_errors = {}
+
+    def stage(k, reps):
+        try:
+            return mixed.time_stage(k, reps)
+        except Exception as exc:  # reported in the line, not fatal
+            stage_errors[k] = str(exc)
+            return None
+
+    ms_spmv = stage(0, 20)
+    ms_prec = stage(1, 20)
+    ms_l0 = stage(2, 20)
+    ms_factor = stage(3, 3)
+    ms_l0_variants = {"tma_staged_x2": stage(4, 20), "tma_staged_x1": stage(5, 20), "registers": stage(6, 20)}
     nbi, bf = info["internal_block_rows"], info["bcsr_blocks"]
     d0 = s.fem_count // 32 if s.fem_count % 32 == 0 else (s.fem_count + 31) // 32
     spmv_bytes = 40 * bf + 4 * (nbi + 1) + 8 * (3 * nbi)
@@ -249,7 +265,7 @@ def run_ours(args, world, rank, local):
             traffic = json.load(open(tfile)).get("dram_bytes_per_launch_full_workload")
         except Exception:
             traffic = None
-    ach = spmv_bytes / (ms_spmv * 1e-3) / 1e9
+    ach = spmv_bytes / (ms_spmv * 1e-3) / 1e9 if ms_spmv else None
 
     value = t_mixed / (world * args.steps)
     line = {
@@ -264,11 +280,19 @@ def run_ours(args, world, rank, local):
         "fp32_plain": {"ms_per_solve": t_plain / args.steps, "iterations": res_plain["iterations"],
                        "rel_res_true": res_plain["rel_res_true"], "status": res_plain["status_name"],
                        "speedup_mixed_vs_fp32": (t_plain / t_mixed) if t_mixed > 0 else None},
-        "stages_ms": {"spmv": ms_spmv, "precondition": ms_prec, "mas_level0": ms_l0, "domain_factor": ms_factor,
+        "solves_per_s": 1000.0 * world * args.steps / t_mixed if t_mixed > 0 else None,
+        "rz_gate_reference_precision": {"ms_per_solve": t_ref / k_ref, "iterations": res_ref["iterations"],
+                                        "rel_res_true": res_ref["rel_res_true"], "status": res_ref["status_name"],
+                                        "gate": "reference rz gate |r.z| <= 1e-4 r0.z0, FP64 PCG + FP32 MAS"},
+        "stages_ms": {"spmv": ms_spmv, "precondition": ms_prec, "mas_level0": ms_l0,
+                      "mas_level0_variants": ms_l0_variants, "domain_factor": ms_factor,
                       "solve_device_ms": res_mixed["solve_ms"]},
-        "roofline": {"kernel": "k_spmv_dot (BCSR SpMV + p.Ap, FP32)", "bound": "hbm", "achieved": ach, "peak": peak,
-                     "unit": "GB/s", "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes": spmv_bytes, "mas_level0_GBps": l0_bytes / (ms_l0 * 1e-3) / 1e9},
+        "stage_errors": stage_errors or None,
+        "roofline": {"kernel": "k_spmv (BCSR SpMV + p.Ap, FP32 32-block tiles)", "bound": "hbm", "achieved": ach,
+                     "peak": peak,
+                     "unit": "GB/s", "frac": ach / peak if ach else None, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes": spmv_bytes,
+                     "mas_level0_GBps": l0_bytes / (ms_l0 * 1e-3) / 1e9 if ms_l0 else None},
         "e2e": {"value": t_e2e / (world * args.steps), "unit": "ms",
                 "h2d_bytes_per_step": int(80 * len(s.rows) + 24 * s.nb), "d2h_bytes_per_step": int(24 * s.nb)},
         "gpu_launches": int(launches),

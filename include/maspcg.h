@@ -225,15 +225,32 @@ MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out
 MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* out);
 
 /* Benchmark introspection (no counterpart in the reference): run one stage
- * `repeats` times between two CUDA events on the handle's stream and return
- * the mean device milliseconds per run.  Stages:
+ * `repeats` times on the handle's stream, each run after reading a 256 MB
+ * buffer that evicts L2 (clean lines only) and between its own two CUDA
+ * events, and return the mean device milliseconds per run (allocates the
+ * buffer on first use).  Stages:
  *   0  PCG SpMV with the p.Ap reduction, working precision
  *   1  full preconditioner apply z = M^-1 r, working precision
  *   2  MAS level-0 domain apply alone (restriction/coarse levels excluded)
  *   3  MAS domain assembly + inversion (build)
- *   4  PCG SpMV without the TMA staging (direct loads), for comparison
+ *   4  MAS level-0 domain apply, 16-bit inverses staged in shared memory by
+ *      TMA bulk copies, two slots per warp
+ *   5  the same with one slot per warp (more warps per SM)
+ *   6  the same apply with the inverse loaded into registers (no staging)
+ *   (stage 2 times the variant the solve uses; 4-6 exist to compare them)
  * Vector contents are left unspecified afterwards. */
 MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);
+
+/* Matrix adjoint of the solve (no counterpart in the reference; the backward
+ * of the differentiable Newton-step solve).  For L(x) with x = A^-1 b and
+ * lam = A^-1 dL/dx, writes dL/d(values) for every input block t of an upper
+ * BCOO list, (r, c) = (rows[t], cols[t]):
+ *   r != c:  grad9[t] = -(lam_r x_c^T + x_r lam_c^T)
+ *   r == c:  grad9[t] = -lam_r x_r^T
+ * column-major 3x3 like values9_colmajor.  lam and x: 3*block_rows doubles in
+ * the caller's order.  Host or device pointers. */
+MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n_blocks,
+                                              const double* lam, const double* x, double* grad9_colmajor);
 
 /* Most vectors one maspcg_residual_norms_noalloc call accepts. */
 #define MASPCG_RESIDUAL_MAX_VECTORS 8

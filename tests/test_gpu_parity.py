@@ -204,6 +204,23 @@ def test_lower_precision_forms_reach_tolerance(which, precision, inverse, reques
     assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) == pytest.approx(res["rel_res_true"], rel=1e-6)
 
 
+@pytest.mark.parametrize("inverse", ["bf16", "fp16"])
+def test_mixed_solve_with_several_domains_per_warp(inverse):
+    """A 40^3 contact system has 2,000 level-0 domains, more than one per warp
+    of the staged apply, so the per-warp copy slots are reused and the r.z
+    reduction spans more partial sums than at the smaller sizes above."""
+    s = synth.config_system(1, scale=40)
+    with MasPcg.from_system(s, gate="euclid", precision="reference") as m:
+        _, ref = m.solve(s.b)
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse=inverse) as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged", res
+    assert res["rel_res_true"] <= 1e-4
+    assert res["iterations"] <= 1.15 * ref["iterations"] + 16, (res["iterations"], ref["iterations"])
+    Ax = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
+    assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) <= 1e-4
+
+
 def test_block_jacobi_matches_oracle(cfg0):
     s = cfg0
     xo, ro, _ = oracle.solve_system(s, precond=oracle.PRECOND_DIAG3, gate=oracle.GATE_EUCLID)
