@@ -32,6 +32,10 @@ PREC_MIXED = 2
 GATE_RZ = 0
 GATE_EUCLID = 1
 
+FLAG_PDL = 1
+FLAG_APPLY_STAGED2 = 2
+FLAG_APPLY_REGISTERS = 4
+
 INV_FP32 = 0
 INV_BF16 = 1
 INV_FP16 = 2
@@ -55,7 +59,7 @@ class Config(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("max_iter_ratio", ctypes.c_double), ("max_iterations", ctypes.c_int),
                 ("gate", ctypes.c_int), ("precision", ctypes.c_int), ("inverse_storage", ctypes.c_int),
                 ("preconditioner", ctypes.c_int), ("refinement_period", ctypes.c_int), ("bank_size", ctypes.c_int),
-                ("iterations_per_launch", ctypes.c_int)]
+                ("iterations_per_launch", ctypes.c_int), ("flags", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):

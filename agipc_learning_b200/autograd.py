@@ -1,0 +1,97 @@
+"""The Newton-step solve as a differentiable PyTorch operation.
+
+`newton_solve(vals, b, solver, rows, cols, nb)` returns x = A^-1 b for the
+block-sparse A given by upper BCOO blocks (`vals`: [n, 9] FP64, Eigen
+column-major; repeated (row, col) entries add), through the C ABI of
+libmaspcg.  Its backward:
+
+  lam     = A^-1 dL/dx           (adjoint solve: A is symmetric, so the same
+                                  operator and preconditioner are reused)
+  dL/db   = lam
+  dL/dval = maspcg_bcoo_gradient(lam, x): -(lam_r x_c^T + x_r lam_c^T) per
+            off-diagonal block, -lam_r x_r^T per diagonal block
+
+x is kept from the forward pass (no Krylov history is stored).  The chain to
+per-tet Young's modulus uses the fact that a tet's Hessian blocks scale with
+its modulus (stable Neo-Hookean with the Lame pair linear in E, and the PSD
+projection commutes with a positive scale): dL/dE_t = sum over the tet's
+element blocks k of <dL/dval_k, val_k> / E_t.
+
+Torch is plumbing here: device memory and the autograd graph.  All
+arithmetic runs in the library's kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from .solver import MasPcg
+
+
+def _ptr(t: torch.Tensor):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class NewtonSolveFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, vals, b, solver: MasPcg, rows, cols, nb: int, fem_offset: int = 0, abd_bodies: int = 0):
+        for t, dt in ((vals, torch.float64), (b, torch.float64), (rows, torch.int32), (cols, torch.int32)):
+            if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
+                raise ValueError("vals/b must be contiguous CUDA float64, rows/cols contiguous CUDA int32")
+        solver.set_matrix(vals, rows, cols, nb, fem_offset, abd_bodies)
+        solver.build()
+        x = torch.empty_like(b)
+        _, res = solver.solve(b, x)
+        if res["status_name"] != "converged":
+            raise RuntimeError(f"forward solve did not converge: {res}")
+        ctx.solver = solver
+        ctx.version = solver.matrix_version
+        ctx.dims = (nb, fem_offset, abd_bodies)
+        ctx.save_for_backward(vals, rows, cols, x)
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        vals, rows, cols, x = ctx.saved_tensors
+        solver = ctx.solver
+        if solver.matrix_version != ctx.version:  # the handle was reused: restore this system
+            solver.set_matrix(vals, rows, cols, *ctx.dims)
+            solver.build()
+        gx = gx.contiguous().to(torch.float64)
+        lam = torch.empty_like(gx)
+        _, res = solver.solve(gx, lam)
+        if res["status_name"] != "converged":
+            raise RuntimeError(f"adjoint solve did not converge: {res}")
+        gvals = torch.empty_like(vals)
+        solver.bcoo_gradient(rows, cols, lam, x, gvals)
+        return gvals, lam, None, None, None, None, None, None
+
+
+def newton_solve(vals: torch.Tensor, b: torch.Tensor, solver: MasPcg, rows: torch.Tensor, cols: torch.Tensor,
+                 nb: int, fem_offset: int = 0, abd_bodies: int = 0) -> torch.Tensor:
+    """x = A^-1 b, differentiable in `vals` and `b` (see the module docstring)."""
+    return NewtonSolveFunction.apply(vals, b, solver, rows, cols, nb, fem_offset, abd_bodies)
+
+
+def modulus_gradient(grad_vals: torch.Tensor, vals: torch.Tensor, E_tet: torch.Tensor,
+                     blocks_per_tet: int = 10) -> torch.Tensor:
+    """dL/dE per tet from dL/d(vals) of the raw triplets whose first
+    blocks_per_tet * ntet entries are the element blocks in tet order."""
+    ntet = E_tet.shape[0]
+    k = blocks_per_tet * ntet
+    s = (grad_vals[:k] * vals[:k]).sum(dim=1).view(ntet, blocks_per_tet).sum(dim=1)
+    return s / E_tet
+
+
+def scale_element_blocks(vals: torch.Tensor, factor: torch.Tensor, blocks_per_tet: int = 10) -> torch.Tensor:
+    """Triplet values after scaling each tet's modulus by `factor` (per tet)."""
+    out = vals.clone()
+    ntet = factor.shape[0]
+    k = blocks_per_tet * ntet
+    out[:k] *= factor.repeat_interleave(blocks_per_tet).unsqueeze(1)
+    return out
+
+
+__all__ = ["NewtonSolveFunction", "newton_solve", "modulus_gradient", "scale_element_blocks", "np"]

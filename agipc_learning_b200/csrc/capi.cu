@@ -139,6 +139,7 @@ MASPCG_API void maspcg_config_default(maspcg_config* c)
   c->refinement_period = 16;
   c->bank_size = 32;
   c->iterations_per_launch = 8;
+  c->flags = 0;
 }
 
 MASPCG_API const char* maspcg_status_string(int s)
@@ -181,7 +182,8 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_NONE) ||
-      c.max_iterations < 0 || !(c.max_iter_ratio >= 0)) {
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~7) != 0 ||
+      ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_REGISTERS))) {
     g_create_error = "invalid configuration";
     return MASPCG_ERR_INVALID_ARGUMENT;
   }
@@ -206,6 +208,8 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     MCK(cudaMallocHost(reinterpret_cast<void**>(&h->h_scal), sizeof(maspcg::PcgScalars)));
     h->scal.resize(1);
     h->grid_stream = 4 * h->sm_count;
+    h->use_pdl = (c.flags & MASPCG_FLAG_PDL) != 0;
+    h->apply_variant = (c.flags & MASPCG_FLAG_APPLY_STAGED2) ? 1 : (c.flags & MASPCG_FLAG_APPLY_REGISTERS) ? 0 : 2;
     h->failed.resize(8);
     MCK(cudaMemset(h->failed.get(), 0, 8 * sizeof(int)));
   } catch (const std::exception& e) {

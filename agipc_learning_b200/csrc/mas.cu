@@ -542,18 +542,34 @@ __device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const f
   }
 }
 
-// Leader of each key group gets the group sum in ascending lane order.
+// Leader of each key group gets the group sum: with kFast a butterfly when
+// the whole warp is one group (the common case at level 0: one coarse node
+// per bank), else the group's lanes in ascending order.  Both orders are
+// fixed.  (The walk over coarse levels uses the general form only: ptxas
+// fails to allocate registers for the butterfly inside that loop.)
+template <bool kFast>
 __device__ __forceinline__ void group_sum(int key, const float v[3], float out[3], bool& leader)
 {
   const unsigned grp = __match_any_sync(kFull, key);
-  float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-  for (int src = 0; src < 32; ++src) {
-    const float a0 = __shfl_sync(kFull, v[0], src), a1 = __shfl_sync(kFull, v[1], src),
-                a2 = __shfl_sync(kFull, v[2], src);
-    if ((grp >> src) & 1u) {
-      s0 += a0;
-      s1 += a1;
-      s2 += a2;
+  float s0, s1, s2;
+  if (kFast && grp == kFull) {  // warp-uniform
+    s0 = v[0], s1 = v[1], s2 = v[2];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(kFull, s0, o);
+      s1 += __shfl_xor_sync(kFull, s1, o);
+      s2 += __shfl_xor_sync(kFull, s2, o);
+    }
+  } else {
+    s0 = s1 = s2 = 0.f;
+    for (int src = 0; src < 32; ++src) {
+      const float a0 = __shfl_sync(kFull, v[0], src), a1 = __shfl_sync(kFull, v[1], src),
+                  a2 = __shfl_sync(kFull, v[2], src);
+      if ((grp >> src) & 1u) {
+        s0 += a0;
+        s1 += a1;
+        s2 += a2;
+      }
     }
   }
   out[0] = s0;
@@ -613,6 +629,12 @@ constexpr int kApplyTpb = 128;
 // nothing waits.  Counters return to zero as they complete.
 constexpr int kChainWarps = 8;
 constexpr int kChainQueue = 64;
+constexpr int kChainApplySlots = 4;  // 16-bit domain records staged in shared memory at a time
+
+// Dynamic shared memory of k_coarse_chain: 16-bit records are staged (their
+// two passes then read shared memory), FP32 records are read from global.
+template <typename TI>
+constexpr int chain_smem_bytes() { return sizeof(TI) == 2 ? kChainApplySlots * kInvElems16 * 2 : 0; }
 
 // One thread counts a finished unit, whose parents span global slots
 // [lo, hi], into the parent domains; domains it completes are appended to
@@ -649,7 +671,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
 {
   __shared__ int queue[kChainQueue];
   __shared__ int tail_s, lo_s, hi_s;
-  pdl_enter();
+  pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -667,7 +689,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
     const float v[3] = {(float)rp[0], (float)rp[1], (float)rp[2]};
     float o[3];
     bool leader;
-    group_sum(key >= 0 ? key : -1 - lane, v, o, leader);
+    group_sum<true>(key >= 0 ? key : -1 - lane, v, o, leader);
     if (leader && key >= 0) {
       float* d = a.coarse_r + 3 * (size_t)key;
       d[0] = o[0];
@@ -682,6 +704,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
       atomicMax(&hi_s, a.c0 + hi);
     }
   }
+  pdl_trigger();
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0 && hi_s >= 0) {
@@ -714,7 +737,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
       }
       float o[3];
       bool leader;
-      group_sum(key, v, o, leader);
+      group_sum<false>(key, v, o, leader);
       if (leader && valid) {
         float* d = a.coarse_r + 3 * (size_t)(key - a.c0);
         d[0] = o[0];
@@ -729,18 +752,34 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
     if (lane == 0) tail_s = t;
   }
   __syncthreads();
-  // all warps: apply the completed domains' inverses
+  // apply the completed domains' inverses: 16-bit records are copied into a
+  // shared-memory slot per warp with 77 coalesced loads per lane, so the
+  // per-diagonal reads of both passes hit shared memory
+  extern __shared__ __align__(16) uint32_t chain_slots[];
   const int n = tail_s;
-  for (int i = w; i < n; i += kChainWarps) {
-    const int g = queue[i];
-    const size_t base = (size_t)(kBank * g + lane - a.c0) * 3;
-    const float x[3] = {__ldcg(a.coarse_r + base), __ldcg(a.coarse_r + base + 1), __ldcg(a.coarse_r + base + 2)};
-    float y[3];
-    domain_apply<TI, true>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>(),
-                           a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
-    a.coarse_z[base] = y[0];
-    a.coarse_z[base + 1] = y[1];
-    a.coarse_z[base + 2] = y[2];
+  constexpr bool kStage = sizeof(TI) == 2;
+  constexpr int kSlots = kStage ? kChainApplySlots : kChainWarps;
+  if (w < kSlots) {
+    for (int i = w; i < n; i += kSlots) {
+      const int g = queue[i];
+      const size_t base = (size_t)(kBank * g + lane - a.c0) * 3;
+      const float x[3] = {__ldcg(a.coarse_r + base), __ldcg(a.coarse_r + base + 1), __ldcg(a.coarse_r + base + 2)};
+      float y[3];
+      const TI* rec = reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>();
+      if constexpr (kStage) {
+        uint32_t* slot = chain_slots + (size_t)w * kInvWords16 * kBank;
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(rec);
+        __syncwarp();
+#pragma unroll 11
+        for (int k = 0; k < kInvWords16; ++k) slot[k * kBank + lane] = __ldcs(src + k * kBank + lane);
+        __syncwarp();
+        rec = reinterpret_cast<const TI*>(slot);
+      }
+      domain_apply<TI, true>(rec, a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
+      a.coarse_z[base] = y[0];
+      a.coarse_z[base + 1] = y[1];
+      a.coarse_z[base + 2] = y[2];
+    }
   }
 }
 
@@ -789,7 +828,7 @@ template <typename TI, typename Tv, typename Tacc>
 __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
                                                       int part_base, int total_parts, int mode, PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   const int lane = threadIdx.x & 31;
   const int warps_total = gridDim.x * (blockDim.x >> 5);
@@ -815,6 +854,7 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
     z[row3 + 2] = (Tv)y[2];
     dot += (Tacc)r0 * (Tacc)(Tv)y[0] + (Tacc)r1 * (Tacc)(Tv)y[1] + (Tacc)r2 * (Tacc)(Tv)y[2];
   }
+  pdl_trigger();
   if (partial) {
     Tacc total = 0;
     if (grid_finish<Tacc, kApplyTpb>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
@@ -842,7 +882,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kApplyWarps][kBuf];
-  pdl_enter();
+  pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   constexpr unsigned kBytes = inv_elems<TI>() * sizeof(TI);
   const int lw = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -923,6 +963,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
       a.coarse_z[base + 2] = y[2];
     }
   }
+  pdl_trigger();
   if (!ok && lane == 0) {
     // drain this warp's copies still in flight (bounded), report
     atomicExch(err, 1);
@@ -1169,9 +1210,16 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
   const int variant = std::is_same<TI, float>::value ? (int)kApplyRegisters : h->apply_variant;
-  if (lv.levelnum > 1)
-    launch_pdl(h, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainWarps)), dim3(kChainWarps * 32), 0, a,
-               r, s);
+  if (lv.levelnum > 1) {
+    constexpr int bytes = chain_smem_bytes<TI>();
+    static bool configured = false;
+    if (!configured && bytes > 48 * 1024) {
+      MCK(cudaFuncSetAttribute(k_coarse_chain<TI, Tv>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    }
+    configured = true;
+    launch_pdl(h, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainWarps)), dim3(kChainWarps * 32), bytes,
+               a, r, s);
+  }
   level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0);
 }
 }  // namespace

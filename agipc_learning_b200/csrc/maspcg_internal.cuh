@@ -227,8 +227,8 @@ struct maspcg_handle {
   int grid_stream = 0;  // CTAs for grid-stride kernels
   long long kernel_launches = 0;  // this library's kernels launched on the handle
   long long graph_kernels = 0;    // kernel nodes of the captured batch graph
-  bool use_pdl = true;            // programmatic dependent launch for the iteration kernels
-  int apply_variant = 1;          // 16-bit level-0 apply: 0 registers, 1 TMA-staged x2 buffers, 2 TMA-staged x1
+  bool use_pdl = false;           // programmatic dependent launch for the iteration kernels (MASPCG_FLAG_PDL)
+  int apply_variant = 2;          // 16-bit level-0 apply: 0 registers, 1 TMA-staged x2 buffers, 2 TMA-staged x1
 };
 
 namespace maspcg {
@@ -292,15 +292,14 @@ __device__ __forceinline__ T block_sum(T v, T* smem /* NT/32 */)
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// Programmatic dependent launch: an iteration kernel lets its successor be
-// scheduled at once and then waits for its predecessor's completion (and
-// memory) before touching anything it produced.  Without the launch
-// attribute both instructions are no-ops.
-__device__ __forceinline__ void pdl_enter()
-{
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-}
+// Programmatic dependent launch.  An iteration kernel waits at entry for its
+// predecessor's completion (and memory) before touching anything it
+// produced, and lets its successor be scheduled once its own main loop is
+// done, so the successor's launch overlaps this kernel's tail (the last-block
+// reduction) without its CTAs taking SM resources from the main loop.
+// Without the launch attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <typename... KArgs, typename... Args>
 void launch_pdl(maspcg_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args)

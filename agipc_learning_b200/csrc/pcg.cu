@@ -91,66 +91,40 @@ __device__ __forceinline__ void st_p4(double* p4, int v, double x, double y, dou
   reinterpret_cast<double2*>(p4)[2 * v + 1] = make_double2(z, 0.0);
 }
 
-// Four consecutive block rows (12 values) of a 3-per-row vector as 16-byte
-// vector loads/stores; `v0` is a multiple of 4.
+// Entries [4q, 4q + 4) of a vector as 16-byte (FP32) / 2 x 16-byte (FP64)
+// accesses.
 template <typename T>
-__device__ __forceinline__ void ld12(const T* p, int v0, T o[12])
+__device__ __forceinline__ void ld4(const T* p, int q, T o[4])
 {
   if constexpr (sizeof(T) == 4) {
-    const float4* q = reinterpret_cast<const float4*>(p + 3 * (size_t)v0);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float4 w = q[k];
-      o[4 * k] = w.x, o[4 * k + 1] = w.y, o[4 * k + 2] = w.z, o[4 * k + 3] = w.w;
-    }
+    const float4 w = reinterpret_cast<const float4*>(p)[q];
+    o[0] = w.x, o[1] = w.y, o[2] = w.z, o[3] = w.w;
   } else {
-    const double2* q = reinterpret_cast<const double2*>(p + 3 * (size_t)v0);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const double2 w = q[k];
-      o[2 * k] = w.x, o[2 * k + 1] = w.y;
-    }
+    const double2 a = reinterpret_cast<const double2*>(p)[2 * q], b = reinterpret_cast<const double2*>(p)[2 * q + 1];
+    o[0] = a.x, o[1] = a.y, o[2] = b.x, o[3] = b.y;
   }
 }
 template <typename T>
-__device__ __forceinline__ void st12(T* p, int v0, const T o[12])
+__device__ __forceinline__ void st4(T* p, int q, const T o[4])
 {
   if constexpr (sizeof(T) == 4) {
-    float4* q = reinterpret_cast<float4*>(p + 3 * (size_t)v0);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) q[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+    reinterpret_cast<float4*>(p)[q] = make_float4(o[0], o[1], o[2], o[3]);
   } else {
-    double2* q = reinterpret_cast<double2*>(p + 3 * (size_t)v0);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) q[k] = make_double2(o[2 * k], o[2 * k + 1]);
+    reinterpret_cast<double2*>(p)[2 * q] = make_double2(o[0], o[1]);
+    reinterpret_cast<double2*>(p)[2 * q + 1] = make_double2(o[2], o[3]);
   }
 }
 
-// p = z (k == 1) or z + beta p, written into the padded layout.  Each thread
-// takes four block rows with 16-byte accesses (a scalar tail for the rest).
+// p = z (k == 1) or z + beta p, written into the padded layout; one block
+// row per thread (many threads in flight: the kernel is latency-bound).
 template <typename Tv>
 __global__ void __launch_bounds__(kTpb) k_update_p(const Tv* __restrict__ z, Tv* p4, int nrows, const PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (!running(s)) return;
   const bool first = s->k == 1;
   const Tv beta = (Tv)s->beta;
-  const int quads = nrows >> 2;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x) {
-    Tv zz[12];
-    ld12(z, 4 * q, zz);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int v = 4 * q + j;
-      if (first) {
-        st_p4(p4, v, zz[3 * j], zz[3 * j + 1], zz[3 * j + 2]);
-      } else {
-        const P4<Tv> o = ld_p4(p4, v);
-        st_p4(p4, v, zz[3 * j] + beta * o.x, zz[3 * j + 1] + beta * o.y, zz[3 * j + 2] + beta * o.z);
-      }
-    }
-  }
-  for (int v = 4 * quads + blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
     const Tv z0 = z[3 * (size_t)v], z1 = z[3 * (size_t)v + 1], z2 = z[3 * (size_t)v + 2];
     if (first) {
       st_p4(p4, v, z0, z1, z2);
@@ -186,7 +160,7 @@ __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, c
                                                 const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap,
                                                 int nrows, Tacc* partial, PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (!running(s)) return;
   using A = typename AccOf<Tm>::type;
   constexpr int kRows = kTpb / LPR;
@@ -237,6 +211,7 @@ __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, c
     rs = nrs;
     re = nre;
   }
+  pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0) {
@@ -256,48 +231,45 @@ __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, c
 
 // x += alpha p, r -= alpha Ap, r.r; last block: stopping gate.
 // MIXED: x is the FP32 correction since the last replacement and a met gate
-// asks for the FP64 true residual instead of stopping.  Four block rows per
-// thread with 16-byte accesses (a scalar tail for the rest).
+// asks for the FP64 true residual instead of stopping.  Each thread takes
+// four consecutive entries of x, r and Ap (16-byte accesses) and gathers the
+// matching entries of the padded p; a scalar tail covers n % 4.
 template <typename Tv, typename Tacc>
 __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p4, const Tv* __restrict__ ap,
                                                      int nrows, int mixed, Tacc* partial, PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (!running(s)) return;
   const Tv alpha = (Tv)s->alpha;
   Tacc acc = 0;
-  const int quads = nrows >> 2;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x) {
-    Tv xx[12], rr[12], ww[12], pp[12];
-    ld12(x, 4 * q, xx);
-    ld12(r, 4 * q, rr);
-    ld12(ap, 4 * q, ww);
+  const int n = 3 * nrows, n4 = n >> 2;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += gridDim.x * blockDim.x) {
+    Tv xx[4], rr[4], ww[4], pp[4];
+    ld4(x, q, xx);
+    ld4(r, q, rr);
+    ld4(ap, q, ww);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const P4<Tv> o = ld_p4(p4, 4 * q + j);
-      pp[3 * j] = o.x, pp[3 * j + 1] = o.y, pp[3 * j + 2] = o.z;
+    for (int k = 0; k < 4; ++k) {
+      const int j = 4 * q + k;
+      pp[k] = p4[4 * (j / 3) + j % 3];
     }
 #pragma unroll
-    for (int k = 0; k < 12; ++k) {
+    for (int k = 0; k < 4; ++k) {
       xx[k] = xx[k] + alpha * pp[k];
       rr[k] = rr[k] - alpha * ww[k];
       acc += (Tacc)rr[k] * (Tacc)rr[k];
     }
-    st12(x, 4 * q, xx);
-    st12(r, 4 * q, rr);
+    st4(x, q, xx);
+    st4(r, q, rr);
   }
-  for (int v = 4 * quads + blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
-    const size_t i = 3 * (size_t)v;
-    const P4<Tv> o = ld_p4(p4, v);
-    const Tv pv[3] = {o.x, o.y, o.z};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      x[i + k] = x[i + k] + alpha * pv[k];
-      const Tv rn = r[i + k] - alpha * ap[i + k];
-      r[i + k] = rn;
-      acc += (Tacc)rn * (Tacc)rn;
-    }
+  for (int j = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const Tv pv = p4[4 * (j / 3) + j % 3];
+    x[j] = x[j] + alpha * pv;
+    const Tv rn = r[j] - alpha * ap[j];
+    r[j] = rn;
+    acc += (Tacc)rn * (Tacc)rn;
   }
+  pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
       threadIdx.x == 0) {
@@ -323,7 +295,7 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
 // MIXED: fold the FP32 correction into the FP64 iterate.
 __global__ void __launch_bounds__(kTpb) k_fold_x(double* xhi, float* xlo, int n, int force, const PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (!force && !(s->status == MASPCG_SOLVE_RUNNING || s->status == kNeedTrue)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     xhi[i] += (double)xlo[i];
@@ -339,7 +311,7 @@ __global__ void __launch_bounds__(kTpb) k_true_residual(const int* __restrict__ 
                                                          const double* __restrict__ b, float* r32, int nrows,
                                                          double* partial, PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (!(s->status == MASPCG_SOLVE_RUNNING || s->status == kNeedTrue)) return;
   const int groups_per_block = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
@@ -357,6 +329,7 @@ __global__ void __launch_bounds__(kTpb) k_true_residual(const int* __restrict__ 
       acc2 += v * v;
     }
   }
+  pdl_trigger();
   double total = 0.0;
   if (grid_finish<double>(acc2, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketTrue], gridDim.x, total) &&
       threadIdx.x == 0) {
@@ -384,7 +357,7 @@ __global__ void __launch_bounds__(kTpb) k_other_apply(const Tv* __restrict__ r, 
                                                        const Tinv* __restrict__ diag_inv, Tacc* partial, int part_base,
                                                        int total_parts, int finalize, int mode, PcgScalars* s)
 {
-  pdl_enter();
+  pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
   Tacc dot = 0;
   const int stride = gridDim.x * blockDim.x;
@@ -427,6 +400,7 @@ __global__ void __launch_bounds__(kTpb) k_other_apply(const Tv* __restrict__ r, 
     if (threadIdx.x == 0) partial[part_base + blockIdx.x] = bsum;
     return;
   }
+  pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x, total) &&
       threadIdx.x == 0 && mode > 0)
@@ -490,7 +464,7 @@ struct Engine {
     mixed = h->cfg.precision == MASPCG_PREC_MIXED;
     gstream = h->grid_stream;
     gspmv = std::max(1, std::min(ceil_div(h->nb_int, kTpb / 16), 4 * h->sm_count));
-    grows = std::max(1, std::min(ceil_div(std::max(h->nb_int / 4, 1), kTpb), 8 * h->sm_count));
+    grows = std::max(1, std::min(ceil_div(h->nb_int, kTpb), 8 * h->sm_count));
     gl0 = mas ? mas_level0_grid(h) : 0;
     const bool other = !mas || h->abd_bodies > 0 || h->fem_off > 0 || h->nb_int > h->fem_off + h->c0;
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;

@@ -58,7 +58,7 @@ class MasPcg:
     """One linear system on one GPU: graph -> contacts -> matrix -> build -> solve."""
 
     def __init__(self, *, tolerance=1e-4, max_iter_ratio=0.3, max_iterations=0, gate="rz", precision="reference",
-                 inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8):
+                 inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8, flags=0):
         lib = N.load()
         cfg = N.Config()
         lib.maspcg_config_default(ctypes.byref(cfg))
@@ -71,6 +71,7 @@ class MasPcg:
         cfg.preconditioner = _PC[preconditioner]
         cfg.refinement_period = refinement_period
         cfg.iterations_per_launch = iterations_per_launch
+        cfg.flags = flags
         self.cfg = cfg
         h = ctypes.c_void_p()
         N.check(lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)), None)
@@ -124,6 +125,7 @@ class MasPcg:
         self._ck(self.lib.maspcg_set_matrix_bcoo(self.h, v.ptr, r.ptr, c.ptr, int(len(rows)), int(block_rows),
                                                  int(fem_offset), int(abd_bodies)))
         self.nb = int(block_rows)
+        self.matrix_version = getattr(self, "matrix_version", 0) + 1
 
     def build(self):
         self._ck(self.lib.maspcg_build_preconditioner(self.h))
@@ -166,6 +168,17 @@ class MasPcg:
         ya = _Arg(y, np.float64, writable=True)
         self._ck(self.lib.maspcg_spmv(self.h, float(a), xa.ptr, float(b), ya.ptr))
         return y
+
+    def bcoo_gradient(self, rows, cols, lam, x, out=None):
+        """dL/d(values) of upper BCOO blocks for lam = A^-1 dL/dx (maspcg_bcoo_gradient)."""
+        n = int(len(rows))
+        r, c = _Arg(rows, np.int32), _Arg(cols, np.int32)
+        la, xa = _Arg(lam, np.float64), _Arg(x, np.float64)
+        if out is None:
+            out = np.zeros((n, 9), np.float64)
+        oa = _Arg(out, np.float64, writable=True)
+        self._ck(self.lib.maspcg_bcoo_gradient(self.h, r.ptr, c.ptr, n, la.ptr, xa.ptr, oa.ptr))
+        return out
 
     def residual_norms_noalloc(self, x, b):
         """FP64 ||b_j - A x_j|| and ||b_j|| for the rows of two CUDA float64

@@ -177,8 +177,13 @@ def _fem_block(X, tets, x, E, nu, dt, rho, row_offset, E_tet=None):
 def cube_system(n: int, *, E: float = 1e5, nu: float = 0.45, rho: float = 1000.0, dt: float = 1 / 60,
                 h: float = 0.01, noise: float = 0.1, seed: int = SEED_BASE, pt_pairs: int = 0, ee_pairs: int = 0,
                 dhat: float = 1e-3, kappa: float = 1e7, E_tet=None, name: str | None = None,
-                nxyz: tuple[int, int, int] | None = None) -> System:
-    """FEM box (n^3 vertices unless nxyz is given) with optional IPC contacts."""
+                nxyz: tuple[int, int, int] | None = None, keep_raw: bool = False) -> System:
+    """FEM box (n^3 vertices unless nxyz is given) with optional IPC contacts.
+
+    keep_raw: also keep the unmerged triplets in meta["raw"] = (rows, cols,
+    vals), element blocks first (10 per tet, in tet order, each proportional
+    to the tet's Young's modulus), then the mass and contact blocks;
+    meta["elem_blocks"] is the element-block count."""
     lib = _lib()
     nx, ny, nz = nxyz if nxyz else (n, n, n)
     X, tets = box_mesh(nx, ny, nz, h)
@@ -210,15 +215,19 @@ def cube_system(n: int, *, E: float = 1e5, nu: float = 0.45, rho: float = 1000.0
             k = lib.syn_contacts_ee(nx, ny, nz, h, _p(X), ne, _p(edges), ee_pairs, dhat, kappa * dt * dt, seed + 202, 0, 0,
                                     _p(p4), _p(r), _p(c), _p(v))
             pairs.append(p4[:k]); R.append(r[:10 * k]); C.append(c[:10 * k]); V.append(v[:10 * k])
-    rows, cols, vals = assemble(np.concatenate(R), np.concatenate(C), np.concatenate(V))
+    raw = (np.concatenate(R), np.concatenate(C), np.concatenate(V))
+    rows, cols, vals = assemble(*raw)
     start, num, lst = vertex_neighbors(nv, tets)
     pmr, rmp = morton_partition(X)
     b = normal_rhs(3 * nv, seed + 7, fp32=True)
+    meta = {"projected_tets": projected, "E": E, "nu": nu, "dt": dt, "rho": rho, "h": h}
+    if keep_raw:
+        meta["raw"] = raw
+        meta["elem_blocks"] = 10 * len(tets)
     return System(name=name or f"cube{n}", nb=nv, rows=rows, cols=cols, vals=vals, b=b, fem_offset=0,
                   fem_count=nv, neighbor_start=start, neighbor_num=num, neighbor_list=lst, part_map_real=pmr,
                   real_map_part=rmp, pairs=np.concatenate(pairs) if pairs else np.zeros((0, 4), np.int32),
-                  node_offset=0, X=X, tets=tets, E_tet=None if E_tet is None else np.asarray(E_tet),
-                  meta={"projected_tets": projected, "E": E, "nu": nu, "dt": dt, "rho": rho, "h": h})
+                  node_offset=0, X=X, tets=tets, E_tet=None if E_tet is None else np.asarray(E_tet), meta=meta)
 
 
 def hybrid_system(bodies: int = 2000, slab=(100, 100, 10), *, E: float = 1e8, nu: float = 0.3, rho: float = 1000.0,
@@ -295,7 +304,7 @@ def config_system(cid: int, scale: int | None = None) -> System:
         n = scale or 32
         ntet = 6 * (n - 1) ** 3
         E_tet = log_uniform_E(ntet, 1e4, 1e6, seed + 5)
-        return cube_system(n, E=1e5, nu=0.45, seed=seed, E_tet=E_tet, name="cfg3")
+        return cube_system(n, E=1e5, nu=0.45, seed=seed, E_tet=E_tet, name="cfg3", keep_raw=True)
     if cid == 4:
         n = scale or 128
         npairs = 400000 if n == 128 else max(2, int(400000 * (n / 128) ** 2))

@@ -108,6 +108,22 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(ms: float, dist=None, device=None) -> float:
+    """The slowest rank's time: every rank takes part in one MAX all-reduce."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_ms_per_solve(max_ms: float, world: int, steps: int) -> float:
+    """Whole-job ms per solve of N replicas that each ran `steps` solves in
+    `max_ms` (slowest rank): the job finishes world * steps solves."""
+    return max_ms / (world * steps)
+
+
 def oracle_solve_ms(s, max_iter=0):
     """Reference algorithm on the host cores: MAS32 build + FP64 PCG."""
     import oracle
@@ -199,10 +215,7 @@ def run_ours(args, world, rank, local):
             res = fn(m)
         e1.record(stream)
         torch.cuda.synchronize()
-        t = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-        if dist:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), res
+        return max_over_ranks(e0.elapsed_time(e1), dist, dev), res
 
     mixed = make("mixed", "bf16")
     plain = make("fp32", "fp32")
@@ -267,7 +280,7 @@ def run_ours(args, world, rank, local):
             traffic = None
     ach = spmv_bytes / (ms_spmv * 1e-3) / 1e9 if ms_spmv else None
 
-    value = t_mixed / (world * args.steps)
+    value = job_ms_per_solve(t_mixed, world, args.steps)
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_mixed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -293,7 +306,7 @@ def run_ours(args, world, rank, local):
                      "unit": "GB/s", "frac": ach / peak if ach else None, "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes": spmv_bytes,
                      "mas_level0_GBps": l0_bytes / (ms_l0 * 1e-3) / 1e9 if ms_l0 else None},
-        "e2e": {"value": t_e2e / (world * args.steps), "unit": "ms",
+        "e2e": {"value": job_ms_per_solve(t_e2e, world, args.steps), "unit": "ms",
                 "h2d_bytes_per_step": int(80 * len(s.rows) + 24 * s.nb), "d2h_bytes_per_step": int(24 * s.nb)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

@@ -88,7 +88,16 @@ typedef struct {
   int refinement_period; /* MIXED: iterations between FP64 true residuals (default 16) */
   int bank_size;         /* MAS bank; 32 (GPU_MAS_BANKSIZE) is the only supported value */
   int iterations_per_launch; /* PCG iterations per CUDA-graph launch (default 8) */
+  int flags;             /* maspcg_flags: kernel-schedule choices, 0 = defaults */
 } maspcg_config;
+
+/* Kernel-schedule choices (bits of maspcg_config.flags); results do not depend
+ * on them beyond floating-point summation order. */
+typedef enum {
+  MASPCG_FLAG_PDL = 1,                 /* launch iteration kernels with programmatic dependent launch */
+  MASPCG_FLAG_APPLY_STAGED2 = 2,       /* 16-bit level-0 apply: two TMA slots per warp */
+  MASPCG_FLAG_APPLY_REGISTERS = 4      /* 16-bit level-0 apply: inverse held in registers */
+} maspcg_flags;
 
 typedef struct {
   int iterations;           /* PCGSolver::pcg return value semantics */
@@ -235,7 +244,7 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
  *   3  MAS domain assembly + inversion (build)
  *   4  MAS level-0 domain apply, 16-bit inverses staged in shared memory by
  *      TMA bulk copies, two slots per warp
- *   5  the same with one slot per warp (more warps per SM)
+ *   5  the same with one slot per warp (more warps per SM; the solve's choice)
  *   6  the same apply with the inverse loaded into registers (no staging)
  *   (stage 2 times the variant the solve uses; 4-6 exist to compare them)
  * Vector contents are left unspecified afterwards. */

@@ -139,6 +139,13 @@ def test_pcg_reference_precision_matches_oracle(cfg1_small, gate):
         x, res = m.solve(s.b)
     assert res["status_name"] == "converged"
     assert abs(res["iterations"] - ro["iterations"]) <= max(1, int(0.1 * ro["iterations"]))
+    if res["iterations"] != ro["iterations"]:
+        # The rz gate stops far from convergence (||r||/||b|| ~ 0.2 here), where
+        # a different FP32 summation order in the MAS apply can move the stop
+        # by an iteration: compare the iterate after the oracle's count.
+        with MasPcg.from_system(s, gate=gate, precision="reference", tolerance=1e-30,
+                                max_iterations=ro["iterations"] + 1) as m:  # the cap counts the initial apply
+            x, _ = m.solve(s.b)
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-4
     # the residual at the stopping iteration: same gate, same order of magnitude
     if gate == "euclid":
@@ -161,6 +168,18 @@ def test_kat257_through_abi():
     assert res["rel_res_true"] == pytest.approx(pub["true_relative_residual"], abs=5e-7)
     d = np.linalg.norm(x - k["ref"]) / np.linalg.norm(k["ref"])
     assert d == pytest.approx(pub["relative_direction_difference"], abs=5e-5)
+
+
+def test_coarse_snapshot_replay_through_the_package():
+    """frozen_io's replay of the reference's coarse snapshot format reproduces
+    the published MAS32 result of the 257-block KAT."""
+    import os
+    from agipc_learning_b200 import frozen_io
+    snap = frozen_io.read_coarse_snapshot(os.path.join(H.GOLDEN, "kat257"))
+    x, res = frozen_io.solve_coarse_snapshot(snap)
+    pub = H.load_kat257()[6]["mas32"]
+    assert res["iterations"] == pub["iterations"]
+    assert res["rel_res_true"] == pytest.approx(pub["true_relative_residual"], abs=5e-7)
 
 
 @pytest.mark.parametrize("inverse", ["bf16", "fp16"])
