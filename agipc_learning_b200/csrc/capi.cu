@@ -182,7 +182,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_NONE) ||
-      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~7) != 0 ||
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~15) != 0 ||
       ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_REGISTERS))) {
     g_create_error = "invalid configuration";
     return MASPCG_ERR_INVALID_ARGUMENT;
@@ -209,6 +209,10 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     h->scal.resize(1);
     h->grid_stream = 4 * h->sm_count;
     h->use_pdl = (c.flags & MASPCG_FLAG_PDL) != 0;
+    h->overlap_coarse = (c.flags & MASPCG_FLAG_SEQUENTIAL_COARSE) == 0;
+    MCK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+    MCK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    MCK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     h->apply_variant = (c.flags & MASPCG_FLAG_APPLY_STAGED2) ? 1 : (c.flags & MASPCG_FLAG_APPLY_REGISTERS) ? 0 : 2;
     h->failed.resize(8);
     MCK(cudaMemset(h->failed.get(), 0, 8 * sizeof(int)));
@@ -225,10 +229,14 @@ MASPCG_API maspcg_status maspcg_destroy(maspcg_handle* h)
 {
   if (!h) return MASPCG_ERR_NULL_HANDLE;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->side_stream) cudaStreamSynchronize(h->side_stream);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   if (h->h_scal) cudaFreeHost(h->h_scal);
+  if (h->side_stream) cudaStreamDestroy(h->side_stream);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return MASPCG_OK;

@@ -589,6 +589,7 @@ struct ApplyArgs {
   const float* scale;
   int* chain_count;             // per coarse domain: arrivals so far (zero between launches)
   const int* chain_target;      // per coarse domain: arrivals that complete it
+  double* chain_dot;            // per coarse domain: R.Z
   int* err;
   int fem_off, c0;
   LevelInfo lv;
@@ -665,9 +666,13 @@ __device__ __forceinline__ int domain_level(const LevelInfo& lv, int g)
   return l;
 }
 
+// pair: the level-0 apply runs concurrently and leaves the coarse correction
+// to the p update; this kernel then also sums r.z of the coarse levels,
+// sum over domains of R.Z (= r . P Z), and completes r.z with the level-0
+// part (rz_part_done, mode as in rz_update).
 template <typename TI, typename Tv>
 __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, const Tv* __restrict__ r,
-                                                                  const PcgScalars* s)
+                                                                  PcgScalars* s, int mode, int pair)
 {
   __shared__ int queue[kChainQueue];
   __shared__ int tail_s, lo_s, hi_s;
@@ -779,6 +784,28 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
       a.coarse_z[base] = y[0];
       a.coarse_z[base + 1] = y[1];
       a.coarse_z[base + 2] = y[2];
+      if (pair && s) {
+        // this domain's R.Z; the warp applying the last coarse domain adds
+        // them up in domain order and completes r.z
+        const int d1 = a.lv.dom_begin[1], nd = a.lv.domains - d1;
+        const double dz = warp_sum((double)x[0] * y[0] + (double)x[1] * y[1] + (double)x[2] * y[2]);
+        int last = 0;
+        if (lane == 0) {
+          a.chain_dot[g - d1] = dz;
+          __threadfence();
+          last = atomicAdd(&s->tickets[kTicketCoarse], 1u) == (unsigned)nd - 1u;
+        }
+        if (__shfl_sync(kFull, last, 0)) {
+          __threadfence();
+          double t = 0.0;
+          for (int q = lane; q < nd; q += 32) t += __ldcg(a.chain_dot + q);
+          t = warp_sum(t);
+          if (lane == 0) {
+            s->tickets[kTicketCoarse] = 0u;
+            rz_part_done(s, 1, t, mode);
+          }
+        }
+      }
     }
   }
 }
@@ -826,7 +853,8 @@ __global__ void k_chain_targets(ApplyArgs a, int* target)
 // updates the PCG scalars (rz0 / beta / k).
 template <typename TI, typename Tv, typename Tacc>
 __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
-                                                      int part_base, int total_parts, int mode, PcgScalars* s)
+                                                      int part_base, int total_parts, int mode, PcgScalars* s,
+                                                      int coarse_add, int pair)
 {
   pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
@@ -842,12 +870,13 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
     domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>(),
                      a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
     float cc[3];
-    if (coarse_correction(a, slot, cc)) {
+    const bool real = coarse_add ? coarse_correction(a, slot, cc) : a.pmr[slot] >= 0;
+    if (!real) {
+      y[0] = y[1] = y[2] = 0.f;
+    } else if (coarse_add) {
       y[0] += cc[0];
       y[1] += cc[1];
       y[2] += cc[2];
-    } else {
-      y[0] = y[1] = y[2] = 0.f;
     }
     z[row3] = (Tv)y[0];
     z[row3 + 1] = (Tv)y[1];
@@ -859,8 +888,12 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
     Tacc total = 0;
     if (grid_finish<Tacc, kApplyTpb>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
                           total) &&
-        threadIdx.x == 0 && mode > 0)
-      rz_update(s, (double)total, mode);
+        threadIdx.x == 0 && mode > 0) {
+      if (pair)
+        rz_part_done(s, 0, (double)total, mode);
+      else
+        rz_update(s, (double)total, mode);
+    }
   }
 }
 
@@ -878,7 +911,7 @@ constexpr int kApplyWarps = 4;
 template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf>
 __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
     k_apply_tma(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-                PcgScalars* s, int g_begin, int g_end, int* err)
+                PcgScalars* s, int g_begin, int g_end, int* err, int coarse_add, int pair)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kApplyWarps][kBuf];
@@ -944,12 +977,13 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
     if (kLevel0) {
       const int slot = kBank * g + lane;
       float cc[3];
-      if (coarse_correction(a, slot, cc)) {
+      const bool real = coarse_add ? coarse_correction(a, slot, cc) : a.pmr[slot] >= 0;
+      if (!real) {
+        y[0] = y[1] = y[2] = 0.f;
+      } else if (coarse_add) {
         y[0] += cc[0];
         y[1] += cc[1];
         y[2] += cc[2];
-      } else {
-        y[0] = y[1] = y[2] = 0.f;
       }
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
@@ -980,8 +1014,12 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
     Tacc total = 0;
     if (grid_finish<Tacc, kApplyWarps * 32>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz],
                                             gridDim.x, total) &&
-        threadIdx.x == 0 && mode > 0)
-      rz_update(s, (double)total, mode);
+        threadIdx.x == 0 && mode > 0) {
+      if (pair)
+        rz_part_done(s, 0, (double)total, mode);
+      else
+        rz_update(s, (double)total, mode);
+    }
   }
 }
 
@@ -1033,6 +1071,7 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   const int coarse_domains = lv.domains - lv.dom_begin[1];
   h->chain_count.resize((size_t)std::max(coarse_domains, 1));
   h->chain_target.resize((size_t)std::max(coarse_domains, 1));
+  h->chain_dot.resize((size_t)std::max(coarse_domains, 1));
   MCK(cudaMemsetAsync(h->chain_count.get(), 0, h->chain_count.bytes(), st));
   MCK(cudaMemsetAsync(h->chain_target.get(), 0, h->chain_target.bytes(), st));
   if (lv.levelnum > 1) {
@@ -1135,6 +1174,7 @@ ApplyArgs make_apply_args(maspcg_handle* h)
   a.pmr = h->pmr.get();
   a.chain_count = h->chain_count.get();
   a.chain_target = h->chain_target.get();
+  a.chain_dot = h->chain_dot.get();
   a.err = h->failed.get() + 4;
   a.inv = h->inv.get();
   a.scale = h->cfg.inverse_storage == MASPCG_INV_FP32 ? nullptr : h->inv_scale.get();
@@ -1149,7 +1189,8 @@ enum ApplyVariant { kApplyRegisters = 0, kApplyStaged2 = 1, kApplyStaged1 = 2 };
 
 template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf>
 void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, Tacc* partial, int part_base,
-                      int total_parts, int mode, PcgScalars* s, int g_begin, int g_end, int grid)
+                      int total_parts, int mode, PcgScalars* s, int g_begin, int g_end, int grid, int coarse_add,
+                      int pair)
 {
   constexpr int bytes = kApplyWarps * kBuf * inv_elems<TI>() * (int)sizeof(TI);
   static bool configured = false;
@@ -1159,7 +1200,7 @@ void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, 
     configured = true;
   }
   launch_pdl(h, k_apply_tma<TI, Tv, Tacc, kLevel0, kBuf>, dim3(grid), dim3(kApplyWarps * 32), bytes, a, r, z, partial,
-             part_base, total_parts, mode, s, g_begin, g_end, h->failed.get() + 4);
+             part_base, total_parts, mode, s, g_begin, g_end, h->failed.get() + 4, coarse_add, pair);
 }
 
 // CTAs of a staged apply over `domains` domains: one wave of resident CTAs.
@@ -1181,62 +1222,125 @@ inline int level0_grid(const maspcg_handle* h, int variant)
   }
 }
 
-// Level-0 apply (with the coarse correction and r.z) in the given variant.
+// Level-0 apply (with r.z) in the given variant; coarse_add: z includes the
+// coarse correction (else the p update adds it); pair: r.z is completed
+// together with the concurrently running coarse levels.
 template <typename TI, typename Tv, typename Tacc>
 void level0_apply(maspcg_handle* h, const ApplyArgs& a, int variant, const Tv* r, Tv* z, Tacc* partial, int part_base,
-                  int total_parts, int mode, PcgScalars* s, int grid0)
+                  int total_parts, int mode, PcgScalars* s, int grid0, int coarse_add = 1, int pair = 0)
 {
   const int d0 = h->lv.dom_begin[1];
   if (std::is_same<TI, float>::value) variant = kApplyRegisters;
   // grid0 == level0_grid(h, variant): every CTA owns one r.z slot
   switch (variant) {
     case kApplyStaged2:
-      launch_apply_tma<TI, Tv, Tacc, true, 2>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0);
+      launch_apply_tma<TI, Tv, Tacc, true, 2>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
+                                              coarse_add, pair);
       break;
     case kApplyStaged1:
-      launch_apply_tma<TI, Tv, Tacc, true, 1>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0);
+      launch_apply_tma<TI, Tv, Tacc, true, 1>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
+                                              coarse_add, pair);
       break;
     default:
       launch_pdl(h, k_level0_apply<TI, Tv, Tacc>, dim3(grid0), dim3(kApplyTpb), 0, a, r, z, partial, part_base,
-                 total_parts, mode, s);
+                 total_parts, mode, s, coarse_add, pair);
       break;
   }
 }
 
+template <typename TI, typename Tv>
+void launch_chain(maspcg_handle* h, cudaStream_t st, const ApplyArgs& a, const Tv* r, PcgScalars* s, int mode, int pair)
+{
+  constexpr int bytes = chain_smem_bytes<TI>();
+  static bool configured = false;
+  if (!configured && bytes > 48 * 1024)
+    MCK(cudaFuncSetAttribute(k_coarse_chain<TI, Tv>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  configured = true;
+  launch_pdl_on(h, st, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainWarps)), dim3(kChainWarps * 32),
+                bytes, a, r, s, mode, pair);
+}
+
+// The MAS apply.  Sequential form: the coarse levels, then the level-0 apply
+// adding the coarse correction.  Overlapped form (inside the solve): the
+// coarse levels run on the side stream beside the level-0 apply, the two
+// complete r.z together, and the next p update adds the coarse correction.
 template <typename TI, typename Tv, typename Tacc>
 void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-                 int grid0, PcgScalars* s)
+                 int grid0, PcgScalars* s, bool overlap)
 {
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
   const int variant = std::is_same<TI, float>::value ? (int)kApplyRegisters : h->apply_variant;
-  if (lv.levelnum > 1) {
-    constexpr int bytes = chain_smem_bytes<TI>();
-    static bool configured = false;
-    if (!configured && bytes > 48 * 1024) {
-      MCK(cudaFuncSetAttribute(k_coarse_chain<TI, Tv>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    }
-    configured = true;
-    launch_pdl(h, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainWarps)), dim3(kChainWarps * 32), bytes,
-               a, r, s);
+  if (lv.levelnum <= 1) {
+    level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0);
+    return;
   }
-  level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0);
+  if (!overlap || !s) {
+    launch_chain<TI, Tv>(h, h->stream, a, r, s, mode, 0);
+    level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0);
+    return;
+  }
+  MCK(cudaEventRecord(h->ev_fork, h->stream));
+  MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+  launch_chain<TI, Tv>(h, h->side_stream, a, r, s, mode, 1);
+  MCK(cudaEventRecord(h->ev_join, h->side_stream));
+  level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0, 0, 1);
+  MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+}
+
+// p = (z + coarse correction) + beta p (p = z + correction when k == 1) for
+// the overlapped apply, whose level-0 z leaves the correction out; rows
+// outside the MAS range take z as it is.
+template <typename Tv>
+__global__ void __launch_bounds__(kTpb) k_update_p_coarse(ApplyArgs a, const Tv* __restrict__ z, Tv* p4, int nrows,
+                                                          const PcgScalars* s)
+{
+  pdl_wait();
+  if (s->status != MASPCG_SOLVE_RUNNING) return;
+  const bool first = s->k == 1;
+  const Tv beta = (Tv)s->beta;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
+    Tv z0 = z[3 * (size_t)v], z1 = z[3 * (size_t)v + 1], z2 = z[3 * (size_t)v + 2];
+    const int slot = v - a.fem_off;
+    if (slot >= 0 && slot < a.c0) {
+      float cc[3];
+      if (coarse_correction(a, slot, cc)) {
+        z0 = (Tv)((float)z0 + cc[0]);
+        z1 = (Tv)((float)z1 + cc[1]);
+        z2 = (Tv)((float)z2 + cc[2]);
+      }
+    }
+    if (first) {
+      st_p4(p4, v, z0, z1, z2);
+    } else {
+      const P4<Tv> o = ld_p4(p4, v);
+      st_p4(p4, v, z0 + beta * o.x, z1 + beta * o.y, z2 + beta * o.z);
+    }
+  }
 }
 }  // namespace
+
+template <typename Tv>
+void mas_update_p(maspcg_handle* h, const Tv* z, Tv* p4, int grid, PcgScalars* s)
+{
+  launch_pdl(h, k_update_p_coarse<Tv>, dim3(grid), dim3(kTpb), 0, make_apply_args(h), z, p4, h->nb_int, s);
+}
+template void mas_update_p<float>(maspcg_handle*, const float*, float*, int, PcgScalars*);
+template void mas_update_p<double>(maspcg_handle*, const double*, double*, int, PcgScalars*);
 
 // Explicit launcher used by pcg.cu.
 template <typename Tv, typename Tacc>
 void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-               int grid0, PcgScalars* s)
+               int grid0, PcgScalars* s, bool overlap)
 {
   switch (h->cfg.inverse_storage) {
     case MASPCG_INV_BF16:
-      mas_apply_t<__nv_bfloat16, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s);
+      mas_apply_t<__nv_bfloat16, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s, overlap);
       break;
     case MASPCG_INV_FP16:
-      mas_apply_t<__half, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s);
+      mas_apply_t<__half, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s, overlap);
       break;
-    default: mas_apply_t<float, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s); break;
+    default: mas_apply_t<float, Tv, Tacc>(h, r, z, partial, part_base, total_parts, mode, grid0, s, overlap); break;
   }
   MCK(cudaGetLastError());
 }
@@ -1268,11 +1372,12 @@ template void mas_level0_only<float, double>(maspcg_handle*, const float*, float
 template void mas_level0_only<double, double>(maspcg_handle*, const double*, double*, double*, int, PcgScalars*,
                                               int);
 
-template void mas_apply<float, float>(maspcg_handle*, const float*, float*, float*, int, int, int, int, PcgScalars*);
-template void mas_apply<float, double>(maspcg_handle*, const float*, float*, double*, int, int, int, int,
-                                       PcgScalars*);
+template void mas_apply<float, float>(maspcg_handle*, const float*, float*, float*, int, int, int, int, PcgScalars*,
+                                      bool);
+template void mas_apply<float, double>(maspcg_handle*, const float*, float*, double*, int, int, int, int, PcgScalars*,
+                                       bool);
 template void mas_apply<double, double>(maspcg_handle*, const double*, double*, double*, int, int, int, int,
-                                        PcgScalars*);
+                                        PcgScalars*, bool);
 
 int mas_level0_grid(maspcg_handle* h) { return level0_grid(h, h->apply_variant); }
 

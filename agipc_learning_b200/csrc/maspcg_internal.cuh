@@ -116,13 +116,15 @@ struct PcgScalars {
   int iterations; // reported iteration count once stopped
   int gate;
   double tol;
+  double rz_part[2];  // r.z of the level-0 apply (0) and of the coarse levels (1) when they run concurrently
   unsigned tickets[8];
 };
 
 constexpr int kNeedTrue = 16;  // MIXED: recursive gate met or period end; true residual pending
 constexpr int kCapPending = 32;
 
-enum Ticket { kTicketSpmv = 0, kTicketXr = 1, kTicketRz = 2, kTicketTrue = 3, kTicketAux = 4 };
+enum Ticket { kTicketSpmv = 0, kTicketXr = 1, kTicketRz = 2, kTicketTrue = 3, kTicketAux = 4, kTicketPair = 5,
+              kTicketCoarse = 6 };
 
 struct LevelInfo {
   int levelnum;
@@ -159,6 +161,8 @@ struct maspcg_handle {
   maspcg_config cfg{};
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t side_stream = nullptr;       // the coarse levels run here beside the level-0 apply
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int device = 0;
   int sm_count = 148;
   std::string last_error;
@@ -203,6 +207,7 @@ struct maspcg_handle {
   int failed_domains = 0;
   maspcg::DBuf<float> coarse_r, coarse_z;
   maspcg::DBuf<int> chain_count, chain_target;  // coarse-level dataflow counters (per coarse domain)
+  maspcg::DBuf<double> chain_dot;               // per coarse domain: R.Z (r.z of the coarse levels)
   maspcg::DBuf<double> coarse64;
   maspcg::DBuf<double> abd_inv64;
   maspcg::DBuf<float> abd_inv32;
@@ -228,6 +233,7 @@ struct maspcg_handle {
   long long kernel_launches = 0;  // this library's kernels launched on the handle
   long long graph_kernels = 0;    // kernel nodes of the captured batch graph
   bool use_pdl = false;           // programmatic dependent launch for the iteration kernels (MASPCG_FLAG_PDL)
+  bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
   int apply_variant = 2;          // 16-bit level-0 apply: 0 registers, 1 TMA-staged x2 buffers, 2 TMA-staged x1
 };
 
@@ -302,13 +308,14 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <typename... KArgs, typename... Args>
-void launch_pdl(maspcg_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args)
+void launch_pdl_on(maspcg_handle* h, cudaStream_t stream, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                   Args&&... args)
 {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
-  cfg.stream = h->stream;
+  cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -316,6 +323,12 @@ void launch_pdl(maspcg_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 bloc
   cfg.numAttrs = h->use_pdl ? 1 : 0;
   MCK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
   ++h->kernel_launches;
+}
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(maspcg_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args)
+{
+  launch_pdl_on(h, h->stream, kernel, grid, block, smem, std::forward<Args>(args)...);
 }
 
 }  // namespace maspcg

@@ -26,7 +26,9 @@ namespace maspcg {
 
 template <typename Tv, typename Tacc>
 void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-               int grid0, PcgScalars* s);
+               int grid0, PcgScalars* s, bool overlap);
+template <typename Tv>
+void mas_update_p(maspcg_handle* h, const Tv* z, Tv* p4, int grid, PcgScalars* s);
 template <typename Tv, typename Tacc>
 void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant);
 void launch_factor(maspcg_handle* h, double* assembled_out);
@@ -55,40 +57,6 @@ __global__ void __launch_bounds__(kTpb) k_init(const double* __restrict__ b, Tv*
   if (grid_finish<double>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketAux], gridDim.x, total) &&
       threadIdx.x == 0)
     s->bb = total;
-}
-
-// ---- padded search direction: one 16-byte (FP32) / 32-byte (FP64) slot per
-// block row, so the SpMV gathers a column's three entries with one vector load.
-template <typename T>
-struct P4;
-template <>
-struct P4<float> {
-  float x, y, z, w;
-};
-template <>
-struct P4<double> {
-  double x, y, z, w;
-};
-
-__device__ __forceinline__ P4<float> ld_p4(const float* p4, int v)
-{
-  const float4 q = __ldg(reinterpret_cast<const float4*>(p4) + v);
-  return {q.x, q.y, q.z, q.w};
-}
-__device__ __forceinline__ P4<double> ld_p4(const double* p4, int v)
-{
-  const double2 a = __ldg(reinterpret_cast<const double2*>(p4) + 2 * v);
-  const double2 b = __ldg(reinterpret_cast<const double2*>(p4) + 2 * v + 1);
-  return {a.x, a.y, b.x, b.y};
-}
-__device__ __forceinline__ void st_p4(float* p4, int v, float x, float y, float z)
-{
-  reinterpret_cast<float4*>(p4)[v] = make_float4(x, y, z, 0.f);
-}
-__device__ __forceinline__ void st_p4(double* p4, int v, double x, double y, double z)
-{
-  reinterpret_cast<double2*>(p4)[2 * v] = make_double2(x, y);
-  reinterpret_cast<double2*>(p4)[2 * v + 1] = make_double2(z, 0.0);
 }
 
 // Entries [4q, 4q + 4) of a vector as 16-byte (FP32) / 2 x 16-byte (FP64)
@@ -455,7 +423,7 @@ template <typename Tm, typename Tv, typename Tacc>
 struct Engine {
   maspcg_handle* h;
   int n, gstream, gspmv, grows, gl0, gother, parts_other, parts_total;
-  bool mas, mixed;
+  bool mas, mixed, ovl;
 
   explicit Engine(maspcg_handle* hh) : h(hh)
   {
@@ -466,6 +434,7 @@ struct Engine {
     gspmv = std::max(1, std::min(ceil_div(h->nb_int, kTpb / 16), 4 * h->sm_count));
     grows = std::max(1, std::min(ceil_div(h->nb_int, kTpb), 8 * h->sm_count));
     gl0 = mas ? mas_level0_grid(h) : 0;
+    ovl = mas && h->lv.levelnum > 1 && h->overlap_coarse;
     const bool other = !mas || h->abd_bodies > 0 || h->fem_off > 0 || h->nb_int > h->fem_off + h->c0;
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;
     parts_other = gother;
@@ -475,7 +444,9 @@ struct Engine {
   Tacc* partial() { return reinterpret_cast<Tacc*>(h->partial.get()); }
   Tacc* partial_rz() { return reinterpret_cast<Tacc*>(h->partial_rz.get()); }
 
-  void precondition(const Tv* r, Tv* z, int mode, PcgScalars* s)
+  // overlap: the coarse levels run beside the level-0 apply and z leaves the
+  // coarse correction to the next p update (inside the solve only).
+  void precondition(const Tv* r, Tv* z, int mode, PcgScalars* s, bool overlap = false)
   {
     const bool ref = h->cfg.precision == MASPCG_PREC_REFERENCE;
     if (gother) {
@@ -491,13 +462,16 @@ struct Engine {
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv32.get(), bj ? h->diag_inv32.get() : nullptr,
             s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
     }
-    if (mas) mas_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s);
+    if (mas) mas_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s, overlap);
     MCK(cudaGetLastError());
   }
 
   void iteration_head(PcgScalars* s)
   {
-    launch_pdl(h, k_update_p<Tv>, dim3(grows), dim3(kTpb), 0, V(h->vz), V(h->vp4), h->nb_int, s);
+    if (ovl)
+      mas_update_p<Tv>(h, V(h->vz), V(h->vp4), grows, s);
+    else
+      launch_pdl(h, k_update_p<Tv>, dim3(grows), dim3(kTpb), 0, V(h->vz), V(h->vp4), h->nb_int, s);
     spmv(s);
     launch_pdl(h, k_update_xr<Tv, Tacc>, dim3(grows), dim3(kTpb), 0, V(h->vx), V(h->vr), V(h->vp4), V(h->vap),
                h->nb_int, mixed ? 1 : 0, partial(), s);
@@ -537,7 +511,7 @@ struct Engine {
     for (int it = 0; it < batch; ++it) {
       iteration_head(s);
       if (mixed && it == batch - 1) true_residual(s);
-      precondition(V(h->vr), V(h->vz), 2, s);
+      precondition(V(h->vr), V(h->vz), 2, s, ovl);
     }
   }
 
@@ -627,7 +601,7 @@ struct Engine {
     MCK(cudaEventRecord(h->ev0, st));
     k_init<Tv><<<gstream, kTpb, 0, st>>>(b_int, V(h->vx), V(h->vr), mixed ? h->x64.get() : nullptr, n,
                                          h->partial_rz.get(), s); MLAUNCHED(h);
-    precondition(V(h->vr), V(h->vz), 1, s);
+    precondition(V(h->vr), V(h->vz), 1, s, ovl);
     // graph of one batch
     const int batch = mixed ? std::max(1, h->cfg.refinement_period) : std::max(1, h->cfg.iterations_per_launch);
     if (h->graph_dirty || h->graph_batch != batch) {

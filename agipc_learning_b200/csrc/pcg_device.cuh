@@ -77,4 +77,54 @@ __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode
   }
 }
 
+// r.z summed by two concurrent kernels (the level-0 apply and the coarse
+// levels): each stores its part and takes a ticket; the second adds the two
+// parts in a fixed order and updates the scalars (mode as in rz_update).
+__device__ __forceinline__ void rz_part_done(PcgScalars* s, int part, double value, int mode)
+{
+  s->rz_part[part] = value;
+  __threadfence();
+  const unsigned t = atomicAdd(&s->tickets[kTicketPair], 1u);
+  if (t == 1u) {
+    __threadfence();
+    const double total = __ldcg(&s->rz_part[0]) + __ldcg(&s->rz_part[1]);
+    s->tickets[kTicketPair] = 0u;
+    if (mode > 0) rz_update(s, total, mode);
+  }
+}
+
+// ---- padded search direction: one 16-byte (FP32) / 32-byte (FP64) slot per
+// block row, so the SpMV gathers a column's three entries with one vector load.
+template <typename T>
+struct P4;
+template <>
+struct P4<float> {
+  float x, y, z, w;
+};
+template <>
+struct P4<double> {
+  double x, y, z, w;
+};
+
+__device__ __forceinline__ P4<float> ld_p4(const float* p4, int v)
+{
+  const float4 q = __ldg(reinterpret_cast<const float4*>(p4) + v);
+  return {q.x, q.y, q.z, q.w};
+}
+__device__ __forceinline__ P4<double> ld_p4(const double* p4, int v)
+{
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p4) + 2 * v);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p4) + 2 * v + 1);
+  return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st_p4(float* p4, int v, float x, float y, float z)
+{
+  reinterpret_cast<float4*>(p4)[v] = make_float4(x, y, z, 0.f);
+}
+__device__ __forceinline__ void st_p4(double* p4, int v, double x, double y, double z)
+{
+  reinterpret_cast<double2*>(p4)[2 * v] = make_double2(x, y);
+  reinterpret_cast<double2*>(p4)[2 * v + 1] = make_double2(z, 0.0);
+}
+
 }  // namespace maspcg

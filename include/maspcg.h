@@ -96,7 +96,8 @@ typedef struct {
 typedef enum {
   MASPCG_FLAG_PDL = 1,                 /* launch iteration kernels with programmatic dependent launch */
   MASPCG_FLAG_APPLY_STAGED2 = 2,       /* 16-bit level-0 apply: two TMA slots per warp */
-  MASPCG_FLAG_APPLY_REGISTERS = 4      /* 16-bit level-0 apply: inverse held in registers */
+  MASPCG_FLAG_APPLY_REGISTERS = 4,     /* 16-bit level-0 apply: inverse held in registers */
+  MASPCG_FLAG_SEQUENTIAL_COARSE = 8    /* run the MAS coarse levels before the level-0 apply, not beside it */
 } maspcg_flags;
 
 typedef struct {
