@@ -280,78 +280,103 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
     return;
   }
 
-  // ---- Cholesky, right-looking, lower blocks (w >= lane) hold L afterwards
+  // ---- blocked Cholesky, right-looking over the 32 block columns: thread
+  // (q,q) factors its 3x3 diagonal block and inverts the factor, the block
+  // column below it is solved against that factor, then the trailing lower
+  // blocks take the rank-3 update.  Lower blocks (w >= lane) hold L after.
+  // The step buffers reuse `stage` (assembly is over once every thread has
+  // passed the first barrier below).
+  __shared__ double dinv[kBank][9];          // L_qq^-1 (lower, row-major), kept for W below
+  double(*panel)[kBank][9] = reinterpret_cast<double(*)[kBank][9]>(&stage[0][0]);               // L_wq, x2
+  double(*wrow)[kBank][9] = reinterpret_cast<double(*)[kBank][9]>(&stage[0][0] + 2 * kBank * 9);  // W_ql, x2
   for (int q = 0; q < kBank; ++q) {
+    const int b = q & 1;
+    if (w == q && lane == q) {
+      double p0 = acc[0];
+      if (!(p0 > 0.0) || !isfinite(p0)) fail = 1, p0 = 1.0;
+      const double l00 = sqrt(p0), i00 = 1.0 / l00;
+      const double l10 = acc[3] * i00, l20 = acc[6] * i00;
+      double p1 = acc[4] - l10 * l10;
+      if (!(p1 > 0.0) || !isfinite(p1)) fail = 1, p1 = 1.0;
+      const double l11 = sqrt(p1), i11 = 1.0 / l11;
+      const double l21 = (acc[7] - l20 * l10) * i11;
+      double p2 = acc[8] - l20 * l20 - l21 * l21;
+      if (!(p2 > 0.0) || !isfinite(p2)) fail = 1, p2 = 1.0;
+      const double l22 = sqrt(p2), i22 = 1.0 / l22;
+      const double i10 = -(l10 * i00) * i11;
+      const double i21 = -(l21 * i11) * i22;
+      const double i20 = -(l20 * i00 + l21 * i10) * i22;
+      const double L[9] = {l00, 0.0, 0.0, l10, l11, 0.0, l20, l21, l22};
+      const double I[9] = {i00, 0.0, 0.0, i10, i11, 0.0, i20, i21, i22};
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int k = 3 * q + c;
-      double* col = buf[k & 1];
-      if (lane == q) {
-        col[3 * w + 0] = acc[c];
-        col[3 * w + 1] = acc[3 + c];
-        col[3 * w + 2] = acc[6 + c];
-        if (w == q) {  // the pivot's owner takes its square root once
-          double pv = acc[4 * c];
-          if (!(pv > 0.0) || !isfinite(pv)) {
-            fail = 1;
-            pv = 1.0;
-          }
-          const double r = sqrt(pv);
-          spiv[k & 1][0] = r;
-          spiv[k & 1][1] = 1.0 / r;
-        }
+      for (int e = 0; e < 9; ++e) {
+        acc[e] = L[e];
+        dinv[q][e] = I[e];
       }
-      __syncthreads();
-      const double dk = spiv[k & 1][0], invd = spiv[k & 1][1];
-      const double lr[3] = {col[3 * w] * invd, col[3 * w + 1] * invd, col[3 * w + 2] * invd};
-      const double ls[3] = {col[3 * lane] * invd, col[3 * lane + 1] * invd, col[3 * lane + 2] * invd};
+    }
+    __syncthreads();
+    if (lane == q && w > q) {  // L_wq = A_wq L_qq^-T
+      double l[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int jj = 0; jj < 3; ++jj) {
-          const int r = 3 * w + i, sc = 3 * lane + jj;
-          double& x = acc[3 * i + jj];
-          if (sc == k && r >= k)
-            x = (r == k) ? dk : lr[i];
-          else if (r > k && sc > k && sc <= r)
-            x = fma(-lr[i], ls[jj], x);
-        }
+        for (int j = 0; j < 3; ++j)
+          l[3 * i + j] = acc[3 * i] * dinv[q][3 * j] + acc[3 * i + 1] * dinv[q][3 * j + 1] +
+                         acc[3 * i + 2] * dinv[q][3 * j + 2];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        acc[e] = l[e];
+        panel[b][w][e] = l[e];
+      }
+    }
+    __syncthreads();
+    if (w > q && lane > q && lane <= w) {  // A_wl -= L_wq L_lq^T
+      const double* pw = panel[b][w];
+      const double* pl = panel[b][lane];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          acc[3 * i + j] -= pw[3 * i] * pl[3 * j] + pw[3 * i + 1] * pl[3 * j + 1] + pw[3 * i + 2] * pl[3 * j + 2];
     }
   }
-  __syncthreads();
-  // ---- W = L^-1 by right-looking elimination on the identity
+  // ---- W = L^-1 by blocked forward substitution on the identity: row
+  // block q of W is L_qq^-1 times the current right-hand side, which is then
+  // eliminated from the rows below.
   double xr[9];
 #pragma unroll
   for (int e = 0; e < 9; ++e) xr[e] = (w == lane && (e % 4) == 0) ? 1.0 : 0.0;
   for (int q = 0; q < kBank; ++q) {
+    const int b = q & 1;
+    if (lane == q && w > q) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int k = 3 * q + c;
-      double* row = buf[k & 1];
-      const double lkk = __shfl_sync(kFull, acc[4 * c], q);  // L[k][k] (warp q, lane q)
-      if (w == q) {
-        const double inv = 1.0 / lkk;
-        xr[3 * c + 0] *= inv;
-        xr[3 * c + 1] *= inv;
-        xr[3 * c + 2] *= inv;
-        row[3 * lane + 0] = xr[3 * c + 0];
-        row[3 * lane + 1] = xr[3 * c + 1];
-        row[3 * lane + 2] = xr[3 * c + 2];
-      }
-      const double m0 = __shfl_sync(kFull, acc[c], q);
-      const double m1 = __shfl_sync(kFull, acc[3 + c], q);
-      const double m2 = __shfl_sync(kFull, acc[6 + c], q);
-      __syncthreads();
-      const double xk[3] = {row[3 * lane], row[3 * lane + 1], row[3 * lane + 2]};
-      const double mm[3] = {m0, m1, m2};
+      for (int e = 0; e < 9; ++e) panel[b][w][e] = acc[e];  // L_wq
+    }
+    if (w == q && lane <= q) {  // W_ql = L_qq^-1 X_ql
+      double y[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
-        if (3 * w + i > k) {
 #pragma unroll
-          for (int jj = 0; jj < 3; ++jj) xr[3 * i + jj] = fma(-mm[i], xk[jj], xr[3 * i + jj]);
-        }
+        for (int j = 0; j < 3; ++j)
+          y[3 * i + j] = dinv[q][3 * i] * xr[j] + dinv[q][3 * i + 1] * xr[3 + j] + dinv[q][3 * i + 2] * xr[6 + j];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        xr[e] = y[e];
+        wrow[b][lane][e] = y[e];
+      }
+    }
+    __syncthreads();
+    if (w > q && lane <= q) {  // X_wl -= L_wq W_ql
+      const double* lw = panel[b][w];
+      const double* wl = wrow[b][lane];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          xr[3 * i + j] -= lw[3 * i] * wl[j] + lw[3 * i + 1] * wl[3 + j] + lw[3 * i + 2] * wl[6 + j];
     }
   }
+  __syncthreads();
   // ---- column scales and factored store (lower blocks only)
   if (w >= lane) {
 #pragma unroll

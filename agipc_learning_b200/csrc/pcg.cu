@@ -519,8 +519,10 @@ struct Engine {
   // launch a 256 MB zero buffer is read through L2 (clean lines only, so the
   // timed launch pays no write-back), so each launch starts cold as it does
   // inside the solve, where the SpMV streams more than L2 between two
-  // applies; each launch is bracketed by its own events.  Programmatic
-  // dependent launch is off while timing.
+  // applies.  The stage's time is (evict + stage) x repeats minus
+  // evict x repeats, each pair of events around a back-to-back sequence, so
+  // no per-launch event overhead is counted.  Programmatic dependent launch
+  // is off while timing.
   double time_stage(int stage, int repeats)
   {
     cudaStream_t st = h->stream;
@@ -554,21 +556,30 @@ struct Engine {
     };
     const bool pdl = h->use_pdl;
     h->use_pdl = false;
+    auto evict = [&]() {
+      k_l2_evict<<<4 * h->sm_count, kTpb, 0, st>>>(reinterpret_cast<const uint4*>(h->l2_flush.get()),
+                                                   kFlushBytes / 16, reinterpret_cast<unsigned*>(h->l2_flush.get()));
+      MLAUNCHED(h);
+    };
+    auto timed = [&](bool with_stage) {
+      MCK(cudaEventRecord(h->ev0, st));
+      for (int i = 0; i < repeats; ++i) {
+        evict();
+        if (with_stage) once();
+      }
+      MCK(cudaEventRecord(h->ev1, st));
+      MCK(cudaEventSynchronize(h->ev1));
+      float ms = 0.f;
+      MCK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+      return (double)ms;
+    };
     double total = 0.0;
     try {
       once();  // warm
-      for (int i = 0; i < repeats; ++i) {
-        k_l2_evict<<<4 * h->sm_count, kTpb, 0, st>>>(reinterpret_cast<const uint4*>(h->l2_flush.get()),
-                                                     kFlushBytes / 16, reinterpret_cast<unsigned*>(h->l2_flush.get()));
-        MLAUNCHED(h);
-        MCK(cudaEventRecord(h->ev0, st));
-        once();
-        MCK(cudaEventRecord(h->ev1, st));
-        MCK(cudaEventSynchronize(h->ev1));
-        float ms = 0.f;
-        MCK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-        total += ms;
-      }
+      evict();
+      const double both = timed(true);
+      const double alone = timed(false);
+      total = std::max(0.0, both - alone);
     } catch (...) {
       h->use_pdl = pdl;
       throw;

@@ -272,7 +272,7 @@ def run_ours(args, world, rank, local):
     l0_bytes = d0 * (528 * 9 * 2 + 96 * 4) + 3 * 4 * 32 * d0 * 3
     peak, peak_kind = peaks()
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "k_spmv_cube64_contacts_traffic.json")
     if os.path.exists(tfile):
         try:
             traffic = json.load(open(tfile)).get("dram_bytes_per_launch_full_workload")

@@ -236,9 +236,10 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
 
 /* Benchmark introspection (no counterpart in the reference): run one stage
  * `repeats` times on the handle's stream, each run after reading a 256 MB
- * buffer that evicts L2 (clean lines only) and between its own two CUDA
- * events, and return the mean device milliseconds per run (allocates the
- * buffer on first use).  Stages:
+ * buffer that evicts L2 (clean lines only), and return the mean device
+ * milliseconds per run: CUDA events around the whole sequence, minus the
+ * same sequence of evictions alone (allocates the buffer on first use).
+ * Stages:
  *   0  PCG SpMV with the p.Ap reduction, working precision
  *   1  full preconditioner apply z = M^-1 r, working precision
  *   2  MAS level-0 domain apply alone (restriction/coarse levels excluded)
