@@ -36,6 +36,7 @@ FLAG_PDL = 1
 FLAG_APPLY_STAGED2 = 2
 FLAG_APPLY_REGISTERS = 4
 FLAG_SEQUENTIAL_COARSE = 8
+FLAG_FUSED_HEAD = 16
 
 INV_FP32 = 0
 INV_BF16 = 1

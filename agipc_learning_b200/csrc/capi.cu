@@ -182,7 +182,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_NONE) ||
-      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~15) != 0 ||
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~31) != 0 ||
       ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_REGISTERS))) {
     g_create_error = "invalid configuration";
     return MASPCG_ERR_INVALID_ARGUMENT;
@@ -210,6 +210,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     h->grid_stream = 4 * h->sm_count;
     h->use_pdl = (c.flags & MASPCG_FLAG_PDL) != 0;
     h->overlap_coarse = (c.flags & MASPCG_FLAG_SEQUENTIAL_COARSE) == 0;
+    h->fused_head = (c.flags & MASPCG_FLAG_FUSED_HEAD) != 0;
     MCK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
     MCK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     MCK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));

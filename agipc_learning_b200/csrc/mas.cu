@@ -29,6 +29,7 @@
 #include "maspcg_internal.cuh"
 #include "pcg_device.cuh"
 #include "tma.cuh"
+#include "mas_args.cuh"
 
 namespace maspcg {
 namespace {
@@ -601,39 +602,6 @@ __device__ __forceinline__ void group_sum(int key, const float v[3], float out[3
   out[1] = s1;
   out[2] = s2;
   leader = (__ffs(grp) - 1) == (int)(threadIdx.x & 31);
-}
-
-struct ApplyArgs {
-  const int* cmap1;
-  const int* cmap[kMaxLevels];  // fine slot -> level-l local node (-1 padding), l >= 1
-  const int* pmr;               // part_map_real: -1 marks a padding slot
-  const int* going_next;
-  float* coarse_r;
-  float* coarse_z;
-  const void* inv;
-  const float* scale;
-  int* chain_count;             // per coarse domain: arrivals so far (zero between launches)
-  const int* chain_target;      // per coarse domain: arrivals that complete it
-  double* chain_dot;            // per coarse domain: R.Z
-  int* err;
-  int fem_off, c0;
-  LevelInfo lv;
-};
-
-// Coarse correction of a level-0 slot: the sum over the coarse levels of the
-// level's z at the slot's ancestor (the prolongation, CollectFinalZ).  Returns
-// false for a padding slot, whose z is zero.
-__device__ __forceinline__ bool coarse_correction(const ApplyArgs& a, int slot, float c[3])
-{
-  c[0] = c[1] = c[2] = 0.f;
-  if (a.pmr[slot] < 0) return false;
-  for (int l = 1; l < a.lv.levelnum; ++l) {
-    const float* q = a.coarse_z + 3 * (size_t)(a.lv.begin[l] - a.c0 + a.cmap[l][slot]);
-    c[0] += q[0];
-    c[1] += q[1];
-    c[2] += q[2];
-  }
-  return true;
 }
 
 // Domain-apply kernels: 4 warps per CTA; 16-bit storage keeps a domain's 77
@@ -1313,45 +1281,11 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
   MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
 }
 
-// p = (z + coarse correction) + beta p (p = z + correction when k == 1) for
-// the overlapped apply, whose level-0 z leaves the correction out; rows
-// outside the MAS range take z as it is.
-template <typename Tv>
-__global__ void __launch_bounds__(kTpb) k_update_p_coarse(ApplyArgs a, const Tv* __restrict__ z, Tv* p4, int nrows,
-                                                          const PcgScalars* s)
-{
-  pdl_wait();
-  if (s->status != MASPCG_SOLVE_RUNNING) return;
-  const bool first = s->k == 1;
-  const Tv beta = (Tv)s->beta;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
-    Tv z0 = z[3 * (size_t)v], z1 = z[3 * (size_t)v + 1], z2 = z[3 * (size_t)v + 2];
-    const int slot = v - a.fem_off;
-    if (slot >= 0 && slot < a.c0) {
-      float cc[3];
-      if (coarse_correction(a, slot, cc)) {
-        z0 = (Tv)((float)z0 + cc[0]);
-        z1 = (Tv)((float)z1 + cc[1]);
-        z2 = (Tv)((float)z2 + cc[2]);
-      }
-    }
-    if (first) {
-      st_p4(p4, v, z0, z1, z2);
-    } else {
-      const P4<Tv> o = ld_p4(p4, v);
-      st_p4(p4, v, z0 + beta * o.x, z1 + beta * o.y, z2 + beta * o.z);
-    }
-  }
-}
 }  // namespace
 
-template <typename Tv>
-void mas_update_p(maspcg_handle* h, const Tv* z, Tv* p4, int grid, PcgScalars* s)
-{
-  launch_pdl(h, k_update_p_coarse<Tv>, dim3(grid), dim3(kTpb), 0, make_apply_args(h), z, p4, h->nb_int, s);
-}
-template void mas_update_p<float>(maspcg_handle*, const float*, float*, int, PcgScalars*);
-template void mas_update_p<double>(maspcg_handle*, const double*, double*, int, PcgScalars*);
+ApplyArgs mas_apply_args(maspcg_handle* h) { return make_apply_args(h); }
+
+
 
 // Explicit launcher used by pcg.cu.
 template <typename Tv, typename Tacc>

@@ -118,13 +118,14 @@ struct PcgScalars {
   double tol;
   double rz_part[2];  // r.z of the level-0 apply (0) and of the coarse levels (1) when they run concurrently
   unsigned tickets[8];
+  unsigned barrier_gen;  // generation of the grid barrier of the fused iteration kernel
 };
 
 constexpr int kNeedTrue = 16;  // MIXED: recursive gate met or period end; true residual pending
 constexpr int kCapPending = 32;
 
 enum Ticket { kTicketSpmv = 0, kTicketXr = 1, kTicketRz = 2, kTicketTrue = 3, kTicketAux = 4, kTicketPair = 5,
-              kTicketCoarse = 6 };
+              kTicketCoarse = 6, kTicketBarrier = 7 };
 
 struct LevelInfo {
   int levelnum;
@@ -233,6 +234,7 @@ struct maspcg_handle {
   long long kernel_launches = 0;  // this library's kernels launched on the handle
   long long graph_kernels = 0;    // kernel nodes of the captured batch graph
   bool use_pdl = false;           // programmatic dependent launch for the iteration kernels (MASPCG_FLAG_PDL)
+  bool fused_head = false;        // p update + SpMV + x/r update as one cooperative kernel (MASPCG_FLAG_FUSED_HEAD)
   bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
   int apply_variant = 2;          // 16-bit level-0 apply: 0 registers, 1 TMA-staged x2 buffers, 2 TMA-staged x1
 };
@@ -321,6 +323,25 @@ void launch_pdl_on(maspcg_handle* h, cudaStream_t stream, void (*kernel)(KArgs..
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = h->use_pdl ? 1 : 0;
+  MCK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+  ++h->kernel_launches;
+}
+
+// Cooperative launch (all CTAs resident at once) for kernels with a grid
+// barrier; the caller sizes the grid from the occupancy API.
+template <typename... KArgs, typename... Args>
+void launch_cooperative(maspcg_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args)
+{
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   MCK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
   ++h->kernel_launches;
 }

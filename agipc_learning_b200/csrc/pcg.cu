@@ -20,6 +20,7 @@
 
 #include "maspcg_internal.cuh"
 #include "pcg_device.cuh"
+#include "mas_args.cuh"
 #include "spmv_row.cuh"
 
 namespace maspcg {
@@ -27,8 +28,7 @@ namespace maspcg {
 template <typename Tv, typename Tacc>
 void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                int grid0, PcgScalars* s, bool overlap);
-template <typename Tv>
-void mas_update_p(maspcg_handle* h, const Tv* z, Tv* p4, int grid, PcgScalars* s);
+
 template <typename Tv, typename Tacc>
 void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant);
 void launch_factor(maspcg_handle* h, double* assembled_out);
@@ -83,17 +83,29 @@ __device__ __forceinline__ void st4(T* p, int q, const T o[4])
   }
 }
 
-// p = z (k == 1) or z + beta p, written into the padded layout; one block
-// row per thread (many threads in flight: the kernel is latency-bound).
-template <typename Tv>
-__global__ void __launch_bounds__(kTpb) k_update_p(const Tv* __restrict__ z, Tv* p4, int nrows, const PcgScalars* s)
+// ---- the three steps of one iteration head as device bodies, shared by
+// the separate kernels and by the fused cooperative kernel below.
+
+// p = z (k == 1) or z + beta p for the rows this thread strides over, written
+// into the padded layout.  With `coarse` the MAS rows first add the coarse
+// correction (the overlapped apply leaves it out of z).
+template <typename Tv, bool kCoarse>
+__device__ __forceinline__ void update_p_rows(const ApplyArgs& a, const Tv* __restrict__ z, Tv* p4, int nrows,
+                                              bool first, Tv beta)
 {
-  pdl_wait();
-  if (!running(s)) return;
-  const bool first = s->k == 1;
-  const Tv beta = (Tv)s->beta;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nrows; v += gridDim.x * blockDim.x) {
-    const Tv z0 = z[3 * (size_t)v], z1 = z[3 * (size_t)v + 1], z2 = z[3 * (size_t)v + 2];
+    Tv z0 = z[3 * (size_t)v], z1 = z[3 * (size_t)v + 1], z2 = z[3 * (size_t)v + 2];
+    if (kCoarse) {
+      const int slot = v - a.fem_off;
+      if (slot >= 0 && slot < a.c0) {
+        float cc[3];
+        if (coarse_correction(a, slot, cc)) {
+          z0 = (Tv)((float)z0 + cc[0]);
+          z1 = (Tv)((float)z1 + cc[1]);
+          z2 = (Tv)((float)z2 + cc[2]);
+        }
+      }
+    }
     if (first) {
       st_p4(p4, v, z0, z1, z2);
     } else {
@@ -101,6 +113,15 @@ __global__ void __launch_bounds__(kTpb) k_update_p(const Tv* __restrict__ z, Tv*
       st_p4(p4, v, z0 + beta * o.x, z1 + beta * o.y, z2 + beta * o.z);
     }
   }
+}
+
+template <typename Tv, bool kCoarse>
+__global__ void __launch_bounds__(kTpb) k_update_p(ApplyArgs a, const Tv* __restrict__ z, Tv* p4, int nrows,
+                                                    const PcgScalars* s)
+{
+  pdl_wait();
+  if (!running(s)) return;
+  update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
 }
 
 // One 3x3 block of the matrix.  FP32: tiles of 32 blocks stored element-major
@@ -120,16 +141,14 @@ __device__ __forceinline__ void load_block(const Tm* __restrict__ val, int t, Tm
   }
 }
 
-// Ap = A p and p.Ap; last block: alpha.  LPR lanes per block row, each lane
-// takes two blocks per step with every load issued before the arithmetic;
-// the next row's extent is fetched while the current row is processed.
+// Ap = A p for the rows this CTA strides over; returns this thread's share of
+// p.Ap.  LPR lanes per block row, each lane takes two blocks per step with
+// every load issued before the arithmetic; the next row's extent is fetched
+// while the current row is processed.
 template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
-__global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                                const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap,
-                                                int nrows, Tacc* partial, PcgScalars* s)
+__device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                          const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap, int nrows)
 {
-  pdl_wait();
-  if (!running(s)) return;
   using A = typename AccOf<Tm>::type;
   constexpr int kRows = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
@@ -179,36 +198,47 @@ __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, c
     rs = nrs;
     re = nre;
   }
-  pdl_trigger();
-  Tacc total = 0;
-  if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
-      threadIdx.x == 0) {
-    const double pap = (double)total;
-    s->pap = pap;
-    if (!isfinite(pap)) {
-      s->status = MASPCG_SOLVE_NONFINITE;
-      s->iterations = s->k;
-    } else if (!(pap > 0.0)) {
-      s->status = MASPCG_SOLVE_NONPOSITIVE_CURVATURE;
-      s->iterations = s->k;
-    } else {
-      s->alpha = s->rz / pap;
-    }
+  return dot;
+}
+
+// Last block of the SpMV: p.Ap and alpha (or a stop on curvature / NaN).
+__device__ __forceinline__ void spmv_finish(PcgScalars* s, double pap)
+{
+  s->pap = pap;
+  if (!isfinite(pap)) {
+    s->status = MASPCG_SOLVE_NONFINITE;
+    s->iterations = s->k;
+  } else if (!(pap > 0.0)) {
+    s->status = MASPCG_SOLVE_NONPOSITIVE_CURVATURE;
+    s->iterations = s->k;
+  } else {
+    s->alpha = s->rz / pap;
   }
 }
 
-// x += alpha p, r -= alpha Ap, r.r; last block: stopping gate.
-// MIXED: x is the FP32 correction since the last replacement and a met gate
-// asks for the FP64 true residual instead of stopping.  Each thread takes
-// four consecutive entries of x, r and Ap (16-byte accesses) and gathers the
-// matching entries of the padded p; a scalar tail covers n % 4.
-template <typename Tv, typename Tacc>
-__global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p4, const Tv* __restrict__ ap,
-                                                     int nrows, int mixed, Tacc* partial, PcgScalars* s)
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
+__global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                                const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap,
+                                                int nrows, Tacc* partial, PcgScalars* s)
 {
   pdl_wait();
   if (!running(s)) return;
-  const Tv alpha = (Tv)s->alpha;
+  const Tacc dot = spmv_rows<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, p4, ap, nrows);
+  pdl_trigger();
+  Tacc total = 0;
+  if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
+      threadIdx.x == 0)
+    spmv_finish(s, (double)total);
+}
+
+// x += alpha p, r -= alpha Ap for the entries this thread strides over;
+// returns its share of r.r.  Four consecutive entries of x, r and Ap per
+// step (16-byte accesses) with the matching entries of the padded p; a
+// scalar tail covers n % 4.
+template <typename Tv, typename Tacc>
+__device__ __forceinline__ Tacc update_xr_rows(Tv* x, Tv* r, const Tv* __restrict__ p4, const Tv* __restrict__ ap,
+                                               int nrows, Tv alpha)
+{
   Tacc acc = 0;
   const int n = 3 * nrows, n4 = n >> 2;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += gridDim.x * blockDim.x) {
@@ -237,27 +267,72 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
     r[j] = rn;
     acc += (Tacc)rn * (Tacc)rn;
   }
+  return acc;
+}
+
+// Last block of the x/r update: r.r and the stopping gate.  MIXED: x is the
+// FP32 correction since the last replacement and a met gate asks for the
+// FP64 true residual instead of stopping.
+__device__ __forceinline__ void xr_finish(PcgScalars* s, double rr, int mixed)
+{
+  s->rr = rr;
+  if (!isfinite(rr)) {
+    s->status = MASPCG_SOLVE_NONFINITE;
+    s->iterations = s->k;
+    return;
+  }
+  const bool conv = (s->gate == MASPCG_GATE_RZ) ? (fabs(s->rz) <= s->tol * s->rz0) : (rr <= s->tol * s->tol * s->bb);
+  if (conv) {
+    if (mixed) {
+      s->status = kNeedTrue;
+    } else {
+      s->status = MASPCG_SOLVE_CONVERGED;
+      s->iterations = s->k;
+    }
+  }
+}
+
+template <typename Tv, typename Tacc>
+__global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p4, const Tv* __restrict__ ap,
+                                                     int nrows, int mixed, Tacc* partial, PcgScalars* s)
+{
+  pdl_wait();
+  if (!running(s)) return;
+  const Tacc acc = update_xr_rows<Tv, Tacc>(x, r, p4, ap, nrows, (Tv)s->alpha);
   pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
-      threadIdx.x == 0) {
-    const double rr = (double)total;
-    s->rr = rr;
-    if (!isfinite(rr)) {
-      s->status = MASPCG_SOLVE_NONFINITE;
-      s->iterations = s->k;
-      return;
-    }
-    const bool conv = (s->gate == MASPCG_GATE_RZ) ? (fabs(s->rz) <= s->tol * s->rz0) : (rr <= s->tol * s->tol * s->bb);
-    if (conv) {
-      if (mixed) {
-        s->status = kNeedTrue;
-      } else {
-        s->status = MASPCG_SOLVE_CONVERGED;
-        s->iterations = s->k;
-      }
-    }
-  }
+      threadIdx.x == 0)
+    xr_finish(s, (double)total, mixed);
+}
+
+// The iteration head as one cooperative kernel (every CTA resident): the p
+// update, a grid barrier, the SpMV with p.Ap and alpha, a grid barrier, the
+// x/r update with r.r and the gate.  Saves two kernel boundaries per
+// iteration; the barriers are bounded (grid_barrier).
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, bool kCoarse>
+__global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, const int* __restrict__ rowptr,
+                                                          const int* __restrict__ colidx, const Tm* __restrict__ val,
+                                                          const Tv* __restrict__ z, Tv* p4, Tv* ap, Tv* x, Tv* r,
+                                                          int nrows, int mixed, Tacc* partial, PcgScalars* s, int* err)
+{
+  if (!running(s)) return;  // uniform: no CTA of this launch has written the status yet
+  update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
+  if (!grid_barrier(s, err)) return;
+  const Tacc dot = spmv_rows<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, p4, ap, nrows);
+  Tacc total = 0;
+  if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
+      threadIdx.x == 0)
+    spmv_finish(s, (double)total);
+  if (!grid_barrier(s, err)) return;
+  // status and alpha were written by another CTA before the barrier: read
+  // them past L1 (this CTA cached the scalars' line at entry)
+  if (__ldcg(&s->status) != MASPCG_SOLVE_RUNNING) return;  // uniform
+  const Tacc acc = update_xr_rows<Tv, Tacc>(x, r, p4, ap, nrows, (Tv)__ldcg(&s->alpha));
+  total = 0;
+  if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
+      threadIdx.x == 0)
+    xr_finish(s, (double)total, mixed);
 }
 
 // MIXED: fold the FP32 correction into the FP64 iterate.
@@ -468,13 +543,43 @@ struct Engine {
 
   void iteration_head(PcgScalars* s)
   {
+    if (h->fused_head) {
+      fused_head(s);
+      return;
+    }
+    const ApplyArgs a = ovl ? mas_apply_args(h) : ApplyArgs{};
     if (ovl)
-      mas_update_p<Tv>(h, V(h->vz), V(h->vp4), grows, s);
+      launch_pdl(h, k_update_p<Tv, true>, dim3(grows), dim3(kTpb), 0, a, V(h->vz), V(h->vp4), h->nb_int, s);
     else
-      launch_pdl(h, k_update_p<Tv>, dim3(grows), dim3(kTpb), 0, V(h->vz), V(h->vp4), h->nb_int, s);
+      launch_pdl(h, k_update_p<Tv, false>, dim3(grows), dim3(kTpb), 0, a, V(h->vz), V(h->vp4), h->nb_int, s);
     spmv(s);
     launch_pdl(h, k_update_xr<Tv, Tacc>, dim3(grows), dim3(kTpb), 0, V(h->vx), V(h->vr), V(h->vp4), V(h->vap),
                h->nb_int, mixed ? 1 : 0, partial(), s);
+  }
+
+  // The iteration head as one cooperative launch: one resident wave of CTAs.
+  template <bool kCoarse>
+  void fused_head_t(PcgScalars* s, const ApplyArgs& a)
+  {
+    constexpr bool kTiled = std::is_same<Tm, float>::value;
+    auto kern = k_iteration_head<Tm, Tv, Tacc, kTiled, kSpmvLanes, kCoarse>;
+    static int per_sm = 0;
+    if (!per_sm) {
+      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
+      MREQ(per_sm > 0, MASPCG_ERR_CUDA, "fused iteration kernel cannot be resident");
+    }
+    const int grid = std::max(1, std::min(ceil_div(h->nb_int, kTpb / kSpmvLanes), per_sm * h->sm_count));
+    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, h->rowptr.get(), h->colidx.get(), matrix(), V(h->vz),
+                       V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0, partial(), s,
+                       h->failed.get() + 4);
+  }
+
+  void fused_head(PcgScalars* s)
+  {
+    if (ovl)
+      fused_head_t<true>(s, mas_apply_args(h));
+    else
+      fused_head_t<false>(s, ApplyArgs{});
   }
 
   const Tm* matrix();
@@ -653,8 +758,9 @@ struct Engine {
       int terr = 0;
       MCK(cudaMemcpy(&terr, h->failed.get() + 4, sizeof(int), cudaMemcpyDeviceToHost));
       MREQ(terr == 0, MASPCG_ERR_CUDA,
-           terr == 2 ? "coarse-level dataflow queue overflow in the preconditioner apply"
-                     : "a TMA mbarrier wait expired in the preconditioner apply");
+           terr == 2   ? "coarse-level dataflow queue overflow in the preconditioner apply"
+           : terr == 3 ? "a grid barrier of the fused iteration kernel timed out"
+                       : "a TMA mbarrier wait expired in the preconditioner apply");
     }
     // final FP64 iterate
     if (mixed) {

@@ -77,6 +77,44 @@ __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode
   }
 }
 
+// Grid-wide barrier of a cooperative launch (every CTA resident).  The last
+// CTA to arrive resets the count and advances the generation word the
+// others wait on.  The wait is bounded: on expiry the CTA records error 3
+// and the barrier returns false (the caller then leaves; the host reports
+// the error after the graph).
+constexpr long long kBarrierLimit = 1ll << 24;
+
+__device__ __forceinline__ bool grid_barrier(PcgScalars* s, int* err)
+{
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &s->barrier_gen;
+    const unsigned g0 = *gen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&s->tickets[kTicketBarrier], 1u) == gridDim.x - 1) {
+      s->tickets[kTicketBarrier] = 0u;
+      __threadfence();
+      atomicAdd(&s->barrier_gen, 1u);
+    } else {
+      long long it = 0;
+      while (*gen == g0) {
+        if (++it > kBarrierLimit) {
+          ok = 0;
+          atomicExch(err, 3);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
 // r.z summed by two concurrent kernels (the level-0 apply and the coarse
 // levels): each stores its part and takes a ticket; the second adds the two
 // parts in a fixed order and updates the scalars (mode as in rz_update).

@@ -240,6 +240,25 @@ def test_mixed_solve_with_several_domains_per_warp(inverse):
     assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) <= 1e-4
 
 
+@pytest.mark.parametrize("flag", ["FLAG_FUSED_HEAD", "FLAG_PDL", "FLAG_SEQUENTIAL_COARSE", "FLAG_APPLY_STAGED2",
+                                  "FLAG_APPLY_REGISTERS"])
+def test_schedule_flags_solve_the_same_system(flag):
+    """Every kernel-schedule choice reaches the FP64-verified tolerance on a
+    system with several domains per warp, in about the same iterations
+    (the schedules differ only in floating-point summation order)."""
+    from agipc_learning_b200 import _native as N
+    s = synth.config_system(1, scale=40)
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16") as m:
+        _, base = m.solve(s.b)
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16", flags=getattr(N, flag)) as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged", res
+    assert res["rel_res_true"] <= 1e-4
+    assert abs(res["iterations"] - base["iterations"]) <= max(8, int(0.05 * base["iterations"]))
+    Ax = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
+    assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) <= 1e-4
+
+
 def test_block_jacobi_matches_oracle(cfg0):
     s = cfg0
     xo, ro, _ = oracle.solve_system(s, precond=oracle.PRECOND_DIAG3, gate=oracle.GATE_EUCLID)
