@@ -209,7 +209,9 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     h->scal.resize(1);
     h->grid_stream = 4 * h->sm_count;
     h->use_pdl = (c.flags & MASPCG_FLAG_PDL) != 0;
-    h->overlap_coarse = (c.flags & MASPCG_FLAG_SEQUENTIAL_COARSE) == 0;
+    // reference precision keeps the reference's r.z: summed over the fine
+    // rows after the coarse correction is added to z
+    h->overlap_coarse = (c.flags & MASPCG_FLAG_SEQUENTIAL_COARSE) == 0 && c.precision != MASPCG_PREC_REFERENCE;
     h->fused_head = (c.flags & MASPCG_FLAG_FUSED_HEAD) != 0;
     MCK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
     MCK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));

@@ -100,9 +100,9 @@ __device__ __forceinline__ void update_p_rows(const ApplyArgs& a, const Tv* __re
       if (slot >= 0 && slot < a.c0) {
         float cc[3];
         if (coarse_correction(a, slot, cc)) {
-          z0 = (Tv)((float)z0 + cc[0]);
-          z1 = (Tv)((float)z1 + cc[1]);
-          z2 = (Tv)((float)z2 + cc[2]);
+          z0 += (Tv)cc[0];
+          z1 += (Tv)cc[1];
+          z2 += (Tv)cc[2];
         }
       }
     }
@@ -141,45 +141,103 @@ __device__ __forceinline__ void load_block(const Tm* __restrict__ val, int t, Tm
   }
 }
 
-// Ap = A p for the rows this CTA strides over; returns this thread's share of
-// p.Ap.  LPR lanes per block row, each lane takes two blocks per step with
-// every load issued before the arithmetic; the next row's extent is fetched
-// while the current row is processed.
+// Ap = A p for block rows [lo, nrows) in the matrix's own precision;
+// returns this thread's share of p.Ap.  LPR lanes per block row and two row
+// groups per thread in flight at once (rows r and r + stride); each lane
+// takes two blocks of each row per step and issues all four blocks' loads
+// before the arithmetic.
 template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
 __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                          const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap, int nrows)
+                                          const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap, int lo,
+                                          int nrows)
 {
   using A = typename AccOf<Tm>::type;
   constexpr int kRows = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
   const int step = gridDim.x * kRows;
   Tacc dot = 0;
-  int row = blockIdx.x * kRows + threadIdx.x / LPR;
-  int rs = row < nrows ? __ldg(rowptr + row) : 0, re = row < nrows ? __ldg(rowptr + row + 1) : 0;
-  for (int row0 = blockIdx.x * kRows; row0 < nrows; row0 += step) {
-    const int nrow = row + step;
-    const int nrs = nrow < nrows ? __ldg(rowptr + nrow) : 0, nre = nrow < nrows ? __ldg(rowptr + nrow + 1) : 0;
-    A a0 = 0, a1 = 0, a2 = 0;
-    for (int t = rs + sub; t < re; t += 2 * LPR) {
-      const int u = t + LPR;
-      const bool two = u < re;
-      Tm m[9], q[9];
-      const int c = __ldcs(colidx + t);
-      const int d = two ? __ldcs(colidx + u) : c;
-      load_block<kTiled>(val, t, m);
-      if (two) {
-        load_block<kTiled>(val, u, q);
-      } else {
+  for (int row0 = lo + blockIdx.x * kRows; row0 < nrows; row0 += 2 * step) {
+    const int ra = row0 + threadIdx.x / LPR, rb = ra + step;
+    const bool oka = ra < nrows, okb = rb < nrows;
+    const int sa = oka ? __ldg(rowptr + ra) : 0, ea = oka ? __ldg(rowptr + ra + 1) : 0;
+    const int sb = okb ? __ldg(rowptr + rb) : 0, eb = okb ? __ldg(rowptr + rb + 1) : 0;
+    A a[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    const int na = (ea - sa + 2 * LPR - 1) / (2 * LPR), nbk = (eb - sb + 2 * LPR - 1) / (2 * LPR);
+    const int steps = max(__reduce_max_sync(kFull, (unsigned)na), __reduce_max_sync(kFull, (unsigned)nbk));
+    for (int k = 0; k < steps; ++k) {
+      int tt[4] = {sa + sub + 2 * LPR * k, sa + sub + 2 * LPR * k + LPR, sb + sub + 2 * LPR * k,
+                   sb + sub + 2 * LPR * k + LPR};
+      const bool in[4] = {tt[0] < ea, tt[1] < ea, tt[2] < eb, tt[3] < eb};
+      Tm m[4][9];
+      int c[4];
 #pragma unroll
-        for (int e = 0; e < 9; ++e) q[e] = Tm(0);
+      for (int j = 0; j < 4; ++j) {
+        c[j] = in[j] ? __ldcs(colidx + tt[j]) : 0;
+        if (in[j]) {
+          load_block<kTiled>(val, tt[j], m[j]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 9; ++e) m[j][e] = Tm(0);
+        }
       }
-      const P4<Tv> x = ld_p4(p4, c), y = ld_p4(p4, d);
-      a0 += (A)m[0] * (A)x.x + (A)m[1] * (A)x.y + (A)m[2] * (A)x.z;
-      a1 += (A)m[3] * (A)x.x + (A)m[4] * (A)x.y + (A)m[5] * (A)x.z;
-      a2 += (A)m[6] * (A)x.x + (A)m[7] * (A)x.y + (A)m[8] * (A)x.z;
-      a0 += (A)q[0] * (A)y.x + (A)q[1] * (A)y.y + (A)q[2] * (A)y.z;
-      a1 += (A)q[3] * (A)y.x + (A)q[4] * (A)y.y + (A)q[5] * (A)y.z;
-      a2 += (A)q[6] * (A)y.x + (A)q[7] * (A)y.y + (A)q[8] * (A)y.z;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const P4<Tv> x = ld_p4(p4, c[j]);
+        A* o = a[j >> 1];
+        o[0] += (A)m[j][0] * (A)x.x + (A)m[j][1] * (A)x.y + (A)m[j][2] * (A)x.z;
+        o[1] += (A)m[j][3] * (A)x.x + (A)m[j][4] * (A)x.y + (A)m[j][5] * (A)x.z;
+        o[2] += (A)m[j][6] * (A)x.x + (A)m[j][7] * (A)x.y + (A)m[j][8] * (A)x.z;
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) {
+        a[h][0] += __shfl_xor_sync(kFull, a[h][0], o, LPR);
+        a[h][1] += __shfl_xor_sync(kFull, a[h][1], o, LPR);
+        a[h][2] += __shfl_xor_sync(kFull, a[h][2], o, LPR);
+      }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = h ? rb : ra;
+      if (row < nrows && sub < 3) {
+        const Tv y = (Tv)(sub == 0 ? a[h][0] : (sub == 1 ? a[h][1] : a[h][2]));
+        ap[3 * (size_t)row + sub] = y;
+        const P4<Tv> pr = ld_p4(p4, row);
+        const Tv pv = sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z);
+        dot += (Tacc)pv * (Tacc)y;
+      }
+    }
+  }
+  return dot;
+}
+
+// Ap for block rows [0, n64) from the FP64 matrix with FP64 sums, used when
+// the iteration runs on the FP32 tiles: these are the affine-body rows, whose
+// 12x12 blocks carry the orthogonality stiffness (~1e7 on the diagonal)
+// beside rotation modes held only by the mass (~1e-4), a spread FP32 values
+// or sums cannot keep positive definite.
+template <typename Tv, typename Tacc, int LPR>
+__device__ __forceinline__ Tacc spmv_rows_exact(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                                const double* __restrict__ val64, const Tv* __restrict__ p4, Tv* ap,
+                                                int n64)
+{
+  constexpr int kRows = kTpb / LPR;
+  const int sub = threadIdx.x % LPR;
+  double dot = 0.0;
+  for (int row0 = blockIdx.x * kRows; row0 < n64; row0 += gridDim.x * kRows) {
+    const int row = row0 + threadIdx.x / LPR;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (row < n64) {
+      const int re = __ldg(rowptr + row + 1);
+      for (int t = __ldg(rowptr + row) + sub; t < re; t += LPR) {
+        double m[9];
+        load_block<false>(val64, t, m);
+        const P4<Tv> x = ld_p4(p4, __ldcs(colidx + t));
+        a0 += m[0] * (double)x.x + m[1] * (double)x.y + m[2] * (double)x.z;
+        a1 += m[3] * (double)x.x + m[4] * (double)x.y + m[5] * (double)x.z;
+        a2 += m[6] * (double)x.x + m[7] * (double)x.y + m[8] * (double)x.z;
+      }
     }
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) {
@@ -187,18 +245,26 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
       a1 += __shfl_xor_sync(kFull, a1, o, LPR);
       a2 += __shfl_xor_sync(kFull, a2, o, LPR);
     }
-    if (row < nrows && sub < 3) {
+    if (row < n64 && sub < 3) {
       const Tv y = (Tv)(sub == 0 ? a0 : (sub == 1 ? a1 : a2));
       ap[3 * (size_t)row + sub] = y;
       const P4<Tv> pr = ld_p4(p4, row);
-      const Tv pv = sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z);
-      dot += (Tacc)pv * (Tacc)y;
+      dot += (double)(sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z)) * (double)y;
     }
-    row = nrow;
-    rs = nrs;
-    re = nre;
   }
-  return dot;
+  return (Tacc)dot;
+}
+
+// Both parts of the product: rows [0, n64) exact (n64 is 0 for the FP64
+// matrix), the rest from `val`.
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
+__device__ __forceinline__ Tacc spmv_all(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                         const Tm* __restrict__ val, const double* __restrict__ val64, int n64,
+                                         const Tv* __restrict__ p4, Tv* ap, int nrows)
+{
+  Tacc dot = 0;
+  if (n64 > 0) dot = spmv_rows_exact<Tv, Tacc, LPR>(rowptr, colidx, val64, p4, ap, n64);
+  return dot + spmv_rows<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, p4, ap, n64, nrows);
 }
 
 // Last block of the SpMV: p.Ap and alpha (or a stop on curvature / NaN).
@@ -218,12 +284,13 @@ __device__ __forceinline__ void spmv_finish(PcgScalars* s, double pap)
 
 template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
 __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                                const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap,
-                                                int nrows, Tacc* partial, PcgScalars* s)
+                                                const Tm* __restrict__ val, const double* __restrict__ val64, int n64,
+                                                const Tv* __restrict__ p4, Tv* ap, int nrows, Tacc* partial,
+                                                PcgScalars* s)
 {
   pdl_wait();
   if (!running(s)) return;
-  const Tacc dot = spmv_rows<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, p4, ap, nrows);
+  const Tacc dot = spmv_all<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, val64, n64, p4, ap, nrows);
   pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
@@ -313,13 +380,14 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
 template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, bool kCoarse>
 __global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, const int* __restrict__ rowptr,
                                                           const int* __restrict__ colidx, const Tm* __restrict__ val,
+                                                          const double* __restrict__ val64, int n64,
                                                           const Tv* __restrict__ z, Tv* p4, Tv* ap, Tv* x, Tv* r,
                                                           int nrows, int mixed, Tacc* partial, PcgScalars* s, int* err)
 {
   if (!running(s)) return;  // uniform: no CTA of this launch has written the status yet
   update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
   if (!grid_barrier(s, err)) return;
-  const Tacc dot = spmv_rows<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, p4, ap, nrows);
+  const Tacc dot = spmv_all<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, val64, n64, p4, ap, nrows);
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0)
@@ -528,7 +596,9 @@ struct Engine {
       const bool bj = h->cfg.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI;
       const int mas_lo = mas ? h->fem_off : 0, mas_hi = mas ? h->fem_off + h->c0 : 0;
       const int bodies = (h->cfg.preconditioner == MASPCG_PRECOND_NONE) ? 0 : h->abd_bodies;
-      if (ref)
+      // affine bodies always apply their FP64 inverses: the 12x12 inverse
+      // spans the same ~1e11 spread as the body's Hessian block
+      if (ref || bodies > 0)
         launch_pdl(h, k_other_apply<Tv, Tacc, double>, dim3(gother), dim3(kTpb), 0, 
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv64.get(), bj ? h->diag_inv64.get() : nullptr,
             s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
@@ -569,8 +639,8 @@ struct Engine {
       MREQ(per_sm > 0, MASPCG_ERR_CUDA, "fused iteration kernel cannot be resident");
     }
     const int grid = std::max(1, std::min(ceil_div(h->nb_int, kTpb / kSpmvLanes), per_sm * h->sm_count));
-    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, h->rowptr.get(), h->colidx.get(), matrix(), V(h->vz),
-                       V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0, partial(), s,
+    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, h->rowptr.get(), h->colidx.get(), matrix(),
+                       h->val64.get(), exact_rows(), V(h->vz), V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0, partial(), s,
                        h->failed.get() + 4);
   }
 
@@ -583,6 +653,8 @@ struct Engine {
   }
 
   const Tm* matrix();
+  // block rows the FP32-tile SpMV takes from the FP64 matrix (the affine bodies)
+  int exact_rows() const { return std::is_same<Tm, float>::value ? 4 * h->abd_bodies : 0; }
 
   // SpMV rows per CTA step: kTpb / kSpmvLanes.
   static constexpr int kSpmvLanes = 8;
@@ -599,8 +671,10 @@ struct Engine {
     }
     const int grid = std::max(1, std::min(ceil_div(h->nb_int, rows), per_sm * h->sm_count));
     launch_pdl(h, k_spmv<Tm, Tv, Tacc, kTiled, kSpmvLanes>, dim3(grid), dim3(kTpb), 0, h->rowptr.get(),
-               h->colidx.get(), matrix(), V(h->vp4), V(h->vap), h->nb_int, partial(), s);
+               h->colidx.get(), matrix(), h->val64.get(), exact_rows(), V(h->vp4), V(h->vap), h->nb_int, partial(), s);
   }
+
+
 
   void true_residual(PcgScalars* s)
   {

@@ -97,7 +97,9 @@ typedef enum {
   MASPCG_FLAG_PDL = 1,                 /* launch iteration kernels with programmatic dependent launch */
   MASPCG_FLAG_APPLY_STAGED2 = 2,       /* 16-bit level-0 apply: two TMA slots per warp */
   MASPCG_FLAG_APPLY_REGISTERS = 4,     /* 16-bit level-0 apply: inverse held in registers */
-  MASPCG_FLAG_SEQUENTIAL_COARSE = 8,   /* run the MAS coarse levels before the level-0 apply, not beside it */
+  MASPCG_FLAG_SEQUENTIAL_COARSE = 8,   /* run the MAS coarse levels before the level-0 apply, not beside it
+                                          (always so in MASPCG_PREC_REFERENCE, whose r.z is then summed over
+                                          the fine rows as the reference sums it) */
   MASPCG_FLAG_FUSED_HEAD = 16          /* p update, SpMV and x/r update as one cooperative kernel with grid barriers */
 } maspcg_flags;
 

@@ -52,7 +52,7 @@ def _library_gradient(s, E, x_star, tol):
         loss = ((x - torch.tensor(x_star, device=dev)) ** 2).sum()
         loss.backward()
         gE = modulus_gradient(vals.grad, vals.detach(), torch.tensor(E, device=dev))
-    return x.detach().cpu().numpy(), b.grad.cpu().numpy(), gE.cpu().numpy(), float(loss)
+    return x.detach().cpu().numpy(), b.grad.cpu().numpy(), gE.cpu().numpy(), float(loss.detach())
 
 
 def test_adjoint_matches_dense_reference_and_fd_on_6cube():
