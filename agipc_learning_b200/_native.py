@@ -34,7 +34,7 @@ GATE_EUCLID = 1
 
 FLAG_PDL = 1
 FLAG_APPLY_STAGED2 = 2
-FLAG_APPLY_REGISTERS = 4
+FLAG_APPLY_DIRECT = 4
 FLAG_SEQUENTIAL_COARSE = 8
 FLAG_FUSED_HEAD = 16
 

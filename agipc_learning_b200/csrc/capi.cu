@@ -183,7 +183,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_NONE) ||
       c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~31) != 0 ||
-      ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_REGISTERS))) {
+      ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_DIRECT))) {
     g_create_error = "invalid configuration";
     return MASPCG_ERR_INVALID_ARGUMENT;
   }
@@ -216,7 +216,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     MCK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
     MCK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     MCK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-    h->apply_variant = (c.flags & MASPCG_FLAG_APPLY_STAGED2) ? 1 : (c.flags & MASPCG_FLAG_APPLY_REGISTERS) ? 0 : 2;
+    h->apply_variant = (c.flags & MASPCG_FLAG_APPLY_STAGED2) ? 1 : (c.flags & MASPCG_FLAG_APPLY_DIRECT) ? 0 : 2;
     h->failed.resize(8);
     MCK(cudaMemset(h->failed.get(), 0, 8 * sizeof(int)));
   } catch (const std::exception& e) {

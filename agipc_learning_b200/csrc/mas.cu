@@ -159,18 +159,6 @@ __global__ void __launch_bounds__(256) k_coarse_assemble(CoarseArgs a)
   if (node >= 0) flush(node);
 }
 
-// Location of the lower block (a,b), a >= b, in the 17-diagonal layout.
-__device__ __forceinline__ void lower_slot(int a, int b, int& l, int& d)
-{
-  if (a - b <= 16) {
-    l = b;
-    d = a - b;
-  } else {
-    l = a;
-    d = 32 - (a - b);
-  }
-}
-
 // One CTA per domain; thread (w,lane) owns block (w,lane) of the 96x96 FP64
 // matrix.  FP32 storage: in-place Gauss-Jordan inverse, symmetric layout.
 // 16-bit storage: Cholesky A = L L^T, W = L^-1, stored W S^-1 with column
@@ -395,177 +383,254 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
   }
   __syncthreads();
   if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
-  if (w >= lane) {
-    int l, d;
-    lower_slot(w, lane, l, d);
+  // tile store: lower blocks, and zeros for the upper elements that fall in
+  // a diagonal tile
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int jj = 0; jj < 3; ++jj) {
-        const double v = (w == lane && jj > i) ? 0.0 : xr[3 * i + jj] / (double)sscale[3 * lane + jj];
-        out[inv16_pos(d * 9 + 3 * i + jj, l)] = from_d<TI>(v);
-        if (w - lane == 16) out[inv16_pos(16 * 9 + 3 * i + jj, w)] = from_d<TI>(0.0);
-      }
-    if (w == lane) out[inv16_pos(kDiags * 9, lane)] = from_d<TI>(0.0);  // pad half of the last word
-  }
+    for (int jj = 0; jj < 3; ++jj) {
+      // (an upper element outside the diagonal tiles has no slot: a 3x3
+      // diagonal block can straddle a tile boundary)
+      const int row = 3 * w + i, col = 3 * lane + jj;
+      if (row >= col)
+        out[inv16_pos(row, col)] = from_d<TI>(xr[3 * i + jj] / (double)sscale[3 * lane + jj]);
+      else if ((row >> 4) == (col >> 4))
+        out[inv16_pos(row, col)] = from_d<TI>(0.0);
+    }
 }
 
 // ------------------------------------------------------------------ apply --
 
-// 16-bit halves of a packed word (element 2k low, 2k+1 high).
-template <typename TI>
-__device__ __forceinline__ float lo16(uint32_t w);
-template <typename TI>
-__device__ __forceinline__ float hi16(uint32_t w);
-template <>
-__device__ __forceinline__ float lo16<__nv_bfloat16>(uint32_t w)
+// z = (M x) for one domain held by one warp, FP32 storage: the symmetric
+// inverse, lane l holding block (l, (l + d) % 32) of diagonal d = 0..16, each
+// stored block serving both triangles through a shuffle.  x, y: the lane's
+// three rows.
+__device__ __forceinline__ void domain_apply(const float* __restrict__ inv, int lane, const float x[3], float y[3])
 {
-  return __uint_as_float(w << 16);
-}
-template <>
-__device__ __forceinline__ float hi16<__nv_bfloat16>(uint32_t w)
-{
-  return __uint_as_float(w & 0xffff0000u);
-}
-template <>
-__device__ __forceinline__ float lo16<__half>(uint32_t w)
-{
-  return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
-}
-template <>
-__device__ __forceinline__ float hi16<__half>(uint32_t w)
-{
-  return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+  const float x0 = x[0], x1 = x[1], x2 = x[2];
+  float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+#pragma unroll
+  for (int d = 0; d < kDiags; ++d) {
+    const int c = (lane + d) & 31;
+    const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
+    float B[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) B[e] = inv[(d * 9 + e) * kBank + lane];
+    y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
+    y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
+    y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
+    if (d != 0) {
+      const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
+      const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
+      const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
+      const int src = (lane - d) & 31;
+      y0 += __shfl_sync(kFull, t0, src);
+      y1 += __shfl_sync(kFull, t1, src);
+      y2 += __shfl_sync(kFull, t2, src);
+    }
+  }
+  y[0] = y0;
+  y[1] = y1;
+  y[2] = y2;
 }
 
-// z_l = (M x)_l for one domain held by one warp; x, y: the lane's 3 rows.
-// FP32 storage holds the symmetric inverse (each stored block serves both
-// triangles through a shuffle).  16-bit storage holds the scaled factor
-// V = W S^-1 of M = W^T W (W lower); the warp loads the domain's 77 words
-// per lane once (coalesced, streaming) into registers and runs the two
-// passes t = V (S x), y = S V^T t from there.  kShared: `inv` points to a
-// shared-memory copy of the domain record.
-template <typename TI, bool kShared = false>
-__device__ __forceinline__ void domain_apply(const TI* __restrict__ inv, const float* __restrict__ scale, int lane,
-                                             const float x[3], float y[3])
-{
-  if constexpr (std::is_same<TI, float>::value) {
-    const float x0 = x[0], x1 = x[1], x2 = x[2];
-    float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-#pragma unroll
-    for (int d = 0; d < kDiags; ++d) {
-      const int c = (lane + d) & 31;
-      const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
-      float B[9];
-#pragma unroll
-      for (int e = 0; e < 9; ++e) B[e] = inv[(d * 9 + e) * kBank + lane];
-      y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
-      y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
-      y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
-      if (d != 0) {
-        const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
-        const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
-        const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
-        const int src = (lane - d) & 31;
-        y0 += __shfl_sync(kFull, t0, src);
-        y1 += __shfl_sync(kFull, t1, src);
-        y2 += __shfl_sync(kFull, t2, src);
-      }
-    }
-    y[0] = y0;
-    y[1] = y1;
-    y[2] = y2;
-  } else {
-    const uint32_t* wp = reinterpret_cast<const uint32_t*>(inv) + lane;
-    // Global records are loaded once into registers (77 words per lane) and
-    // serve both passes; shared-memory records are read per diagonal in each
-    // pass (volatile: the compiler must not keep them live across passes).
-    uint32_t Wd[kShared ? 1 : kInvWords16];
-    if constexpr (!kShared) {
-#pragma unroll
-      for (int k = 0; k < kInvWords16; ++k) Wd[k] = __ldcs(wp + k * kBank);
-    }
-    auto diag = [&](int d, float B[9]) {
-      const int k0 = 9 * d, w0 = k0 >> 1;
-      uint32_t wv[5];
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        if constexpr (kShared)
-          wv[i] = (w0 + i < kInvWords16) ? reinterpret_cast<const volatile uint32_t*>(wp)[(w0 + i) * kBank] : 0u;
-        else
-          wv[i] = (w0 + i < kInvWords16) ? Wd[w0 + i] : 0u;
-      }
-#pragma unroll
-      for (int e = 0; e < 9; ++e) {
-        const int k = k0 + e;
-        B[e] = (k & 1) ? hi16<TI>(wv[(k >> 1) - w0]) : lo16<TI>(wv[(k >> 1) - w0]);
-      }
-    };
-    const float s0 = scale[3 * lane], s1 = scale[3 * lane + 1], s2 = scale[3 * lane + 2];
-    const float x0 = x[0] * s0, x1 = x[1] * s1, x2 = x[2] * s2;
-    // pass 1: t = V xs
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-#pragma unroll
-    for (int d = 0; d < kDiags; ++d) {
-      float B[9];
-      diag(d, B);
-      if (d == 0) {
-        t0 += B[0] * x0 + B[1] * x1 + B[2] * x2;
-        t1 += B[3] * x0 + B[4] * x1 + B[5] * x2;
-        t2 += B[6] * x0 + B[7] * x1 + B[8] * x2;
-      } else {
-        const int c = (lane + d) & 31;
-        const bool below = lane + d >= 32;  // stored block is V_{lane,c}, c < lane
-        const float c0 = __shfl_sync(kFull, x0, c), c1 = __shfl_sync(kFull, x1, c), c2 = __shfl_sync(kFull, x2, c);
-        const float u0 = below ? c0 : x0, u1 = below ? c1 : x1, u2 = below ? c2 : x2;
-        const float p0 = B[0] * u0 + B[1] * u1 + B[2] * u2;
-        const float p1 = B[3] * u0 + B[4] * u1 + B[5] * u2;
-        const float p2 = B[6] * u0 + B[7] * u1 + B[8] * u2;
-        const int src = (lane - d) & 31;
-        const float r0 = __shfl_sync(kFull, below ? 0.f : p0, src);
-        const float r1 = __shfl_sync(kFull, below ? 0.f : p1, src);
-        const float r2 = __shfl_sync(kFull, below ? 0.f : p2, src);
-        t0 += (below ? p0 : 0.f) + r0;
-        t1 += (below ? p1 : 0.f) + r1;
-        t2 += (below ? p2 : 0.f) + r2;
-      }
-    }
-    // pass 2: z = V^T t.  The empty asm keeps the packed words (77 registers)
-    // live instead of the 153 unpacked floats of pass 1.
-    if constexpr (!kShared) {
-#pragma unroll
-      for (int k = 0; k < kInvWords16; ++k) asm volatile("" : "+r"(Wd[k]));
-    }
-    float z0 = 0.f, z1 = 0.f, z2 = 0.f;
-#pragma unroll
-    for (int d = 0; d < kDiags; ++d) {
-      float B[9];
-      diag(d, B);
-      if (d == 0) {
-        z0 += B[0] * t0 + B[3] * t1 + B[6] * t2;
-        z1 += B[1] * t0 + B[4] * t1 + B[7] * t2;
-        z2 += B[2] * t0 + B[5] * t1 + B[8] * t2;
-      } else {
-        const int c = (lane + d) & 31;
-        const bool below = lane + d >= 32;
-        const float c0 = __shfl_sync(kFull, t0, c), c1 = __shfl_sync(kFull, t1, c), c2 = __shfl_sync(kFull, t2, c);
-        const float u0 = below ? t0 : c0, u1 = below ? t1 : c1, u2 = below ? t2 : c2;
-        const float p0 = B[0] * u0 + B[3] * u1 + B[6] * u2;
-        const float p1 = B[1] * u0 + B[4] * u1 + B[7] * u2;
-        const float p2 = B[2] * u0 + B[5] * u1 + B[8] * u2;
-        const int src = (lane - d) & 31;
-        const float r0 = __shfl_sync(kFull, below ? p0 : 0.f, src);
-        const float r1 = __shfl_sync(kFull, below ? p1 : 0.f, src);
-        const float r2 = __shfl_sync(kFull, below ? p2 : 0.f, src);
-        z0 += (below ? 0.f : p0) + r0;
-        z1 += (below ? 0.f : p1) + r1;
-        z2 += (below ? 0.f : p2) + r2;
-      }
-    }
-    y[0] = z0 * s0;
-    y[1] = z1 * s1;
-    y[2] = z2 * s2;
+// ---- tensor-core apply of a 16-bit factored record -------------------------
+//
+// M = S V^T V S with V the scaled lower factor (96 x 96, 21 tiles of 16 x 16
+// in shared memory, inv16_pos).  Pass 1, t = V (S x), multiplies each tile by
+// the matching 16 entries of the vector with mma.m16n8k16 (the tile as A);
+// pass 2, z = V^T t, does the same with the tiles loaded transposed
+// (ldmatrix .trans).  The FP32 vector enters the 16-bit B operand as three
+// terms, hi + mid + lo (each the rounding of what the previous ones leave),
+// in columns 0, 1, 2 of B, so the products carry the vector to FP32 precision
+// and the FP32 accumulators of the three columns are added afterwards.  FP16
+// records scale the vector by a power of two (its largest entry to [1, 2))
+// first, as FP16 has a narrow exponent range; the scaling is exact.
+constexpr int kPartStride = 104;             // 16-bit split terms: 3 rows of 104 (bank spread)
+constexpr int kApplyScratch = 1024;          // per warp: 96 FP32 + 3 x 104 16-bit
+constexpr int kRecBytes16 = kInvElems16 * 2;  // 10,752
+
+template <typename TI>
+struct Mma16;
+template <>
+struct Mma16<__nv_bfloat16> {
+  static constexpr bool kNormalize = false;
+  static __device__ __forceinline__ void mma(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1)
+  {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
   }
+  static __device__ __forceinline__ unsigned short to16(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+  static __device__ __forceinline__ float from16(unsigned short u) { return __uint_as_float((uint32_t)u << 16); }
+};
+template <>
+struct Mma16<__half> {
+  static constexpr bool kNormalize = true;
+  static __device__ __forceinline__ void mma(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1)
+  {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+  }
+  static __device__ __forceinline__ unsigned short to16(float v) { return __half_as_ushort(__float2half_rn(v)); }
+  static __device__ __forceinline__ float from16(unsigned short u) { return __half2float(__ushort_as_half(u)); }
+};
+
+__device__ __forceinline__ void ldsm(uint32_t addr, uint32_t a[4])
+{
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+               : "r"(addr)
+               : "memory");
+}
+__device__ __forceinline__ void ldsm_t(uint32_t addr, uint32_t a[4])
+{
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+               : "r"(addr)
+               : "memory");
+}
+
+// Power-of-two factor taking the warp's largest |v| to [1, 2) (1 when the
+// vector is zero or not finite), and its inverse.
+__device__ __forceinline__ void pow2_normalizer(const float v[3], float& f, float& fi)
+{
+  const float m = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
+  const unsigned mb = __reduce_max_sync(kFull, __float_as_uint(m));
+  int ex = (int)(mb >> 23) - 127;
+  if (mb == 0u || mb >= 0x7f800000u) ex = 0;
+  ex = max(-120, min(120, ex));
+  f = __uint_as_float((unsigned)(127 - ex) << 23);
+  fi = __uint_as_float((unsigned)(127 + ex) << 23);
+}
+
+// Three 16-bit terms of each of the lane's three entries (rows 3 lane + i).
+template <typename TI>
+__device__ __forceinline__ void split_store(unsigned short* part, int lane, const float v[3])
+{
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float r = v[i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const unsigned short u = Mma16<TI>::to16(r);
+      part[k * kPartStride + 3 * lane + i] = u;
+      r -= Mma16<TI>::from16(u);
+    }
+  }
+}
+
+// B operand of the 16 vector entries [16 K, 16 K + 16): thread (g, q) holds
+// column g (split term g; zero for g >= 3), rows 2q, 2q+1 and 2q+8, 2q+9.
+__device__ __forceinline__ void b_frag(const unsigned short* part, int K, int g, int q, uint32_t& b0, uint32_t& b1)
+{
+  b0 = b1 = 0u;
+  if (g < 3) {
+    const unsigned short* p = part + g * kPartStride + 16 * K + 2 * q;
+    b0 = *reinterpret_cast<const uint32_t*>(p);
+    b1 = *reinterpret_cast<const uint32_t*>(p + 8);
+  }
+}
+
+// Sum of the three split-term columns of 6 accumulator tiles into out[96]:
+// thread (g, q = 0) holds columns 0-1 of rows g and g + 8, thread (g, 1)
+// column 2.
+__device__ __forceinline__ void reduce_columns(float acc[6][4], float* out, int g, int q)
+{
+#pragma unroll
+  for (int I = 0; I < 6; ++I) {
+    float t0 = acc[I][0] + acc[I][1], t1 = acc[I][2] + acc[I][3];
+    t0 += __shfl_down_sync(kFull, t0, 1);
+    t1 += __shfl_down_sync(kFull, t1, 1);
+    if (q == 0) {
+      out[16 * I + g] = t0;
+      out[16 * I + g + 8] = t1;
+    }
+  }
+}
+
+// y = (M x) for one domain held by one warp: rec is the 16-bit record in
+// shared memory, scratch this warp's kApplyScratch bytes of shared memory.
+template <typename TI>
+__device__ __forceinline__ void domain_apply16(const TI* rec, unsigned char* scratch, const float* __restrict__ scale,
+                                               int lane, const float x[3], float y[3])
+{
+  using M = Mma16<TI>;
+  float* vf = reinterpret_cast<float*>(scratch);
+  unsigned short* part = reinterpret_cast<unsigned short*>(scratch + 96 * sizeof(float));
+  const int g = lane >> 2, q = lane & 3;
+  const int m = lane >> 3, rr = lane & 7;
+  const uint32_t base = (uint32_t)__cvta_generic_to_shared(rec);
+  const uint32_t off_n = ((((m & 1) << 3) + rr) << 5) + ((((m >> 1) ^ (rr >> 2)) & 1) << 4);
+  const uint32_t off_t = ((((m >> 1) << 3) + rr) << 5) + ((((m & 1) ^ (rr >> 2)) & 1) << 4);
+  const float s0 = scale[3 * lane], s1 = scale[3 * lane + 1], s2 = scale[3 * lane + 2];
+  float v[3] = {x[0] * s0, x[1] * s1, x[2] * s2};
+  float f1 = 1.f, fi1 = 1.f;
+  if constexpr (M::kNormalize) {
+    pow2_normalizer(v, f1, fi1);
+    v[0] *= f1;
+    v[1] *= f1;
+    v[2] *= f1;
+  }
+  split_store<TI>(part, lane, v);
+  __syncwarp();
+  // pass 1: t = V v
+  {
+    float acc[6][4];
+#pragma unroll
+    for (int I = 0; I < 6; ++I) acc[I][0] = acc[I][1] = acc[I][2] = acc[I][3] = 0.f;
+#pragma unroll
+    for (int K = 0; K < 6; ++K) {
+      uint32_t b0, b1;
+      b_frag(part, K, g, q, b0, b1);
+#pragma unroll
+      for (int I = K; I < 6; ++I) {
+        uint32_t a[4];
+        ldsm(base + (uint32_t)((I * (I + 1) / 2 + K) * 512) + off_n, a);
+        M::mma(acc[I], a, b0, b1);
+      }
+    }
+    reduce_columns(acc, vf, g, q);
+  }
+  __syncwarp();
+  v[0] = vf[3 * lane];
+  v[1] = vf[3 * lane + 1];
+  v[2] = vf[3 * lane + 2];
+  float f2 = 1.f, fi2 = 1.f;
+  if constexpr (M::kNormalize) {
+    pow2_normalizer(v, f2, fi2);
+    v[0] *= f2;
+    v[1] *= f2;
+    v[2] *= f2;
+  }
+  split_store<TI>(part, lane, v);
+  __syncwarp();
+  // pass 2: z = V^T t
+  {
+    float acc[6][4];
+#pragma unroll
+    for (int J = 0; J < 6; ++J) acc[J][0] = acc[J][1] = acc[J][2] = acc[J][3] = 0.f;
+#pragma unroll
+    for (int K = 0; K < 6; ++K) {
+      uint32_t b0, b1;
+      b_frag(part, K, g, q, b0, b1);
+#pragma unroll
+      for (int J = 0; J <= K; ++J) {
+        uint32_t a[4];
+        ldsm_t(base + (uint32_t)((K * (K + 1) / 2 + J) * 512) + off_t, a);
+        M::mma(acc[J], a, b0, b1);
+      }
+    }
+    reduce_columns(acc, vf, g, q);
+  }
+  __syncwarp();
+  const float back = fi1 * fi2;
+  y[0] = vf[3 * lane] * back * s0;
+  y[1] = vf[3 * lane + 1] * back * s1;
+  y[2] = vf[3 * lane + 2] * back * s2;
 }
 
 // Leader of each key group gets the group sum: with kFast a butterfly when
@@ -604,10 +669,23 @@ __device__ __forceinline__ void group_sum(int key, const float v[3], float out[3
   leader = (__ffs(grp) - 1) == (int)(threadIdx.x & 31);
 }
 
-// Domain-apply kernels: 4 warps per CTA; 16-bit storage keeps a domain's 77
-// packed words per lane in registers, so those instances get up to 168.
+// Copy a 16-bit domain record to a warp's shared-memory slot with coalesced
+// 16-byte loads (streaming: a record is read once per apply).
+__device__ __forceinline__ void stage_record(const uint4* __restrict__ src, unsigned char* slot, int lane)
+{
+  uint4* dst = reinterpret_cast<uint4*>(slot);
+  __syncwarp();
+#pragma unroll 7
+  for (int k = lane; k < kRecBytes16 / 16; k += 32) dst[k] = __ldcs(src + k);
+  __syncwarp();
+}
+
+// Domain-apply kernels: 4 warps per CTA.  16-bit records are staged in
+// shared memory (a record and the apply scratch per warp: 47,104 bytes per
+// CTA, four CTAs per SM).
 constexpr int kApplyTpb = 128;
-#define MAS_APPLY_BOUNDS(TI) __launch_bounds__(kApplyTpb, sizeof(TI) == 4 ? 4 : 3)
+constexpr int kDirectSmem16 = (kApplyTpb / 32) * (kRecBytes16 + kApplyScratch);
+#define MAS_APPLY_BOUNDS(TI) __launch_bounds__(kApplyTpb, 4)
 
 // ---- coarse levels in one kernel (restriction + coarse domain applies) ----
 //
@@ -628,7 +706,7 @@ constexpr int kChainApplySlots = 4;  // 16-bit domain records staged in shared m
 // Dynamic shared memory of k_coarse_chain: 16-bit records are staged (their
 // two passes then read shared memory), FP32 records are read from global.
 template <typename TI>
-constexpr int chain_smem_bytes() { return sizeof(TI) == 2 ? kChainApplySlots * kInvElems16 * 2 : 0; }
+constexpr int chain_smem_bytes() { return sizeof(TI) == 2 ? kChainApplySlots * (kRecBytes16 + kApplyScratch) : 0; }
 
 // One thread counts a finished unit, whose parents span global slots
 // [lo, hi], into the parent domains; domains it completes are appended to
@@ -752,8 +830,8 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
   __syncthreads();
   // apply the completed domains' inverses: 16-bit records are copied into a
   // shared-memory slot per warp with 77 coalesced loads per lane, so the
-  // per-diagonal reads of both passes hit shared memory
-  extern __shared__ __align__(16) uint32_t chain_slots[];
+  // tensor-core passes read it there
+  extern __shared__ __align__(16) unsigned char chain_slots[];
   const int n = tail_s;
   constexpr bool kStage = sizeof(TI) == 2;
   constexpr int kSlots = kStage ? kChainApplySlots : kChainWarps;
@@ -763,17 +841,14 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
       const size_t base = (size_t)(kBank * g + lane - a.c0) * 3;
       const float x[3] = {__ldcg(a.coarse_r + base), __ldcg(a.coarse_r + base + 1), __ldcg(a.coarse_r + base + 2)};
       float y[3];
-      const TI* rec = reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>();
       if constexpr (kStage) {
-        uint32_t* slot = chain_slots + (size_t)w * kInvWords16 * kBank;
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(rec);
-        __syncwarp();
-#pragma unroll 11
-        for (int k = 0; k < kInvWords16; ++k) slot[k * kBank + lane] = __ldcs(src + k * kBank + lane);
-        __syncwarp();
-        rec = reinterpret_cast<const TI*>(slot);
+        unsigned char* slot = chain_slots + (size_t)w * (kRecBytes16 + kApplyScratch);
+        stage_record(reinterpret_cast<const uint4*>(a.inv) + (size_t)g * (kRecBytes16 / 16), slot, lane);
+        domain_apply16<TI>(reinterpret_cast<const TI*>(slot), slot + kRecBytes16, a.scale + (size_t)g * 96, lane, x,
+                           y);
+      } else {
+        domain_apply(reinterpret_cast<const float*>(a.inv) + (size_t)g * kInvElems, lane, x, y);
       }
-      domain_apply<TI, true>(rec, a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
       a.coarse_z[base] = y[0];
       a.coarse_z[base + 1] = y[1];
       a.coarse_z[base + 2] = y[2];
@@ -860,8 +935,14 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
     const Tv r0 = r[row3], r1 = r[row3 + 1], r2 = r[row3 + 2];
     const float x[3] = {(float)r0, (float)r1, (float)r2};
     float y[3];
-    domain_apply<TI>(reinterpret_cast<const TI*>(a.inv) + (size_t)g * inv_elems<TI>(),
-                     a.scale ? a.scale + (size_t)g * 96 : nullptr, lane, x, y);
+    if constexpr (sizeof(TI) == 2) {
+      extern __shared__ __align__(16) unsigned char direct_slots[];
+      unsigned char* slot = direct_slots + (size_t)(threadIdx.x >> 5) * (kRecBytes16 + kApplyScratch);
+      stage_record(reinterpret_cast<const uint4*>(a.inv) + (size_t)g * (kRecBytes16 / 16), slot, lane);
+      domain_apply16<TI>(reinterpret_cast<const TI*>(slot), slot + kRecBytes16, a.scale + (size_t)g * 96, lane, x, y);
+    } else {
+      domain_apply(reinterpret_cast<const float*>(a.inv) + (size_t)g * kInvElems, lane, x, y);
+    }
     float cc[3];
     const bool real = coarse_add ? coarse_correction(a, slot, cc) : a.pmr[slot] >= 0;
     if (!real) {
@@ -902,7 +983,7 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
 constexpr int kApplyWarps = 4;
 
 template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf>
-__global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
+__global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     k_apply_tma(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                 PcgScalars* s, int g_begin, int g_end, int* err, int coarse_add, int pair)
 {
@@ -910,11 +991,12 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
   __shared__ __align__(8) uint64_t bar[kApplyWarps][kBuf];
   pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  constexpr unsigned kBytes = inv_elems<TI>() * sizeof(TI);
+  static_assert(sizeof(TI) == 2, "the staged apply holds 16-bit records");
+  constexpr unsigned kBytes = kRecBytes16;
   const int lw = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warps_total = gridDim.x * kApplyWarps;
   const int gw = blockIdx.x * kApplyWarps + lw;
-  unsigned char* buf = smem + (size_t)lw * kBuf * kBytes;
+  unsigned char* buf = smem + (size_t)lw * (kBuf * kBytes + kApplyScratch);
   const TI* inv = reinterpret_cast<const TI*>(a.inv);
   if (lane == 0) {
 #pragma unroll
@@ -959,7 +1041,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 5 : 2)
       x[1] = a.coarse_r[base + 1];
       x[2] = a.coarse_r[base + 2];
     }
-    domain_apply<TI, true>(blk, sc, lane, x, y);
+    domain_apply16<TI>(blk, buf + kBuf * kBytes, sc, lane, x, y);
     __syncwarp();
     const int gn = g + kBuf * warps_total;
     if (lane == 0 && gn < g_end) {
@@ -1178,14 +1260,14 @@ ApplyArgs make_apply_args(maspcg_handle* h)
 }
 
 // Level-0 domain apply variants (the solve uses h->apply_variant).
-enum ApplyVariant { kApplyRegisters = 0, kApplyStaged2 = 1, kApplyStaged1 = 2 };
+enum ApplyVariant { kApplyDirect = 0, kApplyStaged2 = 1, kApplyStaged1 = 2 };
 
 template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf>
 void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, Tacc* partial, int part_base,
                       int total_parts, int mode, PcgScalars* s, int g_begin, int g_end, int grid, int coarse_add,
                       int pair)
 {
-  constexpr int bytes = kApplyWarps * kBuf * inv_elems<TI>() * (int)sizeof(TI);
+  constexpr int bytes = kApplyWarps * (kBuf * kRecBytes16 + kApplyScratch);
   static bool configured = false;
   if (!configured) {
     MCK(cudaFuncSetAttribute(k_apply_tma<TI, Tv, Tacc, kLevel0, kBuf>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1199,7 +1281,7 @@ void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, 
 // CTAs of a staged apply over `domains` domains: one wave of resident CTAs.
 inline int staged_grid(const maspcg_handle* h, int domains, int kbuf)
 {
-  return std::max(1, std::min(ceil_div(domains, kApplyWarps), (kbuf == 1 ? 5 : 2) * h->sm_count));
+  return std::max(1, std::min(ceil_div(domains, kApplyWarps), (kbuf == 1 ? 4 : 2) * h->sm_count));
 }
 
 // CTAs of the level-0 apply in a variant.  The r.z partial sums occupy one
@@ -1207,11 +1289,13 @@ inline int staged_grid(const maspcg_handle* h, int domains, int kbuf)
 inline int level0_grid(const maspcg_handle* h, int variant)
 {
   const int d0 = h->lv.dom_begin[1];
-  if (h->cfg.inverse_storage == MASPCG_INV_FP32) variant = kApplyRegisters;
+  if (h->cfg.inverse_storage == MASPCG_INV_FP32) variant = kApplyDirect;
   switch (variant) {
     case kApplyStaged2: return staged_grid(h, d0, 2);
     case kApplyStaged1: return staged_grid(h, d0, 1);
-    default: return std::max(1, std::min(ceil_div((long long)d0 * 32, kApplyTpb), 16 * h->sm_count));
+    default:
+      return std::max(1, std::min(ceil_div((long long)d0 * 32, kApplyTpb),
+                                  (h->cfg.inverse_storage == MASPCG_INV_FP32 ? 16 : 4) * h->sm_count));
   }
 }
 
@@ -1223,19 +1307,22 @@ void level0_apply(maspcg_handle* h, const ApplyArgs& a, int variant, const Tv* r
                   int total_parts, int mode, PcgScalars* s, int grid0, int coarse_add = 1, int pair = 0)
 {
   const int d0 = h->lv.dom_begin[1];
-  if (std::is_same<TI, float>::value) variant = kApplyRegisters;
+  if (std::is_same<TI, float>::value) variant = kApplyDirect;
   // grid0 == level0_grid(h, variant): every CTA owns one r.z slot
   switch (variant) {
     case kApplyStaged2:
-      launch_apply_tma<TI, Tv, Tacc, true, 2>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
-                                              coarse_add, pair);
+      if constexpr (sizeof(TI) == 2)
+        launch_apply_tma<TI, Tv, Tacc, true, 2>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
+                                                coarse_add, pair);
       break;
     case kApplyStaged1:
-      launch_apply_tma<TI, Tv, Tacc, true, 1>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
-                                              coarse_add, pair);
+      if constexpr (sizeof(TI) == 2)
+        launch_apply_tma<TI, Tv, Tacc, true, 1>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
+                                                coarse_add, pair);
       break;
     default:
-      launch_pdl(h, k_level0_apply<TI, Tv, Tacc>, dim3(grid0), dim3(kApplyTpb), 0, a, r, z, partial, part_base,
+      launch_pdl(h, k_level0_apply<TI, Tv, Tacc>, dim3(grid0), dim3(kApplyTpb), sizeof(TI) == 2 ? kDirectSmem16 : 0,
+                 a, r, z, partial, part_base,
                  total_parts, mode, s, coarse_add, pair);
       break;
   }
@@ -1263,7 +1350,7 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
 {
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
-  const int variant = std::is_same<TI, float>::value ? (int)kApplyRegisters : h->apply_variant;
+  const int variant = std::is_same<TI, float>::value ? (int)kApplyDirect : h->apply_variant;
   if (lv.levelnum <= 1) {
     level0_apply<TI, Tv, Tacc>(h, a, variant, r, z, partial, part_base, total_parts, mode, s, grid0);
     return;
@@ -1319,9 +1406,9 @@ void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int gr
       break;
     case MASPCG_INV_FP16: level0_apply<__half, Tv, Tacc>(h, a, variant, r, z, partial, 0, grid, 0, s, grid); break;
     default:
-      MREQ(variant == kApplyRegisters || variant == h->apply_variant, MASPCG_ERR_UNSUPPORTED,
+      MREQ(variant == kApplyDirect || variant == h->apply_variant, MASPCG_ERR_UNSUPPORTED,
            "the staged apply exists for 16-bit inverses only");
-      level0_apply<float, Tv, Tacc>(h, a, kApplyRegisters, r, z, partial, 0, grid, 0, s, grid);
+      level0_apply<float, Tv, Tacc>(h, a, kApplyDirect, r, z, partial, 0, grid, 0, s, grid);
       break;
   }
   MCK(cudaGetLastError());
@@ -1402,17 +1489,9 @@ void decode_inverses(maspcg_handle* h, float* out)
   for (int g = 0; g < D; ++g) {
     std::fill(W.begin(), W.end(), 0.0);
     const float* scg = sc.data() + (size_t)g * 96;
-    for (int d = 0; d < kDiags; ++d)
-      for (int l = 0; l < kBank; ++l) {
-        if (d == 16 && l >= 16) continue;
-        const int c = (l + d) & 31;
-        const int ra = (d == 0 || l + d >= 32) ? l : c;  // block row (the larger index)
-        const int cb = (d == 0 || l + d >= 32) ? c : l;
-        for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j)
-            W[(3 * ra + i) * 96 + 3 * cb + j] =
-                (double)elem((size_t)g * kInvElems16 + (size_t)inv16_pos(d * 9 + 3 * i + j, l)) * scg[3 * cb + j];
-      }
+    for (int i = 0; i < 96; ++i)
+      for (int j = 0; j <= i; ++j)
+        W[i * 96 + j] = (double)elem((size_t)g * kInvElems16 + (size_t)inv16_pos(i, j)) * scg[j];
     for (int r = 0; r < 96; ++r)
       for (int q = r; q < 96; ++q) {
         double acc = 0;

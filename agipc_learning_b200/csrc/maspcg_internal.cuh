@@ -34,20 +34,28 @@ constexpr int kBank = 32;
 constexpr int kPacked = kBank * (kBank + 1) / 2;  // 528
 constexpr int kDiags = 17;
 constexpr int kInvElems = kDiags * 9 * kBank;      // 4896 stored elements per domain (FP32)
-// 16-bit storage packs each lane's 153 elements (17 diagonals x 9, in order
-// 9d + e) two per 32-bit word, word-major: word w of lane l at [w][l]; the
-// high half of the last word is zero.  A warp reads a domain in 77 coalesced
-// 128-byte loads and keeps it in registers for the two factored passes.
-constexpr int kInvWords16 = (kDiags * 9 + 1) / 2;  // 77
-constexpr int kInvElems16 = 2 * kInvWords16 * kBank;  // 4928 stored 16-bit elements per domain
+// 16-bit storage holds the lower triangle of the scaled 96x96 factor as the
+// 21 tiles (I >= J, tile T = I(I+1)/2 + J) of 16x16 elements that the
+// tensor-core apply reads with ldmatrix: row r of a tile at 16 r elements,
+// its two 8-element halves swapped when bit 2 of r is set, so the eight rows
+// of one 8x8 ldmatrix operand fall in distinct shared-memory banks.  Upper
+// elements of the diagonal tiles are zero.  A domain record is 10,752 bytes,
+// copied to shared memory as one bulk copy.
+constexpr int kTiles16 = 21;
+constexpr int kInvElems16 = kTiles16 * 256;  // 5376 stored 16-bit elements per domain
 
 // Stored elements per domain for an inverse element type.
 template <typename TI>
 constexpr int inv_elems() { return sizeof(TI) == 4 ? kInvElems : kInvElems16; }
 inline int inv_elems_for(int storage) { return storage == MASPCG_INV_FP32 ? kInvElems : kInvElems16; }
 
-// Position of element k (= 9d + e) of lane l in a 16-bit domain record.
-__host__ __device__ __forceinline__ int inv16_pos(int k, int l) { return ((k >> 1) * kBank + l) * 2 + (k & 1); }
+// Position of element (i, j) of a 16-bit domain record: i >= j, or i < j
+// inside a diagonal tile.
+__host__ __device__ __forceinline__ int inv16_pos(int i, int j)
+{
+  const int I = i >> 4, J = j >> 4, r = i & 15, c = j & 15;
+  return (I * (I + 1) / 2 + J) * 256 + r * 16 + ((((c >> 3) ^ (r >> 2)) & 1) << 3) + (c & 7);
+}
 constexpr int kMaxLevels = 6;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -236,7 +244,7 @@ struct maspcg_handle {
   bool use_pdl = false;           // programmatic dependent launch for the iteration kernels (MASPCG_FLAG_PDL)
   bool fused_head = false;        // p update + SpMV + x/r update as one cooperative kernel (MASPCG_FLAG_FUSED_HEAD)
   bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
-  int apply_variant = 2;          // 16-bit level-0 apply: 0 registers, 1 TMA-staged x2 buffers, 2 TMA-staged x1
+  int apply_variant = 2;          // 16-bit level-0 apply: 0 direct loads, 1 TMA-staged x2 buffers, 2 TMA-staged x1
 };
 
 namespace maspcg {

@@ -265,11 +265,12 @@ def run_ours(args, world, rank, local):
     ms_prec = stage(1, 20)
     ms_l0 = stage(2, 20)
     ms_factor = stage(3, 3)
-    ms_l0_variants = {"tma_staged_x2": stage(4, 20), "tma_staged_x1": stage(5, 20), "registers": stage(6, 20)}
+    ms_l0_variants = {"tma_staged_x2": stage(4, 20), "tma_staged_x1": stage(5, 20), "direct_loads": stage(6, 20)}
     nbi, bf = info["internal_block_rows"], info["bcsr_blocks"]
     d0 = s.fem_count // 32 if s.fem_count % 32 == 0 else (s.fem_count + 31) // 32
     spmv_bytes = 40 * bf + 4 * (nbi + 1) + 8 * (3 * nbi)
-    l0_bytes = d0 * (528 * 9 * 2 + 96 * 4) + 3 * 4 * 32 * d0 * 3
+    # per domain: the 16-bit record (21 tiles of 16x16, 10,752 B), 96 column scales, r and z (FP32) and the slot map
+    l0_bytes = d0 * (10752 + 96 * 4) + 3 * 4 * 32 * d0 * 3
     peak, peak_kind = peaks()
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "k_spmv_cube64_contacts_traffic.json")

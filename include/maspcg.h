@@ -96,7 +96,7 @@ typedef struct {
 typedef enum {
   MASPCG_FLAG_PDL = 1,                 /* launch iteration kernels with programmatic dependent launch */
   MASPCG_FLAG_APPLY_STAGED2 = 2,       /* 16-bit level-0 apply: two TMA slots per warp */
-  MASPCG_FLAG_APPLY_REGISTERS = 4,     /* 16-bit level-0 apply: inverse held in registers */
+  MASPCG_FLAG_APPLY_DIRECT = 4,        /* 16-bit level-0 apply: records staged by per-lane loads, no TMA */
   MASPCG_FLAG_SEQUENTIAL_COARSE = 8,   /* run the MAS coarse levels before the level-0 apply, not beside it
                                           (always so in MASPCG_PREC_REFERENCE, whose r.z is then summed over
                                           the fine rows as the reference sums it) */
@@ -247,10 +247,10 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
  *   1  full preconditioner apply z = M^-1 r, working precision
  *   2  MAS level-0 domain apply alone (restriction/coarse levels excluded)
  *   3  MAS domain assembly + inversion (build)
- *   4  MAS level-0 domain apply, 16-bit inverses staged in shared memory by
- *      TMA bulk copies, two slots per warp
+ *   4  MAS level-0 domain apply (tensor-core passes over 16-bit records staged
+ *      in shared memory by TMA bulk copies), two slots per warp
  *   5  the same with one slot per warp (more warps per SM; the solve's choice)
- *   6  the same apply with the inverse loaded into registers (no staging)
+ *   6  the same apply with each record staged by per-lane 16-byte loads (no TMA)
  *   (stage 2 times the variant the solve uses; 4-6 exist to compare them)
  * Vector contents are left unspecified afterwards. */
 MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);
