@@ -553,10 +553,11 @@ __device__ __forceinline__ void reduce_columns(float acc[6][4], float* out, int 
 }
 
 // y = (M x) for one domain held by one warp: rec is the 16-bit record in
-// shared memory, scratch this warp's kApplyScratch bytes of shared memory.
+// shared memory, scratch this warp's kApplyScratch bytes of shared memory,
+// sc the lane's three column scales.
 template <typename TI>
-__device__ __forceinline__ void domain_apply16(const TI* rec, unsigned char* scratch, const float* __restrict__ scale,
-                                               int lane, const float x[3], float y[3])
+__device__ __forceinline__ void domain_apply16(const TI* rec, unsigned char* scratch, const float sc[3], int lane,
+                                               const float x[3], float y[3])
 {
   using M = Mma16<TI>;
   float* vf = reinterpret_cast<float*>(scratch);
@@ -566,7 +567,7 @@ __device__ __forceinline__ void domain_apply16(const TI* rec, unsigned char* scr
   const uint32_t base = (uint32_t)__cvta_generic_to_shared(rec);
   const uint32_t off_n = ((((m & 1) << 3) + rr) << 5) + ((((m >> 1) ^ (rr >> 2)) & 1) << 4);
   const uint32_t off_t = ((((m >> 1) << 3) + rr) << 5) + ((((m & 1) ^ (rr >> 2)) & 1) << 4);
-  const float s0 = scale[3 * lane], s1 = scale[3 * lane + 1], s2 = scale[3 * lane + 2];
+  const float s0 = sc[0], s1 = sc[1], s2 = sc[2];
   float v[3] = {x[0] * s0, x[1] * s1, x[2] * s2};
   float f1 = 1.f, fi1 = 1.f;
   if constexpr (M::kNormalize) {
@@ -690,8 +691,8 @@ constexpr int kDirectSmem16 = (kApplyTpb / 32) * (kRecBytes16 + kApplyScratch);
 // ---- coarse levels in one kernel (restriction + coarse domain applies) ----
 //
 // BuildMultiLevelR and the coarse part of _schwarzLocalXSym6 as a dataflow
-// over the hierarchy.  CTA c restricts level-0 banks [8c, 8c + 8) (one warp
-// each) into level-1 nodes.  A coarse domain (32 consecutive nodes of level
+// over the hierarchy.  CTA c restricts level-0 banks [16c, 16c + 16) (two
+// per warp, so one resident wave of CTAs covers them) into level-1 nodes.  A coarse domain (32 consecutive nodes of level
 // l >= 1) is complete once every unit that writes one of its nodes has
 // finished; each unit counts itself into the domains its parents fall in,
 // and the unit that completes a domain processes it in the same CTA:
@@ -700,6 +701,8 @@ constexpr int kDirectSmem16 = (kApplyTpb / 32) * (kRecBytes16 + kApplyScratch);
 // in lane order), so the result does not depend on which CTA finishes last;
 // nothing waits.  Counters return to zero as they complete.
 constexpr int kChainWarps = 8;
+constexpr int kChainBanks = 2;                          // level-0 banks each warp restricts
+constexpr int kChainUnitBanks = kChainWarps * kChainBanks;  // banks per CTA: one resident wave covers them
 constexpr int kChainQueue = 64;
 constexpr int kChainApplySlots = 4;  // 16-bit domain records staged in shared memory at a time
 
@@ -756,28 +759,32 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
     hi_s = -1;
   }
   __syncthreads();
-  // level 0 -> level 1 (RestrictR of the fine residual)
-  const int bank = blockIdx.x * kChainWarps + w;
-  if (bank < a.c0 / kBank) {
-    const int slot = bank * kBank + lane;
-    const int key = a.cmap1[slot];
-    const Tv* rp = r + 3 * (size_t)(a.fem_off + slot);
-    const float v[3] = {(float)rp[0], (float)rp[1], (float)rp[2]};
-    float o[3];
-    bool leader;
-    group_sum<true>(key >= 0 ? key : -1 - lane, v, o, leader);
-    if (leader && key >= 0) {
-      float* d = a.coarse_r + 3 * (size_t)key;
-      d[0] = o[0];
-      d[1] = o[1];
-      d[2] = o[2];
-    }
-    const int lo = (int)__reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0x7fffffffu);
-    const int hi = (int)__reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
-    const bool any = __any_sync(kFull, key >= 0);  // every lane votes
-    if (lane == 0 && any) {
-      atomicMin(&lo_s, a.c0 + lo);
-      atomicMax(&hi_s, a.c0 + hi);
+  // level 0 -> level 1 (RestrictR of the fine residual); a level-1 node's
+  // children all lie in one bank, so its sum is written, not accumulated
+#pragma unroll
+  for (int k = 0; k < kChainBanks; ++k) {
+    const int bank = blockIdx.x * kChainUnitBanks + k * kChainWarps + w;
+    if (bank < a.c0 / kBank) {
+      const int slot = bank * kBank + lane;
+      const int key = a.cmap1[slot];
+      const Tv* rp = r + 3 * (size_t)(a.fem_off + slot);
+      const float v[3] = {(float)rp[0], (float)rp[1], (float)rp[2]};
+      float o[3];
+      bool leader;
+      group_sum<true>(key >= 0 ? key : -1 - lane, v, o, leader);
+      if (leader && key >= 0) {
+        float* d = a.coarse_r + 3 * (size_t)key;
+        d[0] = o[0];
+        d[1] = o[1];
+        d[2] = o[2];
+      }
+      const int lo = (int)__reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0x7fffffffu);
+      const int hi = (int)__reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
+      const bool any = __any_sync(kFull, key >= 0);  // every lane votes
+      if (lane == 0 && any) {
+        atomicMin(&lo_s, a.c0 + lo);
+        atomicMax(&hi_s, a.c0 + hi);
+      }
     }
   }
   pdl_trigger();
@@ -844,8 +851,9 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
       if constexpr (kStage) {
         unsigned char* slot = chain_slots + (size_t)w * (kRecBytes16 + kApplyScratch);
         stage_record(reinterpret_cast<const uint4*>(a.inv) + (size_t)g * (kRecBytes16 / 16), slot, lane);
-        domain_apply16<TI>(reinterpret_cast<const TI*>(slot), slot + kRecBytes16, a.scale + (size_t)g * 96, lane, x,
-                           y);
+        const float* scg = a.scale + (size_t)g * 96 + 3 * lane;
+        const float sc[3] = {scg[0], scg[1], scg[2]};
+        domain_apply16<TI>(reinterpret_cast<const TI*>(slot), slot + kRecBytes16, sc, lane, x, y);
       } else {
         domain_apply(reinterpret_cast<const float*>(a.inv) + (size_t)g * kInvElems, lane, x, y);
       }
@@ -885,10 +893,10 @@ __global__ void k_chain_targets(ApplyArgs a, int* target)
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int d1 = a.lv.dom_begin[1];
-  const int units0 = (a.c0 / kBank + kChainWarps - 1) / kChainWarps;
+  const int units0 = (a.c0 / kBank + kChainUnitBanks - 1) / kChainUnitBanks;
   int lo = 0x7fffffff, hi = -1;
   if (gw < units0) {
-    for (int b = gw * kChainWarps; b < min((gw + 1) * kChainWarps, a.c0 / kBank); ++b) {
+    for (int b = gw * kChainUnitBanks; b < min((gw + 1) * kChainUnitBanks, a.c0 / kBank); ++b) {
       const int key = a.cmap1[b * kBank + lane];
       const int l2 = (int)__reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0x7fffffffu);
       const int h2 = (int)__reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
@@ -939,7 +947,9 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
       extern __shared__ __align__(16) unsigned char direct_slots[];
       unsigned char* slot = direct_slots + (size_t)(threadIdx.x >> 5) * (kRecBytes16 + kApplyScratch);
       stage_record(reinterpret_cast<const uint4*>(a.inv) + (size_t)g * (kRecBytes16 / 16), slot, lane);
-      domain_apply16<TI>(reinterpret_cast<const TI*>(slot), slot + kRecBytes16, a.scale + (size_t)g * 96, lane, x, y);
+      const float* scg = a.scale + (size_t)g * 96 + 3 * lane;
+      const float sc[3] = {scg[0], scg[1], scg[2]};
+      domain_apply16<TI>(reinterpret_cast<const TI*>(slot), slot + kRecBytes16, sc, lane, x, y);
     } else {
       domain_apply(reinterpret_cast<const float*>(a.inv) + (size_t)g * kInvElems, lane, x, y);
     }
@@ -1020,6 +1030,28 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
   bool ok = true;
   for (int g = g_begin + gw; g < g_end; g += warps_total, ++i) {
     const int st = kBuf == 1 ? 0 : (i & 1);
+    // loads that do not depend on the record go out before its wait
+    const float* scg = a.scale + (size_t)g * 96 + 3 * lane;
+    const float sc[3] = {__ldg(scg), __ldg(scg + 1), __ldg(scg + 2)};
+    float x[3], y[3];
+    Tv rv[3];
+    size_t base;
+    if (kLevel0) {
+      base = 3 * (size_t)(a.fem_off + kBank * g + lane);
+      rv[0] = r[base];
+      rv[1] = r[base + 1];
+      rv[2] = r[base + 2];
+      x[0] = (float)rv[0];
+      x[1] = (float)rv[1];
+      x[2] = (float)rv[2];
+    } else {
+      base = (size_t)(kBank * g + lane - a.c0) * 3;
+      x[0] = a.coarse_r[base];
+      x[1] = a.coarse_r[base + 1];
+      x[2] = a.coarse_r[base + 2];
+      rv[0] = rv[1] = rv[2] = Tv(0);
+    }
+    const bool padded = kLevel0 && !coarse_add && a.pmr[kBank * g + lane] < 0;
     const bool w = mbar_wait(&bar[lw][st], ph[st]);
     if (w) ph[st] ^= 1u;
     if (!__all_sync(kFull, w)) {
@@ -1027,20 +1059,6 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
       break;
     }
     const TI* blk = reinterpret_cast<const TI*>(buf + st * kBytes);
-    const float* sc = a.scale + (size_t)g * 96;
-    float x[3], y[3];
-    size_t base;
-    if (kLevel0) {
-      base = 3 * (size_t)(a.fem_off + kBank * g + lane);
-      x[0] = (float)r[base];
-      x[1] = (float)r[base + 1];
-      x[2] = (float)r[base + 2];
-    } else {
-      base = (size_t)(kBank * g + lane - a.c0) * 3;
-      x[0] = a.coarse_r[base];
-      x[1] = a.coarse_r[base + 1];
-      x[2] = a.coarse_r[base + 2];
-    }
     domain_apply16<TI>(blk, buf + kBuf * kBytes, sc, lane, x, y);
     __syncwarp();
     const int gn = g + kBuf * warps_total;
@@ -1052,7 +1070,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     if (kLevel0) {
       const int slot = kBank * g + lane;
       float cc[3];
-      const bool real = coarse_add ? coarse_correction(a, slot, cc) : a.pmr[slot] >= 0;
+      const bool real = coarse_add ? coarse_correction(a, slot, cc) : !padded;
       if (!real) {
         y[0] = y[1] = y[2] = 0.f;
       } else if (coarse_add) {
@@ -1064,7 +1082,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
       for (int q = 0; q < 3; ++q) {
         const Tv zv = (Tv)y[q];
         z[base + q] = zv;
-        dot += (Tacc)r[base + q] * (Tacc)zv;
+        dot += (Tacc)rv[q] * (Tacc)zv;
       }
     } else {
       a.coarse_z[base] = y[0];
@@ -1151,7 +1169,7 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   MCK(cudaMemsetAsync(h->chain_target.get(), 0, h->chain_target.bytes(), st));
   if (lv.levelnum > 1) {
     const ApplyArgs aa = make_apply_args(h);
-    const long long units = (c0 / kBank + kChainWarps - 1) / kChainWarps + coarse_domains;
+    const long long units = (c0 / kBank + kChainUnitBanks - 1) / kChainUnitBanks + coarse_domains;
     k_chain_targets<<<ceil_div(units * 32, kTpb), kTpb, 0, st>>>(aa, h->chain_target.get());
     MLAUNCHED(h);
   }
@@ -1336,7 +1354,7 @@ void launch_chain(maspcg_handle* h, cudaStream_t st, const ApplyArgs& a, const T
   if (!configured && bytes > 48 * 1024)
     MCK(cudaFuncSetAttribute(k_coarse_chain<TI, Tv>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   configured = true;
-  launch_pdl_on(h, st, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainWarps)), dim3(kChainWarps * 32),
+  launch_pdl_on(h, st, k_coarse_chain<TI, Tv>, dim3(ceil_div(h->c0 / kBank, kChainUnitBanks)), dim3(kChainWarps * 32),
                 bytes, a, r, s, mode, pair);
 }
 
