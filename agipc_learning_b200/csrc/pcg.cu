@@ -156,11 +156,20 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
   const int sub = threadIdx.x % LPR;
   const int step = gridDim.x * kRows;
   Tacc dot = 0;
+  // row extents of the first step; each step fetches the next step's
+  auto extent = [&](int row, int& b, int& e) {
+    const bool ok = row < nrows;
+    b = ok ? __ldg(rowptr + row) : 0;
+    e = ok ? __ldg(rowptr + row + 1) : 0;
+  };
+  int nsa, nea, nsb, neb;
+  extent(lo + blockIdx.x * kRows + threadIdx.x / LPR, nsa, nea);
+  extent(lo + blockIdx.x * kRows + threadIdx.x / LPR + step, nsb, neb);
   for (int row0 = lo + blockIdx.x * kRows; row0 < nrows; row0 += 2 * step) {
     const int ra = row0 + threadIdx.x / LPR, rb = ra + step;
-    const bool oka = ra < nrows, okb = rb < nrows;
-    const int sa = oka ? __ldg(rowptr + ra) : 0, ea = oka ? __ldg(rowptr + ra + 1) : 0;
-    const int sb = okb ? __ldg(rowptr + rb) : 0, eb = okb ? __ldg(rowptr + rb + 1) : 0;
+    const int sa = nsa, ea = nea, sb = nsb, eb = neb;
+    extent(ra + 2 * step, nsa, nea);
+    extent(rb + 2 * step, nsb, neb);
     A a[2][3] = {{0, 0, 0}, {0, 0, 0}};
     const int na = (ea - sa + 2 * LPR - 1) / (2 * LPR), nbk = (eb - sb + 2 * LPR - 1) / (2 * LPR);
     const int steps = max(__reduce_max_sync(kFull, (unsigned)na), __reduce_max_sync(kFull, (unsigned)nbk));
