@@ -51,7 +51,8 @@ EXPORTS = (
     "maspcg_set_stream", "maspcg_set_graph", "maspcg_set_contacts", "maspcg_set_matrix_bcoo",
     "maspcg_build_preconditioner", "maspcg_solve", "maspcg_apply_preconditioner", "maspcg_spmv", "maspcg_get_info",
     "maspcg_get_hierarchy", "maspcg_get_bcsr", "maspcg_get_domain_inverses", "maspcg_get_domain_matrices",
-    "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient",
+    "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient", "maspcg_convert_bcoo",
+    "maspcg_partition_contact_triplets",
 )
 
 RESIDUAL_MAX_VECTORS = 8
@@ -120,6 +121,8 @@ def load():
         "maspcg_time_stage": (I, [H, I, I, ctypes.POINTER(ctypes.c_double)]),
         "maspcg_residual_norms_noalloc": (I, [H, I, P, P, P, P]),
         "maspcg_bcoo_gradient": (I, [H, P, P, I, P, P, P]),
+        "maspcg_convert_bcoo": (I, [H, P, P, P, I, P, P, P, P]),
+        "maspcg_partition_contact_triplets": (I, [H, P, P, P, P, I, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -124,6 +124,23 @@ void alloc_vectors(maspcg_handle* h)
 
 }  // namespace
 
+namespace {
+// A device output array, or handle scratch copied back to the host one.
+template <typename T>
+T* device_out(T* user, size_t count, maspcg::DBuf<T>& stage)
+{
+  if (is_device_ptr(user)) return user;
+  stage.resize(std::max<size_t>(count, 1));
+  return stage.get();
+}
+template <typename T>
+void copy_back(maspcg_handle* h, T* user, const T* dev, size_t count)
+{
+  if (count && dev != user)
+    MCK(cudaMemcpyAsync(user, dev, count * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+}
+}  // namespace
+
 extern "C" {
 
 MASPCG_API void maspcg_config_default(maspcg_config* c)
@@ -588,6 +605,59 @@ MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows,
                           h->stream));
     }
     MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_convert_bcoo(maspcg_handle* h, const double* values9, const int* rows,
+                                             const int* cols, int n, double* values9_out, int* rows_out,
+                                             int* cols_out, int* n_out)
+{
+  return guard(h, [&] {
+    MREQ(n >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative triplet count");
+    MREQ(n_out != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null n_out");
+    *n_out = 0;
+    if (n == 0) return;
+    MREQ(values9_out && rows_out && cols_out, MASPCG_ERR_INVALID_ARGUMENT, "null output array");
+    const double* v = device_in(h, values9, (size_t)9 * n, h->asm_vals);
+    const int* r = device_in(h, rows, (size_t)n, h->asm_rows);
+    const int* c = device_in(h, cols, (size_t)n, h->asm_cols);
+    double* vo = device_out(values9_out, (size_t)9 * n, h->asm_vals_out);
+    int* ro = device_out(rows_out, (size_t)n, h->asm_rows_out);
+    int* co = device_out(cols_out, (size_t)n, h->asm_cols_out);
+    const int count = maspcg::convert_bcoo(h, r, c, v, n, ro, co, vo);
+    copy_back(h, values9_out, vo, (size_t)9 * count);
+    copy_back(h, rows_out, ro, (size_t)count);
+    copy_back(h, cols_out, co, (size_t)count);
+    MCK(cudaStreamSynchronize(h->stream));
+    *n_out = count;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, const double* values9, const int* rows,
+                                                           const int* cols, const unsigned long long* type_hash,
+                                                           int n, double* values9_out, int* rows_out,
+                                                           int* cols_out, int counts[4])
+{
+  return guard(h, [&] {
+    MREQ(n >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative triplet count");
+    MREQ(counts != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null counts");
+    counts[0] = counts[1] = counts[2] = counts[3] = 0;
+    if (n == 0) return;
+    MREQ(values9_out && rows_out && cols_out, MASPCG_ERR_INVALID_ARGUMENT, "null output array");
+    const double* v = device_in(h, values9, (size_t)9 * n, h->asm_vals);
+    const int* r = device_in(h, rows, (size_t)n, h->asm_rows);
+    const int* c = device_in(h, cols, (size_t)n, h->asm_cols);
+    const unsigned long long* t = device_in(h, type_hash, (size_t)n, h->asm_types);
+    double* vo = device_out(values9_out, (size_t)9 * n, h->asm_vals_out);
+    int* ro = device_out(rows_out, (size_t)n, h->asm_rows_out);
+    int* co = device_out(cols_out, (size_t)n, h->asm_cols_out);
+    int k[4];
+    maspcg::partition_contacts(h, r, c, v, t, n, ro, co, vo, k);
+    copy_back(h, values9_out, vo, (size_t)9 * n);
+    copy_back(h, rows_out, ro, (size_t)n);
+    copy_back(h, cols_out, co, (size_t)n);
+    MCK(cudaStreamSynchronize(h->stream));
+    for (int q = 0; q < 4; ++q) counts[q] = k[q];
   });
 }
 

@@ -234,6 +234,11 @@ struct maspcg_handle {
   maspcg::DBuf<unsigned char> l2_flush;  // maspcg_time_stage only: written between timed launches
   maspcg::DBuf<int> adj_rows, adj_cols;   // maspcg_bcoo_gradient staging for host arguments
   maspcg::DBuf<double> adj_lam, adj_x, adj_grad;
+  // maspcg_convert_bcoo / maspcg_partition_contact_triplets: sort keys and
+  // permutation, head flags and scan, run starts, and host-argument staging
+  maspcg::DBuf<unsigned long long> asm_keys, asm_types;
+  maspcg::DBuf<int> asm_idx, asm_flags, asm_start, asm_rows, asm_cols, asm_rows_out, asm_cols_out;
+  maspcg::DBuf<double> asm_vals, asm_vals_out;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_batch = 0;
   bool graph_dirty = true;
@@ -274,6 +279,13 @@ void solve(maspcg_handle* h, const double* b_dev, double* x_dev, maspcg_result* 
 // adjoint.cu (device pointers, caller's row order)
 void bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n, const double* lam, const double* x,
                    double* grad);
+
+// assemble.cu (device pointers; returns the unique count / the type counts)
+int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const double* vals, int n, int* rows_out,
+                 int* cols_out, double* vals_out);
+void partition_contacts(maspcg_handle* h, const int* rows, const int* cols, const double* vals,
+                        const unsigned long long* types, int n, int* rows_out, int* cols_out, double* vals_out,
+                        int counts[4]);
 
 // residual_noalloc.cu
 void residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b, double* residual_norms,

@@ -37,7 +37,8 @@ class _Arg:
             return
         if _is_torch(a):
             import torch
-            want = {np.float64: torch.float64, np.int32: torch.int32, np.uint32: torch.int32}[np_dtype]
+            want = {np.float64: torch.float64, np.int32: torch.int32, np.uint32: torch.int32,
+                    np.uint64: torch.int64}[np_dtype]
             if a.dtype != want or not a.is_contiguous():
                 if writable:
                     raise ValueError("output tensor must be contiguous with the right dtype")
@@ -168,6 +169,41 @@ class MasPcg:
         ya = _Arg(y, np.float64, writable=True)
         self._ck(self.lib.maspcg_spmv(self.h, float(a), xa.ptr, float(b), ya.ptr))
         return y
+
+    def _outs(self, like, n):
+        """rows, cols (int32) and values (n x 9 float64) outputs on the device of `like`."""
+        if _is_torch(like) and like.is_cuda:
+            import torch
+            return (torch.empty(n, dtype=torch.int32, device=like.device),
+                    torch.empty(n, dtype=torch.int32, device=like.device),
+                    torch.empty((n, 9), dtype=torch.float64, device=like.device))
+        return np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros((n, 9), np.float64)
+
+    def convert_bcoo(self, rows, cols, values9):
+        """The triplet merge (maspcg_convert_bcoo; Converter::convert): unique
+        (row, col) keys in ascending order with their blocks summed in input
+        order.  Returns (rows, cols, values9) trimmed to the unique count."""
+        n = int(len(rows))
+        ro, co, vo = self._outs(rows, n)
+        r, c, v = _Arg(rows, np.int32), _Arg(cols, np.int32), _Arg(values9, np.float64)
+        ra, ca, va = _Arg(ro, np.int32, True), _Arg(co, np.int32, True), _Arg(vo, np.float64, True)
+        cnt = ctypes.c_int()
+        self._ck(self.lib.maspcg_convert_bcoo(self.h, v.ptr, r.ptr, c.ptr, n, va.ptr, ra.ptr, ca.ptr, ctypes.byref(cnt)))
+        u = cnt.value
+        return ro[:u], co[:u], vo[:u]
+
+    def partition_contact_triplets(self, rows, cols, values9, type_hash):
+        """Contact triplets grouped by type hash 0..3 (maspcg_partition_contact_triplets;
+        GIPC::partitionContactHessian).  Returns (rows, cols, values9, counts[4])."""
+        n = int(len(rows))
+        ro, co, vo = self._outs(rows, n)
+        r, c, v = _Arg(rows, np.int32), _Arg(cols, np.int32), _Arg(values9, np.float64)
+        t = _Arg(type_hash, np.uint64)
+        ra, ca, va = _Arg(ro, np.int32, True), _Arg(co, np.int32, True), _Arg(vo, np.float64, True)
+        counts = (ctypes.c_int * 4)()
+        self._ck(self.lib.maspcg_partition_contact_triplets(self.h, v.ptr, r.ptr, c.ptr, t.ptr, n, va.ptr, ra.ptr,
+                                                            ca.ptr, counts))
+        return ro, co, vo, np.array(list(counts), np.int32)
 
     def bcoo_gradient(self, rows, cols, lam, x, out=None):
         """dL/d(values) of upper BCOO blocks for lam = A^-1 dL/dx (maspcg_bcoo_gradient)."""

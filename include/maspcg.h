@@ -255,6 +255,30 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
  * Vector contents are left unspecified afterwards. */
 MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);
 
+/* The triplet merge in front of the solve: Converter::convert
+ * (StiffGIPC/linear_system/utils/converter.cu:137-284).  Sorts n block
+ * triplets by the key (row << 32) + col, ascending, and sums the 3x3 blocks
+ * of equal keys.  values9 / values9_out are 9 doubles per block in any fixed
+ * layout (summed elementwise; the reference's Eigen column-major).  The
+ * outputs need room for n blocks; *n_out receives the number of unique
+ * blocks.  The blocks of one key are summed in input order, so the result is
+ * deterministic (the reference's FP64 atomics are not).  Negative indices
+ * return MASPCG_ERR_INVALID_ARGUMENT.  Host or device pointers; any handle
+ * (only its stream and scratch are used). */
+MASPCG_API maspcg_status maspcg_convert_bcoo(maspcg_handle* h, const double* values9, const int* rows,
+                                             const int* cols, int n, double* values9_out, int* rows_out,
+                                             int* cols_out, int* n_out);
+
+/* Contact triplets grouped by kind: GIPC::partitionContactHessian
+ * (StiffGIPC/GIPC.cu:9952-10128).  type_hash[t] is 0 (FEM-FEM), 1 (ABD-FEM),
+ * 2 (FEM-ABD) or 3 (ABD-ABD); the outputs hold the n triplets ordered by
+ * type, stable within a type, and counts[k] the number of type k.  A hash
+ * above 3 returns MASPCG_ERR_INVALID_ARGUMENT.  Host or device pointers. */
+MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, const double* values9, const int* rows,
+                                                           const int* cols, const unsigned long long* type_hash,
+                                                           int n, double* values9_out, int* rows_out,
+                                                           int* cols_out, int counts[4]);
+
 /* Matrix adjoint of the solve (no counterpart in the reference; the backward
  * of the differentiable Newton-step solve).  For L(x) with x = A^-1 b and
  * lam = A^-1 dL/dx, writes dL/d(values) for every input block t of an upper

@@ -50,6 +50,7 @@ def lib():
         P, I, D, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
         sig = {
             "orc_convert_triplets": (I, [I, P, P, P, P, P, P]),
+            "orc_partition_contacts": (I, [I, P, P, P, P, P, P, P, P]),
             "orc_sym_spmv": (None, [D, P, P, P, I, I, P, D, P]),
             "orc_upper_to_full_bcsr": (I, [I, I, P, P, P, P, P, P]),
             "orc_bcsr_spmv": (None, [I, P, P, P, P, P]),
@@ -93,6 +94,19 @@ def convert_triplets(rows, cols, vals):
     orow, ocol, oval = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros((n, 9))
     u = lib().orc_convert_triplets(n, _p(r), _p(c), _p(v), _p(orow), _p(ocol), _p(oval))
     return orow[:u].copy(), ocol[:u].copy(), oval[:u].copy()
+
+
+def partition_contacts(rows, cols, vals, types):
+    """Contact triplets ordered by type hash 0..3, stable; and the count of each type."""
+    n = len(rows)
+    r, c, v = _c(rows, np.int32), _c(cols, np.int32), _c(vals, np.float64).reshape(n, 9)
+    t = _c(types, np.uint64)
+    orow, ocol, oval = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros((n, 9))
+    counts = np.zeros(4, np.int32)
+    rc = lib().orc_partition_contacts(n, _p(r), _p(c), _p(v), _p(t), _p(orow), _p(ocol), _p(oval), _p(counts))
+    if rc != 0:
+        raise ValueError("contact type hash outside 0..3")
+    return orow, ocol, oval, counts
 
 
 def sym_spmv(a, vals, rows, cols, x, b=0.0, y=None):

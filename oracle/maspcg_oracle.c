@@ -92,6 +92,30 @@ int orc_convert_triplets(int n, const int* rows, const int* cols, const double* 
   return u + 1;
 }
 
+/* GIPC.cu:9952-10128 (partitionContactHessian) with _partition_collision_
+ * triplets / _reorder_triplets (GIPC.cu:218-283): a stable sort of contact
+ * triplets on their type hash 0..3 (FEM-FEM, ABD-FEM, FEM-ABD, ABD-ABD), here
+ * as a counting sort; counts[k] = triplets of type k.  Returns -1 for a hash
+ * above 3. */
+int orc_partition_contacts(int n, const int* rows, const int* cols, const double* vals9, const uint64_t* type,
+                           int* out_rows, int* out_cols, double* out_vals9, int* counts)
+{
+  int start[4] = {0, 0, 0, 0};
+  for (int k = 0; k < 4; ++k) counts[k] = 0;
+  for (int i = 0; i < n; ++i) {
+    if (type[i] > 3) return -1;
+    counts[type[i]]++;
+  }
+  for (int k = 1; k < 4; ++k) start[k] = start[k - 1] + counts[k - 1];
+  for (int i = 0; i < n; ++i) {
+    const int d = start[type[i]]++;
+    out_rows[d] = rows[i];
+    out_cols[d] = cols[i];
+    memcpy(out_vals9 + 9 * (size_t)d, vals9 + 9 * (size_t)i, 9 * sizeof(double));
+  }
+  return 0;
+}
+
 /* spmv.cu:14-53 and the self-test CPU loop spmv.cu:348-364. */
 void orc_sym_spmv(double a, const double* vals9, const int* rows, const int* cols,
                   int nblocks, int dof, const double* x, double b, double* y)

@@ -36,6 +36,8 @@ extern "C" {
  * must hold n entries. */
 int orc_convert_triplets(int n, const int* rows, const int* cols, const double* vals9,
                          int* out_rows, int* out_cols, double* out_vals9);
+int orc_partition_contacts(int n, const int* rows, const int* cols, const double* vals9, const uint64_t* type,
+                           int* out_rows, int* out_cols, double* out_vals9, int* counts);
 
 /* Spmv::*_sym_spmv (spmv.cu:28-53, CPU loop spmv.cu:348-364):
  * y = a*A*x + b*y with A given as upper BCOO.  Sequential, input order. */
