@@ -52,7 +52,7 @@ EXPORTS = (
     "maspcg_build_preconditioner", "maspcg_solve", "maspcg_apply_preconditioner", "maspcg_spmv", "maspcg_get_info",
     "maspcg_get_hierarchy", "maspcg_get_bcsr", "maspcg_get_domain_inverses", "maspcg_get_domain_matrices",
     "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient", "maspcg_convert_bcoo",
-    "maspcg_partition_contact_triplets",
+    "maspcg_partition_contact_triplets", "maspcg_fem_snk1_gradient_hessian",
 )
 
 RESIDUAL_MAX_VECTORS = 8
@@ -123,6 +123,7 @@ def load():
         "maspcg_bcoo_gradient": (I, [H, P, P, I, P, P, P]),
         "maspcg_convert_bcoo": (I, [H, P, P, P, I, P, P, P, P]),
         "maspcg_partition_contact_triplets": (I, [H, P, P, P, P, I, P, P, P, P]),
+        "maspcg_fem_snk1_gradient_hessian": (I, [H, I, P, I, P, P, P, P, P, D, I, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

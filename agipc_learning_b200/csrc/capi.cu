@@ -661,6 +661,51 @@ MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, con
   });
 }
 
+MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int n_tets, const unsigned* tets,
+                                                          int n_vertices, const double* x, const double* dm_inverse,
+                                                          const double* volume, const double* len_rate,
+                                                          const double* vol_rate, double dt, int hessian_offset,
+                                                          double* gradient, int* rows, int* cols,
+                                                          double* values9_colmajor)
+{
+  return guard(h, [&] {
+    MREQ(n_tets >= 0 && n_vertices >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative count");
+    MREQ(std::isfinite(dt), MASPCG_ERR_INVALID_ARGUMENT, "non-finite dt");
+    if (n_tets == 0) return;
+    MREQ(gradient && rows && cols && values9_colmajor, MASPCG_ERR_INVALID_ARGUMENT, "null output array");
+    MREQ((long long)hessian_offset + n_vertices <= 0x7fffffffLL && hessian_offset >= 0, MASPCG_ERR_CAPACITY,
+         "block index overflow");
+    MREQ(10LL * n_tets <= 0x7fffffffLL, MASPCG_ERR_CAPACITY, "too many tets");
+    // vertex ids must address x (checked on a host copy)
+    {
+      const std::vector<unsigned> ht = host_copy(h, tets, 4 * (size_t)n_tets);
+      for (unsigned v : ht) MREQ(v < (unsigned)n_vertices, MASPCG_ERR_INVALID_ARGUMENT, "tet vertex id out of range");
+    }
+    const unsigned* td = device_in(h, tets, 4 * (size_t)n_tets, h->fem_tets);
+    const double* xd = device_in(h, x, 3 * (size_t)n_vertices, h->fem_x);
+    const double* di = device_in(h, dm_inverse, 9 * (size_t)n_tets, h->fem_dminv);
+    const double* vo = device_in(h, volume, (size_t)n_tets, h->fem_vol);
+    const double* lr = device_in(h, len_rate, (size_t)n_tets, h->fem_len);
+    const double* vr = device_in(h, vol_rate, (size_t)n_tets, h->fem_volr);
+    const bool dev = is_device_ptr(gradient);
+    double* gd = gradient;
+    if (!dev) {
+      h->fem_grad.resize(3 * (size_t)n_vertices);
+      gd = h->fem_grad.get();
+      MCK(cudaMemcpyAsync(gd, gradient, sizeof(double) * 3 * (size_t)n_vertices, cudaMemcpyHostToDevice, h->stream));
+    }
+    int* ro = device_out(rows, 10 * (size_t)n_tets, h->asm_rows_out);
+    int* co = device_out(cols, 10 * (size_t)n_tets, h->asm_cols_out);
+    double* va = device_out(values9_colmajor, 90 * (size_t)n_tets, h->asm_vals_out);
+    maspcg::fem_snk1(h, n_tets, td, xd, di, vo, lr, vr, dt, hessian_offset, gd, ro, co, va);
+    if (!dev) copy_back(h, gradient, gd, 3 * (size_t)n_vertices);
+    copy_back(h, rows, ro, 10 * (size_t)n_tets);
+    copy_back(h, cols, co, 10 * (size_t)n_tets);
+    copy_back(h, values9_colmajor, va, 90 * (size_t)n_tets);
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
 MASPCG_API maspcg_status maspcg_residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b,
                                                        double* residual_norms, double* rhs_norms)
 {

@@ -239,6 +239,9 @@ struct maspcg_handle {
   maspcg::DBuf<unsigned long long> asm_keys, asm_types;
   maspcg::DBuf<int> asm_idx, asm_flags, asm_start, asm_rows, asm_cols, asm_rows_out, asm_cols_out;
   maspcg::DBuf<double> asm_vals, asm_vals_out;
+  // maspcg_fem_snk1_gradient_hessian host-argument staging
+  maspcg::DBuf<unsigned> fem_tets;
+  maspcg::DBuf<double> fem_x, fem_dminv, fem_vol, fem_len, fem_volr, fem_grad;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_batch = 0;
   bool graph_dirty = true;
@@ -286,6 +289,11 @@ int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const doubl
 void partition_contacts(maspcg_handle* h, const int* rows, const int* cols, const double* vals,
                         const unsigned long long* types, int n, int* rows_out, int* cols_out, double* vals_out,
                         int counts[4]);
+
+// fem.cu (device pointers)
+void fem_snk1(maspcg_handle* h, int ntet, const unsigned* tets, const double* x, const double* dm_inv,
+              const double* volume, const double* len_rate, const double* vol_rate, double dt, int offset,
+              double* gradient, int* rows, int* cols, double* vals);
 
 // residual_noalloc.cu
 void residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b, double* residual_norms,

@@ -205,6 +205,24 @@ class MasPcg:
                                                             ca.ptr, counts))
         return ro, co, vo, np.array(list(counts), np.int32)
 
+    def fem_snk1(self, tets, x, dm_inverse, volume, len_rate, vol_rate, dt, hessian_offset=0, gradient=None):
+        """Per-tet SNK1 gradient (accumulated into `gradient`, zeros if None)
+        and projected Hessian triplets (maspcg_fem_snk1_gradient_hessian).
+        numpy in, numpy out.  Returns (gradient, rows, cols, values9)."""
+        tets = np.ascontiguousarray(tets, np.uint32).reshape(-1, 4)
+        x = np.ascontiguousarray(x, np.float64).reshape(-1)
+        nt, nv = len(tets), len(x) // 3
+        grad = np.zeros(3 * nv) if gradient is None else np.ascontiguousarray(gradient, np.float64).copy()
+        rows, cols, vals = np.zeros(10 * nt, np.int32), np.zeros(10 * nt, np.int32), np.zeros((10 * nt, 9))
+        a = [_Arg(tets, np.uint32), _Arg(x, np.float64), _Arg(dm_inverse, np.float64), _Arg(volume, np.float64),
+             _Arg(len_rate, np.float64), _Arg(vol_rate, np.float64)]
+        o = [_Arg(grad, np.float64, True), _Arg(rows, np.int32, True), _Arg(cols, np.int32, True),
+             _Arg(vals, np.float64, True)]
+        self._ck(self.lib.maspcg_fem_snk1_gradient_hessian(self.h, nt, a[0].ptr, nv, a[1].ptr, a[2].ptr, a[3].ptr,
+                                                           a[4].ptr, a[5].ptr, float(dt), int(hessian_offset),
+                                                           o[0].ptr, o[1].ptr, o[2].ptr, o[3].ptr))
+        return grad, rows, cols, vals
+
     def bcoo_gradient(self, rows, cols, lam, x, out=None):
         """dL/d(values) of upper BCOO blocks for lam = A^-1 dL/dx (maspcg_bcoo_gradient)."""
         n = int(len(rows))

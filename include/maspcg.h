@@ -279,6 +279,23 @@ MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, con
                                                            int n, double* values9_out, int* rows_out,
                                                            int* cols_out, int counts[4]);
 
+/* The FEM part of A: per-tet gradient and PSD-projected Hessian of the stable
+ * Neo-Hookean energy, _calculate_fem_gradient_hessian
+ * (StiffGIPC/femEnergy.cu:1720-1856, SNK1 branch; projection
+ * :1641-1717).  Inputs per tet: tets (4 vertex ids), dm_inverse (Dm^-1,
+ * 9 doubles row-major), volume, len_rate and vol_rate (the Lame rates,
+ * gl_main.cu:586-630); x: current positions, 3 doubles per vertex (n_vertices).
+ * gradient (3 doubles per vertex) is accumulated with FP64 atomics, as in the
+ * reference: clear it first.  rows/cols/values9_colmajor receive 10 triplets
+ * per tet at [10t, 10t + 10): the tet's upper 3x3 blocks with vertex ids +
+ * hessian_offset, row <= col.  Host or device pointers (all of one kind). */
+MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int n_tets, const unsigned* tets,
+                                                          int n_vertices, const double* x, const double* dm_inverse,
+                                                          const double* volume, const double* len_rate,
+                                                          const double* vol_rate, double dt, int hessian_offset,
+                                                          double* gradient, int* rows, int* cols,
+                                                          double* values9_colmajor);
+
 /* Matrix adjoint of the solve (no counterpart in the reference; the backward
  * of the differentiable Newton-step solve).  For L(x) with x = A^-1 b and
  * lam = A^-1 dL/dx, writes dL/d(values) for every input block t of an upper

@@ -109,6 +109,102 @@ def partition_contacts(rows, cols, vals, types):
     return orow, ocol, oval, counts
 
 
+def _skew(w):
+    z = np.zeros(w.shape[:-1] + (3, 3))
+    z[..., 0, 1], z[..., 0, 2] = -w[..., 2], w[..., 1]
+    z[..., 1, 0], z[..., 1, 2] = w[..., 2], -w[..., 0]
+    z[..., 2, 0], z[..., 2, 1] = -w[..., 1], w[..., 0]
+    return z
+
+
+def fem_snk1(tets, x, dm_inverse, volume, len_rate, vol_rate, dt, offset=0, project=True):
+    """Per-tet SNK1 gradient and Hessian, StiffGIPC/femEnergy.cu:1720-1856.
+
+    Energy u/2 (I2 - 3) + r/2 (I3 - 1 - u/r)^2 of F = Ds Dm^-1 (u, r: the
+    Lame rates, gl_main.cu:586-630), times dt^2 V.  The gradient
+    (__computePEPF_StableNHK3D1_double, :432-455) is summed per vertex.  The
+    exact 9x9 Hessian in F (vec column-major, index i + 3j) is projected onto
+    the PSD cone by a full eigendecomposition (numpy.linalg.eigh), which is
+    what the reference's closed-form eigensystem (:1641-1717) computes; then
+    H = dF/dx^T H_F dF/dx (:1389, :1814) and the 10 upper 3x3 blocks per tet,
+    row <= col, values column-major (:1821-1852).  Returns (gradient,
+    rows, cols, values9).  project=False keeps the exact Hessian (for finite
+    difference checks)."""
+    T = np.asarray(tets, np.int64).reshape(-1, 4)
+    nt = len(T)
+    X = np.asarray(x, np.float64).reshape(-1, 3)
+    Di = np.asarray(dm_inverse, np.float64).reshape(nt, 3, 3)
+    vol = np.asarray(volume, np.float64)
+    u = np.asarray(len_rate, np.float64)
+    r = np.asarray(vol_rate, np.float64)
+    Ds = np.stack([X[T[:, c + 1]] - X[T[:, 0]] for c in range(3)], axis=2)
+    F = Ds @ Di
+    f = [F[:, :, c] for c in range(3)]
+    cof = np.stack([np.cross(f[1], f[2]), np.cross(f[2], f[0]), np.cross(f[0], f[1])], axis=2)  # dJ/dF
+    J = np.einsum("ti,ti->t", f[0], cof[:, :, 0])
+    s = r * (J - 1.0) - u
+    P = u[:, None, None] * F + s[:, None, None] * cof
+    cf = np.zeros((nt, 4, 3))
+    cf[:, 1:, :] = Di
+    cf[:, 0, :] = -Di.sum(axis=1)
+    scale = dt * dt * vol
+    g12 = scale[:, None, None] * np.einsum("taj,tij->tai", cf, P)  # (nt, 4, 3)
+    grad = np.zeros_like(X)
+    np.add.at(grad, T.reshape(-1), g12.reshape(-1, 3))
+    vg = cof.transpose(0, 2, 1).reshape(nt, 9)  # index i + 3j
+    H9 = u[:, None, None] * np.eye(9) + r[:, None, None] * np.einsum("ta,tb->tab", vg, vg)
+    for c in range(3):
+        c1, c2 = (c + 1) % 3, (c + 2) % 3
+        H9[:, 3 * c:3 * c + 3, 3 * c1:3 * c1 + 3] += -s[:, None, None] * _skew(f[c2])
+        H9[:, 3 * c:3 * c + 3, 3 * c2:3 * c2 + 3] += s[:, None, None] * _skew(f[c1])
+    if project:
+        w, Q = np.linalg.eigh(H9)
+        H9 = np.einsum("tak,tk,tbk->tab", Q, np.maximum(w, 0.0), Q)
+    PF = np.zeros((nt, 9, 12))
+    for a in range(4):
+        for i in range(3):
+            for j in range(3):
+                PF[:, i + 3 * j, 3 * a + i] = cf[:, a, j]
+    H12 = scale[:, None, None] * np.einsum("tpa,tpq,tqb->tab", PF, H9, PF)
+    rows, cols, vals = np.zeros((nt, 10), np.int32), np.zeros((nt, 10), np.int32), np.zeros((nt, 10, 9))
+    k = 0
+    for a in range(4):
+        for b in range(a, 4):
+            ra, rb = T[:, a] + offset, T[:, b] + offset
+            sw = ra > rb
+            rows[:, k] = np.where(sw, rb, ra)
+            cols[:, k] = np.where(sw, ra, rb)
+            B = H12[:, 3 * a:3 * a + 3, 3 * b:3 * b + 3]
+            B = np.where(sw[:, None, None], B.transpose(0, 2, 1), B)
+            vals[:, k, :] = B.transpose(0, 2, 1).reshape(nt, 9)  # column-major: index i + 3j
+            k += 1
+    return grad.reshape(-1), rows.reshape(-1), cols.reshape(-1), vals.reshape(-1, 9)
+
+
+def fem_snk1_energy(tets, x, dm_inverse, volume, len_rate, vol_rate, dt):
+    """Total dt^2 V Psi of the SNK1 energy above (for finite differences)."""
+    T = np.asarray(tets, np.int64).reshape(-1, 4)
+    X = np.asarray(x, np.float64).reshape(-1, 3)
+    Di = np.asarray(dm_inverse, np.float64).reshape(len(T), 3, 3)
+    F = np.stack([X[T[:, c + 1]] - X[T[:, 0]] for c in range(3)], axis=2) @ Di
+    u, r = np.asarray(len_rate, np.float64), np.asarray(vol_rate, np.float64)
+    I2 = np.einsum("tij,tij->t", F, F)
+    J = np.linalg.det(F)
+    psi = 0.5 * u * (I2 - 3.0) + 0.5 * r * (J - 1.0 - u / r) ** 2
+    return float(np.sum(dt * dt * np.asarray(volume) * psi))
+
+
+def fem_rest_data(tets, X, E, nu):
+    """Dm^-1 (row-major), rest volume |det Dm| / 6 and the Lame rates per tet
+    (gl_main.cu:586-630): u = 4/3 mu, r = lambda + 5/6 mu."""
+    T = np.asarray(tets, np.int64).reshape(-1, 4)
+    Xr = np.asarray(X, np.float64).reshape(-1, 3)
+    Dm = np.stack([Xr[T[:, c + 1]] - Xr[T[:, 0]] for c in range(3)], axis=2)
+    E = np.broadcast_to(np.asarray(E, np.float64), (len(T),))
+    mu, la = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    return np.linalg.inv(Dm).reshape(-1, 9), np.abs(np.linalg.det(Dm)) / 6.0, 4 * mu / 3, la + 5 * mu / 6
+
+
 def sym_spmv(a, vals, rows, cols, x, b=0.0, y=None):
     x = _c(x, np.float64)
     y = np.zeros_like(x) if y is None else _c(y, np.float64).copy()
