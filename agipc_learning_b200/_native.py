@@ -52,10 +52,19 @@ EXPORTS = (
     "maspcg_build_preconditioner", "maspcg_solve", "maspcg_apply_preconditioner", "maspcg_spmv", "maspcg_get_info",
     "maspcg_get_hierarchy", "maspcg_get_bcsr", "maspcg_get_domain_inverses", "maspcg_get_domain_matrices",
     "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient", "maspcg_convert_bcoo",
-    "maspcg_partition_contact_triplets", "maspcg_fem_snk1_gradient_hessian",
+    "maspcg_partition_contact_triplets", "maspcg_fem_snk1_gradient_hessian", "maspcg_galerkin_coarse_matrix",
+    "maspcg_galerkin_restrict", "maspcg_galerkin_prolong",
 )
 
 RESIDUAL_MAX_VECTORS = 8
+
+
+class GalerkinMap(ctypes.Structure):
+    """maspcg_galerkin_map: the AGIPC coarse mapping."""
+    _fields_ = [("fine_to_coarse", ctypes.c_void_p), ("coarse_block_bases", ctypes.c_void_p),
+                ("basis_masks", ctypes.c_void_p), ("rest_positions", ctypes.c_void_p),
+                ("prefix_blocks", ctypes.c_int), ("fem_nodes", ctypes.c_int), ("coarse_nodes", ctypes.c_int),
+                ("coarse_block_nodes", ctypes.c_int)]
 
 
 class Config(ctypes.Structure):
@@ -124,6 +133,9 @@ def load():
         "maspcg_convert_bcoo": (I, [H, P, P, P, I, P, P, P, P]),
         "maspcg_partition_contact_triplets": (I, [H, P, P, P, P, I, P, P, P, P]),
         "maspcg_fem_snk1_gradient_hessian": (I, [H, I, P, I, P, P, P, P, P, D, I, P, P, P, P]),
+        "maspcg_galerkin_coarse_matrix": (I, [H, ctypes.POINTER(GalerkinMap), P, P, P, I, P, P, P, I, P]),
+        "maspcg_galerkin_restrict": (I, [H, ctypes.POINTER(GalerkinMap), P, P]),
+        "maspcg_galerkin_prolong": (I, [H, ctypes.POINTER(GalerkinMap), P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

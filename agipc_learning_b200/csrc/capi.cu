@@ -141,6 +141,44 @@ void copy_back(maspcg_handle* h, T* user, const T* dev, size_t count)
 }
 }  // namespace
 
+namespace {
+// Validate a coarse mapping on host copies and stage its arrays on the device.
+maspcg::GalerkinMap galerkin_map(maspcg_handle* h, const maspcg_galerkin_map* map)
+{
+  MREQ(map != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null mapping");
+  const maspcg_galerkin_map& g = *map;
+  MREQ(g.prefix_blocks >= 0 && g.fem_nodes >= 0 && g.coarse_nodes >= 0 && g.coarse_block_nodes >= 0,
+       MASPCG_ERR_INVALID_ARGUMENT, "negative mapping size");
+  MREQ(g.fem_nodes == 0 || g.coarse_nodes > 0, MASPCG_ERR_INVALID_ARGUMENT, "mapping has no coarse owner");
+  MREQ((long long)g.prefix_blocks + g.fem_nodes <= 0x7fffffffLL &&
+           (long long)g.prefix_blocks + g.coarse_block_nodes <= 0x7fffffffLL,
+       MASPCG_ERR_CAPACITY, "block count overflow");
+  if (g.fem_nodes > 0) {
+    const std::vector<int> f2c = host_copy(h, g.fine_to_coarse, (size_t)g.fem_nodes);
+    const std::vector<int> base = host_copy(h, g.coarse_block_bases, (size_t)g.coarse_nodes);
+    const std::vector<int> mask = host_copy(h, g.basis_masks, (size_t)g.coarse_nodes);
+    for (int c : f2c) MREQ(c >= 0 && c < g.coarse_nodes, MASPCG_ERR_INVALID_ARGUMENT, "fine_to_coarse out of range");
+    for (int c = 0; c < g.coarse_nodes; ++c) {
+      MREQ(mask[c] >= 1 && mask[c] <= 15, MASPCG_ERR_INVALID_ARGUMENT, "basis mask outside 1..15");
+      int w = 0;
+      for (int q = 0; q < 4; ++q) w += (mask[c] >> q) & 1;
+      MREQ(base[c] >= 0 && (long long)base[c] + w <= g.coarse_block_nodes, MASPCG_ERR_INVALID_ARGUMENT,
+           "coarse block base out of range");
+    }
+  }
+  maspcg::GalerkinMap m{};
+  m.prefix = g.prefix_blocks;
+  m.fine_blocks = g.prefix_blocks + g.fem_nodes;
+  if (g.fem_nodes > 0) {
+    m.fine_to_coarse = device_in(h, g.fine_to_coarse, (size_t)g.fem_nodes, h->gal_f2c);
+    m.coarse_block_bases = device_in(h, g.coarse_block_bases, (size_t)g.coarse_nodes, h->gal_bases);
+    m.basis_masks = device_in(h, g.basis_masks, (size_t)g.coarse_nodes, h->gal_masks);
+    m.rest = device_in(h, g.rest_positions, 3 * (size_t)g.fem_nodes, h->gal_rest);
+  }
+  return m;
+}
+}  // namespace
+
 extern "C" {
 
 MASPCG_API void maspcg_config_default(maspcg_config* c)
@@ -702,6 +740,73 @@ MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int 
     copy_back(h, rows, ro, 10 * (size_t)n_tets);
     copy_back(h, cols, co, 10 * (size_t)n_tets);
     copy_back(h, values9_colmajor, va, 90 * (size_t)n_tets);
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_galerkin_coarse_matrix(maspcg_handle* h, const maspcg_galerkin_map* map,
+                                                       const double* values9, const int* rows, const int* cols,
+                                                       int n, double* coarse_values9, int* coarse_rows,
+                                                       int* coarse_cols, int capacity, int* n_coarse)
+{
+  return guard(h, [&] {
+    MREQ(n >= 0 && capacity >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative count");
+    MREQ(n_coarse != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null n_coarse");
+    *n_coarse = 0;
+    const maspcg::GalerkinMap m = galerkin_map(h, map);
+    if (n == 0) return;
+    const double* v = device_in(h, values9, (size_t)9 * n, h->gal_in_vals);
+    const int* r = device_in(h, rows, (size_t)n, h->gal_in_rows);
+    const int* c = device_in(h, cols, (size_t)n, h->gal_in_cols);
+    const double* ev;
+    const int *er, *ec;
+    const int expanded = maspcg::galerkin_expand(h, m, v, r, c, n, &ev, &er, &ec);
+    h->gal_out_vals.resize(9 * (size_t)std::max(expanded, 1));
+    h->gal_out_rows.resize((size_t)std::max(expanded, 1));
+    h->gal_out_cols.resize((size_t)std::max(expanded, 1));
+    const int count = maspcg::convert_bcoo(h, er, ec, ev, expanded, h->gal_out_rows.get(), h->gal_out_cols.get(),
+                                           h->gal_out_vals.get());
+    *n_coarse = count;
+    MREQ(count <= capacity, MASPCG_ERR_CAPACITY,
+         "coarse output holds " + std::to_string(capacity) + " blocks, " + std::to_string(count) + " needed");
+    MREQ(count == 0 || (coarse_values9 && coarse_rows && coarse_cols), MASPCG_ERR_INVALID_ARGUMENT,
+         "null output array");
+    const cudaMemcpyKind kind = cudaMemcpyDefault;
+    MCK(cudaMemcpyAsync(coarse_values9, h->gal_out_vals.get(), sizeof(double) * 9 * (size_t)count, kind, h->stream));
+    MCK(cudaMemcpyAsync(coarse_rows, h->gal_out_rows.get(), sizeof(int) * (size_t)count, kind, h->stream));
+    MCK(cudaMemcpyAsync(coarse_cols, h->gal_out_cols.get(), sizeof(int) * (size_t)count, kind, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_galerkin_restrict(maspcg_handle* h, const maspcg_galerkin_map* map,
+                                                  const double* fine_rhs, double* coarse_rhs)
+{
+  return guard(h, [&] {
+    const maspcg::GalerkinMap m = galerkin_map(h, map);
+    const int cb = map->prefix_blocks + map->coarse_block_nodes;
+    if (cb == 0) return;
+    MREQ(coarse_rhs != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null output array");
+    const double* f = m.fine_blocks ? device_in(h, fine_rhs, 3 * (size_t)m.fine_blocks, h->gal_vec_in) : nullptr;
+    double* o = device_out(coarse_rhs, 3 * (size_t)cb, h->gal_vec_out);
+    maspcg::galerkin_restrict(h, m, f, o, cb);
+    copy_back(h, coarse_rhs, o, 3 * (size_t)cb);
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_galerkin_prolong(maspcg_handle* h, const maspcg_galerkin_map* map,
+                                                 const double* coarse_x, double* fine_x)
+{
+  return guard(h, [&] {
+    const maspcg::GalerkinMap m = galerkin_map(h, map);
+    if (m.fine_blocks == 0) return;
+    MREQ(fine_x != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null output array");
+    const int cb = map->prefix_blocks + map->coarse_block_nodes;
+    const double* cx = device_in(h, coarse_x, 3 * (size_t)cb, h->gal_vec_in);
+    double* o = device_out(fine_x, 3 * (size_t)m.fine_blocks, h->gal_vec_out);
+    maspcg::galerkin_prolong(h, m, cx, o);
+    copy_back(h, fine_x, o, 3 * (size_t)m.fine_blocks);
     MCK(cudaStreamSynchronize(h->stream));
   });
 }

@@ -239,6 +239,10 @@ struct maspcg_handle {
   maspcg::DBuf<unsigned long long> asm_keys, asm_types;
   maspcg::DBuf<int> asm_idx, asm_flags, asm_start, asm_rows, asm_cols, asm_rows_out, asm_cols_out;
   maspcg::DBuf<double> asm_vals, asm_vals_out;
+  // maspcg_galerkin_*: expansion counts/offsets, expanded triplets, staging
+  maspcg::DBuf<int> gal_counts, gal_rows, gal_cols, gal_in_rows, gal_in_cols, gal_f2c, gal_bases, gal_masks,
+      gal_out_rows, gal_out_cols;
+  maspcg::DBuf<double> gal_vals, gal_in_vals, gal_rest, gal_vec_in, gal_vec_out, gal_out_vals;
   // maspcg_fem_snk1_gradient_hessian host-argument staging
   maspcg::DBuf<unsigned> fem_tets;
   maspcg::DBuf<double> fem_x, fem_dminv, fem_vol, fem_len, fem_volr, fem_grad;
@@ -289,6 +293,23 @@ int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const doubl
 void partition_contacts(maspcg_handle* h, const int* rows, const int* cols, const double* vals,
                         const unsigned long long* types, int n, int* rows_out, int* cols_out, double* vals_out,
                         int counts[4]);
+
+// galerkin.cu (device pointers).  The AGIPC mapping: fine blocks [0, prefix)
+// pass through; FEM node k (block prefix + k) maps to coarse node
+// fine_to_coarse[k], whose blocks start at prefix + coarse_block_bases[c]
+// with the basis subset basis_masks[c] of (1, x, y, z) at rest[3k..3k+2].
+struct GalerkinMap {
+  const int* fine_to_coarse;
+  const int* coarse_block_bases;
+  const int* basis_masks;
+  const double* rest;
+  int prefix;
+  int fine_blocks;
+};
+int galerkin_expand(maspcg_handle* h, const GalerkinMap& m, const double* vals, const int* rows, const int* cols,
+                    int n, const double** v, const int** r, const int** c);
+void galerkin_restrict(maspcg_handle* h, const GalerkinMap& m, const double* fine, double* coarse, int coarse_blocks);
+void galerkin_prolong(maspcg_handle* h, const GalerkinMap& m, const double* coarse, double* fine);
 
 // fem.cu (device pointers)
 void fem_snk1(maspcg_handle* h, int ntet, const unsigned* tets, const double* x, const double* dm_inv,

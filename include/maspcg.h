@@ -296,6 +296,47 @@ MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int 
                                                           double* gradient, int* rows, int* cols,
                                                           double* values9_colmajor);
 
+/* The AGIPC coarse space (StiffGIPC/agipc/agipc_galerkin.cu, mapping of
+ * agipc_criterion.cuh:13-25).  Fine blocks [0, prefix_blocks) pass through;
+ * FEM node k (fine block prefix_blocks + k, k < fem_nodes) belongs to coarse
+ * node fine_to_coarse[k] (< coarse_nodes), whose blocks start at
+ * prefix_blocks + coarse_block_bases[c] and whose basis is the subset
+ * basis_masks[c] (bits 0-3, 1..15) of (1, x, y, z) at the node's rest
+ * position rest_positions[3k..3k+2]: a translational node has mask 1, an
+ * affine node 15.  The coarse system has prefix_blocks + coarse_block_nodes
+ * block rows. */
+typedef struct maspcg_galerkin_map {
+  const int* fine_to_coarse;
+  const int* coarse_block_bases;
+  const int* basis_masks;
+  const double* rest_positions;
+  int prefix_blocks;
+  int fem_nodes;
+  int coarse_nodes;
+  int coarse_block_nodes;
+} maspcg_galerkin_map;
+
+/* A_c = P^T A P (count_expanded_blocks / emit_expanded_blocks + Converter,
+ * agipc_galerkin.cu:221-283, :921-953): every fine upper triplet expands into
+ * phi_i[a] phi_j[b] A_ij blocks, which are merged as maspcg_convert_bcoo does.
+ * Writes the unique upper coarse blocks (row <= col, ascending keys) and
+ * *n_coarse; if capacity is smaller, returns MASPCG_ERR_CAPACITY with the
+ * needed count in *n_coarse. */
+MASPCG_API maspcg_status maspcg_galerkin_coarse_matrix(maspcg_handle* h, const maspcg_galerkin_map* map,
+                                                       const double* values9, const int* rows, const int* cols,
+                                                       int n, double* coarse_values9, int* coarse_rows,
+                                                       int* coarse_cols, int capacity, int* n_coarse);
+
+/* b_c = P^T b (reduce_mixed_rhs, agipc_galerkin.cu:285-306; FP64 atomics as
+ * in the reference).  fine_rhs: 3 (prefix_blocks + fem_nodes) doubles;
+ * coarse_rhs: 3 (prefix_blocks + coarse_block_nodes). */
+MASPCG_API maspcg_status maspcg_galerkin_restrict(maspcg_handle* h, const maspcg_galerkin_map* map,
+                                                  const double* fine_rhs, double* coarse_rhs);
+
+/* x = P x_c (prolongate_mixed, agipc_galerkin.cu:355-369). */
+MASPCG_API maspcg_status maspcg_galerkin_prolong(maspcg_handle* h, const maspcg_galerkin_map* map,
+                                                 const double* coarse_x, double* fine_x);
+
 /* Matrix adjoint of the solve (no counterpart in the reference; the backward
  * of the differentiable Newton-step solve).  For L(x) with x = A^-1 b and
  * lam = A^-1 dL/dx, writes dL/d(values) for every input block t of an upper

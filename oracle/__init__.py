@@ -205,6 +205,58 @@ def fem_rest_data(tets, X, E, nu):
     return np.linalg.inv(Dm).reshape(-1, 9), np.abs(np.linalg.det(Dm)) / 6.0, 4 * mu / 3, la + 5 * mu / 6
 
 
+def galerkin_transform(block, prefix, fine_to_coarse, bases, masks, rest):
+    """transform_for_block (StiffGIPC/agipc/agipc_galerkin.cu:200-219): the
+    first coarse block, the width and the basis values of a fine block."""
+    if block < prefix:
+        return block, 1, [1.0, 0.0, 0.0, 0.0]
+    k = block - prefix
+    c = int(fine_to_coarse[k])
+    mask = int(masks[c])
+    raw = [1.0, float(rest[3 * k]), float(rest[3 * k + 1]), float(rest[3 * k + 2])]
+    phi = [raw[q] for q in range(4) if mask & (1 << q)] + [0.0] * 4
+    return prefix + int(bases[c]), bin(mask & 15).count("1"), phi[:4]
+
+
+def galerkin_expand(rows, cols, vals, prefix, fine_to_coarse, bases, masks, rest):
+    """count_expanded_blocks + emit_expanded_blocks (agipc_galerkin.cu:221-283):
+    every fine upper triplet as its coarse triplets, in fine order."""
+    rest = np.asarray(rest, np.float64).reshape(-1)
+    V = np.asarray(vals, np.float64).reshape(-1, 9)
+    orow, ocol, oval = [], [], []
+    for i in range(len(rows)):
+        r, c = int(rows[i]), int(cols[i])
+        rb, rw, rp = galerkin_transform(r, prefix, fine_to_coarse, bases, masks, rest)
+        cb, cw, cp = galerkin_transform(c, prefix, fine_to_coarse, bases, masks, rest)
+        M = V[i].reshape(3, 3).T  # Eigen column-major -> (row, col)
+        for a in range(rw):
+            for b in range(cw):
+                if r == c and a > b:
+                    continue
+                mr, mc = rb + a, cb + b
+                w = rp[a] * cp[b]
+                B = w * M
+                if r != c and mr == mc:
+                    B = B + B.T
+                elif mr > mc:
+                    mr, mc, B = mc, mr, B.T
+                orow.append(mr)
+                ocol.append(mc)
+                oval.append(B.T.reshape(9))
+    return (np.array(orow, np.int32), np.array(ocol, np.int32), np.array(oval, np.float64).reshape(-1, 9))
+
+
+def galerkin_prolongation(fine_blocks, coarse_blocks, prefix, fine_to_coarse, bases, masks, rest):
+    """The dense prolongation P (3 fine_blocks x 3 coarse_blocks) of the map."""
+    rest = np.asarray(rest, np.float64).reshape(-1)
+    P = np.zeros((3 * fine_blocks, 3 * coarse_blocks))
+    for blk in range(fine_blocks):
+        base, width, phi = galerkin_transform(blk, prefix, fine_to_coarse, bases, masks, rest)
+        for a in range(width):
+            P[3 * blk:3 * blk + 3, 3 * (base + a):3 * (base + a) + 3] = phi[a] * np.eye(3)
+    return P
+
+
 def sym_spmv(a, vals, rows, cols, x, b=0.0, y=None):
     x = _c(x, np.float64)
     y = np.zeros_like(x) if y is None else _c(y, np.float64).copy()
