@@ -714,11 +714,6 @@ MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int 
     MREQ((long long)hessian_offset + n_vertices <= 0x7fffffffLL && hessian_offset >= 0, MASPCG_ERR_CAPACITY,
          "block index overflow");
     MREQ(10LL * n_tets <= 0x7fffffffLL, MASPCG_ERR_CAPACITY, "too many tets");
-    // vertex ids must address x (checked on a host copy)
-    {
-      const std::vector<unsigned> ht = host_copy(h, tets, 4 * (size_t)n_tets);
-      for (unsigned v : ht) MREQ(v < (unsigned)n_vertices, MASPCG_ERR_INVALID_ARGUMENT, "tet vertex id out of range");
-    }
     const unsigned* td = device_in(h, tets, 4 * (size_t)n_tets, h->fem_tets);
     const double* xd = device_in(h, x, 3 * (size_t)n_vertices, h->fem_x);
     const double* di = device_in(h, dm_inverse, 9 * (size_t)n_tets, h->fem_dminv);
@@ -735,7 +730,7 @@ MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int 
     int* ro = device_out(rows, 10 * (size_t)n_tets, h->asm_rows_out);
     int* co = device_out(cols, 10 * (size_t)n_tets, h->asm_cols_out);
     double* va = device_out(values9_colmajor, 90 * (size_t)n_tets, h->asm_vals_out);
-    maspcg::fem_snk1(h, n_tets, td, xd, di, vo, lr, vr, dt, hessian_offset, gd, ro, co, va);
+    maspcg::fem_snk1(h, n_tets, n_vertices, td, xd, di, vo, lr, vr, dt, hessian_offset, gd, ro, co, va);
     if (!dev) copy_back(h, gradient, gd, 3 * (size_t)n_vertices);
     copy_back(h, rows, ro, 10 * (size_t)n_tets);
     copy_back(h, cols, co, 10 * (size_t)n_tets);

@@ -137,12 +137,17 @@ __global__ void __launch_bounds__(kFemTpb) k_fem_snk1(int ntet, const unsigned* 
                                                       const double* __restrict__ volume,
                                                       const double* __restrict__ len_rate,
                                                       const double* __restrict__ vol_rate, double dt2, int offset,
-                                                      double* gradient, int* rows, int* cols, double* vals)
+                                                      int nverts, double* gradient, int* rows, int* cols,
+                                                      double* vals, int* bad)
 {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntet) return;
   const unsigned v[4] = {tets[4 * (size_t)t], tets[4 * (size_t)t + 1], tets[4 * (size_t)t + 2],
                          tets[4 * (size_t)t + 3]};
+  if (v[0] >= (unsigned)nverts || v[1] >= (unsigned)nverts || v[2] >= (unsigned)nverts || v[3] >= (unsigned)nverts) {
+    atomicExch(bad, 1);  // the tet is skipped; the call reports the error
+    return;
+  }
   const double* Di = dm_inv + 9 * (size_t)t;  // row-major Dm^-1
   double Ds[9];
 #pragma unroll
@@ -282,15 +287,23 @@ __global__ void __launch_bounds__(kFemTpb) k_fem_snk1(int ntet, const unsigned* 
 
 }  // namespace
 
-void fem_snk1(maspcg_handle* h, int ntet, const unsigned* tets, const double* x, const double* dm_inv,
+void fem_snk1(maspcg_handle* h, int ntet, int nverts, const unsigned* tets, const double* x, const double* dm_inv,
               const double* volume, const double* len_rate, const double* vol_rate, double dt, int offset,
               double* gradient, int* rows, int* cols, double* vals)
 {
   if (ntet <= 0) return;
+  h->asm_flags.resize(std::max<size_t>(h->asm_flags.n, 1));
+  int* bad = h->asm_flags.get();
+  MCK(cudaMemsetAsync(bad, 0, sizeof(int), h->stream));
   k_fem_snk1<<<ceil_div(ntet, kFemTpb), kFemTpb, 0, h->stream>>>(ntet, tets, x, dm_inv, volume, len_rate, vol_rate,
-                                                                 dt * dt, offset, gradient, rows, cols, vals);
+                                                                 dt * dt, offset, nverts, gradient, rows, cols, vals,
+                                                                 bad);
   MLAUNCHED(h);
   MCK(cudaGetLastError());
+  int flag = 0;
+  MCK(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  MCK(cudaStreamSynchronize(h->stream));
+  MREQ(flag == 0, MASPCG_ERR_INVALID_ARGUMENT, "tet vertex id out of range");
 }
 
 }  // namespace maspcg

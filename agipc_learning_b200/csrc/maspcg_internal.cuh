@@ -312,7 +312,7 @@ void galerkin_restrict(maspcg_handle* h, const GalerkinMap& m, const double* fin
 void galerkin_prolong(maspcg_handle* h, const GalerkinMap& m, const double* coarse, double* fine);
 
 // fem.cu (device pointers)
-void fem_snk1(maspcg_handle* h, int ntet, const unsigned* tets, const double* x, const double* dm_inv,
+void fem_snk1(maspcg_handle* h, int ntet, int nverts, const unsigned* tets, const double* x, const double* dm_inv,
               const double* volume, const double* len_rate, const double* vol_rate, double dt, int offset,
               double* gradient, int* rows, int* cols, double* vals);
 

@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--scale", type=int, default=None, help="smaller cube edge (debug only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-widened", action="store_true", help="skip the rows in front of the solve")
     return ap.parse_args()
 
 
@@ -166,6 +167,100 @@ def run_reference(args, world, rank):
             "full_solve_ms": full_ms, "rel_res_true": full["rel_res_true"]}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def widened_rows(stream, dev):
+    """Device times of the rows in front of the solve, on the bench workload's
+    64^3 mesh (1,500,282 tets): the SNK1 element kernel, the merge of its
+    15 M triplets, and the Galerkin coarse matrix of the merged matrix for
+    2x2x2 vertex cubes (affine coarse nodes).  CUDA events on the stream the
+    library runs on; mean of 3 launches after one warm-up."""
+    import ctypes
+    import numpy as np
+    import torch
+    from agipc_learning_b200 import fem, galerkin, synth
+    from agipc_learning_b200.solver import MasPcg
+
+    n = 64
+    X, tets = synth.box_mesh(n, n, n, 0.01)
+    rng = np.random.default_rng(20261204)
+    x = X + 0.001 * rng.uniform(-1, 1, X.shape)
+    Di, vol, u, r = fem.rest_data(tets, X, 1e6, 0.45)
+    nt, nv = len(tets), len(X)
+    out = {"workload": f"{n}^3 box, {nt} tets, E=1e6, nu=0.45, positions perturbed by 0.1 h"}
+    with torch.cuda.stream(stream):
+        D = lambda a, t: torch.from_numpy(np.ascontiguousarray(a, t)).to(dev)  # noqa: E731
+        tets_d, x_d, di_d = D(tets, np.int32), D(x, np.float64), D(Di, np.float64)
+        vol_d, u_d, r_d = D(vol, np.float64), D(u, np.float64), D(r, np.float64)
+        m_trip = 10 * nt
+        rows_d = torch.empty(m_trip, dtype=torch.int32, device=dev)
+        cols_d = torch.empty_like(rows_d)
+        vals_d = torch.empty((m_trip, 9), dtype=torch.float64, device=dev)
+        grad_d = torch.zeros(3 * nv, dtype=torch.float64, device=dev)
+        orow_d, ocol_d = torch.empty_like(rows_d), torch.empty_like(rows_d)
+        oval_d = torch.empty_like(vals_d)
+        P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        with MasPcg() as m:
+            m.set_stream(stream.cuda_stream)
+            cnt = ctypes.c_int()
+
+            def fem_call():
+                grad_d.zero_()
+                m._ck(m.lib.maspcg_fem_snk1_gradient_hessian(m.h, nt, P(tets_d), nv, P(x_d), P(di_d), P(vol_d),
+                                                              P(u_d), P(r_d), 1 / 60, 0, P(grad_d), P(rows_d),
+                                                              P(cols_d), P(vals_d)))
+
+            def merge_call():
+                m._ck(m.lib.maspcg_convert_bcoo(m.h, P(vals_d), P(rows_d), P(cols_d), m_trip, P(oval_d), P(orow_d),
+                                                P(ocol_d), ctypes.byref(cnt)))
+
+            def timed3(fn):
+                fn()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(3):
+                    fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1) / 3
+
+            ms_fem = timed3(fem_call)
+            ms_merge = timed3(merge_call)
+            # 12 gathered positions + Dm^-1 + volume + rates + tet in, 10 triplets + gradient atomics out
+            fem_bytes = nt * (16 + 96 + 72 + 24 + 10 * (8 + 72) + 96)
+            out["fem_snk1"] = {"ms": ms_fem, "tets_per_s": nt / (ms_fem * 1e-3), "algorithmic_bytes": fem_bytes,
+                               "GBps": fem_bytes / (ms_fem * 1e-3) / 1e9}
+            out["convert_bcoo"] = {"ms": ms_merge, "triplets": m_trip, "unique_blocks": cnt.value,
+                                   "triplets_per_s": m_trip / (ms_merge * 1e-3)}
+            # Galerkin coarse matrix of the merged fine matrix (host arrays, copies included)
+            u_rows = orow_d[:cnt.value].cpu().numpy()
+            u_cols = ocol_d[:cnt.value].cpu().numpy()
+            u_vals = oval_d[:cnt.value].cpu().numpy()
+            v = np.arange(nv)
+            i, j, k = v % n, (v // n) % n, v // (n * n)
+            h2 = n // 2
+            groups = (((k // 2) * h2 + j // 2) * h2 + i // 2).astype(np.int32)
+            nc = h2 ** 3
+            mp = galerkin.GalerkinMapping(0, groups, (4 * np.arange(nc)).astype(np.int32),
+                                          np.full(nc, 15, np.int32), X, 4 * nc)
+            r_d2, c_d2, v_d2 = (torch.from_numpy(u_rows).to(dev), torch.from_numpy(u_cols).to(dev),
+                                torch.from_numpy(u_vals).to(dev))
+            g, keep = mp._struct()
+            cap = 16 * cnt.value
+            crow_d = torch.empty(cap, dtype=torch.int32, device=dev)
+            ccol_d = torch.empty_like(crow_d)
+            cval_d = torch.empty((cap, 9), dtype=torch.float64, device=dev)
+            ncoarse = ctypes.c_int()
+
+            def gal_call():
+                m._ck(m.lib.maspcg_galerkin_coarse_matrix(m.h, ctypes.byref(g), P(v_d2), P(r_d2), P(c_d2), cnt.value,
+                                                          P(cval_d), P(crow_d), P(ccol_d), cap,
+                                                          ctypes.byref(ncoarse)))
+
+            ms_gal = timed3(gal_call)
+            out["galerkin_coarse_matrix"] = {"ms": ms_gal, "fine_blocks": cnt.value, "coarse_blocks": ncoarse.value,
+                                             "coarse_rows": 4 * nc, "mapping": "2x2x2 vertex cubes, affine"}
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -312,6 +407,11 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if not args.no_widened:
+        try:
+            line["widened_rows"] = widened_rows(stream, dev)
+        except Exception as exc:  # reported, not fatal for the headline
+            line["widened_rows"] = {"error": str(exc)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         oracle.build()

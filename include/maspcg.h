@@ -288,7 +288,9 @@ MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, con
  * gradient (3 doubles per vertex) is accumulated with FP64 atomics, as in the
  * reference: clear it first.  rows/cols/values9_colmajor receive 10 triplets
  * per tet at [10t, 10t + 10): the tet's upper 3x3 blocks with vertex ids +
- * hessian_offset, row <= col.  Host or device pointers (all of one kind). */
+ * hessian_offset, row <= col.  A vertex id >= n_vertices returns
+ * MASPCG_ERR_INVALID_ARGUMENT (checked on the device; that tet is skipped and
+ * the outputs are unspecified).  Host or device pointers. */
 MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int n_tets, const unsigned* tets,
                                                           int n_vertices, const double* x, const double* dm_inverse,
                                                           const double* volume, const double* len_rate,
