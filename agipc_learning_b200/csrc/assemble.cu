@@ -1,8 +1,8 @@
 // assemble.cu -- the two triplet steps in front of the solve, on the device:
 //
 // * convert_bcoo: Converter::convert (StiffGIPC/linear_system/utils/
-//   converter.cu:137-284).  Triplets keyed (row << 32) + col are radix-sorted
-//   (stable), runs of equal keys are found with head flags and an exclusive
+//   converter.cu:137-284).  Triplets keyed (row << 32) + col (packed into as
+//   few bits as the indices need: the same order) are radix-sorted (stable), runs of equal keys are found with head flags and an exclusive
 //   scan, and each run's 3x3 blocks are summed.  The reference sums a run with
 //   a warp head-segmented reduction plus FP64 atomics, whose order varies;
 //   here one thread sums its run in the stable sort order, so the result is
@@ -26,14 +26,33 @@ namespace {
 
 constexpr int kAsmTpb = 256;
 
-__global__ void k_conv_keys(const int* __restrict__ rows, const int* __restrict__ cols, int n,
-                            unsigned long long* keys, int* idx, int* bad)
+// Largest row and column index (for the key width), and a flag for
+// negative indices.
+__global__ void k_conv_range(const int* __restrict__ rows, const int* __restrict__ cols, int n, int* flags)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = -1, c = -1;
+  if (i < n) {
+    r = rows[i];
+    c = cols[i];
+    if (r < 0 || c < 0) atomicExch(flags, 1);
+  }
+  r = __reduce_max_sync(0xffffffffu, (unsigned)max(r, 0));
+  c = __reduce_max_sync(0xffffffffu, (unsigned)max(c, 0));
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(flags + 1, r);
+    atomicMax(flags + 2, c);
+  }
+}
+
+// Key (row << col_bits) + col: the order of (row << 32) + col in as few bits
+// as the indices need, so the radix sort runs only the passes it must.
+__global__ void k_conv_keys(const int* __restrict__ rows, const int* __restrict__ cols, int n, int col_bits,
+                            unsigned long long* keys, int* idx)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int r = rows[i], c = cols[i];
-  if (r < 0 || c < 0) atomicExch(bad, 1);
-  keys[i] = ((unsigned long long)(unsigned)max(r, 0) << 32) + (unsigned long long)(unsigned)max(c, 0);
+  keys[i] = ((unsigned long long)(unsigned)rows[i] << col_bits) + (unsigned long long)(unsigned)cols[i];
   idx[i] = i;
 }
 
@@ -54,15 +73,15 @@ __global__ void k_conv_starts(const int* __restrict__ heads, const int* __restri
 // One thread per unique key: its row and column, and the sum of its run's
 // blocks in sorted (stable) order.
 __global__ void k_conv_sum(const unsigned long long* __restrict__ keys, const int* __restrict__ perm,
-                           const int* __restrict__ start, int count, const double* __restrict__ vals, int* rows_out,
-                           int* cols_out, double* vals_out)
+                           const int* __restrict__ start, int count, int col_bits, const double* __restrict__ vals,
+                           int* rows_out, int* cols_out, double* vals_out)
 {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= count) return;
   const int s = start[u], e = start[u + 1];
   const unsigned long long k = keys[s];
-  rows_out[u] = (int)(k >> 32);
-  cols_out[u] = (int)(k & 0xffffffffull);
+  rows_out[u] = (int)(k >> col_bits);
+  cols_out[u] = (int)(k & ((1ull << col_bits) - 1ull));
   double a[9];
 #pragma unroll
   for (int q = 0; q < 9; ++q) a[q] = 0.0;
@@ -101,14 +120,6 @@ __global__ void k_gather_triplets(const int* __restrict__ perm, int n, const int
   for (int q = 0; q < 9; ++q) vals_out[9 * (size_t)i + q] = vals[9 * (size_t)p + q];
 }
 
-int read_flag(maspcg_handle* h, const int* d)
-{
-  int v = 0;
-  MCK(cudaMemcpyAsync(&v, d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  MCK(cudaStreamSynchronize(h->stream));
-  return v;
-}
-
 }  // namespace
 
 int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const double* vals, int n, int* rows_out,
@@ -118,28 +129,38 @@ int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const doubl
   cudaStream_t st = h->stream;
   h->asm_keys.resize(2 * (size_t)n);
   h->asm_idx.resize(2 * (size_t)n);
-  h->asm_flags.resize(2 * (size_t)n + 2);
+  h->asm_flags.resize(2 * (size_t)n + 4);
   unsigned long long* k0 = h->asm_keys.get();
   unsigned long long* k1 = k0 + n;
   int* i0 = h->asm_idx.get();
   int* i1 = i0 + n;
   int* heads = h->asm_flags.get();
   int* pos = heads + n;
-  int* bad = pos + n;
-  MCK(cudaMemsetAsync(bad, 0, sizeof(int), st));
+  int* flags = pos + n;  // negative index, max row, max col
+  MCK(cudaMemsetAsync(flags, 0, 3 * sizeof(int), st));
   const int grid = ceil_div(n, kAsmTpb);
-  k_conv_keys<<<grid, kAsmTpb, 0, st>>>(rows, cols, n, k0, i0, bad); MLAUNCHED(h);
+  k_conv_range<<<grid, kAsmTpb, 0, st>>>(rows, cols, n, flags); MLAUNCHED(h);
+  int fl[3] = {0, 0, 0};
+  MCK(cudaMemcpyAsync(fl, flags, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaStreamSynchronize(st));
+  MREQ(fl[0] == 0, MASPCG_ERR_INVALID_ARGUMENT, "negative row or column index");
+  auto bits = [](unsigned v) {
+    int b = 1;
+    while (b < 32 && (v >> b) != 0u) ++b;
+    return b;
+  };
+  const int col_bits = bits((unsigned)fl[2]), key_bits = col_bits + bits((unsigned)fl[1]);
+  k_conv_keys<<<grid, kAsmTpb, 0, st>>>(rows, cols, n, col_bits, k0, i0); MLAUNCHED(h);
   size_t need = 0;
-  MCK(cub::DeviceRadixSort::SortPairs(nullptr, need, k0, k1, i0, i1, n, 0, 64, st));
+  MCK(cub::DeviceRadixSort::SortPairs(nullptr, need, k0, k1, i0, i1, n, 0, key_bits, st));
   size_t need2 = 0;
   MCK(cub::DeviceScan::ExclusiveSum(nullptr, need2, heads, pos, n, st));
   h->cub_tmp.resize(std::max(std::max(need, need2), h->cub_tmp.n));
   size_t tb = h->cub_tmp.cap;
-  MCK(cub::DeviceRadixSort::SortPairs(h->cub_tmp.get(), tb, k0, k1, i0, i1, n, 0, 64, st));
+  MCK(cub::DeviceRadixSort::SortPairs(h->cub_tmp.get(), tb, k0, k1, i0, i1, n, 0, key_bits, st));
   k_conv_heads<<<grid, kAsmTpb, 0, st>>>(k1, n, heads); MLAUNCHED(h);
   tb = h->cub_tmp.cap;
   MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), tb, heads, pos, n, st));
-  MREQ(read_flag(h, bad) == 0, MASPCG_ERR_INVALID_ARGUMENT, "negative row or column index");
   int last[2] = {0, 0};
   MCK(cudaMemcpyAsync(&last[0], pos + (n - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
   MCK(cudaMemcpyAsync(&last[1], heads + (n - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -147,8 +168,8 @@ int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const doubl
   const int count = last[0] + last[1];
   h->asm_start.resize((size_t)count + 1);
   k_conv_starts<<<grid, kAsmTpb, 0, st>>>(heads, pos, n, h->asm_start.get()); MLAUNCHED(h);
-  k_conv_sum<<<ceil_div(count, kAsmTpb), kAsmTpb, 0, st>>>(k1, i1, h->asm_start.get(), count, vals, rows_out,
-                                                          cols_out, vals_out); MLAUNCHED(h);
+  k_conv_sum<<<ceil_div(count, kAsmTpb), kAsmTpb, 0, st>>>(k1, i1, h->asm_start.get(), count, col_bits, vals,
+                                                          rows_out, cols_out, vals_out); MLAUNCHED(h);
   MCK(cudaGetLastError());
   return count;
 }
