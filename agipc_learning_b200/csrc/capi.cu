@@ -436,9 +436,25 @@ MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* 
     h->fem_off = fem_offset_blocks;
     h->abd_bodies = abd_body_count;
     h->n_in = n_blocks;
-    const double* v = device_in(h, values9, (size_t)9 * n_blocks, h->in_vals);
     const int* r = device_in(h, rows, (size_t)n_blocks, h->in_rows);
     const int* c = device_in(h, cols, (size_t)n_blocks, h->in_cols);
+    // Host values (the bulk of the input) are copied on the side stream while
+    // the structure is built from the indices; the value fill waits for them.
+    const double* v = values9;
+    h->vals_pending = false;
+    if (n_blocks > 0) {
+      MREQ(values9 != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null array argument");
+      if (!is_device_ptr(values9)) {
+        h->in_vals.resize((size_t)9 * n_blocks);
+        MCK(cudaEventRecord(h->ev_fork, h->stream));  // earlier readers of in_vals are done
+        MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+        MCK(cudaMemcpyAsync(h->in_vals.get(), values9, sizeof(double) * 9 * (size_t)n_blocks,
+                            cudaMemcpyHostToDevice, h->side_stream));
+        MCK(cudaEventRecord(h->ev_join, h->side_stream));
+        h->vals_pending = true;
+        v = h->in_vals.get();
+      }
+    }
     maspcg::build_internal_matrix(h, v, r, c, n_blocks);
     alloc_vectors(h);
     MCK(cudaStreamSynchronize(h->stream));

@@ -255,6 +255,7 @@ struct maspcg_handle {
   long long graph_kernels = 0;    // kernel nodes of the captured batch graph
   bool use_pdl = false;           // programmatic dependent launch for the iteration kernels (MASPCG_FLAG_PDL)
   bool fused_head = false;        // p update + SpMV + x/r update as one cooperative kernel (MASPCG_FLAG_FUSED_HEAD)
+  bool vals_pending = false;      // set_matrix_bcoo: host values still copying on side_stream (ev_join)
   bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
   int apply_variant = 2;          // 16-bit level-0 apply: 0 direct loads, 1 TMA-staged x2 buffers, 2 TMA-staged x1
 };

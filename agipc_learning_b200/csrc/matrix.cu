@@ -320,6 +320,10 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   // rowptr = exclusive scan of the per-row counts (the extra entry gives nnzb)
   tb = h->cub_tmp.cap;
   MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), tb, h->row_count.get(), h->rowptr.get(), nb_int + 1, st));
+  if (h->vals_pending) {  // host values copied on the side stream
+    MCK(cudaStreamWaitEvent(st, h->ev_join, 0));
+    h->vals_pending = false;
+  }
   k_fill_values<<<ceil_div(nnzb, kTpb), kTpb, 0, st>>>(h->keys_sorted.get(), h->kv_sorted.get(), h->seg_start.get(),
                                                       nnzb, m_valid, vals, h->val64.get(), h->val32.get());
   MLAUNCHED(h);
