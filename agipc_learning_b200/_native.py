@@ -22,6 +22,7 @@ ERR_NO_DEVICE = 7
 ERR_UNSUPPORTED = 8
 
 PRECOND_BLOCK_JACOBI = 0
+PRECOND_MAS16 = 1
 PRECOND_MAS32 = 2
 PRECOND_NONE = 3
 

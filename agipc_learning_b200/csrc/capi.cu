@@ -78,15 +78,16 @@ maspcg_status guard(maspcg_handle* h, F&& f)
   }
 }
 
-int compute_num_levels(int vert_num)
+int compute_num_levels(int vert_num, int bank)
 {
-  // computeNumLevels (TraditionalMAS32Preconditioner.cu:2142-2161)
+  // computeNumLevels (TraditionalMAS32Preconditioner.cu:2142-2161,
+  // MASPreconditioner.cu:1727-1746 with BANKSIZE 16)
   int n_level = 1;
-  int level_sz = (vert_num + 31) / 32 * 32;
-  while (level_sz > 32) {
-    level_sz /= 32;
+  int level_sz = (vert_num + bank - 1) / bank * bank;
+  while (level_sz > bank) {
+    level_sz /= bank;
     n_level++;
-    level_sz = (level_sz + 31) / 32 * 32;
+    level_sz = (level_sz + bank - 1) / bank * bank;
   }
   n_level += 1;
   return n_level > 6 ? 6 : n_level;
@@ -229,14 +230,23 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
   maspcg_config c;
   maspcg_config_default(&c);
   if (cfg) c = *cfg;
-  if (c.bank_size != 32) {
-    g_create_error = "only the 32-vertex MAS bank is supported";
+  if (c.bank_size != 32 && c.bank_size != 16) {
+    g_create_error = "the MAS bank is 32 (TraditionalMAS32) or 16 (CEMAS16) vertices";
+    return MASPCG_ERR_UNSUPPORTED;
+  }
+  if ((c.preconditioner == MASPCG_PRECOND_MAS32 && c.bank_size != 32) ||
+      (c.preconditioner == MASPCG_PRECOND_MAS16 && c.bank_size != 16)) {
+    g_create_error = "MAS32 takes the 32-vertex bank, CEMAS16 the 16-vertex bank";
+    return MASPCG_ERR_UNSUPPORTED;
+  }
+  if (c.preconditioner == MASPCG_PRECOND_MAS16 && c.inverse_storage != MASPCG_INV_FP32) {
+    g_create_error = "CEMAS16 stores FP32 inverses";
     return MASPCG_ERR_UNSUPPORTED;
   }
   if (!(c.tolerance > 0) || c.precision < 0 || c.precision > 2 || c.gate < 0 || c.gate > 1 ||
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
-        c.preconditioner == MASPCG_PRECOND_NONE) ||
+        c.preconditioner == MASPCG_PRECOND_MAS16 || c.preconditioner == MASPCG_PRECOND_NONE) ||
       c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~31) != 0 ||
       ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_DIRECT))) {
     g_create_error = "invalid configuration";
@@ -315,9 +325,11 @@ MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int co
                                           const int* part_map_real, int part_map_size, const int* real_map_part)
 {
   return guard(h, [&] {
+    const int bank = h->cfg.bank_size;
     MREQ(vert_num >= 1, MASPCG_ERR_INVALID_ARGUMENT, "vert_num must be >= 1");
-    MREQ(part_map_size >= vert_num && part_map_size % 32 == 0, MASPCG_ERR_INVALID_ARGUMENT,
-         "part_map_size must be a multiple of 32 and >= vert_num");
+    MREQ(part_map_size >= vert_num && part_map_size % bank == 0, MASPCG_ERR_INVALID_ARGUMENT,
+         bank == 16 ? "part_map_size must be a multiple of 16 and >= vert_num"
+                    : "part_map_size must be a multiple of 32 and >= vert_num");
     MREQ(neighbor_list_size >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative neighbor_list_size");
     const auto st = host_copy(h, neighbor_start, vert_num);
     const auto nn = host_copy(h, neighbor_num, vert_num);
@@ -338,15 +350,18 @@ MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int co
       mapped += pmr[s] >= 0;
     }
     MREQ(mapped == vert_num, MASPCG_ERR_INVALID_ARGUMENT, "part_map_real must map every vertex once");
-    for (int b = 0; b < part_map_size / 32; ++b)
-      MREQ(pmr[32 * b] >= 0, MASPCG_ERR_INVALID_ARGUMENT, "lane 0 of every 32-slot bank must hold a vertex");
+    for (int b = 0; b < part_map_size / bank; ++b)
+      MREQ(pmr[bank * b] >= 0, MASPCG_ERR_INVALID_ARGUMENT,
+           bank == 16 ? "lane 0 of every 16-slot bank must hold a vertex"
+                      : "lane 0 of every 32-slot bank must hold a vertex");
 
+    h->bank = bank;
     h->nv = vert_num;
     h->c0 = part_map_size;
     h->node_offset = collision_node_offset;
     h->nlist_size = neighbor_list_size;
-    h->levelnum = compute_num_levels(std::max(part_map_size, vert_num));
-    h->gn_cap = hierarchy_capacity(vert_num, part_map_size, h->levelnum, 32);
+    h->levelnum = compute_num_levels(std::max(part_map_size, vert_num), bank);
+    h->gn_cap = hierarchy_capacity(vert_num, part_map_size, h->levelnum, bank);
     cudaStream_t s = h->stream;
     auto up = [&](auto& buf, const auto& vec) {
       buf.resize(std::max<size_t>(vec.size(), 1));
@@ -365,10 +380,10 @@ MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int co
     const int L = h->levelnum;
     h->fine_mask.resize(vert_num);
     h->next_mask.resize(vert_num);
-    h->next_prefix.resize(vert_num / 32 + 2);
-    h->next_prefix_sum.resize(vert_num / 32 + 2);
-    h->prefix_orig.resize(part_map_size / 32 + 1);
-    h->prefix_sum_orig.resize(part_map_size / 32 + 1);
+    h->next_prefix.resize(vert_num / bank + 2);
+    h->next_prefix_sum.resize(vert_num / bank + 2);
+    h->prefix_orig.resize(part_map_size / bank + 1);
+    h->prefix_sum_orig.resize(part_map_size / bank + 1);
     h->cst.resize((size_t)vert_num * L);
     h->going_next.resize((size_t)h->gn_cap);
     MCK(cudaMemsetAsync(h->going_next.get(), 0xff, (size_t)h->gn_cap * 4, s));
@@ -426,8 +441,8 @@ MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* 
     MREQ(fem_offset_blocks >= 0 && abd_body_count >= 0 && 4LL * abd_body_count <= block_rows,
          MASPCG_ERR_INVALID_ARGUMENT, "invalid offsets");
     MREQ(n_blocks <= (1 << 29), MASPCG_ERR_CAPACITY, "too many blocks");
-    if (h->cfg.preconditioner == MASPCG_PRECOND_MAS32) {
-      MREQ(h->has_graph, MASPCG_ERR_NOT_READY, "MAS32 needs set_graph before set_matrix_bcoo");
+    if (h->cfg.preconditioner == MASPCG_PRECOND_MAS32 || h->cfg.preconditioner == MASPCG_PRECOND_MAS16) {
+      MREQ(h->has_graph, MASPCG_ERR_NOT_READY, "MAS needs set_graph before set_matrix_bcoo");
       MREQ(4LL * abd_body_count <= fem_offset_blocks, MASPCG_ERR_INVALID_ARGUMENT, "ABD rows overlap the FEM range");
       MREQ((long long)fem_offset_blocks + h->nv <= block_rows, MASPCG_ERR_INVALID_ARGUMENT,
            "FEM range exceeds block_rows");
@@ -563,7 +578,7 @@ MASPCG_API maspcg_status maspcg_get_hierarchy(maspcg_handle* h, uint32_t* fine_m
                                               int* level_size, int* coarse_table, int* prefix_original)
 {
   return guard(h, [&] {
-    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS32 preconditioner first");
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS preconditioner first");
     cudaStream_t s = h->stream;
     const size_t nv = h->nv;
     if (fine_mask) MCK(cudaMemcpyAsync(fine_mask, h->fine_mask.get(), nv * 4, cudaMemcpyDeviceToHost, s));
@@ -575,7 +590,8 @@ MASPCG_API maspcg_status maspcg_get_hierarchy(maspcg_handle* h, uint32_t* fine_m
                           s));
     if (coarse_table) MCK(cudaMemcpyAsync(coarse_table, h->coarse_table.get(), nv * 6 * 4, cudaMemcpyDeviceToHost, s));
     if (prefix_original)
-      MCK(cudaMemcpyAsync(prefix_original, h->prefix_orig.get(), (size_t)(h->c0 / 32) * 4, cudaMemcpyDeviceToHost, s));
+      MCK(cudaMemcpyAsync(prefix_original, h->prefix_orig.get(), (size_t)(h->c0 / h->bank) * 4, cudaMemcpyDeviceToHost,
+                          s));
     MCK(cudaStreamSynchronize(s));
   });
 }
@@ -598,7 +614,7 @@ MASPCG_API maspcg_status maspcg_get_bcsr(maspcg_handle* h, int* rowptr, int* col
 MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out)
 {
   return guard(h, [&] {
-    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS32 preconditioner first");
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS preconditioner first");
     MREQ(out, MASPCG_ERR_INVALID_ARGUMENT, "null output");
     maspcg::decode_inverses(h, out);
   });
@@ -607,9 +623,9 @@ MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out
 MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* out)
 {
   return guard(h, [&] {
-    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS32 preconditioner first");
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS preconditioner first");
     MREQ(out, MASPCG_ERR_INVALID_ARGUMENT, "null output");
-    const size_t n = (size_t)h->lv.domains * maspcg::kPacked * 9;
+    const size_t n = (size_t)h->lv.domains * (h->bank == 16 ? maspcg::kMas16Packed : maspcg::kPacked) * 9;
     DBuf<double> tmp;
     tmp.resize(n);
     MCK(cudaMemsetAsync(tmp.get(), 0, n * sizeof(double), h->stream));

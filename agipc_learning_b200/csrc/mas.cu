@@ -66,16 +66,40 @@ __global__ void k_member_offsets(const unsigned* __restrict__ keys, int nreal, i
   if (p == nreal - 1) off[count] = nreal;
 }
 
-__device__ __forceinline__ int pk(int a, int b) { return kBank * a - a * (a + 1) / 2 + b; }
+template <int kB>
+__device__ __forceinline__ int pkb(int a, int b) { return kB * a - a * (a + 1) / 2 + b; }
+
+// CEMAS16 assembly (MASPreconditioner.cu prepare_hessian_bcoo_kernel
+// :1822-1914 and prepare_hessian_bcoo_sum_kernel :1916-2037) differs from
+// MAS32 on the entries (rs, u) of a fine row whose column lies in the row's
+// own level-0 bank (rs, u: level-0 slots):
+//  * an in-bank upper block is kept only when its column's slot is not
+//    below its row's: a pair whose slot order runs against its vertex order
+//    is not transposed (MAS32 transposes it) but dropped, at every level;
+//  * in a bank that is one component, the coarse diagonal block receives
+//    the entries of rows (2k, 2k+1) through the entry (2k, 0), so a row
+//    whose even partner slot is padding adds nothing to the coarse levels.
+// pmr: part_map_real; prefix_orig: components per level-0 bank (null for
+// the level-0 domain itself).
+__device__ __forceinline__ bool cemas16_drops(int rs, int u, const int* __restrict__ pmr,
+                                              const int* __restrict__ prefix_orig)
+{
+  if ((u >> 4) != (rs >> 4)) return false;
+  if (u != rs && ((pmr[rs] < pmr[u]) != (rs < u))) return true;
+  return prefix_orig && prefix_orig[rs >> 4] == 1 && pmr[rs & ~1] < 0;
+}
 
 // Accumulate the fine row `row` into the owner lanes: every block whose
-// column's level node `B` lies in bank `bank` is added by lane B % 32.
+// column's level node `B` lies in bank `bank` is added by lane B % kB.
 // Staging: 16 blocks per chunk through the warp's shared-memory slots, so
 // the 9 doubles of a block are read coalesced and summed in block order.
+// kB = 16 applies the CEMAS16 rules (pmr non-null).
+template <int kB>
 __device__ __forceinline__ void gather_row(const int* __restrict__ rowptr, const int* __restrict__ colidx,
                                            const double* __restrict__ val64, const int* __restrict__ cmap, int row,
                                            int fem_off, int c0, int bank, int lane, double* stage, int* sdest,
-                                           double acc[9])
+                                           double acc[9], const int* __restrict__ pmr = nullptr,
+                                           const int* __restrict__ prefix_orig = nullptr)
 {
   const int rs = rowptr[row], re = rowptr[row + 1];
   for (int t0 = rs; t0 < re; t0 += 16) {
@@ -85,7 +109,8 @@ __device__ __forceinline__ void gather_row(const int* __restrict__ rowptr, const
       const int u = colidx[t0 + lane] - fem_off;
       if (u >= 0 && u < c0) {
         const int B = cmap ? cmap[u] : u;
-        if (B >= 0 && (B >> 5) == bank) dest = B & 31;
+        if (B >= 0 && B / kB == bank) dest = B % kB;
+        if (kB == 16 && dest >= 0 && cemas16_drops(row - fem_off, u, pmr, prefix_orig)) dest = -1;
       }
       sdest[lane] = dest;
     }
@@ -103,6 +128,8 @@ __device__ __forceinline__ void gather_row(const int* __restrict__ rowptr, const
 }
 
 struct CoarseArgs {
+  const int* pmr;          // CEMAS16 rules (bank 16 only)
+  const int* prefix_orig;
   const int* perm[kMaxLevels];
   const int* cmap[kMaxLevels];
   int slice_base[kMaxLevels + 1];  // first warp item of each level (levels >= 1)
@@ -114,12 +141,13 @@ struct CoarseArgs {
   const int* colidx;
   const double* val64;
   int fem_off, c0;
-  double* coarse64;  // (domains - dom_begin[1]) x 32 x 32 blocks, row-major 3x3
+  double* coarse64;  // (domains - dom_begin[1]) x kB x kB blocks, row-major 3x3
 };
 
 // Coarse-level Galerkin sums: one warp per slice of a level's member list
 // (fine rows grouped by node); the slice's partial block-row is reduced in
 // registers and added to the FP64 coarse domain matrix once per node.
+template <int kB>
 __global__ void __launch_bounds__(256) k_coarse_assemble(CoarseArgs a)
 {
   __shared__ double stage_s[8][16 * 9];
@@ -138,8 +166,9 @@ __global__ void __launch_bounds__(256) k_coarse_assemble(CoarseArgs a)
   for (int e = 0; e < 9; ++e) acc[e] = 0.0;
   int node = -1;
   auto flush = [&](int A) {
-    const int local = a.dom_begin[L] + (A >> 5) - a.dom_begin[1];
-    double* dst = a.coarse64 + (((size_t)local * 32 + (A & 31)) * 32 + lane) * 9;
+    if (lane >= kB) return;
+    const int local = a.dom_begin[L] + A / kB - a.dom_begin[1];
+    double* dst = a.coarse64 + (((size_t)local * kB + A % kB) * kB + lane) * 9;
 #pragma unroll
     for (int e = 0; e < 9; ++e)
       if (acc[e] != 0.0) atomicAdd(dst + e, acc[e]);
@@ -153,18 +182,19 @@ __global__ void __launch_bounds__(256) k_coarse_assemble(CoarseArgs a)
       for (int e = 0; e < 9; ++e) acc[e] = 0.0;
       node = A;
     }
-    gather_row(a.rowptr, a.colidx, a.val64, cmap, a.fem_off + v, a.fem_off, a.c0, A >> 5, lane, stage_s[lw],
-               sdest_s[lw], acc);
+    gather_row<kB>(a.rowptr, a.colidx, a.val64, cmap, a.fem_off + v, a.fem_off, a.c0, A / kB, lane, stage_s[lw],
+                   sdest_s[lw], acc, a.pmr, a.prefix_orig);
   }
   if (node >= 0) flush(node);
 }
 
-// One CTA per domain; thread (w,lane) owns block (w,lane) of the 96x96 FP64
-// matrix.  FP32 storage: in-place Gauss-Jordan inverse, symmetric layout.
-// 16-bit storage: Cholesky A = L L^T, W = L^-1, stored W S^-1 with column
-// scales S, so the applied operator S (W S^-1)^T (W S^-1) S stays SPD whatever
-// the rounding.
-template <typename TI, bool kAssembled>
+// One CTA per domain; thread (w,lane) owns block (w,lane) of the 3kB x 3kB
+// FP64 matrix (one warp per block row; for kB = 16 lanes 16..31 only help
+// stage the gathered rows).  FP32 storage: in-place Gauss-Jordan inverse,
+// symmetric layout.  16-bit storage (kB = 32): Cholesky A = L L^T,
+// W = L^-1, stored W S^-1 with column scales S, so the applied operator
+// S (W S^-1)^T (W S^-1) S stays SPD whatever the rounding.
+template <typename TI, bool kAssembled, int kB>
 __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom_offset)
 {
   __shared__ double buf[2][96];
@@ -185,17 +215,17 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
   for (int e = 0; e < 9; ++e) acc[e] = 0.0;
   const int d0 = a.lv.dom_begin[1];
   if (g < d0) {
-    const int slot = kBank * g + w;
+    const int slot = kB * g + w;
     if (a.pmr[slot] >= 0)
-      gather_row(a.rowptr, a.colidx, a.val64, nullptr, a.fem_off + slot, a.fem_off, a.c0, g, lane, stage[w],
-                 sdest[w], acc);
-  } else {
-    const double* src = a.coarse64 + (((size_t)(g - d0) * 32 + w) * 32 + lane) * 9;
+      gather_row<kB>(a.rowptr, a.colidx, a.val64, nullptr, a.fem_off + slot, a.fem_off, a.c0, g, lane, stage[w],
+                     sdest[w], acc, a.pmr);
+  } else if (lane < kB) {
+    const double* src = a.coarse64 + (((size_t)(g - d0) * kB + w) * kB + lane) * 9;
 #pragma unroll
     for (int e = 0; e < 9; ++e) acc[e] = src[e];
   }
-  if (kAssembled && lane >= w) {
-    double* o = a.assembled + ((size_t)g * kPacked + pk(w, lane)) * 9;
+  if (kAssembled && lane >= w && lane < kB) {
+    double* o = a.assembled + ((size_t)g * (kB * (kB + 1) / 2) + pkb<kB>(w, lane)) * 9;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -207,11 +237,12 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
     if (acc[8] == 0.0) acc[8] = 1.0;
   }
   constexpr bool kFactored = !std::is_same<TI, float>::value;
-  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * inv_elems<TI>();
+  static_assert(kB == 32 || !kFactored, "16-slot banks store FP32 inverses");
+  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * (kB == 32 ? inv_elems<TI>() : kMas16InvElems);
 
   if (!kFactored) {
     // ---- in-place Gauss-Jordan inversion (the elimination of __inverse6_P96x96)
-    for (int q = 0; q < kBank; ++q) {
+    for (int q = 0; q < kB; ++q) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const int j = 3 * q + c;
@@ -258,16 +289,24 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
     }
     __syncthreads();
     if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
-    const int d = (lane - w) & 31;
-    if (d <= 16) {
-      const bool zero = (d == 16) && (w >= 16);
+    const int d = (lane - w) & (kB - 1);
+    if (lane < kB && d <= kB / 2) {
+      const bool zero = (d == kB / 2) && (w >= kB / 2);
+      if (kB == 16 && d == 0) {
+        // CEMAS16 stores the diagonal blocks with their lower elements
+        // taken from the upper ones (MASPreconditioner.cu:705-711)
+        acc[3] = acc[1];
+        acc[6] = acc[2];
+        acc[7] = acc[5];
+      }
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) out[(d * 9 + 3 * i + j) * kBank + w] = from_d<TI>(zero ? 0.0 : acc[3 * i + j]);
+        for (int j = 0; j < 3; ++j) out[(d * 9 + 3 * i + j) * kB + w] = from_d<TI>(zero ? 0.0 : acc[3 * i + j]);
     }
     return;
   }
+  if constexpr (kFactored) {
 
   // ---- blocked Cholesky, right-looking over the 32 block columns: thread
   // (q,q) factors its 3x3 diagonal block and inverts the factor, the block
@@ -397,6 +436,7 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
       else if ((row >> 4) == (col >> 4))
         out[inv16_pos(row, col)] = from_d<TI>(0.0);
     }
+  }
 }
 
 // ------------------------------------------------------------------ apply --
@@ -922,6 +962,175 @@ __global__ void k_chain_targets(ApplyArgs a, int* target)
     for (int g = lo / kBank; g <= hi / kBank; ++g) atomicAdd(target + (g - d1), 1);
 }
 
+// ---- CEMAS16 apply (MASPreconditioner::preconditioning, :2250-2291) -------
+//
+// Three launches over 16-slot banks:
+//   * the coarse restriction: R of a coarse node is the sum of its member
+//     slots' residuals, read from the member lists in slot order
+//     (__buildMultiLevelR_optimized_new :729-847 adds the same FP32 terms
+//     with atomics, in no fixed order);
+//   * the domain applies of every level, half a warp per 48x48 domain: lane
+//     l holds block (l, (l + d) % 16) of the wrapped diagonals d = 0..8 and
+//     each stored block serves both triangles through a shuffle of width 16
+//     (_schwarzLocalXSym6 :957-1027); level-0 domains read r directly;
+//   * the prolongation z = Z0 + sum of the coarse Z along the vertex's
+//     coarse table, in level order (__collectFinalZ_new :850-881), with r.z.
+struct Mas16Args {
+  const int* pmr;
+  const int* coarse_table;  // 6 global slots per vertex (levels 1..L-1)
+  const int* perm[kMaxLevels];
+  const int* off[kMaxLevels];
+  int node_base[kMaxLevels + 1];  // first restriction thread of each coarse level
+  LevelInfo lv;
+  const float* inv;  // kMas16InvElems per domain
+  float* coarse_r;   // (total_clusters - c0) x 3
+  float* coarse_z;
+  float* z0;  // c0 x 3
+  int fem_off, c0;
+};
+
+template <typename Tv>
+__global__ void __launch_bounds__(kTpb) k16_restrict(Mas16Args a, const Tv* __restrict__ r, PcgScalars* s)
+{
+  pdl_wait();
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.node_base[a.lv.levelnum]) return;
+  int L = 1;
+  while (L + 1 < a.lv.levelnum && t >= a.node_base[L + 1]) ++L;
+  const int A = t - a.node_base[L];
+  const int* perm = a.perm[L];
+  const int p0 = a.off[L][A], p1 = a.off[L][A + 1];
+  float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+  for (int p = p0; p < p1; ++p) {
+    const size_t base = 3 * (size_t)(a.fem_off + perm[p]);
+    x0 += (float)r[base];
+    x1 += (float)r[base + 1];
+    x2 += (float)r[base + 2];
+  }
+  float* o = a.coarse_r + 3 * (size_t)(a.lv.begin[L] + A - a.c0);
+  o[0] = x0;
+  o[1] = x1;
+  o[2] = x2;
+}
+
+template <typename Tv>
+__global__ void __launch_bounds__(kTpb) k16_apply(Mas16Args a, const Tv* __restrict__ r, PcgScalars* s)
+{
+  pdl_wait();
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((t & ~31) >= a.lv.domains * 16) return;  // whole warp past the last domain
+  const int g = t >> 4, lane = t & 15;
+  const bool in = g < a.lv.domains;
+  const bool level0 = g < a.lv.dom_begin[1];
+  const int slot = 16 * g + lane;
+  float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+  if (in) {
+    if (level0) {
+      if (a.pmr[slot] >= 0) {
+        const size_t base = 3 * (size_t)(a.fem_off + slot);
+        x0 = (float)r[base];
+        x1 = (float)r[base + 1];
+        x2 = (float)r[base + 2];
+      }
+    } else {
+      const float* x = a.coarse_r + 3 * (size_t)(slot - a.c0);
+      x0 = x[0];
+      x1 = x[1];
+      x2 = x[2];
+    }
+  }
+  const float* inv = a.inv + (size_t)(in ? g : 0) * kMas16InvElems;
+  float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+#pragma unroll
+  for (int d = 0; d < kMas16Diags; ++d) {
+    const int c = (lane + d) & 15;
+    const float c0 = __shfl_sync(kFull, x0, c, 16), c1 = __shfl_sync(kFull, x1, c, 16),
+                c2 = __shfl_sync(kFull, x2, c, 16);
+    float B[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) B[e] = in ? __ldcs(inv + (d * 9 + e) * 16 + lane) : 0.f;
+    y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
+    y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
+    y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
+    if (d != 0) {
+      const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
+      const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
+      const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
+      const int src = (lane - d) & 15;
+      y0 += __shfl_sync(kFull, t0, src, 16);
+      y1 += __shfl_sync(kFull, t1, src, 16);
+      y2 += __shfl_sync(kFull, t2, src, 16);
+    }
+  }
+  if (!in) return;
+  float* o = level0 ? a.z0 + 3 * (size_t)slot : a.coarse_z + 3 * (size_t)(slot - a.c0);
+  o[0] = y0;
+  o[1] = y1;
+  o[2] = y2;
+}
+
+template <typename Tv, typename Tacc>
+__global__ void __launch_bounds__(kTpb) k16_collect(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
+                                                    int part_base, int total_parts, int mode, PcgScalars* s)
+{
+  pdl_wait();
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  Tacc dot = 0;
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < a.c0; slot += gridDim.x * blockDim.x) {
+    const int v = a.pmr[slot];
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    if (v >= 0) {
+      c0 = a.z0[3 * (size_t)slot];
+      c1 = a.z0[3 * (size_t)slot + 1];
+      c2 = a.z0[3 * (size_t)slot + 2];
+      for (int l = 1; l < a.lv.levelnum; ++l) {
+        const float* zc = a.coarse_z + 3 * (size_t)(a.coarse_table[6 * (size_t)v + l - 1] - a.c0);
+        c0 += zc[0];
+        c1 += zc[1];
+        c2 += zc[2];
+      }
+    }
+    const size_t base = 3 * (size_t)(a.fem_off + slot);
+    const Tv z0 = (Tv)c0, z1 = (Tv)c1, z2 = (Tv)c2;
+    z[base] = z0;
+    z[base + 1] = z1;
+    z[base + 2] = z2;
+    dot += (Tacc)r[base] * (Tacc)z0 + (Tacc)r[base + 1] * (Tacc)z1 + (Tacc)r[base + 2] * (Tacc)z2;
+  }
+  pdl_trigger();
+  if (!partial) return;
+  Tacc total = 0;
+  if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x, total) &&
+      threadIdx.x == 0 && mode > 0)
+    rz_update(s, (double)total, mode);
+}
+
+Mas16Args make_mas16_args(maspcg_handle* h)
+{
+  Mas16Args a{};
+  const LevelInfo& lv = h->lv;
+  a.pmr = h->pmr.get();
+  a.coarse_table = h->coarse_table.get();
+  int n = 0;
+  for (int l = 1; l < lv.levelnum && l < kMaxLevels; ++l) {
+    a.perm[l] = h->perm[l].get();
+    a.off[l] = h->off[l].get();
+    a.node_base[l] = n;
+    n += lv.count[l];
+  }
+  for (int l = std::max(lv.levelnum, 1); l <= kMaxLevels; ++l) a.node_base[l] = n;
+  a.lv = lv;
+  a.inv = reinterpret_cast<const float*>(h->inv.get());
+  a.coarse_r = h->coarse_r.get();
+  a.coarse_z = h->coarse_z.get();
+  a.z0 = h->mas16_z0.get();
+  a.fem_off = h->fem_off;
+  a.c0 = h->c0;
+  return a;
+}
+
 }  // namespace
 
 // Level-0 apply + prolongation + r.z; with `partial` set, the last block
@@ -1150,10 +1359,10 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
     k_member_offsets<<<ceil_div(h->nv, kTpb), kTpb, 0, st>>>(
         reinterpret_cast<const unsigned*>(h->sort_keys_out.get()), h->nv, count, h->off[l].get()); MLAUNCHED(h);
   }
-  // storage
-  const int storage = h->cfg.inverse_storage;
+  // storage (16-slot banks: FP32 only)
+  const int storage = h->bank == 16 ? (int)MASPCG_INV_FP32 : h->cfg.inverse_storage;
   const size_t esize = storage == MASPCG_INV_FP32 ? 4 : 2;
-  h->inv.resize((size_t)lv.domains * inv_elems_for(storage) * esize, 16);
+  h->inv.resize((size_t)lv.domains * (h->bank == 16 ? kMas16InvElems : inv_elems_for(storage)) * esize, 16);
   if (storage != MASPCG_INV_FP32) h->inv_scale.resize((size_t)lv.domains * 96);
   MCK(cudaMemsetAsync(h->failed.get() + 3, 0, sizeof(int), st));
   launch_factor(h, assembled_out);
@@ -1161,6 +1370,16 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   const size_t coarse = (size_t)(lv.total_clusters - c0) * 3;
   h->coarse_r.resize(coarse > 0 ? coarse : 3);
   h->coarse_z.resize(coarse > 0 ? coarse : 3);
+  if (h->bank == 16) {
+    h->mas16_z0.resize(3 * (size_t)c0);
+    MCK(cudaMemsetAsync(h->coarse_r.get(), 0, h->coarse_r.bytes(), st));
+    MCK(cudaMemsetAsync(h->coarse_z.get(), 0, h->coarse_z.bytes(), st));
+    int f = 0;
+    MCK(cudaMemcpyAsync(&f, h->failed.get() + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MCK(cudaStreamSynchronize(st));
+    h->failed_domains = f;
+    return;
+  }
   const int coarse_domains = lv.domains - lv.dom_begin[1];
   h->chain_count.resize((size_t)std::max(coarse_domains, 1));
   h->chain_target.resize((size_t)std::max(coarse_domains, 1));
@@ -1181,18 +1400,21 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   h->failed_domains = f;
 }
 
-void launch_factor(maspcg_handle* h, double* assembled_out)
+template <int kB>
+void launch_factor_t(maspcg_handle* h, double* assembled_out)
 {
   cudaStream_t st = h->stream;
   const LevelInfo& lv = h->lv;
   const int c0 = h->c0;
-  const int storage = h->cfg.inverse_storage;
+  const int storage = kB == 16 ? (int)MASPCG_INV_FP32 : h->cfg.inverse_storage;
   const int d0 = lv.dom_begin[1];
   const int coarse_domains = lv.domains - d0;
   // coarse-level Galerkin sums
-  h->coarse64.resize((size_t)std::max(coarse_domains, 1) * 1024 * 9);
-  MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * 1024 * 9 * sizeof(double), st));
+  h->coarse64.resize((size_t)std::max(coarse_domains, 1) * kB * kB * 9);
+  MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * kB * kB * 9 * sizeof(double), st));
   CoarseArgs ca{};
+  ca.pmr = h->pmr.get();
+  ca.prefix_orig = h->prefix_orig.get();
   ca.levelnum = lv.levelnum;
   ca.slice_rows = 64;
   ca.nv = h->nv;
@@ -1212,7 +1434,7 @@ void launch_factor(maspcg_handle* h, double* assembled_out)
   ca.c0 = c0;
   ca.coarse64 = h->coarse64.get();
   if (items > 0) {
-    k_coarse_assemble<<<ceil_div((long long)items * 32, 256), 256, 0, st>>>(ca);
+    k_coarse_assemble<kB><<<ceil_div((long long)items * 32, 256), 256, 0, st>>>(ca);
     MLAUNCHED(h);
   }
   FactorArgs fa{};
@@ -1234,8 +1456,13 @@ void launch_factor(maspcg_handle* h, double* assembled_out)
   fa.assembled = assembled_out;
   fa.coarse64 = h->coarse64.get();
   const int grid = lv.domains;
-#define MAS_FACTOR(TI, ASM) k_domain_factor<TI, ASM><<<grid, 1024, 0, st>>>(fa, 0)
-  if (assembled_out) {
+#define MAS_FACTOR(TI, ASM) k_domain_factor<TI, ASM, kB><<<grid, 32 * kB, 0, st>>>(fa, 0)
+  if constexpr (kB == 16) {
+    if (assembled_out)
+      MAS_FACTOR(float, true);
+    else
+      MAS_FACTOR(float, false);
+  } else if (assembled_out) {
     if (storage == MASPCG_INV_FP32)
       MAS_FACTOR(float, true);
     else if (storage == MASPCG_INV_BF16)
@@ -1253,6 +1480,14 @@ void launch_factor(maspcg_handle* h, double* assembled_out)
 #undef MAS_FACTOR
   MLAUNCHED(h);
   MCK(cudaGetLastError());
+}
+
+void launch_factor(maspcg_handle* h, double* assembled_out)
+{
+  if (h->bank == 16)
+    launch_factor_t<16>(h, assembled_out);
+  else
+    launch_factor_t<32>(h, assembled_out);
 }
 
 namespace {
@@ -1445,13 +1680,37 @@ template void mas_apply<double, double>(maspcg_handle*, const double*, double*, 
 
 int mas_level0_grid(maspcg_handle* h) { return level0_grid(h, h->apply_variant); }
 
+int mas16_grid(maspcg_handle* h) { return std::max(1, std::min(ceil_div(h->c0, kTpb), 4 * h->sm_count)); }
+
+// CEMAS16 apply: restriction, domain applies of all levels, prolongation
+// with r.z (the last block completes r.z over [0, total_parts)).
+template <typename Tv, typename Tacc>
+void mas16_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
+                 int grid, PcgScalars* s)
+{
+  const Mas16Args a = make_mas16_args(h);
+  const int nodes = a.node_base[std::min(h->lv.levelnum, kMaxLevels)];
+  if (h->lv.levelnum > 1 && nodes > 0)
+    launch_pdl(h, k16_restrict<Tv>, dim3(ceil_div(nodes, kTpb)), dim3(kTpb), 0, a, r, s);
+  launch_pdl(h, k16_apply<Tv>, dim3(ceil_div((long long)h->lv.domains * 16, kTpb)), dim3(kTpb), 0, a, r, s);
+  launch_pdl(h, k16_collect<Tv, Tacc>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base, total_parts, mode,
+             s);
+  MCK(cudaGetLastError());
+}
+template void mas16_apply<float, float>(maspcg_handle*, const float*, float*, float*, int, int, int, int,
+                                        PcgScalars*);
+template void mas16_apply<float, double>(maspcg_handle*, const float*, float*, double*, int, int, int, int,
+                                         PcgScalars*);
+template void mas16_apply<double, double>(maspcg_handle*, const double*, double*, double*, int, int, int, int,
+                                          PcgScalars*);
+
 // Decode the stored inverses into the reference's packed FP32 layout.
 void decode_inverses(maspcg_handle* h, float* out)
 {
   const int D = h->lv.domains;
-  const int storage = h->cfg.inverse_storage;
+  const int storage = h->bank == 16 ? (int)MASPCG_INV_FP32 : h->cfg.inverse_storage;
   const size_t esize = storage == MASPCG_INV_FP32 ? 4 : 2;
-  std::vector<unsigned char> raw((size_t)D * inv_elems_for(storage) * esize);
+  std::vector<unsigned char> raw((size_t)D * (h->bank == 16 ? kMas16InvElems : inv_elems_for(storage)) * esize);
   std::vector<float> sc;
   MCK(cudaMemcpyAsync(raw.data(), h->inv.get(), raw.size(), cudaMemcpyDeviceToHost, h->stream));
   if (storage != MASPCG_INV_FP32) {
@@ -1484,6 +1743,22 @@ void decode_inverses(maspcg_handle* h, float* out)
       f = std::ldexp((float)(man | 0x400), (int)ex - 25);
     return sign ? -f : f;
   };
+  if (h->bank == 16) {
+    for (int g = 0; g < D; ++g)
+      for (int a = 0; a < 16; ++a)
+        for (int b = a; b < 16; ++b) {
+          const int d = b - a;
+          const bool direct = d <= 8;
+          const int lane = direct ? a : b, dd = direct ? d : 16 - d;
+          float* o = out + ((size_t)g * kMas16Packed + (16 * a - a * (a + 1) / 2 + b)) * 9;
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+              const int ei = direct ? 3 * i + j : 3 * j + i;
+              o[i + 3 * j] = elem((size_t)g * kMas16InvElems + (size_t)(dd * 9 + ei) * 16 + lane);
+            }
+        }
+    return;
+  }
   if (storage == MASPCG_INV_FP32) {
     for (int g = 0; g < D; ++g)
       for (int a = 0; a < kBank; ++a)

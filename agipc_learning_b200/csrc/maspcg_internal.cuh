@@ -44,6 +44,12 @@ constexpr int kInvElems = kDiags * 9 * kBank;      // 4896 stored elements per d
 constexpr int kTiles16 = 21;
 constexpr int kInvElems16 = kTiles16 * 256;  // 5376 stored 16-bit elements per domain
 
+// CEMAS16 (16-slot banks, 48x48 domains): FP32 inverses stored as 9 wrapped
+// diagonals x 9 elements x 16 lanes, lane l holding block (l, (l + d) % 16).
+constexpr int kMas16Packed = 16 * 17 / 2;                 // 136 packed upper blocks
+constexpr int kMas16Diags = 9;
+constexpr int kMas16InvElems = kMas16Diags * 9 * 16;      // 1296 per domain
+
 // Stored elements per domain for an inverse element type.
 template <typename TI>
 constexpr int inv_elems() { return sizeof(TI) == 4 ? kInvElems : kInvElems16; }
@@ -177,6 +183,7 @@ struct maspcg_handle {
   std::string last_error;
 
   // ---- graph (set_graph)
+  int bank = 32;  // MAS bank: 32 (TraditionalMAS32) or 16 (CEMAS16)
   bool has_graph = false;
   int nv = 0, c0 = 0, levelnum = 0, node_offset = 0, nlist_size = 0;
   long long gn_cap = 0;
@@ -215,6 +222,7 @@ struct maspcg_handle {
   maspcg::DBuf<int> failed;
   int failed_domains = 0;
   maspcg::DBuf<float> coarse_r, coarse_z;
+  maspcg::DBuf<float> mas16_z0;                 // CEMAS16: level-0 domain outputs (3 per slot)
   maspcg::DBuf<int> chain_count, chain_target;  // coarse-level dataflow counters (per coarse domain)
   maspcg::DBuf<double> chain_dot;               // per coarse domain: R.Z (r.z of the coarse levels)
   maspcg::DBuf<double> coarse64;

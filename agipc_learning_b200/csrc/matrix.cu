@@ -246,7 +246,8 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   const int nb = h->nb;
   // ---- internal row order
   std::vector<int> iof(nb);
-  h->mas_layout = (h->cfg.preconditioner == MASPCG_PRECOND_MAS32) && h->has_graph && h->nv > 0;
+  h->mas_layout = (h->cfg.preconditioner == MASPCG_PRECOND_MAS32 || h->cfg.preconditioner == MASPCG_PRECOND_MAS16) &&
+                  h->has_graph && h->nv > 0;
   int nb_int = nb;
   if (h->mas_layout) {
     MREQ(h->fem_off + h->nv <= nb, MASPCG_ERR_INVALID_ARGUMENT, "FEM range exceeds the block rows");

@@ -33,6 +33,10 @@ template <typename Tv, typename Tacc>
 void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant);
 void launch_factor(maspcg_handle* h, double* assembled_out);
 int mas_level0_grid(maspcg_handle* h);
+template <typename Tv, typename Tacc>
+void mas16_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
+                 int grid, PcgScalars* s);
+int mas16_grid(maspcg_handle* h);
 
 namespace {
 
@@ -575,19 +579,20 @@ template <typename Tm, typename Tv, typename Tacc>
 struct Engine {
   maspcg_handle* h;
   int n, gstream, gspmv, grows, gl0, gother, parts_other, parts_total;
-  bool mas, mixed, ovl;
+  bool mas, mas16, mixed, ovl;
 
   explicit Engine(maspcg_handle* hh) : h(hh)
   {
     n = 3 * h->nb_int;
     mas = h->mas_layout && h->cfg.preconditioner == MASPCG_PRECOND_MAS32;
+    mas16 = h->mas_layout && h->cfg.preconditioner == MASPCG_PRECOND_MAS16;
     mixed = h->cfg.precision == MASPCG_PREC_MIXED;
     gstream = h->grid_stream;
     gspmv = std::max(1, std::min(ceil_div(h->nb_int, kTpb / 16), 4 * h->sm_count));
     grows = std::max(1, std::min(ceil_div(h->nb_int, kTpb), 8 * h->sm_count));
-    gl0 = mas ? mas_level0_grid(h) : 0;
+    gl0 = mas ? mas_level0_grid(h) : (mas16 ? mas16_grid(h) : 0);
     ovl = mas && h->lv.levelnum > 1 && h->overlap_coarse;
-    const bool other = !mas || h->abd_bodies > 0 || h->fem_off > 0 || h->nb_int > h->fem_off + h->c0;
+    const bool other = !(mas || mas16) || h->abd_bodies > 0 || h->fem_off > 0 || h->nb_int > h->fem_off + h->c0;
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;
     parts_other = gother;
     parts_total = gother + gl0;
@@ -603,20 +608,22 @@ struct Engine {
     const bool ref = h->cfg.precision == MASPCG_PREC_REFERENCE;
     if (gother) {
       const bool bj = h->cfg.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI;
-      const int mas_lo = mas ? h->fem_off : 0, mas_hi = mas ? h->fem_off + h->c0 : 0;
+      const bool any_mas = mas || mas16;
+      const int mas_lo = any_mas ? h->fem_off : 0, mas_hi = any_mas ? h->fem_off + h->c0 : 0;
       const int bodies = (h->cfg.preconditioner == MASPCG_PRECOND_NONE) ? 0 : h->abd_bodies;
       // affine bodies always apply their FP64 inverses: the 12x12 inverse
       // spans the same ~1e11 spread as the body's Hessian block
       if (ref || bodies > 0)
         launch_pdl(h, k_other_apply<Tv, Tacc, double>, dim3(gother), dim3(kTpb), 0, 
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv64.get(), bj ? h->diag_inv64.get() : nullptr,
-            s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
+            s ? partial_rz() : nullptr, 0, parts_total, any_mas ? 0 : 1, mode, s);
       else
         launch_pdl(h, k_other_apply<Tv, Tacc, float>, dim3(gother), dim3(kTpb), 0, 
             r, z, h->nb_int, mas_lo, mas_hi, bodies, h->abd_inv32.get(), bj ? h->diag_inv32.get() : nullptr,
-            s ? partial_rz() : nullptr, 0, parts_total, mas ? 0 : 1, mode, s);
+            s ? partial_rz() : nullptr, 0, parts_total, any_mas ? 0 : 1, mode, s);
     }
     if (mas) mas_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s, overlap);
+    if (mas16) mas16_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s);
     MCK(cudaGetLastError());
   }
 
@@ -723,7 +730,7 @@ struct Engine {
     init.max_iter = 1 << 30;
     init.tol = 0.0;
     init.gate = MASPCG_GATE_EUCLID;
-    MREQ(stage != 3 || mas, MASPCG_ERR_NOT_READY, "stage 3 needs a MAS32 preconditioner");
+    MREQ(stage != 3 || mas || mas16, MASPCG_ERR_NOT_READY, "stage 3 needs a MAS preconditioner");
     MREQ(stage != 2 || mas, MASPCG_ERR_NOT_READY, "stage 2 needs a MAS32 preconditioner");
     MREQ(stage < 4 || stage > 6 || mas, MASPCG_ERR_NOT_READY, "stages 4-6 need a MAS32 preconditioner");
     MREQ(stage >= 0 && stage <= 6, MASPCG_ERR_INVALID_ARGUMENT, "unknown stage");

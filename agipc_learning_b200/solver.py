@@ -20,7 +20,8 @@ from . import _native as N
 _PREC = {"reference": N.PREC_REFERENCE, "fp32": N.PREC_FP32, "mixed": N.PREC_MIXED}
 _GATE = {"rz": N.GATE_RZ, "euclid": N.GATE_EUCLID}
 _INV = {"fp32": N.INV_FP32, "bf16": N.INV_BF16, "fp16": N.INV_FP16}
-_PC = {"mas32": N.PRECOND_MAS32, "block_jacobi": N.PRECOND_BLOCK_JACOBI, "none": N.PRECOND_NONE}
+_PC = {"mas32": N.PRECOND_MAS32, "cemas16": N.PRECOND_MAS16, "block_jacobi": N.PRECOND_BLOCK_JACOBI,
+       "none": N.PRECOND_NONE}
 
 
 def _is_torch(a) -> bool:
@@ -70,6 +71,7 @@ class MasPcg:
         cfg.precision = _PREC[precision]
         cfg.inverse_storage = _INV[inverse]
         cfg.preconditioner = _PC[preconditioner]
+        cfg.bank_size = 16 if preconditioner == "cemas16" else 32
         cfg.refinement_period = refinement_period
         cfg.iterations_per_launch = iterations_per_launch
         cfg.flags = flags
@@ -135,7 +137,7 @@ class MasPcg:
     def from_system(cls, s, **cfg):
         """Set up graph, contacts and matrix of a synth.System and build."""
         m = cls(**cfg)
-        if m.cfg.preconditioner == N.PRECOND_MAS32 and s.fem_count > 0:
+        if m.cfg.preconditioner in (N.PRECOND_MAS32, N.PRECOND_MAS16) and s.fem_count > 0:
             m.set_graph(s.fem_count, s.node_offset, s.neighbor_start, s.neighbor_num, s.neighbor_list,
                         s.part_map_real, s.real_map_part)
             m.set_contacts(s.pairs)
@@ -270,7 +272,7 @@ class MasPcg:
         gn = np.zeros(i["going_next_capacity"], np.int32)
         ls = np.zeros(2 * (L + 1), np.int32)
         ct = np.zeros(6 * nv, np.int32)
-        po = np.zeros(i["part_map_size"] // 32, np.int32)
+        po = np.zeros(i["part_map_size"] // self.cfg.bank_size, np.int32)
         p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
         self._ck(self.lib.maspcg_get_hierarchy(self.h, p(fm), p(cst), p(gn), p(ls), p(ct), p(po)))
         return {"fine_mask": fm, "coarse_space_tables": cst.reshape(L, nv), "going_next": gn,
@@ -289,7 +291,8 @@ class MasPcg:
 
     def domain_inverses(self):
         d = self.info()["domains"]
-        out = np.zeros((d, 528, 9), np.float32)
+        B = self.cfg.bank_size
+        out = np.zeros((d, B * (B + 1) // 2, 9), np.float32)
         self._ck(self.lib.maspcg_get_domain_inverses(self.h, out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
@@ -302,7 +305,8 @@ class MasPcg:
 
     def domain_matrices(self):
         d = self.info()["domains"]
-        out = np.zeros((d, 528, 9), np.float64)
+        B = self.cfg.bank_size
+        out = np.zeros((d, B * (B + 1) // 2, 9), np.float64)
         self._ck(self.lib.maspcg_get_domain_matrices(self.h, out.ctypes.data_as(ctypes.c_void_p)))
         return out
 

@@ -271,6 +271,60 @@ def hybrid_system(bodies: int = 2000, slab=(100, 100, 10), *, E: float = 1e8, nu
                   meta={"projected_tets": projected, "E": E, "nu": nu, "dt": dt, "rho": rho, "h": h})
 
 
+def partition_for_bank(s: System, bank: int, *, sorted_ids: bool = True) -> System:
+    """The system with a MAS partition of `bank`-slot banks (16: CEMAS16).
+
+    sorted_ids=True renumbers the FEM vertices in Morton order, as the app's
+    METIS-sorted meshes number a part's vertices consecutively for CEMAS16
+    (gl_main.cu:1118-1145), so vertex v sits in slot v and the slots of every
+    bank follow the vertex order.  sorted_ids=False keeps the numbering and
+    packs the Morton order into banks, so inside a bank the slot order runs
+    against the vertex order."""
+    import dataclasses
+    nv, fo = s.fem_count, s.fem_offset
+    order = np.asarray(s.part_map_real)[np.asarray(s.part_map_real) >= 0].astype(np.int64)  # Morton order
+    padded = (nv + bank - 1) // bank * bank
+    pmr = np.full(padded, -1, np.int32)
+    if not sorted_ids:
+        pmr[:nv] = order
+        rmp = np.zeros(nv, np.int32)
+        rmp[order] = np.arange(nv, dtype=np.int32)
+        return dataclasses.replace(s, part_map_real=pmr, real_map_part=rmp)
+    new = np.empty(nv, np.int64)
+    new[order] = np.arange(nv)
+    gmap = np.arange(s.nb, dtype=np.int64)
+    gmap[fo:fo + nv] = fo + new
+    r, c = gmap[s.rows], gmap[s.cols]
+    v = np.asarray(s.vals, np.float64).reshape(-1, 3, 3).copy()
+    swap = r > c
+    r2, c2 = np.where(swap, c, r), np.where(swap, r, c)
+    v[swap] = v[swap].transpose(0, 2, 1)
+    rows, cols, vals = assemble(r2, c2, v.reshape(-1, 9))
+    b = np.asarray(s.b, np.float64).reshape(-1, 3).copy()
+    b[fo + new] = np.asarray(s.b).reshape(-1, 3)[fo:fo + nv]
+    st, nn, nl = (np.asarray(a) for a in (s.neighbor_start, s.neighbor_num, s.neighbor_list))
+    lists = [new[nl[st[o]:st[o] + nn[o]]] for o in order]
+    num = np.array([len(x) for x in lists], np.uint32)
+    start = np.zeros(nv, np.uint32)
+    start[1:] = np.cumsum(num)[:-1]
+    lst = np.concatenate(lists).astype(np.uint32) if nv else np.zeros(0, np.uint32)
+    pairs = np.asarray(s.pairs, np.int64).copy()
+    if pairs.size:
+        vtx = np.where(pairs >= 0, pairs, -pairs - 1)
+        loc = vtx - s.node_offset
+        inr = (loc >= 0) & (loc < nv)
+        mapped = np.where(inr, s.node_offset + new[np.clip(loc, 0, nv - 1)], vtx)
+        pairs = np.where(pairs >= 0, mapped, -mapped - 1)
+    pmr[:nv] = np.arange(nv, dtype=np.int32)
+    meta = {k: v_ for k, v_ in s.meta.items() if k not in ("raw", "elem_blocks")}
+    X = None if s.X is None else np.asarray(s.X)[order]
+    tets = None if s.tets is None else new[np.asarray(s.tets)].astype(np.int32)
+    return dataclasses.replace(s, rows=rows, cols=cols, vals=vals, b=b.reshape(-1), neighbor_start=start,
+                               neighbor_num=num, neighbor_list=lst, part_map_real=pmr,
+                               real_map_part=np.arange(nv, dtype=np.int32), pairs=pairs.astype(np.int32), X=X,
+                               tets=tets, meta=meta, name=f"{s.name}_b{bank}")
+
+
 def log_uniform_E(ntet: int, lo: float, hi: float, seed: int) -> np.ndarray:
     """Per-tet Young's modulus, log-uniform in [lo, hi] (numpy PCG64 stream)."""
     u = np.random.default_rng(seed).random(ntet)

@@ -3,7 +3,7 @@
  * Newton-step linear solve.
  *
  * One handle owns one linear system on one GPU: the neighbour graph and
- * partition of the FEM vertices (MAS32 hierarchy input), the contact pairs of
+ * partition of the FEM vertices (MAS hierarchy input), the contact pairs of
  * the current Newton step, the assembled block-sparse Hessian, the
  * preconditioner built from it, and the PCG work space.  All entry points
  * return a maspcg_status; none aborts or exits.  A handle is thread-compatible
@@ -55,6 +55,7 @@ typedef enum {
 /* Preconditioner ids follow the reference's P_type (gl_main.cu:1248-1250). */
 typedef enum {
   MASPCG_PRECOND_BLOCK_JACOBI = 0, /* DiagPreconditioner: 3x3 block inverse */
+  MASPCG_PRECOND_MAS16 = 1,        /* MASPreconditioner (CEMAS16, 16-vertex banks) on the FEM range + ABD 12x12 */
   MASPCG_PRECOND_MAS32 = 2,        /* TraditionalMAS32 on the FEM range + ABD 12x12 */
   MASPCG_PRECOND_NONE = 3
 } maspcg_preconditioner;
@@ -83,10 +84,10 @@ typedef struct {
   int max_iterations;    /* > 0 overrides max_iter_ratio */
   int gate;              /* maspcg_gate */
   int precision;         /* maspcg_precision */
-  int inverse_storage;   /* maspcg_inverse_storage (FP32 unless MIXED) */
+  int inverse_storage;   /* maspcg_inverse_storage (FP32 unless MIXED; always FP32 for CEMAS16) */
   int preconditioner;    /* maspcg_preconditioner */
   int refinement_period; /* MIXED: iterations between FP64 true residuals (default 16) */
-  int bank_size;         /* MAS bank; 32 (GPU_MAS_BANKSIZE) is the only supported value */
+  int bank_size;         /* MAS bank: 32 (GPU_MAS_BANKSIZE) for MAS32, 16 (BANKSIZE) for CEMAS16 */
   int iterations_per_launch; /* PCG iterations per CUDA-graph launch (default 8) */
   int flags;             /* maspcg_flags: kernel-schedule choices, 0 = defaults */
 } maspcg_config;
@@ -150,10 +151,14 @@ MASPCG_API maspcg_status maspcg_set_stream(maspcg_handle* h, void* stream);
  *   vert_num              FEM vertices (totalNodes)
  *   collision_node_offset vertex-number offset of the FEM range in contact pairs
  *   neighbor_*            vertex neighbour CSR (u32), list of neighbor_list_size
- *   part_map_real         part_map_size slots (multiple of 32): slot -> vertex or -1
+ *   part_map_real         part_map_size slots (multiple of bank_size): slot -> vertex or -1
  *   real_map_part         vert_num entries: vertex -> slot
- * Lane 0 of every 32-slot bank must hold a vertex (the reference leaves the
- * bank's component count undefined otherwise). */
+ * Lane 0 of every bank must hold a vertex (the reference leaves the bank's
+ * component count undefined otherwise).  CEMAS16 (MASPreconditioner.cu:
+ * 2293-2362, the same inputs with 16-slot banks, METIS-sorted in the app)
+ * drops an in-bank block whose slots run against its vertex order
+ * (prepare_hessian_bcoo_kernel :1822-1914); a partition whose slots follow
+ * the vertex order inside every bank loses nothing. */
 MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int collision_node_offset,
                                           const uint32_t* neighbor_start, const uint32_t* neighbor_num,
                                           const uint32_t* neighbor_list, int neighbor_list_size,
@@ -176,10 +181,10 @@ MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* 
                                                 int abd_body_count);
 
 /* Replaces LocalPreconditioner::assemble of TraditionalMAS32_Preconditioner /
- * ABDPreconditioner / DiagPreconditioner
- * (traditional_mas32_preconditioner.cu:20-32, abd_preconditioner.cu:33-36,
- * diag_preconditioner.cu:74-80): hierarchy for the current contacts,
- * domain matrices, inverses. */
+ * MAS_Preconditioner (CEMAS16) / ABDPreconditioner / DiagPreconditioner
+ * (traditional_mas32_preconditioner.cu:20-32, fem_mas_preconditioner.cu:18-31,
+ * abd_preconditioner.cu:33-36, diag_preconditioner.cu:74-80): hierarchy for
+ * the current contacts, domain matrices, inverses. */
 MASPCG_API maspcg_status maspcg_build_preconditioner(maspcg_handle* h);
 
 /* Replaces IterativeSolver::solve(x, b) -> iterations
@@ -200,7 +205,7 @@ MASPCG_API maspcg_status maspcg_spmv(maspcg_handle* h, double a, const double* x
 typedef struct {
   int levelnum;          /* computeNumLevels */
   int total_clusters;    /* totalNumberClusters */
-  int domains;           /* total_clusters / 32 */
+  int domains;           /* total_clusters / bank_size */
   int vert_num;          /* totalNodes */
   int part_map_size;     /* totalMapNodes */
   long long going_next_capacity;
@@ -217,7 +222,7 @@ MASPCG_API maspcg_status maspcg_get_info(maspcg_handle* h, maspcg_info* info);
  * (TraditionalMAS32Preconditioner.cuh:35-64); any pointer may be NULL; host
  * pointers.  fine_mask[vert_num], coarse_space_tables[levelnum*vert_num],
  * going_next[going_next_capacity], level_size[2*(levelnum+1)],
- * coarse_table[6*vert_num], prefix_original[part_map_size/32]. */
+ * coarse_table[6*vert_num], prefix_original[part_map_size/bank_size]. */
 MASPCG_API maspcg_status maspcg_get_hierarchy(maspcg_handle* h, uint32_t* fine_mask, int* coarse_space_tables,
                                               int* going_next, int* level_size, int* coarse_table,
                                               int* prefix_original);
@@ -228,13 +233,15 @@ MASPCG_API maspcg_status maspcg_get_hierarchy(maspcg_handle* h, uint32_t* fine_m
 MASPCG_API maspcg_status maspcg_get_bcsr(maspcg_handle* h, int* rowptr, int* colidx, double* values_rowmajor,
                                          int* internal_of_row);
 
-/* Domain inverses in the reference's packed layout (GPUMas32MatrixSymf):
- * 528 upper 3x3 blocks per domain, block (a,b) at 32a - a(a+1)/2 + b, 9 floats
- * column-major; decoded from whatever precision is stored.  out: domains*528*9. */
+/* Domain inverses in the reference's packed layout (GPUMas32MatrixSymf;
+ * MasMatrixSymf for CEMAS16): P = B(B+1)/2 upper 3x3 blocks per domain for
+ * bank B (528 or 136), block (a,b) at Ba - a(a+1)/2 + b, 9 floats
+ * column-major; decoded from whatever precision is stored.  out: domains*P*9. */
 MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out);
 
-/* Assembled FP64 domain matrices (GPUMas32MatrixSymT layout) of the last
- * build, before the zero-diagonal rule: recomputed on demand. out: domains*528*9. */
+/* Assembled FP64 domain matrices (GPUMas32MatrixSymT / MasMatrixSymT layout)
+ * of the last build, before the zero-diagonal rule: recomputed on demand.
+ * out: domains*P*9 (P as above). */
 MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* out);
 
 /* Benchmark introspection (no counterpart in the reference): run one stage

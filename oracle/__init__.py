@@ -1,7 +1,9 @@
 """ctypes binding of the CPU oracle (test infrastructure only).
 
 The oracle restates the reference's Newton-step linear solve in plain C
-(``maspcg_oracle.c``).  It is the parity checker for the CUDA path and the
+(``maspcg_oracle.c``), built for the 32-vertex MAS bank (``liboracle.so``,
+TraditionalMAS32Preconditioner) and the 16-vertex bank (``liboracle16.so``,
+CEMAS16 / MASPreconditioner).  It is the parity checker for the CUDA path and the
 timed CPU baseline; nothing in ``agipc_learning_b200`` imports it.
 """
 from __future__ import annotations
@@ -13,9 +15,10 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
 
 PRECOND_DIAG3 = 0
+PRECOND_MAS16 = 1
 PRECOND_MAS32 = 2
 PRECOND_NONE = -1
 GATE_RZ = 0
@@ -40,10 +43,9 @@ class _PcgResult(ctypes.Structure):
                 ("rel_res_true", ctypes.c_double)]
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        path = os.path.join(_HERE, "liboracle.so")
+def lib(bank=32):
+    if bank not in _LIBS:
+        path = os.path.join(_HERE, "liboracle.so" if bank == 32 else "liboracle16.so")
         if not os.path.exists(path):
             build()
         L = ctypes.CDLL(path)
@@ -76,8 +78,8 @@ def lib():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        _LIB = L
-    return _LIB
+        _LIBS[bank] = L
+    return _LIBS[bank]
 
 
 def _p(a):
@@ -284,8 +286,8 @@ def bcsr_spmv(rowptr, col, vals, x):
     return y
 
 
-def compute_num_levels(n):
-    return lib().orc_compute_num_levels(int(n))
+def compute_num_levels(n, bank=32):
+    return lib(bank).orc_compute_num_levels(int(n))
 
 
 def hierarchy_capacity(vertices, mapped, levels, bank):
@@ -295,19 +297,22 @@ def hierarchy_capacity(vertices, mapped, levels, bank):
 class Mas32:
     """TraditionalMAS32Preconditioner restated on the CPU."""
 
+    BANK = 32
+
     def __init__(self, vert_num, node_offset, neighbor_start, neighbor_num, neighbor_list, part_map_real,
                  real_map_part):
+        self._lib = lib(self.BANK)
         self._keep = [_c(neighbor_start, np.uint32), _c(neighbor_num, np.uint32),
                       _c(neighbor_list if len(neighbor_list) else np.zeros(1), np.uint32),
                       _c(part_map_real, np.int32), _c(real_map_part, np.int32)]
         s, n, l, pm, rm = self._keep
-        self.h = lib().orc_mas_create(int(vert_num), int(node_offset), _p(s), _p(n), _p(l), int(len(neighbor_list)),
-                                      _p(pm), int(len(pm)), _p(rm))
+        self.h = self._lib.orc_mas_create(int(vert_num), int(node_offset), _p(s), _p(n), _p(l),
+                                          int(len(neighbor_list)), _p(pm), int(len(pm)), _p(rm))
         if not self.h:
-            raise ValueError("invalid MAS32 inputs")
+            raise ValueError("invalid MAS inputs")
         self.nv = int(vert_num)
         self.c0 = len(pm)
-        self.levelnum = lib().orc_mas_levelnum(self.h)
+        self.levelnum = self._lib.orc_mas_levelnum(self.h)
         self.total_clusters = 0
 
     @classmethod
@@ -317,24 +322,24 @@ class Mas32:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().orc_mas_free(self.h)
+            self._lib.orc_mas_free(self.h)
             self.h = None
 
     def reorder(self, pairs=None):
         p = None if pairs is None or len(pairs) == 0 else _c(pairs, np.int32).reshape(-1, 4)
-        self.total_clusters = lib().orc_mas_reorder(self.h, _p(p), 0 if p is None else len(p))
+        self.total_clusters = self._lib.orc_mas_reorder(self.h, _p(p), 0 if p is None else len(p))
         return self.total_clusters
 
     def hierarchy(self):
         L = self.levelnum
-        cap = lib().orc_mas_going_next_capacity(self.h)
+        cap = self._lib.orc_mas_going_next_capacity(self.h)
         fm = np.zeros(self.nv, np.uint32)
         cst = np.zeros(self.nv * L, np.int32)
         gn = np.zeros(cap, np.int32)
         ls = np.zeros(2 * (L + 1), np.int32)
         ct = np.zeros(self.nv * 6, np.int32)
-        po = np.zeros(self.c0 // 32, np.int32)
-        lib().orc_mas_get_hierarchy(self.h, _p(fm), _p(cst), _p(gn), _p(ls), _p(ct), _p(po))
+        po = np.zeros(self.c0 // self.BANK, np.int32)
+        self._lib.orc_mas_get_hierarchy(self.h, _p(fm), _p(cst), _p(gn), _p(ls), _p(ct), _p(po))
         return {"fine_mask": fm, "coarse_space_tables": cst.reshape(L, self.nv), "going_next": gn,
                 "level_size": ls.reshape(L + 1, 2), "coarse_table": ct.reshape(self.nv, 6),
                 "prefix_original": po, "total_clusters": self.total_clusters, "levelnum": L}
@@ -343,29 +348,38 @@ class Mas32:
         n = len(rows) if indices is None else len(indices)
         self._mat = (_c(vals, np.float64), _c(rows, np.int32), _c(cols, np.int32))
         ind = None if indices is None else _c(indices, np.uint32)
-        lib().orc_mas_prepare_hessian(self.h, _p(self._mat[0]), _p(self._mat[1]), _p(self._mat[2]), _p(ind),
-                                      int(offset), int(n))
+        self._lib.orc_mas_prepare_hessian(self.h, _p(self._mat[0]), _p(self._mat[1]), _p(self._mat[2]), _p(ind),
+                                          int(offset), int(n))
 
     def domains(self):
-        nd = self.total_clusters // 32
-        p64 = np.zeros((nd, 528, 9))
-        i32 = np.zeros((nd, 528, 9), np.float32)
-        lib().orc_mas_get_domains(self.h, _p(p64), _p(i32))
+        B = self.BANK
+        nd = self.total_clusters // B
+        p64 = np.zeros((nd, B * (B + 1) // 2, 9))
+        i32 = np.zeros((nd, B * (B + 1) // 2, 9), np.float32)
+        self._lib.orc_mas_get_domains(self.h, _p(p64), _p(i32))
         return p64, i32
 
     def precondition(self, R):
         R = _c(R, np.float64)
         Z = np.zeros_like(R)
-        lib().orc_mas_precondition(self.h, _p(R), _p(Z))
+        self._lib.orc_mas_precondition(self.h, _p(R), _p(Z))
         return Z
 
 
-def local_checks(packed64, inverse32):
+class Mas16(Mas32):
+    """CEMAS16 (MASPreconditioner, 16-vertex banks, 48x48 domains) restated on
+    the CPU: the MAS32 restatement built with a 16-vertex bank, plus the three
+    places where CEMAS16's kernels differ (maspcg_oracle.c, ORC_BANK == 16)."""
+
+    BANK = 16
+
+
+def local_checks(packed64, inverse32, bank=32):
     packed64 = _c(packed64, np.float64)
     inverse32 = _c(inverse32, np.float32)
     n = packed64.shape[0]
     out = np.zeros((n, 7))
-    lib().orc_local_checks(n, _p(packed64), _p(inverse32), _p(out))
+    lib(bank).orc_local_checks(n, _p(packed64), _p(inverse32), _p(out))
     keys = ["local_finite", "inverse_finite", "local_spd", "inverse_spd", "minimum_local_diagonal",
             "minimum_inverse_diagonal", "inverse_residual"]
     return [dict(zip(keys, row)) for row in out]
@@ -392,8 +406,9 @@ def pcg(vals, rows, cols, nb, b, *, precond=PRECOND_MAS32, gate=GATE_RZ, tol=1e-
     res = _PcgResult()
     b = _c(b, np.float64)
     x = np.zeros_like(b)
-    lib().orc_pcg(ctypes.byref(o), _p(_c(vals, np.float64)), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)),
-                  len(rows), None if mas is None else mas.h, _p(b), _p(x), ctypes.byref(res))
+    L = lib() if mas is None else mas._lib
+    L.orc_pcg(ctypes.byref(o), _p(_c(vals, np.float64)), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)),
+              len(rows), None if mas is None else mas.h, _p(b), _p(x), ctypes.byref(res))
     return x, {"iterations": res.iterations, "status": STATUS_NAMES.get(res.status, res.status), "rz0": res.rz0,
                "rz_last": res.rz_last, "rel_res_recursive": res.rel_res_recursive, "rel_res_true": res.rel_res_true}
 
@@ -401,8 +416,8 @@ def pcg(vals, rows, cols, nb, b, *, precond=PRECOND_MAS32, gate=GATE_RZ, tol=1e-
 def solve_system(s, *, precond=PRECOND_MAS32, gate=GATE_RZ, tol=1e-4, max_iter=0, replay_checks=False):
     """Full reference pipeline on a synth.System: MAS build then PCG."""
     mas = None
-    if precond == PRECOND_MAS32 and s.fem_count > 0:
-        mas = Mas32.from_system(s)
+    if precond in (PRECOND_MAS32, PRECOND_MAS16) and s.fem_count > 0:
+        mas = (Mas32 if precond == PRECOND_MAS32 else Mas16).from_system(s)
         mas.reorder(s.pairs)
         sel = np.nonzero((s.rows >= s.fem_offset) & (s.rows < s.fem_offset + s.fem_count) &
                          (s.cols >= s.fem_offset) & (s.cols < s.fem_offset + s.fem_count))[0].astype(np.uint32)

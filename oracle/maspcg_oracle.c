@@ -9,6 +9,11 @@
  * matrices, FP64 Gauss-Jordan inverse cast to FP32, FP32 MAS apply) with a
  * fixed summation order where the reference uses atomics.
  *
+ * Built twice: liboracle.so (ORC_BANK 32, TraditionalMAS32Preconditioner.cu)
+ * and liboracle16.so (ORC_BANK 16, CEMAS16: MASPreconditioner.cu, whose
+ * kernels are the MAS32 ones with BANKSIZE 16 apart from the three places
+ * marked ORC_BANK == 16 below).
+ *
  * Parity pins: the spmv self-test KAT (spmv.cu:301-459), the MAS32 hierarchy
  * self-test KAT (TraditionalMAS32Preconditioner.cu:257-427), the local
  * diagnostics cases (:182-215), hierarchy_capacity asserts
@@ -670,9 +675,14 @@ void orc_mas_prepare_hessian(orc_mas* m, const double* vals9, const int* rows, c
       if (vc >= vr) {
         memcpy(blk64(m, cp, pk(a, b)), H, 9 * sizeof(double));
       } else {
+#if ORC_BANK == 16
+        /* CEMAS16 keeps an in-bank block only when its slots follow its
+         * vertex order (MASPreconditioner.cu:1846-1857): dropped */
+#else
         double* d = blk64(m, cp, pk(b, a));
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j) d[i + 3 * j] = H[j + 3 * i];
+#endif
       }
     } else {
       for (int level = 1; level < levels; ++level) {
@@ -712,6 +722,11 @@ void orc_mas_prepare_hessian(orc_mas* m, const double* vals9, const int* rows, c
       if (rdx0 < 0) continue;
       if (prefix == 1) {
         if (m->pmr[hid * BANK] < 0) continue; /* lane 0 carries the row sum */
+#if ORC_BANK == 16
+        /* CEMAS16: a warp of 32 entries spans rows (2k, 2k+1) and its sum is
+         * added by entry (2k, 0) (MASPreconditioner.cu:1955-2005) */
+        if (m->pmr[hid * BANK + (lr & ~1)] < 0) continue;
+#endif
         double mat[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, b9[9];
         for (int lc = 0; lc < BANK; ++lc) {
           if (m->pmr[hid * BANK + lc] < 0) continue;
@@ -773,6 +788,16 @@ void orc_mas_prepare_hessian(orc_mas* m, const double* vals9, const int* rows, c
           for (int i = 0; i < DIM; ++i) a[k * DIM + i] = fma(rate, a[j * DIM + i], a[k * DIM + i]);
         }
       }
+#if ORC_BANK == 16
+      /* CEMAS16 copies the upper elements of each diagonal 3x3 block onto
+       * the lower ones before the store (MASPreconditioner.cu:705-711) */
+      for (int i = 0; i < DIM; ++i) {
+        if (i % 3 < 2)
+          a[(i + 1) * DIM + i] = a[i * DIM + i + 1];
+        else
+          a[i * DIM + i - 2] = a[(i - 2) * DIM + i];
+      }
+#endif
       float* out = m->inv32 + (size_t)d * NPACK * 9;
       for (int r = 0; r < DIM; ++r)
         for (int c = 0; c < DIM; ++c) {
@@ -1077,7 +1102,7 @@ static void apply_precond(const precond_ctx* p, const double* r, double* z, int 
       }
     }
   }
-  if (o->precond == ORC_PRECOND_MAS32 && o->fem_count > 0 && p->mas)
+  if ((o->precond == ORC_PRECOND_MAS32 || o->precond == ORC_PRECOND_MAS16) && o->fem_count > 0 && p->mas)
     orc_mas_precondition(p->mas, r + 3 * (size_t)o->fem_offset, z + 3 * (size_t)o->fem_offset);
 }
 

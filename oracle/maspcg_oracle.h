@@ -56,7 +56,12 @@ void orc_bcsr_spmv(int nb, const int* rowptr, const int* colidx, const double* v
 
 /* ---------------------------------------------------------------- MAS32 -- */
 
+/* MAS bank: 32 (TraditionalMAS32), or 16 for the CEMAS16 build (-DORC_BANK=16,
+ * liboracle16.so: MASPreconditioner.cu, the same algorithm with BANKSIZE 16
+ * and the differences marked ORC_BANK == 16 in maspcg_oracle.c). */
+#ifndef ORC_BANK
 #define ORC_BANK 32
+#endif
 #define ORC_MAX_LEVELS 6
 
 typedef struct orc_mas orc_mas;
@@ -129,7 +134,8 @@ int orc_abd_inverse(int bodies, int nblocks, const int* rows, const int* cols, c
 
 enum {
   ORC_PRECOND_DIAG3 = 0, /* DiagPreconditioner (global) + ABD local */
-  ORC_PRECOND_MAS32 = 2, /* identity copy + ABD local + MAS32 on the FEM range */
+  ORC_PRECOND_MAS16 = 1, /* the same with CEMAS16 (liboracle16.so only) */
+  ORC_PRECOND_MAS32 = 2, /* identity copy + ABD local + MAS on the FEM range (bank ORC_BANK) */
   ORC_PRECOND_NONE = -1
 };
 enum {

@@ -129,17 +129,160 @@ def permute_full_bcsr(nb_int, iof, rowptr, col, vals):
     return rp, np.array(cs, np.int64), np.array(vs).reshape(-1, 9) if vs else np.zeros((0, 9))
 
 
-def unpack_domain(packed):
-    """96x96 symmetric matrix from a domain's 528 packed upper 3x3 blocks
-    (block (a, b), a <= b, at 32a - a(a+1)/2 + b; column-major blocks)."""
-    p = np.asarray(packed, np.float64).reshape(528, 9)
-    A = np.zeros((96, 96))
-    for a in range(32):
-        for b in range(a, 32):
-            blk = p[32 * a - a * (a + 1) // 2 + b].reshape(3, 3).T
+def unpack_domain(packed, bank=32):
+    """3B x 3B symmetric matrix from a domain's B(B+1)/2 packed upper 3x3
+    blocks (block (a, b), a <= b, at Ba - a(a+1)/2 + b; column-major blocks)."""
+    B = bank
+    p = np.asarray(packed, np.float64).reshape(B * (B + 1) // 2, 9)
+    A = np.zeros((3 * B, 3 * B))
+    for a in range(B):
+        for b in range(a, B):
+            blk = p[B * a - a * (a + 1) // 2 + b].reshape(3, 3).T
             A[3 * a:3 * a + 3, 3 * b:3 * b + 3] = blk
             A[3 * b:3 * b + 3, 3 * a:3 * a + 3] = blk.T
     return A
+
+
+def _decode_pairs(pairs, node_offset, nv):
+    """FEM-local vertex tuples of int4 contact pairs (the sign encoding of
+    _buildCollisionConnection_new)."""
+    out = []
+    for x, y, z, w in np.asarray(pairs, np.int64).reshape(-1, 4):
+        if x >= 0:
+            v = [x, y, z, -w - 1 if w < 0 else w]
+        else:
+            x = -x - 1
+            if z < 0:
+                v = [x, -y - 1, -z - 1, -w - 1] if y < 0 else [x, y]
+            elif w < 0:
+                v = [x, -y - 1, z, -w - 1] if y < 0 else [x, y, z]
+            else:
+                v = [x, y, z, w]
+        loc = [int(t) - node_offset for t in v]
+        out.append([t for t in loc if 0 <= t < nv])
+    return out
+
+
+def mas_levels(s, bank):
+    """The MAS hierarchy by its meaning, independent of the mask kernels: the
+    nodes of level l+1 are the connected components, inside each bank of B
+    consecutive level-l nodes, of the graph of mesh edges and contact pairs;
+    they are numbered bank by bank, inside a bank by their lowest lane.
+    Level 0 nodes are the partition slots.  Returns fine_mask, per-level
+    node ids (levels 1..L), level sizes [L+1, 2] and components per level-0
+    bank."""
+    import oracle
+    B = bank
+    nv, pmr, rmp = s.fem_count, np.asarray(s.part_map_real), np.asarray(s.real_map_part)
+    L = oracle.compute_num_levels(max(len(pmr), nv), bank)
+    st, nn, nl = (np.asarray(a) for a in (s.neighbor_start, s.neighbor_num, s.neighbor_list))
+    edges = [(v, int(u)) for v in range(nv) for u in nl[st[v]:st[v] + nn[v]]]
+    for grp in _decode_pairs(s.pairs, s.node_offset, nv):
+        edges += [(grp[i], grp[j]) for i in range(len(grp)) for j in range(i + 1, len(grp))]
+    node = rmp.astype(np.int64).copy()  # level-0 node = slot
+    count, begin = len(pmr), 0
+    ids, sizes = [], [(len(pmr), 0)]
+    fine_mask = prefix = None
+    for level in range(L):
+        parent = list(range(count))
+
+        def find(a):
+            while parent[a] != a:
+                parent[a] = parent[parent[a]]
+                a = parent[a]
+            return a
+        for u, v in edges:
+            a, b = int(node[u]), int(node[v])
+            if a // B == b // B and a != b:
+                ra, rb = find(a), find(b)
+                if ra != rb:
+                    parent[max(ra, rb)] = min(ra, rb)  # root: lowest member
+        live = np.zeros(count, bool)
+        live[node] = True
+        new = np.full(count, -1, np.int64)
+        comps = np.zeros((count + B - 1) // B, np.int64)
+        nxt = 0
+        for a in range(count):
+            if live[a] and find(a) == a:
+                new[a] = nxt
+                comps[a // B] += 1
+                nxt += 1
+        for a in range(count):
+            if live[a]:
+                new[a] = new[find(a)]
+        if level == 0:
+            fine_mask = np.zeros(nv, np.uint32)
+            for v in range(nv):
+                a = node[v]
+                for u in range(a - a % B, a - a % B + B):
+                    if u < count and live[u] and find(u) == find(a):
+                        fine_mask[v] |= np.uint32(1 << (u % B))
+            prefix = comps
+        begin += (count + B - 1) // B * B
+        node = new[node]
+        ids.append(node.copy())
+        count = nxt
+        sizes.append((count, begin))
+    return {"fine_mask": fine_mask, "ids": np.array(ids), "level_size": np.array(sizes), "prefix": prefix,
+            "levelnum": L}
+
+
+def galerkin_domains(s, lev, bank, cemas16):
+    """Packed upper FP64 domain matrices of every level by their meaning: the
+    Galerkin sum over the FEM entries A_ij whose level-l nodes share a bank,
+    minus the entries CEMAS16 leaves out (cemas16=True): an in-bank pair of
+    level-0 slots whose order runs against the vertex order, and, above
+    level 0, the in-bank entries of a row whose even partner slot is padding
+    when the bank is one component."""
+    B = bank
+    nv, fo = s.fem_count, s.fem_offset
+    pmr, rmp = np.asarray(s.part_map_real), np.asarray(s.real_map_part)
+    L = lev["levelnum"]
+    begins = [0] + [int(lev["level_size"][l][1]) for l in range(1, L)]
+    total = int(lev["level_size"][L][1])
+    P = B * (B + 1) // 2
+    out = np.zeros((total // B, P, 9))
+    r, c, v = np.asarray(s.rows), np.asarray(s.cols), np.asarray(s.vals).reshape(-1, 3, 3).transpose(0, 2, 1)
+    sel = (r >= fo) & (r < fo + nv) & (c >= fo) & (c < fo + nv)
+    ent = []
+    for i, j, blk in zip(r[sel] - fo, c[sel] - fo, v[sel]):
+        ent.append((i, j, blk))
+        if i != j:
+            ent.append((j, i, blk.T))
+    for i, j, blk in ent:
+        si, sj = rmp[i], rmp[j]
+        same0 = si // B == sj // B
+        if cemas16 and same0 and i != j and ((i < j) != (si < sj)):
+            continue
+        for l in range(L):
+            if l == 0:
+                a, b = si, sj
+            else:
+                if cemas16 and same0 and lev["prefix"][si // B] == 1 and pmr[si & ~1] < 0:
+                    continue
+                a, b = begins[l] + lev["ids"][l - 1][i], begins[l] + lev["ids"][l - 1][j]
+            if a // B != b // B or a > b:
+                continue
+            g, la, lb = a // B, a % B, b % B
+            out[g, B * la - la * (la + 1) // 2 + lb] += blk.T.reshape(9)  # column-major
+    return out
+
+
+def gapped_partition(s, bank=16, gap=2):
+    """Partition of a vertex-sorted system (partition_for_bank) with slot
+    `gap` of every bank left empty: B - 1 consecutive vertices per bank."""
+    import dataclasses
+    nv, B = s.fem_count, bank
+    per = B - 1
+    nbanks = (nv + per - 1) // per
+    pmr = np.full(nbanks * B, -1, np.int32)
+    rmp = np.zeros(nv, np.int32)
+    for v in range(nv):
+        b, k = divmod(v, per)
+        slot = b * B + (k if k < gap else k + 1)
+        pmr[slot] = v
+        rmp[v] = slot
+    return dataclasses.replace(s, part_map_real=pmr, real_map_part=rmp, name=s.name + "_gap")
 
 
 def expand_unused(A):

@@ -51,10 +51,18 @@ def test_create_rejects_bad_config(lib):
     from agipc_learning_b200 import _native as N
     cfg = N.Config()
     lib.maspcg_config_default(ctypes.byref(cfg))
-    cfg.bank_size = 16
+    cfg.bank_size = 16  # MAS32 with a 16-vertex bank
     h = ctypes.c_void_p()
     assert lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)) == N.ERR_UNSUPPORTED
     assert b"32-vertex" in lib.maspcg_last_error(None)
+    cfg.bank_size = 24
+    assert lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)) == N.ERR_UNSUPPORTED
+    cfg.preconditioner, cfg.bank_size = N.PRECOND_MAS16, 32  # CEMAS16 with a 32-vertex bank
+    assert lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)) == N.ERR_UNSUPPORTED
+    assert b"16-vertex" in lib.maspcg_last_error(None)
+    cfg.bank_size, cfg.inverse_storage = 16, N.INV_BF16  # CEMAS16 stores FP32 inverses
+    assert lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)) == N.ERR_UNSUPPORTED
+    assert b"FP32" in lib.maspcg_last_error(None)
 
 
 def test_create_without_device_fails_cleanly(lib):
