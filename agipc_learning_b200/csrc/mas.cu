@@ -964,90 +964,86 @@ __global__ void k_chain_targets(ApplyArgs a, int* target)
 
 // ---- CEMAS16 apply (MASPreconditioner::preconditioning, :2250-2291) -------
 //
-// Three launches over 16-slot banks:
-//   * the coarse restriction: R of a coarse node is the sum of its member
-//     slots' residuals, read from the member lists in slot order
-//     (__buildMultiLevelR_optimized_new :729-847 adds the same FP32 terms
-//     with atomics, in no fixed order);
-//   * the domain applies of every level, half a warp per 48x48 domain: lane
-//     l holds block (l, (l + d) % 16) of the wrapped diagonals d = 0..8 and
-//     each stored block serves both triangles through a shuffle of width 16
-//     (_schwarzLocalXSym6 :957-1027); level-0 domains read r directly;
-//   * the prolongation z = Z0 + sum of the coarse Z along the vertex's
-//     coarse table, in level order (__collectFinalZ_new :850-881), with r.z.
+// Over 16-slot banks:
+//   * the restriction, one launch per coarse level (L-1 launches): a node of
+//     level l+1 is a connected component inside one bank of level l, so its
+//     children sit in one half-warp; each group is summed in lane order and
+//     its lowest lane writes the parent's R once (no atomics; the reference
+//     adds the same FP32 terms with atomics, __buildMultiLevelR_optimized_new
+//     :729-847);
+//   * the coarse domain applies (levels >= 1) and the level-0 domain apply:
+//     half a warp per 48x48 domain, lane l holding block (l, (l + d) % 16) of
+//     the wrapped diagonals d = 0..8, each stored block serving both
+//     triangles through a shuffle of width 16 (_schwarzLocalXSym6 :957-1027);
+//   * the prolongation: a vertex's z is its level-0 result plus the coarse
+//     results along its coarse table, in level order (__collectFinalZ_new
+//     :850-881), with r.z.  Sequentially it is fused into the level-0 apply;
+//     with the coarse levels on the side stream beside the level-0 apply it
+//     is a pass of its own after the join (the same FP32 sums either way).
 struct Mas16Args {
   const int* pmr;
+  const int* going_next;
   const int* coarse_table;  // 6 global slots per vertex (levels 1..L-1)
-  const int* perm[kMaxLevels];
-  const int* off[kMaxLevels];
-  int node_base[kMaxLevels + 1];  // first restriction thread of each coarse level
   LevelInfo lv;
   const float* inv;  // kMas16InvElems per domain
   float* coarse_r;   // (total_clusters - c0) x 3
   float* coarse_z;
-  float* z0;  // c0 x 3
   int fem_off, c0;
 };
 
+// R of level l+1 from level l (l = 0: from r).
 template <typename Tv>
-__global__ void __launch_bounds__(kTpb) k16_restrict(Mas16Args a, const Tv* __restrict__ r, PcgScalars* s)
+__global__ void __launch_bounds__(kTpb) k16_restrict(Mas16Args a, const Tv* __restrict__ r, int level, PcgScalars* s)
 {
   pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int count = level == 0 ? a.c0 : a.lv.count[level];
+  const int padded = (count + 15) & ~15;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.node_base[a.lv.levelnum]) return;
-  int L = 1;
-  while (L + 1 < a.lv.levelnum && t >= a.node_base[L + 1]) ++L;
-  const int A = t - a.node_base[L];
-  const int* perm = a.perm[L];
-  const int p0 = a.off[L][A], p1 = a.off[L][A + 1];
-  float x0 = 0.f, x1 = 0.f, x2 = 0.f;
-  for (int p = p0; p < p1; ++p) {
-    const size_t base = 3 * (size_t)(a.fem_off + perm[p]);
-    x0 += (float)r[base];
-    x1 += (float)r[base + 1];
-    x2 += (float)r[base + 2];
-  }
-  float* o = a.coarse_r + 3 * (size_t)(a.lv.begin[L] + A - a.c0);
-  o[0] = x0;
-  o[1] = x1;
-  o[2] = x2;
-}
-
-template <typename Tv>
-__global__ void __launch_bounds__(kTpb) k16_apply(Mas16Args a, const Tv* __restrict__ r, PcgScalars* s)
-{
-  pdl_wait();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if ((t & ~31) >= a.lv.domains * 16) return;  // whole warp past the last domain
-  const int g = t >> 4, lane = t & 15;
-  const bool in = g < a.lv.domains;
-  const bool level0 = g < a.lv.dom_begin[1];
-  const int slot = 16 * g + lane;
-  float x0 = 0.f, x1 = 0.f, x2 = 0.f;
-  if (in) {
-    if (level0) {
-      if (a.pmr[slot] >= 0) {
-        const size_t base = 3 * (size_t)(a.fem_off + slot);
-        x0 = (float)r[base];
-        x1 = (float)r[base + 1];
-        x2 = (float)r[base + 2];
+  if ((t & ~31) >= padded) return;  // whole warp past the level
+  float v[3] = {0.f, 0.f, 0.f};
+  int parent = -1;
+  if (t < count) {
+    if (level == 0) {
+      const int vtx = a.pmr[t];
+      if (vtx >= 0) {
+        const size_t base = 3 * (size_t)(a.fem_off + t);
+        v[0] = (float)r[base];
+        v[1] = (float)r[base + 1];
+        v[2] = (float)r[base + 2];
+        parent = a.going_next[vtx];
       }
     } else {
+      const int slot = a.lv.begin[level] + t;
       const float* x = a.coarse_r + 3 * (size_t)(slot - a.c0);
-      x0 = x[0];
-      x1 = x[1];
-      x2 = x[2];
+      v[0] = x[0];
+      v[1] = x[1];
+      v[2] = x[2];
+      parent = a.going_next[slot];
     }
   }
-  const float* inv = a.inv + (size_t)(in ? g : 0) * kMas16InvElems;
+  float o[3];
+  bool leader;
+  group_sum<false>(parent >= 0 ? parent : -1 - (int)(threadIdx.x & 31), v, o, leader);
+  if (parent >= 0 && leader) {
+    float* d = a.coarse_r + 3 * (size_t)(parent - a.c0);
+    d[0] = o[0];
+    d[1] = o[1];
+    d[2] = o[2];
+  }
+}
+
+// y = M x for the domain of this half-warp (lane = t & 15); x of the lane's
+// node; all 32 lanes of the warp take part (in = false: x = 0, no loads).
+__device__ __forceinline__ void domain_apply16(const float* __restrict__ inv, bool in, int lane, const float x[3],
+                                               float y[3])
+{
   float y0 = 0.f, y1 = 0.f, y2 = 0.f;
 #pragma unroll
   for (int d = 0; d < kMas16Diags; ++d) {
     const int c = (lane + d) & 15;
-    const float c0 = __shfl_sync(kFull, x0, c, 16), c1 = __shfl_sync(kFull, x1, c, 16),
-                c2 = __shfl_sync(kFull, x2, c, 16);
+    const float c0 = __shfl_sync(kFull, x[0], c, 16), c1 = __shfl_sync(kFull, x[1], c, 16),
+                c2 = __shfl_sync(kFull, x[2], c, 16);
     float B[9];
 #pragma unroll
     for (int e = 0; e < 9; ++e) B[e] = in ? __ldcs(inv + (d * 9 + e) * 16 + lane) : 0.f;
@@ -1055,51 +1051,73 @@ __global__ void __launch_bounds__(kTpb) k16_apply(Mas16Args a, const Tv* __restr
     y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
     y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
     if (d != 0) {
-      const float t0 = B[0] * x0 + B[3] * x1 + B[6] * x2;
-      const float t1 = B[1] * x0 + B[4] * x1 + B[7] * x2;
-      const float t2 = B[2] * x0 + B[5] * x1 + B[8] * x2;
+      const float t0 = B[0] * x[0] + B[3] * x[1] + B[6] * x[2];
+      const float t1 = B[1] * x[0] + B[4] * x[1] + B[7] * x[2];
+      const float t2 = B[2] * x[0] + B[5] * x[1] + B[8] * x[2];
       const int src = (lane - d) & 15;
       y0 += __shfl_sync(kFull, t0, src, 16);
       y1 += __shfl_sync(kFull, t1, src, 16);
       y2 += __shfl_sync(kFull, t2, src, 16);
     }
   }
-  if (!in) return;
-  float* o = level0 ? a.z0 + 3 * (size_t)slot : a.coarse_z + 3 * (size_t)(slot - a.c0);
-  o[0] = y0;
-  o[1] = y1;
-  o[2] = y2;
+  y[0] = y0;
+  y[1] = y1;
+  y[2] = y2;
 }
 
-template <typename Tv, typename Tacc>
-__global__ void __launch_bounds__(kTpb) k16_collect(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
-                                                    int part_base, int total_parts, int mode, PcgScalars* s)
+__global__ void __launch_bounds__(kTpb) k16_apply_coarse(Mas16Args a, PcgScalars* s)
 {
   pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  Tacc dot = 0;
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < a.c0; slot += gridDim.x * blockDim.x) {
-    const int v = a.pmr[slot];
-    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-    if (v >= 0) {
-      c0 = a.z0[3 * (size_t)slot];
-      c1 = a.z0[3 * (size_t)slot + 1];
-      c2 = a.z0[3 * (size_t)slot + 2];
-      for (int l = 1; l < a.lv.levelnum; ++l) {
-        const float* zc = a.coarse_z + 3 * (size_t)(a.coarse_table[6 * (size_t)v + l - 1] - a.c0);
-        c0 += zc[0];
-        c1 += zc[1];
-        c2 += zc[2];
-      }
-    }
-    const size_t base = 3 * (size_t)(a.fem_off + slot);
-    const Tv z0 = (Tv)c0, z1 = (Tv)c1, z2 = (Tv)c2;
-    z[base] = z0;
-    z[base + 1] = z1;
-    z[base + 2] = z2;
-    dot += (Tacc)r[base] * (Tacc)z0 + (Tacc)r[base + 1] * (Tacc)z1 + (Tacc)r[base + 2] * (Tacc)z2;
+  const int d1 = a.lv.dom_begin[1];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((t & ~31) >= (a.lv.domains - d1) * 16) return;
+  const int g = d1 + (t >> 4), lane = t & 15;
+  const bool in = g < a.lv.domains;
+  const size_t base = 3 * (size_t)(16 * g + lane - a.c0);
+  float x[3] = {0.f, 0.f, 0.f}, y[3];
+  if (in) {
+    x[0] = a.coarse_r[base];
+    x[1] = a.coarse_r[base + 1];
+    x[2] = a.coarse_r[base + 2];
   }
-  pdl_trigger();
+  domain_apply16(a.inv + (size_t)(in ? g : 0) * kMas16InvElems, in, lane, x, y);
+  if (!in) return;
+  a.coarse_z[base] = y[0];
+  a.coarse_z[base + 1] = y[1];
+  a.coarse_z[base + 2] = y[2];
+}
+
+// The coarse correction and r.z of one slot's z (y holds the level-0 result
+// in FP32 precision).
+template <typename Tv, typename Tacc>
+__device__ __forceinline__ Tacc prolong16(const Mas16Args& a, int vtx, const Tv rv[3], float y[3], Tv* zp)
+{
+  if (vtx >= 0) {
+    const int* ct = a.coarse_table + 6 * (size_t)vtx;
+    for (int l = 1; l < a.lv.levelnum; ++l) {
+      const float* zc = a.coarse_z + 3 * (size_t)(ct[l - 1] - a.c0);
+      y[0] += zc[0];
+      y[1] += zc[1];
+      y[2] += zc[2];
+    }
+  } else {
+    y[0] = y[1] = y[2] = 0.f;
+  }
+  Tacc dot = 0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const Tv zv = (Tv)y[q];
+    zp[q] = zv;
+    dot += (Tacc)rv[q] * (Tacc)zv;
+  }
+  return dot;
+}
+
+template <typename Tacc>
+__device__ __forceinline__ void rz_finish(Tacc dot, Tacc* partial, int part_base, int total_parts, int mode,
+                                          PcgScalars* s)
+{
   if (!partial) return;
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x, total) &&
@@ -1107,25 +1125,80 @@ __global__ void __launch_bounds__(kTpb) k16_collect(Mas16Args a, const Tv* __res
     rz_update(s, (double)total, mode);
 }
 
+// kProlong: add the coarse correction and sum r.z (the coarse levels ran
+// before); else z = the level-0 result only.
+template <typename Tv, typename Tacc, bool kProlong>
+__global__ void __launch_bounds__(kTpb) k16_apply_level0(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
+                                                         int part_base, int total_parts, int mode, PcgScalars* s)
+{
+  pdl_wait();
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  const int d0 = a.lv.dom_begin[1];
+  Tacc dot = 0;
+  const int stride = gridDim.x * blockDim.x;
+  const int span = (d0 * 16 + 31) & ~31;  // whole warps
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < span; t += stride) {
+    const int g = t >> 4, lane = t & 15;
+    const bool in = g < d0;
+    const int slot = 16 * g + lane;
+    const int vtx = in ? a.pmr[slot] : -1;
+    const size_t base = 3 * (size_t)(a.fem_off + slot);
+    Tv rv[3] = {0, 0, 0};
+    float x[3] = {0.f, 0.f, 0.f}, y[3];
+    if (vtx >= 0) {
+      rv[0] = r[base];
+      rv[1] = r[base + 1];
+      rv[2] = r[base + 2];
+      x[0] = (float)rv[0];
+      x[1] = (float)rv[1];
+      x[2] = (float)rv[2];
+    }
+    domain_apply16(a.inv + (size_t)(in ? g : 0) * kMas16InvElems, in, lane, x, y);
+    if (!in) continue;
+    if (kProlong) {
+      dot += prolong16<Tv, Tacc>(a, vtx, rv, y, z + base);
+    } else {
+      const bool real = vtx >= 0;
+      z[base] = real ? (Tv)y[0] : Tv(0);
+      z[base + 1] = real ? (Tv)y[1] : Tv(0);
+      z[base + 2] = real ? (Tv)y[2] : Tv(0);
+    }
+  }
+  pdl_trigger();
+  if (kProlong) rz_finish(dot, partial, part_base, total_parts, mode, s);
+}
+
+// The prolongation after the join: z (the level-0 result) plus the coarse
+// correction, and r.z.
+template <typename Tv, typename Tacc>
+__global__ void __launch_bounds__(kTpb) k16_prolong(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
+                                                    int part_base, int total_parts, int mode, PcgScalars* s)
+{
+  pdl_wait();
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  Tacc dot = 0;
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < a.c0; slot += gridDim.x * blockDim.x) {
+    const int vtx = a.pmr[slot];
+    if (vtx < 0) continue;
+    const size_t base = 3 * (size_t)(a.fem_off + slot);
+    const Tv rv[3] = {r[base], r[base + 1], r[base + 2]};
+    float y[3] = {(float)z[base], (float)z[base + 1], (float)z[base + 2]};
+    dot += prolong16<Tv, Tacc>(a, vtx, rv, y, z + base);
+  }
+  pdl_trigger();
+  rz_finish(dot, partial, part_base, total_parts, mode, s);
+}
+
 Mas16Args make_mas16_args(maspcg_handle* h)
 {
   Mas16Args a{};
-  const LevelInfo& lv = h->lv;
   a.pmr = h->pmr.get();
+  a.going_next = h->going_next.get();
   a.coarse_table = h->coarse_table.get();
-  int n = 0;
-  for (int l = 1; l < lv.levelnum && l < kMaxLevels; ++l) {
-    a.perm[l] = h->perm[l].get();
-    a.off[l] = h->off[l].get();
-    a.node_base[l] = n;
-    n += lv.count[l];
-  }
-  for (int l = std::max(lv.levelnum, 1); l <= kMaxLevels; ++l) a.node_base[l] = n;
-  a.lv = lv;
+  a.lv = h->lv;
   a.inv = reinterpret_cast<const float*>(h->inv.get());
   a.coarse_r = h->coarse_r.get();
   a.coarse_z = h->coarse_z.get();
-  a.z0 = h->mas16_z0.get();
   a.fem_off = h->fem_off;
   a.c0 = h->c0;
   return a;
@@ -1371,7 +1444,6 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   h->coarse_r.resize(coarse > 0 ? coarse : 3);
   h->coarse_z.resize(coarse > 0 ? coarse : 3);
   if (h->bank == 16) {
-    h->mas16_z0.resize(3 * (size_t)c0);
     MCK(cudaMemsetAsync(h->coarse_r.get(), 0, h->coarse_r.bytes(), st));
     MCK(cudaMemsetAsync(h->coarse_z.get(), 0, h->coarse_z.bytes(), st));
     int f = 0;
@@ -1680,29 +1752,54 @@ template void mas_apply<double, double>(maspcg_handle*, const double*, double*, 
 
 int mas_level0_grid(maspcg_handle* h) { return level0_grid(h, h->apply_variant); }
 
-int mas16_grid(maspcg_handle* h) { return std::max(1, std::min(ceil_div(h->c0, kTpb), 4 * h->sm_count)); }
+// CTAs of the kernel that completes r.z (level-0 apply or prolongation).
+int mas16_grid(maspcg_handle* h) { return std::max(1, std::min(ceil_div(h->c0, kTpb), 8 * h->sm_count)); }
 
-// CEMAS16 apply: restriction, domain applies of all levels, prolongation
-// with r.z (the last block completes r.z over [0, total_parts)).
+// CEMAS16 apply.  Sequential: the restriction level by level, the coarse
+// domain applies, then the level-0 apply with the prolongation and r.z.
+// overlap: the restriction and the coarse applies run on the side stream
+// beside the level-0 apply, and the prolongation with r.z follows the join.
+// The last block of the final kernel completes r.z over [0, total_parts).
 template <typename Tv, typename Tacc>
 void mas16_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-                 int grid, PcgScalars* s)
+                 int grid, PcgScalars* s, bool overlap)
 {
   const Mas16Args a = make_mas16_args(h);
-  const int nodes = a.node_base[std::min(h->lv.levelnum, kMaxLevels)];
-  if (h->lv.levelnum > 1 && nodes > 0)
-    launch_pdl(h, k16_restrict<Tv>, dim3(ceil_div(nodes, kTpb)), dim3(kTpb), 0, a, r, s);
-  launch_pdl(h, k16_apply<Tv>, dim3(ceil_div((long long)h->lv.domains * 16, kTpb)), dim3(kTpb), 0, a, r, s);
-  launch_pdl(h, k16_collect<Tv, Tacc>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base, total_parts, mode,
-             s);
+  const LevelInfo& lv = h->lv;
+  const int g0 = std::max(1, ceil_div(h->c0, kTpb));
+  auto coarse_levels = [&](cudaStream_t st) {
+    for (int l = 0; l + 1 < lv.levelnum; ++l) {
+      const int count = l == 0 ? h->c0 : lv.count[l];
+      launch_pdl_on(h, st, k16_restrict<Tv>, dim3(std::max(1, ceil_div((count + 15) & ~15, kTpb))), dim3(kTpb), 0,
+                    a, r, l, s);
+    }
+    const int coarse = lv.domains - lv.dom_begin[1];
+    launch_pdl_on(h, st, k16_apply_coarse, dim3(std::max(1, ceil_div((long long)coarse * 16, kTpb))), dim3(kTpb), 0,
+                  a, s);
+  };
+  if (lv.levelnum > 1 && overlap) {
+    MCK(cudaEventRecord(h->ev_fork, h->stream));
+    MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+    coarse_levels(h->side_stream);
+    MCK(cudaEventRecord(h->ev_join, h->side_stream));
+    launch_pdl(h, k16_apply_level0<Tv, Tacc, false>, dim3(g0), dim3(kTpb), 0, a, r, z, partial, part_base,
+               total_parts, mode, s);
+    MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    launch_pdl(h, k16_prolong<Tv, Tacc>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base, total_parts, mode,
+               s);
+  } else {
+    if (lv.levelnum > 1) coarse_levels(h->stream);
+    launch_pdl(h, k16_apply_level0<Tv, Tacc, true>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base,
+               total_parts, mode, s);
+  }
   MCK(cudaGetLastError());
 }
 template void mas16_apply<float, float>(maspcg_handle*, const float*, float*, float*, int, int, int, int,
-                                        PcgScalars*);
+                                        PcgScalars*, bool);
 template void mas16_apply<float, double>(maspcg_handle*, const float*, float*, double*, int, int, int, int,
-                                         PcgScalars*);
+                                         PcgScalars*, bool);
 template void mas16_apply<double, double>(maspcg_handle*, const double*, double*, double*, int, int, int, int,
-                                          PcgScalars*);
+                                          PcgScalars*, bool);
 
 // Decode the stored inverses into the reference's packed FP32 layout.
 void decode_inverses(maspcg_handle* h, float* out)

@@ -222,7 +222,6 @@ struct maspcg_handle {
   maspcg::DBuf<int> failed;
   int failed_domains = 0;
   maspcg::DBuf<float> coarse_r, coarse_z;
-  maspcg::DBuf<float> mas16_z0;                 // CEMAS16: level-0 domain outputs (3 per slot)
   maspcg::DBuf<int> chain_count, chain_target;  // coarse-level dataflow counters (per coarse domain)
   maspcg::DBuf<double> chain_dot;               // per coarse domain: R.Z (r.z of the coarse levels)
   maspcg::DBuf<double> coarse64;

@@ -35,7 +35,7 @@ void launch_factor(maspcg_handle* h, double* assembled_out);
 int mas_level0_grid(maspcg_handle* h);
 template <typename Tv, typename Tacc>
 void mas16_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-                 int grid, PcgScalars* s);
+                 int grid, PcgScalars* s, bool overlap);
 int mas16_grid(maspcg_handle* h);
 
 namespace {
@@ -623,7 +623,9 @@ struct Engine {
             s ? partial_rz() : nullptr, 0, parts_total, any_mas ? 0 : 1, mode, s);
     }
     if (mas) mas_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s, overlap);
-    if (mas16) mas16_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s);
+    if (mas16)
+      mas16_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s,
+                            h->overlap_coarse);
     MCK(cudaGetLastError());
   }
 

@@ -263,6 +263,58 @@ def widened_rows(stream, dev):
     return out
 
 
+def cemas16_row(s, stream, dev, steps):
+    """The same Newton system under CEMAS16 (16-vertex banks, 48x48 domains)
+    with the vertex-sorted partition the app's METIS-sorted meshes give:
+    build + solve device time in the reference precision with the reference's
+    rz gate, and with FP32 vectors / FP64 refinement to the bench's FP64
+    gate; the apply and factor stages alone.  CUDA events on the library's
+    stream; one warm-up, then the mean of `steps`."""
+    import torch
+    from agipc_learning_b200 import synth
+    from agipc_learning_b200.solver import MasPcg
+
+    t = synth.partition_for_bank(s, 16)
+    D = lambda a: torch.from_numpy(a).to(dev)  # noqa: E731
+    vals_d, rows_d, cols_d, b_d = D(t.vals), D(t.rows), D(t.cols), D(t.b)
+    x_d = torch.zeros_like(b_d)
+    out = {"partition": "16-slot banks, vertices renumbered in Morton order (slot = vertex)"}
+    for key, precision, gate in (("reference_rz_gate", "reference", "rz"), ("mixed_fp32_inverse", "mixed", "euclid")):
+        with MasPcg(preconditioner="cemas16", precision=precision, gate=gate, tolerance=1e-4) as m:
+            m.set_stream(stream.cuda_stream)
+            m.set_graph(t.fem_count, t.node_offset, t.neighbor_start, t.neighbor_num, t.neighbor_list,
+                        t.part_map_real, t.real_map_part)
+            m.set_contacts(t.pairs)
+
+            def step():
+                m.set_matrix(vals_d, rows_d, cols_d, t.nb, t.fem_offset, t.abd_bodies)
+                m.build()
+                return m.solve(b_d, x_d)[1]
+
+            step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                res = step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            row = {"ms_per_solve": e0.elapsed_time(e1) / steps, "iterations": res["iterations"],
+                   "rel_res_true": res["rel_res_true"], "status": res["status_name"]}
+            if precision == "mixed":
+                info = m.info()
+                ms_prec, ms_fac = m.time_stage(1, 20), m.time_stage(3, 3)
+                c0 = len(t.part_map_real)
+                # FP32 records (9 diagonals x 9 x 16 floats) of every domain; r read
+                # twice, z written, read and written again (FP32), 24 B of coarse table
+                apply_bytes = info["domains"] * 5184 + (5 * 12 + 24) * c0
+                row.update({"domains": info["domains"], "levels": info["levelnum"], "precondition_ms": ms_prec,
+                            "domain_factor_ms": ms_fac, "precondition_algorithmic_bytes": apply_bytes,
+                            "precondition_GBps": apply_bytes / (ms_prec * 1e-3) / 1e9})
+            out[key] = row
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -412,6 +464,10 @@ def run_ours(args, world, rank, local):
             line["widened_rows"] = widened_rows(stream, dev)
         except Exception as exc:  # reported, not fatal for the headline
             line["widened_rows"] = {"error": str(exc)}
+        try:
+            line["cemas16"] = cemas16_row(s, stream, dev, max(1, min(args.steps, 3)))
+        except Exception as exc:
+            line["cemas16"] = {"error": str(exc)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         oracle.build()
