@@ -1035,18 +1035,21 @@ __global__ void __launch_bounds__(kTpb) k16_restrict(Mas16Args a, const Tv* __re
 
 // y = M x for the domain of this half-warp (lane = t & 15); x of the lane's
 // node; all 32 lanes of the warp take part (in = false: x = 0, no loads).
+// The lane's 81 record elements are all loaded before the arithmetic, so a
+// warp has its whole 10 KB in flight at once.
 __device__ __forceinline__ void domain_apply16(const float* __restrict__ inv, bool in, int lane, const float x[3],
                                                float y[3])
 {
+  float Bm[kMas16Diags * 9];
+#pragma unroll
+  for (int k = 0; k < kMas16Diags * 9; ++k) Bm[k] = in ? __ldcs(inv + k * 16 + lane) : 0.f;
   float y0 = 0.f, y1 = 0.f, y2 = 0.f;
 #pragma unroll
   for (int d = 0; d < kMas16Diags; ++d) {
     const int c = (lane + d) & 15;
     const float c0 = __shfl_sync(kFull, x[0], c, 16), c1 = __shfl_sync(kFull, x[1], c, 16),
                 c2 = __shfl_sync(kFull, x[2], c, 16);
-    float B[9];
-#pragma unroll
-    for (int e = 0; e < 9; ++e) B[e] = in ? __ldcs(inv + (d * 9 + e) * 16 + lane) : 0.f;
+    const float* B = Bm + 9 * d;
     y0 += B[0] * c0 + B[1] * c1 + B[2] * c2;
     y1 += B[3] * c0 + B[4] * c1 + B[5] * c2;
     y2 += B[6] * c0 + B[7] * c1 + B[8] * c2;
@@ -1065,7 +1068,7 @@ __device__ __forceinline__ void domain_apply16(const float* __restrict__ inv, bo
   y[2] = y2;
 }
 
-__global__ void __launch_bounds__(kTpb) k16_apply_coarse(Mas16Args a, PcgScalars* s)
+__global__ void __launch_bounds__(kTpb, 2) k16_apply_coarse(Mas16Args a, PcgScalars* s)
 {
   pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
@@ -1128,7 +1131,7 @@ __device__ __forceinline__ void rz_finish(Tacc dot, Tacc* partial, int part_base
 // kProlong: add the coarse correction and sum r.z (the coarse levels ran
 // before); else z = the level-0 result only.
 template <typename Tv, typename Tacc, bool kProlong>
-__global__ void __launch_bounds__(kTpb) k16_apply_level0(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
+__global__ void __launch_bounds__(kTpb, 2) k16_apply_level0(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
                                                          int part_base, int total_parts, int mode, PcgScalars* s)
 {
   pdl_wait();
