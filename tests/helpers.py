@@ -319,3 +319,16 @@ def inverse_residual(A, M):
     """Root-mean-square entry of A M - I (the oracle's local check)."""
     R = A @ M - np.eye(A.shape[0])
     return float(np.sqrt((R * R).sum() / A.shape[0]))
+
+
+def compare_hierarchy(g, o):
+    """GPU hierarchy (MasPcg.hierarchy) equals the oracle's, bit for bit."""
+    L = o["levelnum"]
+    assert g["levelnum"] == L
+    assert np.array_equal(g["fine_mask"], o["fine_mask"])
+    assert np.array_equal(g["coarse_space_tables"], o["coarse_space_tables"])
+    assert np.array_equal(g["going_next"], o["going_next"])
+    assert np.array_equal(g["level_size"][1:], o["level_size"][1:])
+    assert np.array_equal(g["coarse_table"][:, :L - 1], o["coarse_table"][:, :L - 1])
+    assert np.array_equal(g["prefix_original"], o["prefix_original"])
+    assert g["total_clusters"] == o["total_clusters"]
