@@ -357,6 +357,8 @@ class TraditionalMAS32Preconditioner:
     initPreconditioner_Neighbor, fill the public arrays, initPreconditioner_Matrix,
     then per Newton step setPreconditioner_bcoo and preconditioning."""
 
+    _PRECONDITIONER = "mas32"
+
     def __init__(self, **engine_cfg):
         self.engine_cfg = engine_cfg
         self.neighborListSize = 0
@@ -376,7 +378,7 @@ class TraditionalMAS32Preconditioner:
         self.totalMapNodes = int(partMapSize)
 
     def initPreconditioner_Matrix(self):
-        e = MasPcg(preconditioner="mas32", **self.engine_cfg)
+        e = MasPcg(preconditioner=self._PRECONDITIONER, **self.engine_cfg)
         lst = np.asarray(self.d_neighborListInit)[: self.neighborListSize]
         e.set_graph(self.totalNodes, self.collision_node_Offset, self.d_neighborStart, self.d_neighborNumInit, lst,
                     np.asarray(self.d_partId_map_real)[: self.totalMapNodes], self.d_real_map_partId)
@@ -399,3 +401,12 @@ class TraditionalMAS32Preconditioner:
         if self._engine is not None:
             self._engine.close()
             self._engine = None
+
+
+class MASPreconditioner(TraditionalMAS32Preconditioner):
+    """MASPreconditioner, CEMAS16 (MASPreconditioner.cuh; MASPreconditioner.cu:
+    2209-2364): the same caller sequence (initPreconditioner_Neighbor,
+    initPreconditioner_Matrix, setPreconditioner_bcoo, preconditioning,
+    FreeMAS) with d_partId_map_real in 16-slot banks."""
+
+    _PRECONDITIONER = "cemas16"

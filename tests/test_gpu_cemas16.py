@@ -120,3 +120,27 @@ def test_hybrid_abd_fem_matches_oracle():
     assert res["status_name"] == ro["status"] == "converged"
     assert abs(res["iterations"] - ro["iterations"]) <= max(2, int(0.1 * ro["iterations"]))
     assert res["rel_res_true"] <= 1e-5 * 1.01
+
+
+@pytest.mark.parametrize("bank", [32, 16])
+def test_reference_call_sequence(bank):
+    """The reference's caller sequence (gl_main.cu:1502-1536) on the mirror
+    classes: TraditionalMAS32Preconditioner and MASPreconditioner (CEMAS16)."""
+    from agipc_learning_b200.solver import MASPreconditioner, TraditionalMAS32Preconditioner
+    base = synth.config_system(0)
+    s = synth.partition_for_bank(base, 16) if bank == 16 else base
+    p = (MASPreconditioner if bank == 16 else TraditionalMAS32Preconditioner)()
+    p.initPreconditioner_Neighbor(s.fem_count, s.node_offset, len(s.neighbor_list), s.pairs, len(s.part_map_real))
+    p.neighborListSize = len(s.neighbor_list)
+    p.d_neighborListInit, p.d_neighborStart, p.d_neighborNumInit = s.neighbor_list, s.neighbor_start, s.neighbor_num
+    p.d_partId_map_real, p.d_real_map_partId = s.part_map_real, s.real_map_part
+    p.initPreconditioner_Matrix()
+    p.setPreconditioner_bcoo(s.vals, s.rows, s.cols, np.arange(len(s.rows)), 0, len(s.rows), len(s.pairs))
+    z = p.preconditioning(s.b)
+    p.FreeMAS()
+    o = _oracle(s) if bank == 16 else oracle.Mas32.from_system(s)
+    if bank == 32:
+        o.reorder(s.pairs)
+        o.prepare_hessian(s.vals, s.rows, s.cols, None, 0)
+    z_ref = o.precondition(s.b)
+    assert np.linalg.norm(z - z_ref) / np.linalg.norm(z_ref) <= 2e-4
