@@ -307,16 +307,57 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
     return;
   }
   if constexpr (kFactored) {
+    // 16-bit storage: the lower blocks go to dom64 for k_domain_chol16
+    if (lane <= w) {
+      double* o = a.dom64 + ((size_t)g * kPacked + w * (w + 1) / 2 + lane) * 9;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) o[e] = acc[e];
+    }
+  }
+}
 
+// 16-bit storage, second pass: the Cholesky factor of one domain from its
+// lower FP64 blocks (dom64, written by k_domain_factor), then W = L^-1 and
+// the scaled tile store.  Thread t < 528 owns lower block (w, lane),
+// t = w(w+1)/2 + lane; only the lower triangle takes part, so two CTAs fit
+// on an SM and hide each other's step latency.  The steps talk through
+// shared memory only, so the thread layout is free.
+constexpr int kCholThreads = 544;  // 528 lower blocks in 17 warps
+template <typename TI>
+__global__ void __launch_bounds__(kCholThreads, 2) k_domain_chol16(FactorArgs a)
+{
+  __shared__ double dinv[kBank][9];      // L_qq^-1 (lower, row-major), kept for W below
+  __shared__ double panel[2][kBank][9];  // L_wq
+  __shared__ double wrow[2][kBank][9];   // W_ql
+  __shared__ float sscale[96];
+  __shared__ unsigned smax[96];
+  __shared__ int fail;
+  const int g = blockIdx.x;
+  const bool act = threadIdx.x < kPacked;
+  int w = -1, lane = -1;
+  if (act) {
+    const int t = threadIdx.x;
+    w = (int)((sqrtf(8.f * t + 1.f) - 1.f) * 0.5f);
+    while (w * (w + 1) / 2 > t) --w;
+    while ((w + 1) * (w + 2) / 2 <= t) ++w;
+    lane = t - w * (w + 1) / 2;
+  }
+  if (threadIdx.x == 0) fail = 0;
+  if (threadIdx.x < 96) smax[threadIdx.x] = 0u;
+  double acc[9];
+  if (act) {
+    const double* src = a.dom64 + ((size_t)g * kPacked + threadIdx.x) * 9;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = src[e];
+  } else {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+  }
+  __syncthreads();
   // ---- blocked Cholesky, right-looking over the 32 block columns: thread
   // (q,q) factors its 3x3 diagonal block and inverts the factor, the block
   // column below it is solved against that factor, then the trailing lower
   // blocks take the rank-3 update.  Lower blocks (w >= lane) hold L after.
-  // The step buffers reuse `stage` (assembly is over once every thread has
-  // passed the first barrier below).
-  __shared__ double dinv[kBank][9];          // L_qq^-1 (lower, row-major), kept for W below
-  double(*panel)[kBank][9] = reinterpret_cast<double(*)[kBank][9]>(&stage[0][0]);               // L_wq, x2
-  double(*wrow)[kBank][9] = reinterpret_cast<double(*)[kBank][9]>(&stage[0][0] + 2 * kBank * 9);  // W_ql, x2
   for (int q = 0; q < kBank; ++q) {
     const int b = q & 1;
     if (w == q && lane == q) {
@@ -406,7 +447,7 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
   }
   __syncthreads();
   // ---- column scales and factored store (lower blocks only)
-  if (w >= lane) {
+  if (act) {
 #pragma unroll
     for (int jj = 0; jj < 3; ++jj) {
       const float m = (float)fmax(fmax(fabs(xr[jj]), fabs(xr[3 + jj])), fabs(xr[6 + jj]));
@@ -424,6 +465,8 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
   if (threadIdx.x == 0 && fail) atomicAdd(a.failed, 1);
   // tile store: lower blocks, and zeros for the upper elements that fall in
   // a diagonal tile
+  if (!act) return;
+  TI* out = reinterpret_cast<TI*>(a.inv) + (size_t)g * kInvElems16;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -435,8 +478,10 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
         out[inv16_pos(row, col)] = from_d<TI>(xr[3 * i + jj] / (double)sscale[3 * lane + jj]);
       else if ((row >> 4) == (col >> 4))
         out[inv16_pos(row, col)] = from_d<TI>(0.0);
+      // the mirror upper block (lane, w): its elements inside a diagonal tile are zero
+      const int mr = 3 * lane + i, mc = 3 * w + jj;
+      if (w > lane && (mr >> 4) == (mc >> 4)) out[inv16_pos(mr, mc)] = from_d<TI>(0.0);
     }
-  }
 }
 
 // ------------------------------------------------------------------ apply --
@@ -1530,6 +1575,10 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out)
   fa.failed = h->failed.get() + 3;
   fa.assembled = assembled_out;
   fa.coarse64 = h->coarse64.get();
+  if (kB == 32 && storage != MASPCG_INV_FP32) {
+    h->dom64.resize((size_t)lv.domains * kPacked * 9);
+    fa.dom64 = h->dom64.get();
+  }
   const int grid = lv.domains;
 #define MAS_FACTOR(TI, ASM) k_domain_factor<TI, ASM, kB><<<grid, 32 * kB, 0, st>>>(fa, 0)
   if constexpr (kB == 16) {
@@ -1554,6 +1603,15 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out)
   }
 #undef MAS_FACTOR
   MLAUNCHED(h);
+  if constexpr (kB == 32) {
+    if (storage == MASPCG_INV_BF16) {
+      k_domain_chol16<__nv_bfloat16><<<grid, kCholThreads, 0, st>>>(fa);
+      MLAUNCHED(h);
+    } else if (storage == MASPCG_INV_FP16) {
+      k_domain_chol16<__half><<<grid, kCholThreads, 0, st>>>(fa);
+      MLAUNCHED(h);
+    }
+  }
   MCK(cudaGetLastError());
 }
 

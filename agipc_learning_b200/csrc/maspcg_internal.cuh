@@ -167,6 +167,7 @@ struct FactorArgs {
   int* failed;                   // count of domains with a pivot <= 0
   double* assembled;             // optional: packed FP64 domain matrices (reference layout)
   const double* coarse64;        // coarse-level domain matrices (32x32 blocks, row-major 3x3)
+  double* dom64;                 // 16-bit storage: lower FP64 blocks per domain (kPacked x 9, row-major)
 };
 
 }  // namespace maspcg
@@ -225,6 +226,7 @@ struct maspcg_handle {
   maspcg::DBuf<int> chain_count, chain_target;  // coarse-level dataflow counters (per coarse domain)
   maspcg::DBuf<double> chain_dot;               // per coarse domain: R.Z (r.z of the coarse levels)
   maspcg::DBuf<double> coarse64;
+  maspcg::DBuf<double> dom64;  // 16-bit storage: assembled lower blocks between the two factor passes
   maspcg::DBuf<double> abd_inv64;
   maspcg::DBuf<float> abd_inv32;
   maspcg::DBuf<double> diag_inv64;
