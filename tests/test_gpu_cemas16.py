@@ -102,10 +102,15 @@ def test_pcg_reference_precision_matches_oracle(systems, gate):
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-4
 
 
-@pytest.mark.parametrize("precision", ["fp32", "mixed"])
-def test_lower_precision_forms_reach_tolerance(systems, precision):
+@pytest.mark.parametrize("precision,sequential", [("fp32", False), ("mixed", False), ("mixed", True)])
+def test_lower_precision_forms_reach_tolerance(systems, precision, sequential):
+    # sequential: the coarse levels before the level-0 apply, which then adds
+    # the coarse correction itself (else they run beside it on the side stream)
+    from agipc_learning_b200 import _native as N
     s = systems["cube0"]
-    with MasPcg.from_system(s, preconditioner="cemas16", gate="euclid", tolerance=1e-6, precision=precision) as m:
+    flags = N.FLAG_SEQUENTIAL_COARSE if sequential else 0
+    with MasPcg.from_system(s, preconditioner="cemas16", gate="euclid", tolerance=1e-6, precision=precision,
+                            flags=flags) as m:
         x, res = m.solve(s.b)
     assert res["status_name"] == "converged"
     tol = 1e-6 if precision == "mixed" else 1e-4
@@ -143,4 +148,14 @@ def test_reference_call_sequence(bank):
         o.reorder(s.pairs)
         o.prepare_hessian(s.vals, s.rows, s.cols, None, 0)
     z_ref = o.precondition(s.b)
+    assert np.linalg.norm(z - z_ref) / np.linalg.norm(z_ref) <= 2e-4
+
+
+def test_apply_with_fp32_vectors(systems):
+    """The apply of the FP32-vector forms (r rounded to FP32 on entry, z
+    widened on exit) against the oracle's FP64-edged apply."""
+    s = systems["sorted"]
+    z_ref = _oracle(s).precondition(s.b)
+    with MasPcg.from_system(s, preconditioner="cemas16", precision="mixed") as m:
+        z = m.apply_preconditioner(s.b)
     assert np.linalg.norm(z - z_ref) / np.linalg.norm(z_ref) <= 2e-4
