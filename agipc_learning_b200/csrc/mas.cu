@@ -1827,7 +1827,10 @@ void mas16_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
 {
   const Mas16Args a = make_mas16_args(h);
   const LevelInfo& lv = h->lv;
-  const int g0 = std::max(1, ceil_div(h->c0, kTpb));
+  // Beside the coarse chain the level-0 apply leaves 16 SMs' worth of CTA
+  // slots free (its CTAs take all of an SM's registers, two per SM), so the
+  // chain's small launches start at once instead of after the apply drains.
+  const int g0 = std::max(1, std::min(ceil_div(h->c0, kTpb), 2 * std::max(h->sm_count - 16, 1)));
   auto coarse_levels = [&](cudaStream_t st) {
     for (int l = 0; l + 1 < lv.levelnum; ++l) {
       const int count = l == 0 ? h->c0 : lv.count[l];
