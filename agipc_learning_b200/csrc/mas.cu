@@ -1113,13 +1113,16 @@ __device__ __forceinline__ void domain_apply16(const float* __restrict__ inv, bo
   y[2] = y2;
 }
 
-__global__ void __launch_bounds__(kTpb, 2) k16_apply_coarse(Mas16Args a, PcgScalars* s)
+// All coarse domains (levels >= 1).  pair: the grid's R.Z (= r . P Z, the
+// coarse part of r.z) completes part 1 of the pair r.z.
+template <typename Tacc>
+__global__ void __launch_bounds__(kTpb, 2) k16_apply_coarse(Mas16Args a, Tacc* cpart, PcgScalars* s, int mode,
+                                                           int pair)
 {
   pdl_wait();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
+  if (s && s->status != MASPCG_SOLVE_RUNNING) return;  // uniform: nothing changes the status meanwhile
   const int d1 = a.lv.dom_begin[1];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if ((t & ~31) >= (a.lv.domains - d1) * 16) return;
   const int g = d1 + (t >> 4), lane = t & 15;
   const bool in = g < a.lv.domains;
   const size_t base = 3 * (size_t)(16 * g + lane - a.c0);
@@ -1130,10 +1133,24 @@ __global__ void __launch_bounds__(kTpb, 2) k16_apply_coarse(Mas16Args a, PcgScal
     x[2] = a.coarse_r[base + 2];
   }
   domain_apply16(a.inv + (size_t)(in ? g : 0) * kMas16InvElems, in, lane, x, y);
-  if (!in) return;
-  a.coarse_z[base] = y[0];
-  a.coarse_z[base + 1] = y[1];
-  a.coarse_z[base + 2] = y[2];
+  Tacc dot = 0;
+  if (in) {
+    a.coarse_z[base] = y[0];
+    a.coarse_z[base + 1] = y[1];
+    a.coarse_z[base + 2] = y[2];
+    dot = (Tacc)x[0] * (Tacc)y[0] + (Tacc)x[1] * (Tacc)y[1] + (Tacc)x[2] * (Tacc)y[2];
+  }
+  if (!pair || !s) return;
+  Tacc total = 0;
+  if (grid_finish<Tacc>(dot, cpart, blockIdx.x, gridDim.x, &s->tickets[kTicketCoarse], gridDim.x, total) &&
+      threadIdx.x == 0)
+    rz_part_done(s, 1, (double)total, mode);
+}
+
+// CTAs of k16_apply_coarse.
+inline int mas16_coarse_grid(const maspcg_handle* h)
+{
+  return std::max(1, ceil_div((long long)(h->lv.domains - h->lv.dom_begin[1]) * 16, kTpb));
 }
 
 // The coarse correction and r.z of one slot's z (y holds the level-0 result
@@ -1174,7 +1191,8 @@ __device__ __forceinline__ void rz_finish(Tacc dot, Tacc* partial, int part_base
 }
 
 // kProlong: add the coarse correction and sum r.z (the coarse levels ran
-// before); else z = the level-0 result only.
+// before).  Else z = the level-0 result (the next p update adds the coarse
+// correction), and r.z0 completes part 0 of the pair r.z.
 template <typename Tv, typename Tacc, bool kProlong>
 __global__ void __launch_bounds__(kTpb, 2) k16_apply_level0(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
                                                          int part_base, int total_parts, int mode, PcgScalars* s)
@@ -1207,34 +1225,24 @@ __global__ void __launch_bounds__(kTpb, 2) k16_apply_level0(Mas16Args a, const T
       dot += prolong16<Tv, Tacc>(a, vtx, rv, y, z + base);
     } else {
       const bool real = vtx >= 0;
-      z[base] = real ? (Tv)y[0] : Tv(0);
-      z[base + 1] = real ? (Tv)y[1] : Tv(0);
-      z[base + 2] = real ? (Tv)y[2] : Tv(0);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const Tv zv = real ? (Tv)y[q] : Tv(0);
+        z[base + q] = zv;
+        dot += (Tacc)rv[q] * (Tacc)zv;
+      }
     }
   }
   pdl_trigger();
-  if (kProlong) rz_finish(dot, partial, part_base, total_parts, mode, s);
-}
-
-// The prolongation after the join: z (the level-0 result) plus the coarse
-// correction, and r.z.
-template <typename Tv, typename Tacc>
-__global__ void __launch_bounds__(kTpb) k16_prolong(Mas16Args a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
-                                                    int part_base, int total_parts, int mode, PcgScalars* s)
-{
-  pdl_wait();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  Tacc dot = 0;
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < a.c0; slot += gridDim.x * blockDim.x) {
-    const int vtx = a.pmr[slot];
-    if (vtx < 0) continue;
-    const size_t base = 3 * (size_t)(a.fem_off + slot);
-    const Tv rv[3] = {r[base], r[base + 1], r[base + 2]};
-    float y[3] = {(float)z[base], (float)z[base + 1], (float)z[base + 2]};
-    dot += prolong16<Tv, Tacc>(a, vtx, rv, y, z + base);
+  if (kProlong) {
+    rz_finish(dot, partial, part_base, total_parts, mode, s);
+  } else if (partial) {
+    Tacc total = 0;
+    if (grid_finish<Tacc>(dot, partial, part_base + blockIdx.x, total_parts, &s->tickets[kTicketRz], gridDim.x,
+                          total) &&
+        threadIdx.x == 0)
+      rz_part_done(s, 0, (double)total, mode);
   }
-  pdl_trigger();
-  rz_finish(dot, partial, part_base, total_parts, mode, s);
 }
 
 Mas16Args make_mas16_args(maspcg_handle* h)
@@ -1492,6 +1500,7 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
   h->coarse_r.resize(coarse > 0 ? coarse : 3);
   h->coarse_z.resize(coarse > 0 ? coarse : 3);
   if (h->bank == 16) {
+    h->chain_dot.resize((size_t)mas16_coarse_grid(h));  // k16_apply_coarse's R.Z partials
     MCK(cudaMemsetAsync(h->coarse_r.get(), 0, h->coarse_r.bytes(), st));
     MCK(cudaMemsetAsync(h->coarse_z.get(), 0, h->coarse_z.bytes(), st));
     int f = 0;
@@ -1814,43 +1823,47 @@ template void mas_apply<double, double>(maspcg_handle*, const double*, double*, 
 int mas_level0_grid(maspcg_handle* h) { return level0_grid(h, h->apply_variant); }
 
 // CTAs of the kernel that completes r.z (level-0 apply or prolongation).
-int mas16_grid(maspcg_handle* h) { return std::max(1, std::min(ceil_div(h->c0, kTpb), 8 * h->sm_count)); }
+// CTAs of the level-0 apply, which completes r.z (or part 0 of it).  When
+// the coarse levels run beside it (inside the solve, outside the reference
+// precision) it leaves 16 SMs' worth of CTA slots free: its CTAs take every
+// register of an SM, two per SM, so the chain's small launches start at once
+// instead of after the apply drains.
+int mas16_grid(maspcg_handle* h)
+{
+  const int sms = (h->overlap_coarse && h->lv.levelnum > 1) ? std::max(h->sm_count - 16, 1) : 4 * h->sm_count;
+  return std::max(1, std::min(ceil_div(h->c0, kTpb), 2 * sms));
+}
 
 // CEMAS16 apply.  Sequential: the restriction level by level, the coarse
 // domain applies, then the level-0 apply with the prolongation and r.z.
-// overlap: the restriction and the coarse applies run on the side stream
-// beside the level-0 apply, and the prolongation with r.z follows the join.
-// The last block of the final kernel completes r.z over [0, total_parts).
+// overlap (with s): the restriction and the coarse applies on the side
+// stream beside the level-0 apply; z leaves the coarse correction to the
+// next p update (as the MAS32 apply does) and r.z is completed from a pair
+// of parts, r.z0 over the fine rows and R.Z over the coarse domains.
 template <typename Tv, typename Tacc>
 void mas16_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                  int grid, PcgScalars* s, bool overlap)
 {
   const Mas16Args a = make_mas16_args(h);
   const LevelInfo& lv = h->lv;
-  // Beside the coarse chain the level-0 apply leaves 16 SMs' worth of CTA
-  // slots free (its CTAs take all of an SM's registers, two per SM), so the
-  // chain's small launches start at once instead of after the apply drains.
-  const int g0 = std::max(1, std::min(ceil_div(h->c0, kTpb), 2 * std::max(h->sm_count - 16, 1)));
+  const bool pair = overlap && s && lv.levelnum > 1;
   auto coarse_levels = [&](cudaStream_t st) {
     for (int l = 0; l + 1 < lv.levelnum; ++l) {
       const int count = l == 0 ? h->c0 : lv.count[l];
       launch_pdl_on(h, st, k16_restrict<Tv>, dim3(std::max(1, ceil_div((count + 15) & ~15, kTpb))), dim3(kTpb), 0,
                     a, r, l, s);
     }
-    const int coarse = lv.domains - lv.dom_begin[1];
-    launch_pdl_on(h, st, k16_apply_coarse, dim3(std::max(1, ceil_div((long long)coarse * 16, kTpb))), dim3(kTpb), 0,
-                  a, s);
+    launch_pdl_on(h, st, k16_apply_coarse<Tacc>, dim3(mas16_coarse_grid(h)), dim3(kTpb), 0, a,
+                  reinterpret_cast<Tacc*>(h->chain_dot.get()), s, mode, pair ? 1 : 0);
   };
-  if (lv.levelnum > 1 && overlap) {
+  if (pair) {
     MCK(cudaEventRecord(h->ev_fork, h->stream));
     MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
     coarse_levels(h->side_stream);
     MCK(cudaEventRecord(h->ev_join, h->side_stream));
-    launch_pdl(h, k16_apply_level0<Tv, Tacc, false>, dim3(g0), dim3(kTpb), 0, a, r, z, partial, part_base,
+    launch_pdl(h, k16_apply_level0<Tv, Tacc, false>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base,
                total_parts, mode, s);
     MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
-    launch_pdl(h, k16_prolong<Tv, Tacc>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base, total_parts, mode,
-               s);
   } else {
     if (lv.levelnum > 1) coarse_levels(h->stream);
     launch_pdl(h, k16_apply_level0<Tv, Tacc, true>, dim3(grid), dim3(kTpb), 0, a, r, z, partial, part_base,

@@ -591,7 +591,7 @@ struct Engine {
     gspmv = std::max(1, std::min(ceil_div(h->nb_int, kTpb / 16), 4 * h->sm_count));
     grows = std::max(1, std::min(ceil_div(h->nb_int, kTpb), 8 * h->sm_count));
     gl0 = mas ? mas_level0_grid(h) : (mas16 ? mas16_grid(h) : 0);
-    ovl = mas && h->lv.levelnum > 1 && h->overlap_coarse;
+    ovl = (mas || mas16) && h->lv.levelnum > 1 && h->overlap_coarse;
     const bool other = !(mas || mas16) || h->abd_bodies > 0 || h->fem_off > 0 || h->nb_int > h->fem_off + h->c0;
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;
     parts_other = gother;
@@ -624,8 +624,7 @@ struct Engine {
     }
     if (mas) mas_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s, overlap);
     if (mas16)
-      mas16_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s,
-                            h->overlap_coarse);
+      mas16_apply<Tv, Tacc>(h, r, z, s ? partial_rz() : nullptr, parts_other, parts_total, mode, gl0, s, overlap);
     MCK(cudaGetLastError());
   }
 
