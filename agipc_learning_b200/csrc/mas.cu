@@ -1,4 +1,6 @@
-// mas.cu -- MAS32 domain matrices, inverses and the preconditioner apply.
+// mas.cu -- MAS domain matrices, inverses and the preconditioner apply:
+// TraditionalMAS32 (32-slot banks, 96x96 domains) and, where marked, CEMAS16
+// (16-slot banks, 48x48 domains, MASPreconditioner.cu).
 //
 // Build (once per Newton step, after the hierarchy):
 //   * member lists: for every coarse level a stable radix sort of the fine
@@ -11,15 +13,19 @@
 //     prepare_hessian_bcoo_sum_kernel (TraditionalMAS32Preconditioner.cu:
 //     2234-2464) without atomics and in a fixed order;
 //   * the 96x96 FP64 matrix stays in registers (thread (a,b) holds block
-//     (a,b)); zero diagonals become 1 (expand_symmetric_mas32 :1062-1096) and
-//     it is inverted in place by Gauss-Jordan elimination without pivoting,
-//     as __inverse6_P96x96 (:1099-1146) does, with the pivot (= the squared
-//     Cholesky diagonal) checked > 0;
-//   * the inverse is stored as 17 wrapped diagonals x 9 elements x 32 lanes,
-//     in FP32 or scaled BF16/FP16.
-// Apply (every PCG iteration): restriction by in-warp segmented sums, one warp
-// per domain for the symmetric 96x96 matvec (each stored block is used for
-// both triangles through a shuffle), prolongation by the goingNext chain.
+//     (a,b)); zero diagonals become 1 (expand_symmetric_mas32 :1062-1096);
+//     FP32 storage inverts it in place by Gauss-Jordan elimination without
+//     pivoting, as __inverse6_P96x96 (:1099-1146) does, with the pivot (=
+//     the squared Cholesky diagonal) checked > 0, and stores 17 wrapped
+//     diagonals x 9 elements x 32 lanes; 16-bit storage writes the lower
+//     blocks out and k_domain_chol16 factors them (scaled BF16/FP16 tiles);
+//   * CEMAS16: the same with 16-slot banks (48x48, FP32, 9 wrapped
+//     diagonals), with its assembly and store rules.
+// Apply (every PCG iteration): MAS32 runs the coarse levels as one dataflow
+// kernel beside a tensor-core level-0 apply of the 16-bit records (or a warp
+// per domain on FP32 records, each stored block used for both triangles
+// through a shuffle); CEMAS16 runs half a warp per domain (see the CEMAS16
+// apply kernels).
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
