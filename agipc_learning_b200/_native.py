@@ -54,7 +54,8 @@ EXPORTS = (
     "maspcg_get_hierarchy", "maspcg_get_bcsr", "maspcg_get_domain_inverses", "maspcg_get_domain_matrices",
     "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient", "maspcg_convert_bcoo",
     "maspcg_partition_contact_triplets", "maspcg_fem_snk1_gradient_hessian", "maspcg_galerkin_coarse_matrix",
-    "maspcg_galerkin_restrict", "maspcg_galerkin_prolong",
+    "maspcg_galerkin_restrict", "maspcg_galerkin_prolong", "maspcg_adjust_contact_triplets",
+    "maspcg_zero_boundary_triplets", "maspcg_spmv_working",
 )
 
 RESIDUAL_MAX_VECTORS = 8
@@ -79,7 +80,7 @@ class Result(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("status", ctypes.c_int), ("refinements", ctypes.c_int),
                 ("launches", ctypes.c_int), ("rz0", ctypes.c_double), ("rz_final", ctypes.c_double),
                 ("rel_res_recursive", ctypes.c_double), ("rel_res_true", ctypes.c_double),
-                ("solve_ms", ctypes.c_double)]
+                ("solve_ms", ctypes.c_double), ("fp64_gate_met", ctypes.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -137,6 +138,9 @@ def load():
         "maspcg_galerkin_coarse_matrix": (I, [H, ctypes.POINTER(GalerkinMap), P, P, P, I, P, P, P, I, P]),
         "maspcg_galerkin_restrict": (I, [H, ctypes.POINTER(GalerkinMap), P, P]),
         "maspcg_galerkin_prolong": (I, [H, ctypes.POINTER(GalerkinMap), P, P]),
+        "maspcg_adjust_contact_triplets": (I, [H, I, P, P, P, P, I, I]),
+        "maspcg_zero_boundary_triplets": (I, [H, I, P, P, P, P, I, I]),
+        "maspcg_spmv_working": (I, [H, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

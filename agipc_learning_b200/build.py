@@ -44,18 +44,38 @@ def build_synth(force: bool = False) -> str:
 
 
 def build_cuda(force: bool = False, verbose_ptxas: bool = False, extra=()) -> str:
+    """Compile every ``csrc/*.cu`` to an object under ``_build/`` (in parallel;
+    a source is recompiled when it or any shared header changed), then link
+    ``libmaspcg.so``.  No file shares device symbols with another, so the
+    objects are whole-program device code and need no device link step."""
+    from concurrent.futures import ThreadPoolExecutor
+
     out = os.path.join(HERE, "libmaspcg.so")
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    deps = srcs + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(INCLUDE, "*.h")))
-    if not (force or _newer(out, deps)):
-        return out
-    cmd = [_nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC,
-           "-o", out, *srcs, "-lcudart"]
+    headers = sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(INCLUDE, "*.h")))
+    objdir = os.path.join(ROOT, "_build", "maspcg")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
+             "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC, *extra]
     if verbose_ptxas:
-        cmd.insert(1, "-Xptxas=-v")
-    cmd.extend(extra)
-    subprocess.run(cmd, check=True)
+        flags.insert(0, "-Xptxas=-v")
+    objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or verbose_ptxas or extra or _newer(o, [s, *headers])]
+    if not todo and not _newer(out, objs):
+        return out
+
+    def compile_one(so):
+        src, obj = so
+        return subprocess.run([_nvcc(), *flags, "-c", "-o", obj, src], capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, todo))
+    for (src, _), r in zip(todo, results):
+        if verbose_ptxas or r.returncode:
+            print(r.stdout + r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, f"nvcc {src}")
+    subprocess.run([_nvcc(), *NVCC_ARCH, "-shared", "-o", out, *objs, "-lcudart"], check=True)
     return out
 
 

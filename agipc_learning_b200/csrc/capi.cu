@@ -16,6 +16,14 @@ namespace {
 
 thread_local std::string g_create_error;
 
+// The device of the handle the current entry point serves (set by guard), so
+// a device pointer can be checked against it.
+thread_local int g_call_device = -1;
+
+// True for memory a kernel on the handle's device can read: managed memory,
+// or device memory of that device.  Device memory of another GPU is refused
+// (MASPCG_ERR_INVALID_ARGUMENT): without peer access a kernel given it would
+// fault.
 bool is_device_ptr(const void* p)
 {
   if (!p) return false;
@@ -25,7 +33,11 @@ bool is_device_ptr(const void* p)
     cudaGetLastError();
     return false;
   }
-  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+  if (at.type == cudaMemoryTypeManaged) return true;
+  if (at.type != cudaMemoryTypeDevice) return false;
+  MREQ(g_call_device < 0 || at.device == g_call_device, MASPCG_ERR_INVALID_ARGUMENT,
+       "device pointer on GPU " + std::to_string(at.device) + ", handle on GPU " + std::to_string(g_call_device));
+  return true;
 }
 
 // A device view of a caller array: the caller's pointer when it is device
@@ -56,13 +68,34 @@ std::vector<T> host_copy(maspcg_handle* h, const T* user, size_t count)
   return v;
 }
 
+// Runs one entry point on the handle's device and puts the caller's current
+// device back afterwards, on every path: the reference runs on the caller's
+// device and never changes it.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int device)
+  {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    if (prev != device) MCK(cudaSetDevice(device));
+    g_call_device = device;
+  }
+  ~DeviceScope()
+  {
+    g_call_device = -1;
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 template <typename F>
 maspcg_status guard(maspcg_handle* h, F&& f)
 {
   if (!h) return MASPCG_ERR_NULL_HANDLE;
   try {
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess && dev != h->device) MCK(cudaSetDevice(h->device));
+    DeviceScope scope(h->device);
     f();
     h->last_error.clear();
     return MASPCG_OK;
@@ -177,6 +210,32 @@ maspcg::GalerkinMap galerkin_map(maspcg_handle* h, const maspcg_galerkin_map* ma
     m.rest = device_in(h, g.rest_positions, 3 * (size_t)g.fem_nodes, h->gal_rest);
   }
   return m;
+}
+}  // namespace
+
+namespace {
+// In-place triplet fix-up shared by the two entry points below: stage host
+// arrays, run the kernel, copy them back.
+maspcg_status triplet_fixup(maspcg_handle* h, int n, int* rows, int* cols, double* values9, const int* bd_type,
+                            int n_vertices, int offset, bool zero_boundary_only)
+{
+  return guard(h, [&] {
+    MREQ(n >= 0 && n_vertices >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative count");
+    if (n == 0) return;
+    MREQ(rows && cols && values9 && bd_type, MASPCG_ERR_INVALID_ARGUMENT, "null array argument");
+    MREQ(n_vertices > 0, MASPCG_ERR_INVALID_ARGUMENT, "no vertices");
+    const bool dev_rows = is_device_ptr(rows), dev_cols = is_device_ptr(cols), dev_vals = is_device_ptr(values9);
+    int* r = dev_rows ? rows : const_cast<int*>(device_in(h, (const int*)rows, (size_t)n, h->asm_rows));
+    int* c = dev_cols ? cols : const_cast<int*>(device_in(h, (const int*)cols, (size_t)n, h->asm_cols));
+    double* v = dev_vals ? values9 : const_cast<double*>(device_in(h, (const double*)values9, 9 * (size_t)n, h->asm_vals));
+    const int* bd = device_in(h, bd_type, (size_t)n_vertices, h->asm_start);
+    const bool ok = maspcg::adjust_contacts(h, n, r, c, v, bd, n_vertices, offset, zero_boundary_only);
+    if (!zero_boundary_only && !dev_rows) copy_back(h, rows, (const int*)r, (size_t)n);
+    if (!zero_boundary_only && !dev_cols) copy_back(h, cols, (const int*)c, (size_t)n);
+    if (!dev_vals) copy_back(h, values9, (const double*)v, 9 * (size_t)n);
+    MCK(cudaStreamSynchronize(h->stream));
+    MREQ(ok, MASPCG_ERR_INVALID_ARGUMENT, "a triplet names a vertex outside [0, n_vertices); it was left unchanged");
+  });
 }
 }  // namespace
 
@@ -555,6 +614,26 @@ MASPCG_API maspcg_status maspcg_spmv(maspcg_handle* h, double a, const double* x
   });
 }
 
+MASPCG_API maspcg_status maspcg_spmv_working(maspcg_handle* h, const double* x, double* y)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    MREQ(x && y, MASPCG_ERR_INVALID_ARGUMENT, "null vector");
+    const size_t n = 3 * (size_t)h->nb;
+    const double* xd = device_in(h, x, n, h->io_a);
+    maspcg::permute_in(h, xd, h->io_b.get());
+    maspcg::spmv_working(h, h->io_b.get(), h->r64.get());
+    if (is_device_ptr(y)) {
+      maspcg::permute_out(h, h->r64.get(), y);
+    } else {
+      maspcg::permute_out(h, h->r64.get(), h->io_a.get());
+      MCK(cudaMemcpyAsync(y, h->io_a.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    MCK(cudaStreamSynchronize(h->stream));
+    h->graph_dirty = true;
+  });
+}
+
 MASPCG_API maspcg_status maspcg_get_info(maspcg_handle* h, maspcg_info* info)
 {
   return guard(h, [&] {
@@ -729,6 +808,22 @@ MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, con
     MCK(cudaStreamSynchronize(h->stream));
     for (int q = 0; q < 4; ++q) counts[q] = k[q];
   });
+}
+
+
+MASPCG_API maspcg_status maspcg_adjust_contact_triplets(maspcg_handle* h, int n, int* rows, int* cols,
+                                                        double* values9_colmajor, const int* bd_type, int n_vertices,
+                                                        int fem_offset)
+{
+  return triplet_fixup(h, n, rows, cols, values9_colmajor, bd_type, n_vertices, fem_offset, false);
+}
+
+MASPCG_API maspcg_status maspcg_zero_boundary_triplets(maspcg_handle* h, int n, const int* rows, const int* cols,
+                                                       double* values9_colmajor, const int* bd_type, int n_vertices,
+                                                       int index_offset)
+{
+  return triplet_fixup(h, n, const_cast<int*>(rows), const_cast<int*>(cols), values9_colmajor, bd_type, n_vertices,
+                       index_offset, true);
 }
 
 MASPCG_API maspcg_status maspcg_fem_snk1_gradient_hessian(maspcg_handle* h, int n_tets, const unsigned* tets,

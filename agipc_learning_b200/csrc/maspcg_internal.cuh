@@ -292,6 +292,7 @@ void decode_inverses(maspcg_handle* h, float* out_host);
 // pcg.cu
 double time_stage(maspcg_handle* h, int stage, int repeats);
 void solve(maspcg_handle* h, const double* b_dev, double* x_dev, maspcg_result* res);
+void spmv_working(maspcg_handle* h, const double* x_int, double* y_int);  // internal order, FP64 in/out
 
 // adjoint.cu (device pointers, caller's row order)
 void bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n, const double* lam, const double* x,
@@ -303,6 +304,14 @@ int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const doubl
 void partition_contacts(maspcg_handle* h, const int* rows, const int* cols, const double* vals,
                         const unsigned long long* types, int n, int* rows_out, int* cols_out, double* vals_out,
                         int counts[4]);
+
+// contact.cu (device pointers, in place).  zero_boundary_only: clear the
+// triplets touching a boundary vertex (indices minus `offset`); else the
+// contact adjustment (lower copies moved up and cleared, boundary pairs
+// cleared, indices plus `offset`).  Returns false when an index fell outside
+// [0, n_vertices) (that triplet is left as it was).
+bool adjust_contacts(maspcg_handle* h, int n, int* rows, int* cols, double* values9, const int* bd_type,
+                     int n_vertices, int offset, bool zero_boundary_only);
 
 // galerkin.cu (device pointers).  The AGIPC mapping: fine blocks [0, prefix)
 // pass through; FEM node k (block prefix + k) maps to coarse node

@@ -561,6 +561,14 @@ __global__ void k_from_f64(const double* __restrict__ x, Tv* y, int n)
   if (i < n) y[i] = (Tv)x[i];
 }
 
+// FP64 vector (3 per block row) into the padded search-direction layout.
+template <typename Tv>
+__global__ void k_to_p4(const double* __restrict__ x, Tv* p4, int nrows)
+{
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nrows) st_p4(p4, v, (Tv)x[3 * (size_t)v], (Tv)x[3 * (size_t)v + 1], (Tv)x[3 * (size_t)v + 2]);
+}
+
 // Reads `n` 16-byte words through L2 (evicting what was cached) without
 // dirtying any line; writes only if the data is nonzero (never, in use).
 __global__ void __launch_bounds__(kTpb) k_l2_evict(const uint4* __restrict__ p, size_t n, unsigned* sink)
@@ -699,6 +707,30 @@ struct Engine {
     launch_pdl(h, k_true_residual<16>, dim3(gspmv), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(), h->x64.get(),
                                                h->b64.get(), reinterpret_cast<float*>(h->vr.get()), h->nb_int,
                                                h->partial.get(), s);
+  }
+
+  // y = A x through the iteration's own SpMV kernel: x (internal order, FP64)
+  // rounded into the padded search-direction layout, the kernel run once,
+  // its working-precision output widened into y.
+  void spmv_working(const double* x_int, double* y_int)
+  {
+    cudaStream_t st = h->stream;
+    PcgScalars* s = h->scal.get();
+    PcgScalars init{};
+    init.status = MASPCG_SOLVE_RUNNING;
+    init.k = 2;
+    init.rz = 1.0;
+    init.max_iter = 1 << 30;
+    MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_to_p4<Tv><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, V(h->vp4), h->nb_int);
+    MLAUNCHED(h);
+    const bool pdl = h->use_pdl;
+    h->use_pdl = false;
+    spmv(s);
+    h->use_pdl = pdl;
+    k_to_f64<Tv><<<ceil_div(n, kTpb), kTpb, 0, st>>>(V(h->vap), y_int, n);
+    MLAUNCHED(h);
+    MCK(cudaGetLastError());
   }
 
   // One graph = `batch` iterations.
@@ -878,6 +910,7 @@ struct Engine {
       res->rel_res_recursive = hs.bb > 0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
       res->rel_res_true = hs.bb > 0 ? std::sqrt(hs.rr_true / hs.bb) : std::sqrt(hs.rr_true);
       res->solve_ms = ms;
+      res->fp64_gate_met = (std::isfinite(res->rel_res_true) && res->rel_res_true <= h->cfg.tolerance) ? 1 : 0;
     }
   }
 };
@@ -932,6 +965,15 @@ void solve(maspcg_handle* h, const double* b_int, double* x_int, maspcg_result* 
   }
   MCK(cudaMemcpyAsync(x_int, h->x64.get(), sizeof(double) * 3 * (size_t)h->nb_int, cudaMemcpyDeviceToDevice,
                       h->stream));
+}
+
+void spmv_working(maspcg_handle* h, const double* x_int, double* y_int)
+{
+  switch (h->cfg.precision) {
+    case MASPCG_PREC_REFERENCE: Engine<double, double, double>(h).spmv_working(x_int, y_int); break;
+    case MASPCG_PREC_FP32: Engine<float, float, float>(h).spmv_working(x_int, y_int); break;
+    default: Engine<float, float, double>(h).spmv_working(x_int, y_int); break;
+  }
 }
 
 // z = M^-1 r on internal-order FP64 vectors (standalone apply).

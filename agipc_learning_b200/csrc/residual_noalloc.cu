@@ -16,8 +16,9 @@
 //     [8208]              low 32 bits: completion ticket
 //
 // The ticket must be zero when a launch starts.  Static device storage starts
-// at zero, set-up zeroes it once more, and the last block of every launch puts
-// it back to zero.  The partial sums and results need no initial value.
+// at zero, set-up (the first call that sees the array at a new device address)
+// zeroes it once more, and the last block of every launch puts it back to
+// zero.  The partial sums and results need no initial value.
 //
 // One scratch per device and process: two launches that overlapped on one
 // device would race on it.  The host entry point therefore holds a per-device
@@ -145,15 +146,21 @@ void residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const 
 {
   MREQ(h->device >= 0 && h->device < kMaxDevices, MASPCG_ERR_UNSUPPORTED, "device ordinal beyond the scratch table");
   std::lock_guard<std::mutex> lock(g_res_lock[h->device]);
-  double*& scratch = g_res_scratch[h->device];
-  if (!scratch) {
-    // set-up, once per device, with h->device current
-    void* p = nullptr;
-    MCK(cudaGetSymbolAddress(&p, g_residual_scratch));
+  // The array's device address is looked up on every call (a lookup, not an
+  // allocation): a context created again on this device (after
+  // cudaDeviceReset, or a handle on a non-primary context) loads the module
+  // again at another address, and a cached address would then be stale.
+  void* p = nullptr;
+  MCK(cudaGetSymbolAddress(&p, g_residual_scratch));
+  double*& seen = g_res_scratch[h->device];
+  if (seen != static_cast<double*>(p)) {
+    // set-up for this module instance, with h->device current: a freshly
+    // loaded array is zero already; the ticket is cleared once more
     MCK(cudaMemsetAsync(static_cast<double*>(p) + kResTicketOffset, 0, sizeof(double), h->stream));
     MCK(cudaStreamSynchronize(h->stream));
-    scratch = static_cast<double*>(p);
+    seen = static_cast<double*>(p);
   }
+  double* scratch = seen;
   const int grid = std::max(1, std::min(std::min(2 * h->sm_count, kResMaxBlocks), ceil_div(h->nb_int, kResGroups)));
   k_residual_noalloc<<<grid, kResTpb, 0, h->stream>>>(h->rowptr.get(), h->colidx.get(), h->val64.get(),
                                                       h->row_of_int.get(), h->nb_int, x, b, 3LL * h->nb, count,

@@ -172,6 +172,33 @@ class MasPcg:
         self._ck(self.lib.maspcg_spmv(self.h, float(a), xa.ptr, float(b), ya.ptr))
         return y
 
+    def spmv_working(self, x, y=None):
+        """y = A x as the PCG iteration's own SpMV kernel forms it, in the
+        working precision (maspcg_spmv_working)."""
+        xa = _Arg(x, np.float64)
+        y, ya = self._out(y, 3 * self.nb)
+        self._ck(self.lib.maspcg_spmv_working(self.h, xa.ptr, ya.ptr))
+        return y
+
+    def adjust_contact_triplets(self, rows, cols, values9, bd_type, fem_offset):
+        """Contact-pair dedup in place (maspcg_adjust_contact_triplets;
+        adjust_fem_fem_contact_indices_kernel).  numpy arrays are adjusted in
+        place and returned; CUDA tensors likewise."""
+        r, c, v = _Arg(rows, np.int32, True), _Arg(cols, np.int32, True), _Arg(values9, np.float64, True)
+        bd = _Arg(bd_type, np.int32)
+        self._ck(self.lib.maspcg_adjust_contact_triplets(self.h, int(len(rows)), r.ptr, c.ptr, v.ptr, bd.ptr,
+                                                         int(len(bd_type)), int(fem_offset)))
+        return rows, cols, values9
+
+    def zero_boundary_triplets(self, rows, cols, values9, bd_type, index_offset):
+        """Boundary blocks cleared in place (maspcg_zero_boundary_triplets;
+        zero_fem_boundary_hessian_kernel)."""
+        r, c, v = _Arg(rows, np.int32), _Arg(cols, np.int32), _Arg(values9, np.float64, True)
+        bd = _Arg(bd_type, np.int32)
+        self._ck(self.lib.maspcg_zero_boundary_triplets(self.h, int(len(rows)), r.ptr, c.ptr, v.ptr, bd.ptr,
+                                                        int(len(bd_type)), int(index_offset)))
+        return values9
+
     def _outs(self, like, n):
         """rows, cols (int32) and values (n x 9 float64) outputs on the device of `like`."""
         if _is_torch(like) and like.is_cuda:

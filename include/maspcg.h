@@ -106,7 +106,7 @@ typedef enum {
 
 typedef struct {
   int iterations;           /* PCGSolver::pcg return value semantics */
-  int status;               /* maspcg_solve_status */
+  int status;               /* maspcg_solve_status: which gate stopped the loop (see below) */
   int refinements;          /* FP64 true-residual replacements (MIXED) */
   int launches;             /* CUDA-graph launches */
   double rz0;               /* r0^T z0 */
@@ -114,6 +114,14 @@ typedef struct {
   double rel_res_recursive; /* ||r_k|| / ||b|| of the recursive residual */
   double rel_res_true;      /* ||b - A x|| / ||b|| in FP64 with the FP64 input matrix */
   double solve_ms;          /* device time of maspcg_solve (events) */
+  /* 1 when rel_res_true <= tolerance: the returned x meets the Euclidean
+   * tolerance checked in FP64 against the FP64 input matrix.  MASPCG_SOLVE_
+   * CONVERGED alone says only that the configured gate was met by the loop's
+   * own quantities (the recursive residual or r^T z), which in FP32 can stop
+   * far above the tolerance; a Newton loop that needs the FP64 guarantee
+   * reads this field (MIXED stops on the FP64 residual, so there the two
+   * agree). */
+  int fp64_gate_met;
 } maspcg_result;
 
 typedef enum {
@@ -170,9 +178,16 @@ MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int co
 MASPCG_API maspcg_status maspcg_set_contacts(maspcg_handle* h, const int* pairs4, int n_pairs);
 
 /* The assembled system: GIPCTripletMatrix after Converter::convert
- * (global_matrix.h:18-203, converter.cu:137-284).  Upper BCOO (row <= col; a
- * lower entry is taken as its transposed upper block), any order; duplicate
- * (row,col) blocks are summed.
+ * (global_matrix.h:18-203, converter.cu:137-284).  Upper BCOO in any order;
+ * duplicate (row,col) blocks are summed, as the merge sums them.  Every stored
+ * block (r, c), r != c, stands for A_rc and its mirror A_cr = A_rc^T, as in the
+ * reference's symmetric SpMV (spmv.cu:28-53), which also applies to a block
+ * stored below the diagonal.  The caller passes the triplets the reference
+ * merges, so FEM-FEM contact triplets must already have gone through
+ * maspcg_adjust_contact_triplets (or the reference's own adjust kernel):
+ * before it, a barrier's coupling appears as both (a, b) and (b, a) and would
+ * be counted twice, exactly as the reference would count it without that
+ * step.
  *   block_rows         total block rows of the system
  *   fem_offset_blocks  first block row of the FEM vertices (MAS range)
  *   abd_body_count     affine bodies occupying block rows [0, 4*abd_body_count) */
@@ -201,6 +216,15 @@ MASPCG_API maspcg_status maspcg_apply_preconditioner(maspcg_handle* h, const dou
 MASPCG_API maspcg_status maspcg_spmv(maspcg_handle* h, double a, const double* x, double b, double* y);
 
 /* ---- introspection (parity tests, diagnostics) ---- */
+
+/* y = A x formed by the PCG iteration's own SpMV kernel (no counterpart in
+ * the reference: it exposes the product the solve computes, for parity
+ * checks against the FP64 product of maspcg_spmv).  x is rounded to the
+ * working precision: FP32 in MASPCG_PREC_FP32 and MIXED, where the kernel
+ * reads the FP32 matrix tiles and sums in FP32 (the affine-body rows from the
+ * FP64 matrix in FP64); FP64 in MASPCG_PREC_REFERENCE.  y is that output
+ * widened to FP64.  x, y: 3*block_rows doubles, host or device pointers. */
+MASPCG_API maspcg_status maspcg_spmv_working(maspcg_handle* h, const double* x, double* y);
 
 typedef struct {
   int levelnum;          /* computeNumLevels */
@@ -286,6 +310,32 @@ MASPCG_API maspcg_status maspcg_partition_contact_triplets(maspcg_handle* h, con
                                                            int n, double* values9_out, int* rows_out,
                                                            int* cols_out, int counts[4]);
 
+/* Contact-pair dedup of the FEM-FEM contact triplets, in place:
+ * adjust_fem_fem_contact_indices_kernel (StiffGIPC/GIPC.cu:10130-10160).  A
+ * barrier Hessian emits the full block pattern of its pair, so every coupling
+ * appears as (a, b) and as (b, a).  For triplet i, (r, c) = (rows[i],
+ * cols[i]) in FEM vertex numbering:
+ *   r <= c: rows[i] = r + fem_offset, cols[i] = c + fem_offset; the value is
+ *           cleared (nine +0.0) when bd_type[r] or bd_type[c] is nonzero;
+ *   r >  c: rows[i] = c + fem_offset, cols[i] = r + fem_offset and the value
+ *           is cleared: its upper twin carries the block.
+ * bd_type holds n_vertices ints (TetMesh.BoundaryType).  fem_offset is the
+ * reference's fem_global_hessian_index_offset (4 * ABD bodies - ABD points).
+ * A triplet naming a vertex outside [0, n_vertices) is left unchanged and the
+ * call returns MASPCG_ERR_INVALID_ARGUMENT (the reference does not check).
+ * Host or device pointers. */
+MASPCG_API maspcg_status maspcg_adjust_contact_triplets(maspcg_handle* h, int n, int* rows, int* cols,
+                                                        double* values9_colmajor, const int* bd_type, int n_vertices,
+                                                        int fem_offset);
+
+/* zero_fem_boundary_hessian_kernel (StiffGIPC/GIPC.cu:10162-10181), in
+ * place: the value of triplet i is cleared when bd_type[rows[i] -
+ * index_offset] or bd_type[cols[i] - index_offset] is nonzero; indices are
+ * not changed.  Range rule and pointers as maspcg_adjust_contact_triplets. */
+MASPCG_API maspcg_status maspcg_zero_boundary_triplets(maspcg_handle* h, int n, const int* rows, const int* cols,
+                                                       double* values9_colmajor, const int* bd_type, int n_vertices,
+                                                       int index_offset);
+
 /* The FEM part of A: per-tet gradient and PSD-projected Hessian of the stable
  * Neo-Hookean energy, _calculate_fem_gradient_hessian
  * (StiffGIPC/femEnergy.cu:1720-1856, SNK1 branch; projection
@@ -370,8 +420,10 @@ MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows,
  *
  * The call allocates no memory: its scratch (per-block partial sums, results
  * and a completion ticket) is one fixed 65,696-byte device array per device
- * inside the library, its address looked up once per device.  That set-up
- * runs on the first call for a device: make that first call before any stream
+ * inside the library.  Its device address is looked up on every call; the
+ * first call for a device (and the first after that device's context was
+ * created again) also clears the array's completion ticket with a small
+ * memset and a stream synchronisation: make that first call before any stream
  * capture is active.  Calls for one device are serialised by a lock held until
  * the call's stream has finished; the call synchronises the handle's stream
  * before it returns. */

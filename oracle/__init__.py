@@ -73,6 +73,9 @@ def lib(bank=32):
             "orc_abd_inverse": (I, [I, I, P, P, P, P]),
             "orc_pcg": (I, [ctypes.POINTER(_PcgOpts), P, P, P, I, P, P, P, ctypes.POINTER(_PcgResult)]),
             "orc_num_threads": (I, []),
+            "orc_adjust_contacts": (I, [I, P, P, P, P, I, I]),
+            "orc_zero_boundary": (I, [I, P, P, P, P, I, I]),
+            "orc_mas_set_inverses": (None, [P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -109,6 +112,28 @@ def partition_contacts(rows, cols, vals, types):
     if rc != 0:
         raise ValueError("contact type hash outside 0..3")
     return orow, ocol, oval, counts
+
+
+def adjust_contacts(rows, cols, vals, bd_type, offset):
+    """adjust_fem_fem_contact_indices_kernel restated: returns adjusted copies
+    (rows, cols, vals) and the first out-of-range triplet (-1 if none)."""
+    n = len(rows)
+    r, c = _c(rows, np.int32).copy(), _c(cols, np.int32).copy()
+    v = _c(vals, np.float64).reshape(n, 9).copy()
+    bd = _c(bd_type, np.int32)
+    bad = lib().orc_adjust_contacts(n, _p(r), _p(c), _p(v), _p(bd), len(bd), int(offset))
+    return r, c, v, bad
+
+
+def zero_boundary(rows, cols, vals, bd_type, offset):
+    """zero_fem_boundary_hessian_kernel restated: returns the cleared copy of
+    vals and the first out-of-range triplet (-1 if none)."""
+    n = len(rows)
+    v = _c(vals, np.float64).reshape(n, 9).copy()
+    bd = _c(bd_type, np.int32)
+    bad = lib().orc_zero_boundary(n, _p(_c(rows, np.int32)), _p(_c(cols, np.int32)), _p(v), _p(bd), len(bd),
+                                  int(offset))
+    return v, bad
 
 
 def _skew(w):
@@ -358,6 +383,14 @@ class Mas32:
         i32 = np.zeros((nd, B * (B + 1) // 2, 9), np.float32)
         self._lib.orc_mas_get_domains(self.h, _p(p64), _p(i32))
         return p64, i32
+
+    def set_inverses(self, inverse32):
+        """Replace the domain inverses (packed upper FP32 blocks, the layout of
+        domains()) with the given ones, e.g. the decoded inverses of the GPU
+        build, so precondition() applies exactly those operators."""
+        B = self.BANK
+        inv = _c(inverse32, np.float32).reshape(self.total_clusters // B, B * (B + 1) // 2, 9)
+        self._lib.orc_mas_set_inverses(self.h, _p(inv))
 
     def precondition(self, R):
         R = _c(R, np.float64)

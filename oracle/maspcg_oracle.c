@@ -121,6 +121,49 @@ int orc_partition_contacts(int n, const int* rows, const int* cols, const double
   return 0;
 }
 
+/* adjust_fem_fem_contact_indices_kernel (GIPC.cu:10130-10160): one triplet
+ * at a time, in input order. */
+int orc_adjust_contacts(int n, int* rows, int* cols, double* vals9, const int* bd_type, int nv, int offset)
+{
+  int first_bad = -1;
+  for (int i = 0; i < n; ++i) {
+    const int r = rows[i], c = cols[i];
+    if (r < 0 || c < 0 || r >= nv || c >= nv) {
+      if (first_bad < 0) first_bad = i;
+      continue;
+    }
+    int clear;
+    if (r <= c) {
+      rows[i] = r + offset;
+      cols[i] = c + offset;
+      clear = bd_type[r] != 0 || bd_type[c] != 0;
+    } else {
+      rows[i] = c + offset;
+      cols[i] = r + offset;
+      clear = 1;
+    }
+    if (clear)
+      for (int e = 0; e < 9; ++e) vals9[9 * (size_t)i + e] = 0.0;
+  }
+  return first_bad;
+}
+
+/* zero_fem_boundary_hessian_kernel (GIPC.cu:10162-10181). */
+int orc_zero_boundary(int n, const int* rows, const int* cols, double* vals9, const int* bd_type, int nv, int offset)
+{
+  int first_bad = -1;
+  for (int i = 0; i < n; ++i) {
+    const int a = rows[i] - offset, b = cols[i] - offset;
+    if (a < 0 || b < 0 || a >= nv || b >= nv) {
+      if (first_bad < 0) first_bad = i;
+      continue;
+    }
+    if (bd_type[a] != 0 || bd_type[b] != 0)
+      for (int e = 0; e < 9; ++e) vals9[9 * (size_t)i + e] = 0.0;
+  }
+  return first_bad;
+}
+
 /* spmv.cu:14-53 and the self-test CPU loop spmv.cu:348-364. */
 void orc_sym_spmv(double a, const double* vals9, const int* rows, const int* cols,
                   int nblocks, int dof, const double* x, double b, double* y)
@@ -814,6 +857,11 @@ void orc_mas_get_domains(const orc_mas* m, double* packed64, float* inverse32)
   const size_t n = (size_t)m->ndom * NPACK * 9;
   if (packed64 && m->packed64) memcpy(packed64, m->packed64, n * sizeof(double));
   if (inverse32 && m->inv32) memcpy(inverse32, m->inv32, n * sizeof(float));
+}
+
+void orc_mas_set_inverses(orc_mas* m, const float* inverse32)
+{
+  if (m->inv32 && inverse32) memcpy(m->inv32, inverse32, (size_t)m->ndom * NPACK * 9 * sizeof(float));
 }
 
 /* preconditioning (:2684-2725) = __buildMultiLevelR_optimized_new (:1149-1266)

@@ -39,6 +39,16 @@ int orc_convert_triplets(int n, const int* rows, const int* cols, const double* 
 int orc_partition_contacts(int n, const int* rows, const int* cols, const double* vals9, const uint64_t* type,
                            int* out_rows, int* out_cols, double* out_vals9, int* counts);
 
+/* adjust_fem_fem_contact_indices_kernel (GIPC.cu:10130-10160), in place:
+ * r <= c keeps its order, r > c swaps to the upper slot and is cleared, an
+ * upper triplet touching a nonzero bd_type is cleared; offset added to both
+ * indices.  Returns the first triplet index naming a vertex outside
+ * [0, nv) (that triplet untouched) or -1. */
+int orc_adjust_contacts(int n, int* rows, int* cols, double* vals9, const int* bd_type, int nv, int offset);
+/* zero_fem_boundary_hessian_kernel (GIPC.cu:10162-10181), in place; same
+ * return rule with the vertex index row/col - offset. */
+int orc_zero_boundary(int n, const int* rows, const int* cols, double* vals9, const int* bd_type, int nv, int offset);
+
 /* Spmv::*_sym_spmv (spmv.cu:28-53, CPU loop spmv.cu:348-364):
  * y = a*A*x + b*y with A given as upper BCOO.  Sequential, input order. */
 void orc_sym_spmv(double a, const double* vals9, const int* rows, const int* cols,
@@ -110,6 +120,11 @@ void orc_mas_prepare_hessian(orc_mas* m, const double* vals9, const int* rows, c
  * packed64 gets the FP64 matrices before the zero-diagonal rule,
  * inverse32 the FP32 inverses.  Either may be NULL. */
 void orc_mas_get_domains(const orc_mas* m, double* packed64, float* inverse32);
+
+/* Replace the FP32 inverses (the layout of orc_mas_get_domains) with the
+ * caller's, after orc_mas_prepare_hessian: the apply then uses exactly those
+ * operators (to check another build's inverses through the same apply). */
+void orc_mas_set_inverses(orc_mas* m, const float* inverse32);
 
 /* preconditioning (:2684-2725): R,Z are double3 arrays of length vert_num. */
 void orc_mas_precondition(const orc_mas* m, const double* R, double* Z);

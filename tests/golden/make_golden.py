@@ -1,9 +1,8 @@
 #!/usr/bin/env python3
 """Regenerate the golden fixtures under tests/golden/ from the reference.
 
-Run in a container where the reference checkout is mounted (read-only) at
-$REFERENCE_ROOT (default /root/reference).  The GPU box never runs this: the
-outputs are committed.
+Usage: make_golden.py REFERENCE_ROOT, the path of a read-only checkout of the
+reference project.  The GPU box never runs this: the outputs are committed.
 
 kat257/  -- the reference's own coarse-replay known-answer system
             (reports/agipc_reproduction/make_coarse_replay_fixture.py, default
@@ -18,10 +17,13 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
 
 
 def main() -> int:
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        print("usage: make_golden.py REFERENCE_ROOT (a checkout of the reference project)", file=sys.stderr)
+        return 2
+    REF = sys.argv[1]
     tools = os.path.join(REF, "reports", "agipc_reproduction")
     out = os.path.join(HERE, "kat257")
     subprocess.run([sys.executable, os.path.join(tools, "make_coarse_replay_fixture.py"), out], check=True)

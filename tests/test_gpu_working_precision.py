@@ -1,0 +1,205 @@
+"""Direct parity of the kernels the benchmarked (mixed-precision) solve runs,
+against the oracle, through the C ABI (needs a B200):
+
+* the iteration's SpMV in its working precision (FP32 32-block tiles with
+  FP32 sums; FP64 affine-body rows) against the FP64 product of the same
+  FP32-rounded operands, elementwise within a rounding bound;
+* the tensor-core level-0 apply of 16-bit factored domain records (every
+  staging variant) plus the coarse levels, against the oracle's apply run
+  with the GPU's own decoded inverses;
+* the mixed and FP32 solutions against the oracle's solution, with the
+  iteration counts;
+* the status word and the FP64 gate flag.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from agipc_learning_b200 import _native as N
+from agipc_learning_b200 import synth
+from agipc_learning_b200.solver import MasPcg
+
+pytestmark = pytest.mark.gpu
+
+EPS32 = float(np.finfo(np.float32).eps)
+
+
+@pytest.fixture(scope="module")
+def cfg1_small():
+    return synth.config_system(1, scale=24)
+
+
+@pytest.fixture(scope="module")
+def cfg1_40():
+    return synth.config_system(1, scale=40)
+
+
+def _round32(a):
+    return np.asarray(a, np.float64).astype(np.float32).astype(np.float64)
+
+
+def _abd_rows_mask(s):
+    mask = np.zeros(3 * s.nb, bool)
+    mask[: 12 * s.abd_bodies] = True
+    return mask
+
+
+@pytest.mark.parametrize("which,precision", [("cfg1_small", "mixed"), ("cfg1_small", "fp32"),
+                                             ("hybrid", "mixed"), ("cfg1_small", "reference")])
+def test_working_spmv_against_oracle(which, precision, request):
+    """|y_gpu - A32 x32| <= 48 eps32 (|A32| |x32|) elementwise, where A32 and
+    x32 are the FP32-rounded matrix and vector the kernel reads (rows of the
+    affine bodies, taken from the FP64 matrix in FP64, within 1e-12 of the
+    FP64 product); reference precision within 1e-12 of the FP64 product."""
+    s = synth.config_system(2, scale=16) if which == "hybrid" else request.getfixturevalue(which)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(3 * s.nb)
+    with MasPcg.from_system(s, precision=precision, inverse="bf16" if precision == "mixed" else "fp32",
+                            gate="euclid") as m:
+        y = m.spmv_working(x)
+    if precision == "reference":
+        ref = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
+        mag = oracle.sym_spmv(1.0, np.abs(s.vals), s.rows, s.cols, np.abs(x))
+        assert np.all(np.abs(y - ref) <= 1e-12 * mag + 1e-300)
+        return
+    x32 = _round32(x)
+    ref = oracle.sym_spmv(1.0, _round32(s.vals), s.rows, s.cols, x32)
+    mag = oracle.sym_spmv(1.0, np.abs(_round32(s.vals)), s.rows, s.cols, np.abs(x32))
+    abd = _abd_rows_mask(s)
+    fem = ~abd
+    # the kernel's FP32 output: the FP64 product of the rounded operands, plus
+    # the FP32 summation error and the final rounding
+    assert np.all(np.abs(y[fem] - ref[fem]) <= 48 * EPS32 * mag[fem] + 1e-300)
+    if abd.any():
+        ref64 = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x32)
+        mag64 = oracle.sym_spmv(1.0, np.abs(s.vals), s.rows, s.cols, np.abs(x32))
+        # FP64 sums over the FP64 matrix, rounded once to FP32 at the end
+        assert np.all(np.abs(y[abd] - ref64[abd]) <= EPS32 * np.abs(ref64[abd]) + 1e-12 * mag64[abd] + 1e-300)
+
+
+def _oracle_with_inverses(s, gpu_inverses):
+    o = oracle.Mas32.from_system(s)
+    o.reorder(s.pairs)
+    sel = np.nonzero((s.rows >= s.fem_offset) & (s.rows < s.fem_offset + s.fem_count) &
+                     (s.cols >= s.fem_offset) & (s.cols < s.fem_offset + s.fem_count))[0].astype(np.uint32)
+    o.prepare_hessian(s.vals, s.rows, s.cols, sel, s.fem_offset)
+    o.set_inverses(gpu_inverses)
+    return o
+
+
+@pytest.mark.parametrize("inverse", ["bf16", "fp16"])
+@pytest.mark.parametrize("flag", [0, N.FLAG_APPLY_STAGED2, N.FLAG_APPLY_DIRECT])
+def test_tensor_core_apply_against_oracle(cfg1_40, inverse, flag):
+    """The 16-bit level-0 apply (S V^T V S r on the tensor cores, the vector
+    split into three 16-bit terms) and the coarse levels against the oracle's
+    FP32 apply of the same operators (the GPU's decoded inverses).  The 40^3
+    system has more level-0 domains than warps of one resident wave, so each
+    warp reuses its staging slots."""
+    s = cfg1_40
+    rng = np.random.default_rng(17)
+    with MasPcg.from_system(s, precision="mixed", inverse=inverse, gate="euclid", flags=flag) as m:
+        gi = m.domain_inverses()
+        rs = [s.b, rng.standard_normal(3 * s.nb)]
+        zs = [m.apply_preconditioner(r) for r in rs]
+    o = _oracle_with_inverses(s, gi)
+    for r, z in zip(rs, zs):
+        zo = o.precondition(_round32(r))
+        err = np.linalg.norm(z - zo) / np.linalg.norm(zo)
+        assert err <= 2e-6, err
+        # every row, against the size of its own terms
+        mag = np.abs(zo) + np.linalg.norm(zo) / np.sqrt(len(zo))
+        assert np.max(np.abs(z - zo) / mag) <= 1e-4
+
+
+def test_mixed_apply_inside_the_solve_schedule(cfg1_40):
+    """The solve's overlapped form (coarse levels beside the level-0 apply, the
+    coarse correction added in the p update) gives the same iterate as the
+    sequential form to rounding: both reach the gate in nearly the same
+    number of iterations and their solutions agree."""
+    s = cfg1_40
+    with MasPcg.from_system(s, precision="mixed", inverse="bf16", gate="euclid") as m:
+        x1, r1 = m.solve(s.b)
+    with MasPcg.from_system(s, precision="mixed", inverse="bf16", gate="euclid", flags=N.FLAG_SEQUENTIAL_COARSE) as m:
+        x2, r2 = m.solve(s.b)
+    assert r1["fp64_gate_met"] and r2["fp64_gate_met"]
+    assert abs(r1["iterations"] - r2["iterations"]) <= max(4, int(0.05 * r2["iterations"]))
+    assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) <= 1e-3
+
+
+def _solution_case(name):
+    if name == "cfg0":
+        return synth.config_system(0)
+    if name == "hybrid":
+        return synth.config_system(2, scale=16)
+    return synth.config_system(1, scale=int(name.split("_")[1]))
+
+
+@pytest.mark.parametrize("name", ["cfg0", "cfg1_24", "cfg1_40", "hybrid"])
+@pytest.mark.parametrize("precision,inverse", [("mixed", "bf16"), ("mixed", "fp16"), ("fp32", "fp32")])
+def test_solution_against_oracle(name, precision, inverse):
+    """x of the lower-precision forms against the oracle's FP64 PCG x at the
+    same FP64-verified tolerance: iterations within 10% (mixed), and the two
+    solutions within the distance two iterates with residual <= 1e-4 can
+    have, measured on the oracle's own iterates: ||x - x_o|| <= 2 ||x_o' -
+    x_o|| with x_o' the oracle's solve to 1e-4 / 4.  Plain FP32 is checked
+    only where its FP64 residual reaches the tolerance (it stalls above 1e-4
+    on the stiff contact systems; the FP64 gate flag must then say so)."""
+    s = _solution_case(name)
+    xo, ro, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID)
+    with MasPcg.from_system(s, gate="euclid", precision=precision, inverse=inverse) as m:
+        x, res = m.solve(s.b)
+    assert res["fp64_gate_met"] == (res["rel_res_true"] <= 1e-4)
+    if precision == "fp32" and not res["fp64_gate_met"]:
+        assert res["status_name"] in ("converged", "iteration_cap")
+        pytest.skip(f"plain FP32 stalls at an FP64 residual of {res['rel_res_true']:.2e} on {name}")
+    assert res["status_name"] == "converged" and res["fp64_gate_met"], res
+    if precision == "mixed":
+        assert abs(res["iterations"] - ro["iterations"]) <= max(2, int(0.1 * ro["iterations"])), \
+            (res["iterations"], ro["iterations"])
+    xt, _, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID, tol=2.5e-5)
+    spread = np.linalg.norm(xt - xo)
+    d = np.linalg.norm(x - xo)
+    assert d <= 2.0 * spread + 1e-12 * np.linalg.norm(xo), (d / np.linalg.norm(xo), spread / np.linalg.norm(xo))
+    assert d / np.linalg.norm(xo) <= 1e-2
+
+
+def test_fp32_status_and_fp64_gate_flag(cfg1_40):
+    """Plain FP32 under the Euclidean gate stops on its recursive residual:
+    the status says the loop's gate was met, the FP64 flag says whether the
+    returned x meets the tolerance checked in FP64."""
+    s = cfg1_40
+    with MasPcg.from_system(s, gate="euclid", precision="fp32") as m:
+        _, res = m.solve(s.b)
+    assert res["fp64_gate_met"] == (res["rel_res_true"] <= 1e-4)
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16") as m:
+        _, res = m.solve(s.b)
+    assert res["status_name"] == "converged" and res["fp64_gate_met"] == 1
+
+
+def test_full_size_reference_precision_solve_against_oracle():
+    """The bench system (64^3 cube, 50,000 contacts) solved in the reference
+    precision to the FP64 Euclidean 1e-4: iterations within 10% and the
+    solution within 1e-4 of the oracle's (the same iteration in FP64 up to
+    summation order)."""
+    s = synth.config_system(1)
+    xo, ro, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID)
+    with MasPcg.from_system(s, gate="euclid", precision="reference") as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged" and res["fp64_gate_met"]
+    assert abs(res["iterations"] - ro["iterations"]) <= max(2, int(0.1 * ro["iterations"]))
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-4
+
+
+def test_full_size_mixed_solve_against_oracle():
+    """The benchmarked configuration itself (mixed precision, BF16 inverses)
+    against the oracle on the same system: iterations within 10%, FP64 gate
+    met, the solution within twice the spread of the oracle's own iterates
+    between 1e-4 and 2.5e-5."""
+    s = synth.config_system(1)
+    xo, ro, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID)
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16") as m:
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged" and res["fp64_gate_met"]
+    assert abs(res["iterations"] - ro["iterations"]) <= max(2, int(0.1 * ro["iterations"]))
+    xt, _, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID, tol=2.5e-5)
+    assert np.linalg.norm(x - xo) <= 2.0 * np.linalg.norm(xt - xo)
