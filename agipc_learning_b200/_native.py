@@ -55,7 +55,9 @@ EXPORTS = (
     "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient", "maspcg_convert_bcoo",
     "maspcg_partition_contact_triplets", "maspcg_fem_snk1_gradient_hessian", "maspcg_galerkin_coarse_matrix",
     "maspcg_galerkin_restrict", "maspcg_galerkin_prolong", "maspcg_adjust_contact_triplets",
-    "maspcg_zero_boundary_triplets", "maspcg_spmv_working",
+    "maspcg_zero_boundary_triplets", "maspcg_spmv_working", "maspcg_refresh_matrix_values",
+    "maspcg_set_matrix_bcoo_indexed", "maspcg_local_diagnostics", "maspcg_check_local_matrices",
+    "maspcg_refresh_matrix_values_indexed",
 )
 
 RESIDUAL_MAX_VECTORS = 8
@@ -85,6 +87,28 @@ class Result(ctypes.Structure):
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["status_name"] = SOLVE_STATUS.get(self.status, str(self.status))
+        return d
+
+
+class DomainCheck(ctypes.Structure):
+    """maspcg_domain_check (LocalGpuCheck)."""
+    _fields_ = [("local_finite", ctypes.c_int), ("inverse_finite", ctypes.c_int), ("local_spd", ctypes.c_int),
+                ("inverse_spd", ctypes.c_int), ("minimum_local_diagonal", ctypes.c_double),
+                ("minimum_inverse_diagonal", ctypes.c_double), ("inverse_residual", ctypes.c_double)]
+
+
+class Diagnostics(ctypes.Structure):
+    """maspcg_diagnostics (the summary of gpu_local_checks)."""
+    _fields_ = [("matrix_count", ctypes.c_int), ("local_spd_count", ctypes.c_int),
+                ("inverse_spd_count", ctypes.c_int), ("first_local_spd_failure", ctypes.c_int),
+                ("first_inverse_spd_failure", ctypes.c_int), ("nonfinite_local_count", ctypes.c_int),
+                ("nonfinite_inverse_count", ctypes.c_int), ("passed", ctypes.c_int),
+                ("minimum_local_diagonal", ctypes.c_double), ("minimum_inverse_diagonal", ctypes.c_double),
+                ("maximum_inverse_residual", ctypes.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["passed"] = bool(d["passed"])
         return d
 
 
@@ -141,6 +165,11 @@ def load():
         "maspcg_adjust_contact_triplets": (I, [H, I, P, P, P, P, I, I]),
         "maspcg_zero_boundary_triplets": (I, [H, I, P, P, P, P, I, I]),
         "maspcg_spmv_working": (I, [H, P, P]),
+        "maspcg_refresh_matrix_values": (I, [H, P]),
+        "maspcg_refresh_matrix_values_indexed": (I, [H, P, ctypes.c_longlong, P]),
+        "maspcg_set_matrix_bcoo_indexed": (I, [H, P, P, P, ctypes.c_longlong, P, I, I, I, I, I]),
+        "maspcg_local_diagnostics": (I, [H, P, ctypes.POINTER(Diagnostics)]),
+        "maspcg_check_local_matrices": (I, [H, I, I, P, P, P, ctypes.POINTER(Diagnostics)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -4,6 +4,7 @@
 // maspcg_status and keeps the message for maspcg_last_error; nothing aborts.
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <new>
 #include <vector>
 
@@ -491,50 +492,89 @@ MASPCG_API maspcg_status maspcg_set_contacts(maspcg_handle* h, const int* pairs4
   });
 }
 
+namespace {
+void check_matrix_args(maspcg_handle* h, int n_blocks, int block_rows, int fem_offset_blocks, int abd_body_count)
+{
+  MREQ(n_blocks >= 1 && block_rows >= 1, MASPCG_ERR_INVALID_ARGUMENT, "empty matrix");
+  MREQ(fem_offset_blocks >= 0 && abd_body_count >= 0 && 4LL * abd_body_count <= block_rows,
+       MASPCG_ERR_INVALID_ARGUMENT, "invalid offsets");
+  MREQ(n_blocks <= (1 << 29), MASPCG_ERR_CAPACITY, "too many blocks");
+  if (h->cfg.preconditioner == MASPCG_PRECOND_MAS32 || h->cfg.preconditioner == MASPCG_PRECOND_MAS16) {
+    MREQ(h->has_graph, MASPCG_ERR_NOT_READY, "MAS needs set_graph before set_matrix_bcoo");
+    MREQ(4LL * abd_body_count <= fem_offset_blocks, MASPCG_ERR_INVALID_ARGUMENT, "ABD rows overlap the FEM range");
+    MREQ((long long)fem_offset_blocks + h->nv <= block_rows, MASPCG_ERR_INVALID_ARGUMENT,
+         "FEM range exceeds block_rows");
+  }
+}
+
+// The matrix build from device triplets (values may still be copying on the
+// side stream: h->vals_pending).
+void finish_set_matrix(maspcg_handle* h, const double* v, const int* r, const int* c, int n_blocks, int block_rows,
+                       int fem_offset_blocks, int abd_body_count)
+{
+  h->nb = block_rows;
+  h->fem_off = fem_offset_blocks;
+  h->abd_bodies = abd_body_count;
+  h->n_in = n_blocks;
+  maspcg::build_internal_matrix(h, v, r, c, n_blocks);
+  alloc_vectors(h);
+  MCK(cudaStreamSynchronize(h->stream));
+  h->has_matrix = true;
+  h->has_precond = false;
+  h->graph_dirty = true;
+}
+}  // namespace
+
 MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* values9, const int* rows,
                                                 const int* cols, int n_blocks, int block_rows, int fem_offset_blocks,
                                                 int abd_body_count)
 {
   return guard(h, [&] {
-    MREQ(n_blocks >= 1 && block_rows >= 1, MASPCG_ERR_INVALID_ARGUMENT, "empty matrix");
-    MREQ(fem_offset_blocks >= 0 && abd_body_count >= 0 && 4LL * abd_body_count <= block_rows,
-         MASPCG_ERR_INVALID_ARGUMENT, "invalid offsets");
-    MREQ(n_blocks <= (1 << 29), MASPCG_ERR_CAPACITY, "too many blocks");
-    if (h->cfg.preconditioner == MASPCG_PRECOND_MAS32 || h->cfg.preconditioner == MASPCG_PRECOND_MAS16) {
-      MREQ(h->has_graph, MASPCG_ERR_NOT_READY, "MAS needs set_graph before set_matrix_bcoo");
-      MREQ(4LL * abd_body_count <= fem_offset_blocks, MASPCG_ERR_INVALID_ARGUMENT, "ABD rows overlap the FEM range");
-      MREQ((long long)fem_offset_blocks + h->nv <= block_rows, MASPCG_ERR_INVALID_ARGUMENT,
-           "FEM range exceeds block_rows");
-    }
-    h->nb = block_rows;
-    h->fem_off = fem_offset_blocks;
-    h->abd_bodies = abd_body_count;
-    h->n_in = n_blocks;
+    check_matrix_args(h, n_blocks, block_rows, fem_offset_blocks, abd_body_count);
     const int* r = device_in(h, rows, (size_t)n_blocks, h->in_rows);
     const int* c = device_in(h, cols, (size_t)n_blocks, h->in_cols);
     // Host values (the bulk of the input) are copied on the side stream while
     // the structure is built from the indices; the value fill waits for them.
     const double* v = values9;
     h->vals_pending = false;
-    if (n_blocks > 0) {
-      MREQ(values9 != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null array argument");
-      if (!is_device_ptr(values9)) {
-        h->in_vals.resize((size_t)9 * n_blocks);
-        MCK(cudaEventRecord(h->ev_fork, h->stream));  // earlier readers of in_vals are done
-        MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
-        MCK(cudaMemcpyAsync(h->in_vals.get(), values9, sizeof(double) * 9 * (size_t)n_blocks,
-                            cudaMemcpyHostToDevice, h->side_stream));
-        MCK(cudaEventRecord(h->ev_join, h->side_stream));
-        h->vals_pending = true;
-        v = h->in_vals.get();
-      }
+    MREQ(values9 != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null array argument");
+    if (!is_device_ptr(values9)) {
+      h->in_vals.resize((size_t)9 * n_blocks);
+      MCK(cudaEventRecord(h->ev_fork, h->stream));  // earlier readers of in_vals are done
+      MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+      MCK(cudaMemcpyAsync(h->in_vals.get(), values9, sizeof(double) * 9 * (size_t)n_blocks, cudaMemcpyHostToDevice,
+                          h->side_stream));
+      MCK(cudaEventRecord(h->ev_join, h->side_stream));
+      h->vals_pending = true;
+      v = h->in_vals.get();
     }
-    maspcg::build_internal_matrix(h, v, r, c, n_blocks);
-    alloc_vectors(h);
-    MCK(cudaStreamSynchronize(h->stream));
-    h->has_matrix = true;
-    h->has_precond = false;
-    h->graph_dirty = true;
+    finish_set_matrix(h, v, r, c, n_blocks, block_rows, fem_offset_blocks, abd_body_count);
+  });
+}
+
+MASPCG_API maspcg_status maspcg_set_matrix_bcoo_indexed(maspcg_handle* h, const double* values9, const int* rows,
+                                                        const int* cols, long long source_count,
+                                                        const uint32_t* indices, int n_blocks, int offset,
+                                                        int block_rows, int fem_offset_blocks, int abd_body_count)
+{
+  return guard(h, [&] {
+    check_matrix_args(h, n_blocks, block_rows, fem_offset_blocks, abd_body_count);
+    MREQ(source_count >= 1 && source_count <= (1LL << 31), MASPCG_ERR_INVALID_ARGUMENT, "bad source_count");
+    MREQ(indices != nullptr || n_blocks <= source_count, MASPCG_ERR_INVALID_ARGUMENT,
+         "without indices n_blocks must not exceed source_count");
+    const double* sv = device_in(h, values9, 9 * (size_t)source_count, h->asm_vals);
+    const int* sr = device_in(h, rows, (size_t)source_count, h->asm_rows);
+    const int* sc = device_in(h, cols, (size_t)source_count, h->asm_cols);
+    DBuf<unsigned> idx_stage;
+    const unsigned* ix = indices ? device_in(h, (const unsigned*)indices, (size_t)n_blocks, idx_stage) : nullptr;
+    h->in_vals.resize((size_t)9 * n_blocks);
+    h->in_rows.resize((size_t)n_blocks);
+    h->in_cols.resize((size_t)n_blocks);
+    maspcg::gather_triplets(h, n_blocks, ix, sr, sc, sv, source_count, offset, h->in_rows.get(), h->in_cols.get(),
+                            h->in_vals.get());
+    h->vals_pending = false;
+    finish_set_matrix(h, h->in_vals.get(), h->in_rows.get(), h->in_cols.get(), n_blocks, block_rows,
+                      fem_offset_blocks, abd_body_count);
   });
 }
 
@@ -549,6 +589,43 @@ MASPCG_API maspcg_status maspcg_build_preconditioner(maspcg_handle* h)
     maspcg::build_block_jacobi(h);
     MCK(cudaStreamSynchronize(h->stream));
     h->has_precond = true;
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_refresh_matrix_values(maspcg_handle* h, const double* values9)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix && h->has_precond, MASPCG_ERR_NOT_READY, "set_matrix_bcoo and build_preconditioner first");
+    MREQ(values9 != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null values");
+    const double* v = device_in(h, values9, (size_t)9 * h->n_in, h->in_vals);
+    maspcg::refresh_internal_values(h, v);
+    if (h->mas_layout) maspcg::build_mas_domains(h, nullptr);
+    maspcg::build_block_jacobi(h);
+    MCK(cudaStreamSynchronize(h->stream));
+    h->graph_dirty = true;
+  });
+}
+
+MASPCG_API maspcg_status maspcg_refresh_matrix_values_indexed(maspcg_handle* h, const double* values9,
+                                                             long long source_count, const uint32_t* indices)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix && h->has_precond, MASPCG_ERR_NOT_READY, "set_matrix_bcoo and build_preconditioner first");
+    MREQ(values9 != nullptr && indices != nullptr, MASPCG_ERR_INVALID_ARGUMENT, "null argument");
+    MREQ(source_count >= 1 && source_count <= (1LL << 31), MASPCG_ERR_INVALID_ARGUMENT, "bad source_count");
+    const std::vector<uint32_t> ix = host_copy(h, indices, (size_t)h->n_in);
+    for (uint32_t t : ix) MREQ((long long)t < source_count, MASPCG_ERR_INVALID_ARGUMENT, "index past the source");
+    const double* sv = device_in(h, values9, 9 * (size_t)source_count, h->asm_vals);
+    DBuf<unsigned> idx_stage;
+    const unsigned* id = device_in(h, (const unsigned*)indices, (size_t)h->n_in, idx_stage);
+    h->in_vals.resize((size_t)9 * h->n_in);
+    maspcg::gather_triplets(h, h->n_in, id, nullptr, nullptr, sv, source_count, 0, nullptr, nullptr,
+                            h->in_vals.get());
+    maspcg::refresh_internal_values(h, h->in_vals.get());
+    if (h->mas_layout) maspcg::build_mas_domains(h, nullptr);
+    maspcg::build_block_jacobi(h);
+    MCK(cudaStreamSynchronize(h->stream));
     h->graph_dirty = true;
   });
 }
@@ -711,6 +788,88 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
     maspcg::build_mas_domains(h, tmp.get());
     MCK(cudaMemcpyAsync(out, tmp.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     MCK(cudaStreamSynchronize(h->stream));
+    h->graph_dirty = true;
+  });
+}
+
+namespace {
+// Runs the per-domain checks on device arrays and fills the caller's outputs.
+void run_local_checks(maspcg_handle* h, int count, int bank, const double* p64, const float* i32,
+                      maspcg_domain_check* per_domain, maspcg_diagnostics* summary)
+{
+  DBuf<double> res;
+  res.resize(7 * (size_t)std::max(count, 1));
+  maspcg::check_local_matrices(h, count, bank, p64, i32, res.get());
+  std::vector<double> r(7 * (size_t)count);
+  if (count) MCK(cudaMemcpyAsync(r.data(), res.get(), r.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  MCK(cudaStreamSynchronize(h->stream));
+  maspcg_diagnostics d{};
+  d.matrix_count = count;
+  d.first_local_spd_failure = d.first_inverse_spd_failure = -1;
+  d.minimum_local_diagonal = d.minimum_inverse_diagonal = std::numeric_limits<double>::infinity();
+  for (int i = 0; i < count; ++i) {
+    const double* o = &r[7 * (size_t)i];
+    maspcg_domain_check c{};
+    c.local_finite = o[0] != 0.0;
+    c.inverse_finite = o[1] != 0.0;
+    c.local_spd = o[2] != 0.0;
+    c.inverse_spd = o[3] != 0.0;
+    c.minimum_local_diagonal = o[4];
+    c.minimum_inverse_diagonal = o[5];
+    c.inverse_residual = o[6];
+    if (per_domain) per_domain[i] = c;
+    d.local_spd_count += c.local_spd;
+    d.inverse_spd_count += c.inverse_spd;
+    d.nonfinite_local_count += !c.local_finite;
+    d.nonfinite_inverse_count += !c.inverse_finite;
+    if (!c.local_spd && d.first_local_spd_failure < 0) d.first_local_spd_failure = i;
+    if (!c.inverse_spd && d.first_inverse_spd_failure < 0) d.first_inverse_spd_failure = i;
+    d.minimum_local_diagonal = std::min(d.minimum_local_diagonal, c.minimum_local_diagonal);
+    d.minimum_inverse_diagonal = std::min(d.minimum_inverse_diagonal, c.minimum_inverse_diagonal);
+    if (!std::isfinite(c.inverse_residual))
+      d.maximum_inverse_residual = std::numeric_limits<double>::infinity();
+    else
+      d.maximum_inverse_residual = std::max(d.maximum_inverse_residual, c.inverse_residual);
+  }
+  d.passed = count > 0 && d.local_spd_count == count && d.inverse_spd_count == count && !d.nonfinite_local_count &&
+             !d.nonfinite_inverse_count && d.maximum_inverse_residual <= 1e-3;
+  if (summary) *summary = d;
+}
+}  // namespace
+
+MASPCG_API maspcg_status maspcg_check_local_matrices(maspcg_handle* h, int count, int bank, const double* packed64,
+                                                     const float* inverse32, maspcg_domain_check* per_domain,
+                                                     maspcg_diagnostics* summary)
+{
+  return guard(h, [&] {
+    MREQ(count >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative count");
+    MREQ(bank == 32 || bank == 16, MASPCG_ERR_INVALID_ARGUMENT, "bank must be 32 or 16");
+    const size_t per = (size_t)bank * (bank + 1) / 2 * 9;
+    DBuf<double> a;
+    DBuf<float> b;
+    const double* pa = count ? device_in(h, packed64, per * count, a) : nullptr;
+    const float* pb = count ? device_in(h, inverse32, per * count, b) : nullptr;
+    run_local_checks(h, count, bank, pa, pb, per_domain, summary);
+  });
+}
+
+MASPCG_API maspcg_status maspcg_local_diagnostics(maspcg_handle* h, maspcg_domain_check* per_domain,
+                                                  maspcg_diagnostics* summary)
+{
+  return guard(h, [&] {
+    MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS preconditioner first");
+    const int D = h->lv.domains;
+    const size_t per = (size_t)(h->bank == 16 ? maspcg::kMas16Packed : maspcg::kPacked) * 9;
+    DBuf<double> a;
+    a.resize(per * std::max(D, 1));
+    MCK(cudaMemsetAsync(a.get(), 0, per * D * sizeof(double), h->stream));
+    maspcg::build_mas_domains(h, a.get());
+    std::vector<float> inv(per * D);
+    maspcg::decode_inverses(h, inv.data());
+    DBuf<float> b;
+    b.resize(per * std::max(D, 1));
+    MCK(cudaMemcpyAsync(b.get(), inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    run_local_checks(h, D, h->bank, a.get(), b.get(), per_domain, summary);
     h->graph_dirty = true;
   });
 }

@@ -11,6 +11,10 @@
 //   FEM offset.
 // * zero_boundary: zero_fem_boundary_hessian_kernel (GIPC.cu:10162-10181):
 //   element triplets touching a boundary vertex are cleared.
+// * gather_triplets: a subsystem's triplets picked from the global list by
+//   index and shifted into the subsystem's numbering, as
+//   LocalPreconditioner::calculate_subsystem_bcoo_indices and
+//   setPreconditioner_bcoo pick them (i_preconditioner.cu:54-89).
 //
 // Integer work plus stores of +0.0, so the outputs are bit-exact.  The
 // reference reads bd_type without a bound check; here an index outside
@@ -79,6 +83,32 @@ __global__ void __launch_bounds__(kContactTpb) k_zero_boundary(int n, const int*
   clear_flagged(values9, warp_first, n, clear);
 }
 
+// Triplet t of a sub-range: the source triplet idx[t] (t itself without an
+// index list) with both indices moved down by `offset`.  An index past the
+// source gives the row -1, which the matrix build reports as out of range.
+// Without rows_out only the values are gathered.
+__global__ void __launch_bounds__(kContactTpb) k_gather_triplets(int n, const unsigned* __restrict__ idx,
+                                                                   const int* __restrict__ rows,
+                                                                   const int* __restrict__ cols,
+                                                                   const double* __restrict__ vals9,
+                                                                   long long source, int offset, int* rows_out,
+                                                                   int* cols_out, double* vals_out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long t = idx ? (long long)idx[i] : (long long)i;
+  if (t >= source) {
+    if (rows_out) rows_out[i] = cols_out[i] = -1;
+    return;
+  }
+  if (rows_out) {
+    rows_out[i] = rows[t] - offset;
+    cols_out[i] = cols[t] - offset;
+  }
+#pragma unroll
+  for (int e = 0; e < 9; ++e) vals_out[9 * (size_t)i + e] = vals9[9 * (size_t)t + e];
+}
+
 }  // namespace
 
 bool adjust_contacts(maspcg_handle* h, int n, int* rows, int* cols, double* values9, const int* bd_type,
@@ -98,6 +128,16 @@ bool adjust_contacts(maspcg_handle* h, int n, int* rows, int* cols, double* valu
   MCK(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   MCK(cudaStreamSynchronize(h->stream));
   return flag == 0;
+}
+
+void gather_triplets(maspcg_handle* h, int n, const unsigned* idx, const int* rows, const int* cols,
+                     const double* vals9, long long source, int offset, int* rows_out, int* cols_out,
+                     double* vals_out)
+{
+  k_gather_triplets<<<ceil_div(n, kContactTpb), kContactTpb, 0, h->stream>>>(n, idx, rows, cols, vals9, source, offset,
+                                                                             rows_out, cols_out, vals_out);
+  MLAUNCHED(h);
+  MCK(cudaGetLastError());
 }
 
 }  // namespace maspcg

@@ -206,11 +206,20 @@ struct maspcg_handle {
   // ---- matrix (set_matrix_bcoo)
   bool has_matrix = false;
   int nb = 0, fem_off = 0, abd_bodies = 0, nb_int = 0, n_in = 0, nnzb = 0;
+  int m_valid = 0;  // sorted (key, block) pairs that carry a block (the merge of set_matrix_bcoo)
   bool mas_layout = false;  // internal order uses the MAS partition
   maspcg::DBuf<int> int_of_row, row_of_int;
   maspcg::DBuf<int> rowptr, colidx;
   maspcg::DBuf<double> val64;     // row-major 3x3 blocks
-  maspcg::DBuf<float> val32;      // tiles of 32 blocks, element-major: (t/32)*288 + 32e + t%32
+  // FP32 matrix of the iteration (FP32 / MIXED precision) in the sliced
+  // jagged-diagonal layout of spmv_jds.cuh, and the rows it leaves to the
+  // FP64 row path
+  maspcg::DBuf<int> jds_base, jds_cbase, jds_coff, jds_xrows, jds_xflag, jds_xpos, jds_len;
+  maspcg::DBuf<unsigned char> jds_perm;
+  maspcg::DBuf<float4> jds_a, jds_b;
+  maspcg::DBuf<float2> jds_c;
+  int jds_slices = 0, jds_nx = 0;
+  long long jds_entries = 0;
   maspcg::DBuf<unsigned long long> keys, keys_sorted;
   maspcg::DBuf<int> kv, kv_sorted, seg_head, seg_start, row_count;
   maspcg::DBuf<double> in_vals;
@@ -276,6 +285,11 @@ void build_hierarchy(maspcg_handle* h);
 
 // matrix.cu
 void build_internal_matrix(maspcg_handle* h, const double* vals_dev, const int* rows_dev, const int* cols_dev, int n);
+void build_jds(maspcg_handle* h);  // FP32 sliced layout from the FP64 BCSR (FP32 / MIXED precision)
+void fill_jds(maspcg_handle* h);   // its values only (structure unchanged)
+// New values for the structure of the last build_internal_matrix (same
+// triplets in the same order): the FP64 BCSR values and the FP32 layout.
+void refresh_internal_values(maspcg_handle* h, const double* vals_dev);
 void launch_spmv64(maspcg_handle* h, const double* x, double* y, double a, double b);  // internal order
 void permute_in(maspcg_handle* h, const double* src_orig, double* dst_int);
 void permute_out(maspcg_handle* h, const double* src_int, double* dst_orig);
@@ -312,6 +326,11 @@ void partition_contacts(maspcg_handle* h, const int* rows, const int* cols, cons
 // [0, n_vertices) (that triplet is left as it was).
 bool adjust_contacts(maspcg_handle* h, int n, int* rows, int* cols, double* values9, const int* bd_type,
                      int n_vertices, int offset, bool zero_boundary_only);
+// Sub-range triplets (device pointers): out[t] = source[idx ? idx[t] : t]
+// with indices - offset; an index >= source gives rows_out -1.
+void gather_triplets(maspcg_handle* h, int n, const unsigned* idx, const int* rows, const int* cols,
+                     const double* vals9, long long source, int offset, int* rows_out, int* cols_out,
+                     double* vals_out);
 
 // galerkin.cu (device pointers).  The AGIPC mapping: fine blocks [0, prefix)
 // pass through; FEM node k (block prefix + k) maps to coarse node
@@ -334,6 +353,10 @@ void galerkin_prolong(maspcg_handle* h, const GalerkinMap& m, const double* coar
 void fem_snk1(maspcg_handle* h, int ntet, int nverts, const unsigned* tets, const double* x, const double* dm_inv,
               const double* volume, const double* len_rate, const double* vol_rate, double dt, int offset,
               double* gradient, int* rows, int* cols, double* vals);
+
+// diagnostics.cu (device pointers): 7 doubles per domain into results
+void check_local_matrices(maspcg_handle* h, int count, int bank, const double* packed64_dev,
+                          const float* inverse32_dev, double* results_dev);
 
 // residual_noalloc.cu
 void residual_norms_noalloc(maspcg_handle* h, int count, const double* x, const double* b, double* residual_norms,

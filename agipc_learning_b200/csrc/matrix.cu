@@ -12,6 +12,7 @@
 
 #include "maspcg_internal.cuh"
 #include "spmv_row.cuh"
+#include "spmv_jds.cuh"
 
 namespace maspcg {
 namespace {
@@ -71,7 +72,7 @@ __global__ void k_fill_structure(const unsigned long long* __restrict__ keys, co
 // One thread per stored block: sum its input blocks in sorted (= input) order.
 __global__ void k_fill_values(const unsigned long long* __restrict__ keys, const int* __restrict__ vals_sorted,
                               const int* __restrict__ seg_start, int nnzb, int m_valid,
-                              const double* __restrict__ in_vals, double* val64, float* val32)
+                              const double* __restrict__ in_vals, double* val64)
 {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nnzb) return;
@@ -95,10 +96,7 @@ __global__ void k_fill_values(const unsigned long long* __restrict__ keys, const
     }
   }
 #pragma unroll
-  for (int q = 0; q < 9; ++q) {
-    val64[9 * (size_t)u + q] = a[q];
-    val32[(size_t)(u >> 5) * 288 + 32 * q + (u & 31)] = (float)a[q];  // tiles of 32 blocks, element-major
-  }
+  for (int q = 0; q < 9; ++q) val64[9 * (size_t)u + q] = a[q];
 }
 
 // y = a*A*x + b*y, FP64, half-warp per block row.
@@ -230,6 +228,95 @@ __global__ void k_abd_inverse(const int* __restrict__ rowptr, const int* __restr
     }
 }
 
+// ---- the FP32 sliced jagged-diagonal matrix (spmv_jds.cuh) ---------------
+
+// Rows on the FP64 row path: the affine bodies [0, n64) and rows longer than
+// kJdsMaxLen blocks.
+__global__ void k_jds_flags(const int* __restrict__ rowptr, int nrows, int n64, int* xflag)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  xflag[r] = (r < n64 || rowptr[r + 1] - rowptr[r] > kJdsMaxLen) ? 1 : 0;
+}
+
+__global__ void k_jds_xrows(const int* __restrict__ xflag, const int* __restrict__ xpos, int nrows, int* xrows)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nrows && xflag[r]) xrows[xpos[r]] = r;
+}
+
+// Length of the slice row of lane `lane` in slice s (0 past the end and on
+// the FP64 row path).
+__device__ __forceinline__ int jds_row_len(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows,
+                                           int s, int lane)
+{
+  const int r = 32 * s + lane;
+  return (r < nrows && !xflag[r]) ? rowptr[r + 1] - rowptr[r] : 0;
+}
+
+// One warp per slice: rank the rows by length (longest first, ties by row),
+// the rank -> row map, and the slice's entry count and width + 1.
+__global__ void k_jds_slices(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows, int slices,
+                             unsigned char* perm, int* entries, int* ncols)
+{
+  const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (s >= slices) return;  // whole warp
+  const int r = 32 * s + lane;
+  const int len = jds_row_len(rowptr, xflag, nrows, s, lane);
+  int rank = 0;
+  for (int j = 0; j < 32; ++j) {
+    const int lj = __shfl_sync(kFull, len, j);
+    rank += (lj > len || (lj == len && j < lane)) ? 1 : 0;
+  }
+  const bool skip = r >= nrows || xflag[r];
+  perm[32 * (size_t)s + rank] = (unsigned char)(lane | (skip ? 0x80 : 0));
+  const int width = (int)__reduce_max_sync(kFull, (unsigned)len);
+  const int total = (int)__reduce_add_sync(kFull, (unsigned)len);
+  if (lane == 0) {
+    entries[s] = total;
+    ncols[s] = width + 1;
+  }
+}
+
+// Column offsets of a slice: entries in the columns before column k =
+// sum over its rows of min(length, k).
+__global__ void k_jds_coff(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows, int slices,
+                           const int* __restrict__ cbase, int* coff)
+{
+  const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (s >= slices) return;
+  const int len = jds_row_len(rowptr, xflag, nrows, s, lane);
+  const int c0 = cbase[s], width = cbase[s + 1] - c0 - 1;
+  for (int k = 0; k <= width; ++k) {
+    const int v = (int)__reduce_add_sync(kFull, (unsigned)min(len, k));
+    if (lane == 0) coff[c0 + k] = v;
+  }
+}
+
+// One warp per slice, lane = rank: the row's blocks in column order into the
+// three planes, rounded to FP32.
+__global__ void k_jds_fill(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                           const double* __restrict__ val64, const int* __restrict__ xflag, int nrows, int slices,
+                           const int* __restrict__ base, const int* __restrict__ cbase, const int* __restrict__ coff,
+                           const unsigned char* __restrict__ perm, float4* pa, float4* pb, float2* pc)
+{
+  const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (s >= slices) return;
+  const unsigned pm = perm[32 * (size_t)s + lane];
+  if (pm & 0x80u) return;
+  const int r = 32 * s + (int)(pm & 31u);
+  const int rs = rowptr[r], len = rowptr[r + 1] - rs;
+  const int b0 = base[s], c0 = cbase[s];
+  for (int k = 0; k < len; ++k) {
+    const int t = rs + k;
+    const size_t e = (size_t)b0 + coff[c0 + k] + lane;
+    const double* m = val64 + 9 * (size_t)t;
+    pa[e] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
+    pb[e] = make_float4((float)m[4], (float)m[5], (float)m[6], (float)m[7]);
+    pc[e] = make_float2((float)m[8], __int_as_float(colidx[t]));
+  }
+}
+
 size_t cub_bytes_sort(int m, int end_bit)
 {
   size_t b = 0;
@@ -309,10 +396,10 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   MREQ(flags[0] == 0, MASPCG_ERR_INVALID_ARGUMENT, "matrix block index out of range");
   const int nnzb = tail[0] + tail[1];
   const int m_valid = m - flags[2];  // sentinels (one per diagonal input block) sort last
+  h->m_valid = m_valid;
   h->nnzb = nnzb;
   h->colidx.resize(nnzb, 4);  // 16-byte tail for TMA bulk copies
   h->val64.resize((size_t)9 * nnzb, 2);
-  h->val32.resize((size_t)9 * (((size_t)nnzb + 31) / 32 * 32));
   h->row_count.resize(nb_int + 1);
   h->rowptr.resize(nb_int + 1);
   MCK(cudaMemsetAsync(h->row_count.get(), 0, sizeof(int) * (nb_int + 1), st));
@@ -326,9 +413,90 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
     h->vals_pending = false;
   }
   k_fill_values<<<ceil_div(nnzb, kTpb), kTpb, 0, st>>>(h->keys_sorted.get(), h->kv_sorted.get(), h->seg_start.get(),
-                                                      nnzb, m_valid, vals, h->val64.get(), h->val32.get());
+                                                      nnzb, m_valid, vals, h->val64.get());
   MLAUNCHED(h);
   MCK(cudaGetLastError());
+  if (h->cfg.precision != MASPCG_PREC_REFERENCE) build_jds(h);
+}
+
+void build_jds(maspcg_handle* h)
+{
+  cudaStream_t st = h->stream;
+  const int nrows = h->nb_int;
+  const int slices = ceil_div(nrows, 32);
+  const int n64 = 4 * h->abd_bodies;
+  h->jds_slices = slices;
+  h->jds_xflag.resize(nrows + 1);
+  h->jds_xpos.resize(nrows + 1);
+  h->jds_perm.resize(32 * (size_t)slices);
+  h->jds_base.resize(slices + 1);
+  h->jds_cbase.resize(slices + 1);
+  h->jds_len.resize(2 * (size_t)slices + 2);  // entries and width + 1 per slice
+  int* entries = h->jds_len.get();
+  int* ncols = h->jds_len.get() + slices + 1;
+  MCK(cudaMemsetAsync(h->jds_xflag.get() + nrows, 0, sizeof(int), st));
+  MCK(cudaMemsetAsync(entries + slices, 0, sizeof(int), st));
+  MCK(cudaMemsetAsync(ncols + slices, 0, sizeof(int), st));
+  k_jds_flags<<<ceil_div(nrows, kTpb), kTpb, 0, st>>>(h->rowptr.get(), nrows, n64, h->jds_xflag.get());
+  MLAUNCHED(h);
+  const int wgrid = ceil_div(32LL * slices, kTpb);
+  k_jds_slices<<<wgrid, kTpb, 0, st>>>(h->rowptr.get(), h->jds_xflag.get(), nrows, slices, h->jds_perm.get(), entries,
+                                       ncols);
+  MLAUNCHED(h);
+  size_t need = 0, b = 0;
+  MCK(cub::DeviceScan::ExclusiveSum(nullptr, b, (const int*)nullptr, (int*)nullptr, std::max(nrows, slices) + 1));
+  need = b;
+  h->cub_tmp.resize(std::max(need, h->cub_tmp.n));
+  b = h->cub_tmp.cap;
+  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, h->jds_xflag.get(), h->jds_xpos.get(), nrows + 1, st));
+  b = h->cub_tmp.cap;
+  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, entries, h->jds_base.get(), slices + 1, st));
+  b = h->cub_tmp.cap;
+  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, ncols, h->jds_cbase.get(), slices + 1, st));
+  int tail[3] = {0, 0, 0};
+  MCK(cudaMemcpyAsync(&tail[0], h->jds_xpos.get() + nrows, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaMemcpyAsync(&tail[1], h->jds_base.get() + slices, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaMemcpyAsync(&tail[2], h->jds_cbase.get() + slices, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaStreamSynchronize(st));
+  h->jds_nx = tail[0];
+  h->jds_entries = tail[1];
+  h->jds_xrows.resize(std::max(tail[0], 1));
+  h->jds_coff.resize(std::max(tail[2], 1));
+  h->jds_a.resize(std::max<size_t>(tail[1], 1));
+  h->jds_b.resize(std::max<size_t>(tail[1], 1));
+  h->jds_c.resize(std::max<size_t>(tail[1], 1));
+  k_jds_xrows<<<ceil_div(nrows, kTpb), kTpb, 0, st>>>(h->jds_xflag.get(), h->jds_xpos.get(), nrows,
+                                                      h->jds_xrows.get());
+  MLAUNCHED(h);
+  k_jds_coff<<<wgrid, kTpb, 0, st>>>(h->rowptr.get(), h->jds_xflag.get(), nrows, slices, h->jds_cbase.get(),
+                                     h->jds_coff.get());
+  MLAUNCHED(h);
+  fill_jds(h);
+}
+
+void fill_jds(maspcg_handle* h)
+{
+  const int nrows = h->nb_int, slices = h->jds_slices;
+  k_jds_fill<<<ceil_div(32LL * slices, kTpb), kTpb, 0, h->stream>>>(
+      h->rowptr.get(), h->colidx.get(), h->val64.get(), h->jds_xflag.get(), nrows, slices, h->jds_base.get(),
+      h->jds_cbase.get(), h->jds_coff.get(), h->jds_perm.get(), h->jds_a.get(), h->jds_b.get(), h->jds_c.get());
+  MLAUNCHED(h);
+  MCK(cudaGetLastError());
+}
+
+void refresh_internal_values(maspcg_handle* h, const double* vals)
+{
+  cudaStream_t st = h->stream;
+  if (h->vals_pending) {  // host values copied on the side stream
+    MCK(cudaStreamWaitEvent(st, h->ev_join, 0));
+    h->vals_pending = false;
+  }
+  k_fill_values<<<ceil_div(h->nnzb, kTpb), kTpb, 0, st>>>(h->keys_sorted.get(), h->kv_sorted.get(),
+                                                          h->seg_start.get(), h->nnzb, h->m_valid, vals,
+                                                          h->val64.get());
+  MLAUNCHED(h);
+  MCK(cudaGetLastError());
+  if (h->cfg.precision != MASPCG_PREC_REFERENCE) fill_jds(h);
 }
 
 void launch_spmv64(maspcg_handle* h, const double* x, double* y, double a, double b)

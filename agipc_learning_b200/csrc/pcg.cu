@@ -22,6 +22,7 @@
 #include "pcg_device.cuh"
 #include "mas_args.cuh"
 #include "spmv_row.cuh"
+#include "spmv_jds.cuh"
 
 namespace maspcg {
 
@@ -128,21 +129,13 @@ __global__ void __launch_bounds__(kTpb) k_update_p(ApplyArgs a, const Tv* __rest
   update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
 }
 
-// One 3x3 block of the matrix.  FP32: tiles of 32 blocks stored element-major
-// (element e of block t at (t/32)*288 + 32e + t%32), so a warp's element loads
-// are coalesced and a tile is one contiguous 1152-byte run.  FP64: row-major
-// blocks.
+// One row-major 3x3 block of the FP64 matrix.
 template <bool kTiled, typename Tm>
 __device__ __forceinline__ void load_block(const Tm* __restrict__ val, int t, Tm m[9])
 {
-  if (kTiled) {
-    const Tm* b = val + (size_t)(t >> 5) * 288 + (t & 31);
+  static_assert(!kTiled, "the FP32 matrix uses the sliced layout of spmv_jds.cuh");
 #pragma unroll
-    for (int e = 0; e < 9; ++e) m[e] = __ldcs(b + 32 * e);
-  } else {
-#pragma unroll
-    for (int e = 0; e < 9; ++e) m[e] = __ldcs(val + 9 * (size_t)t + e);
-  }
+  for (int e = 0; e < 9; ++e) m[e] = __ldcs(val + 9 * (size_t)t + e);
 }
 
 // Ap = A p for block rows [lo, nrows) in the matrix's own precision;
@@ -225,61 +218,6 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
   return dot;
 }
 
-// Ap for block rows [0, n64) from the FP64 matrix with FP64 sums, used when
-// the iteration runs on the FP32 tiles: these are the affine-body rows, whose
-// 12x12 blocks carry the orthogonality stiffness (~1e7 on the diagonal)
-// beside rotation modes held only by the mass (~1e-4), a spread FP32 values
-// or sums cannot keep positive definite.
-template <typename Tv, typename Tacc, int LPR>
-__device__ __forceinline__ Tacc spmv_rows_exact(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                                const double* __restrict__ val64, const Tv* __restrict__ p4, Tv* ap,
-                                                int n64)
-{
-  constexpr int kRows = kTpb / LPR;
-  const int sub = threadIdx.x % LPR;
-  double dot = 0.0;
-  for (int row0 = blockIdx.x * kRows; row0 < n64; row0 += gridDim.x * kRows) {
-    const int row = row0 + threadIdx.x / LPR;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    if (row < n64) {
-      const int re = __ldg(rowptr + row + 1);
-      for (int t = __ldg(rowptr + row) + sub; t < re; t += LPR) {
-        double m[9];
-        load_block<false>(val64, t, m);
-        const P4<Tv> x = ld_p4(p4, __ldcs(colidx + t));
-        a0 += m[0] * (double)x.x + m[1] * (double)x.y + m[2] * (double)x.z;
-        a1 += m[3] * (double)x.x + m[4] * (double)x.y + m[5] * (double)x.z;
-        a2 += m[6] * (double)x.x + m[7] * (double)x.y + m[8] * (double)x.z;
-      }
-    }
-#pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) {
-      a0 += __shfl_xor_sync(kFull, a0, o, LPR);
-      a1 += __shfl_xor_sync(kFull, a1, o, LPR);
-      a2 += __shfl_xor_sync(kFull, a2, o, LPR);
-    }
-    if (row < n64 && sub < 3) {
-      const Tv y = (Tv)(sub == 0 ? a0 : (sub == 1 ? a1 : a2));
-      ap[3 * (size_t)row + sub] = y;
-      const P4<Tv> pr = ld_p4(p4, row);
-      dot += (double)(sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z)) * (double)y;
-    }
-  }
-  return (Tacc)dot;
-}
-
-// Both parts of the product: rows [0, n64) exact (n64 is 0 for the FP64
-// matrix), the rest from `val`.
-template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
-__device__ __forceinline__ Tacc spmv_all(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                         const Tm* __restrict__ val, const double* __restrict__ val64, int n64,
-                                         const Tv* __restrict__ p4, Tv* ap, int nrows)
-{
-  Tacc dot = 0;
-  if (n64 > 0) dot = spmv_rows_exact<Tv, Tacc, LPR>(rowptr, colidx, val64, p4, ap, n64);
-  return dot + spmv_rows<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, p4, ap, n64, nrows);
-}
-
 // Last block of the SpMV: p.Ap and alpha (or a stop on curvature / NaN).
 __device__ __forceinline__ void spmv_finish(PcgScalars* s, double pap)
 {
@@ -295,15 +233,44 @@ __device__ __forceinline__ void spmv_finish(PcgScalars* s, double pap)
   }
 }
 
-template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
+// The SpMV of the iteration with p.Ap; the last block computes alpha.
+// FP64 matrix (reference precision): full BCSR, LPR lanes per block row.
+template <int LPR>
 __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                                const Tm* __restrict__ val, const double* __restrict__ val64, int n64,
-                                                const Tv* __restrict__ p4, Tv* ap, int nrows, Tacc* partial,
-                                                PcgScalars* s)
+                                                const double* __restrict__ val, const double* __restrict__ p4,
+                                                double* ap, int nrows, double* partial, PcgScalars* s)
 {
   pdl_wait();
   if (!running(s)) return;
-  const Tacc dot = spmv_all<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, val64, n64, p4, ap, nrows);
+  const double dot = spmv_rows<double, double, double, false, LPR>(rowptr, colidx, val, p4, ap, 0, nrows);
+  pdl_trigger();
+  double total = 0;
+  if (grid_finish<double>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
+      threadIdx.x == 0)
+    spmv_finish(s, total);
+}
+
+// FP32 matrix (FP32 / MIXED precision): the sliced jagged-diagonal layout,
+// with the affine-body and long rows from the FP64 BCSR.
+template <typename Tacc>
+__device__ __forceinline__ Tacc spmv_fp32(const JdsArgs& j, const int* __restrict__ rowptr,
+                                          const int* __restrict__ colidx, const double* __restrict__ val64,
+                                          const float* __restrict__ p4, float* ap)
+{
+  Tacc dot = 0;
+  if (j.nx > 0) dot = spmv_rows_listed<Tacc, 8>(rowptr, colidx, val64, j.xrows, j.nx, p4, ap);
+  return dot + spmv_jds<Tacc, kJdsSlicesPerWarp, kJdsColumnsPerStep>(j, p4, ap);
+}
+
+template <typename Tacc>
+__global__ void __launch_bounds__(kTpb) k_spmv_jds(JdsArgs j, const int* __restrict__ rowptr,
+                                                    const int* __restrict__ colidx, const double* __restrict__ val64,
+                                                    const float* __restrict__ p4, float* ap, Tacc* partial,
+                                                    PcgScalars* s)
+{
+  pdl_wait();
+  if (!running(s)) return;
+  const Tacc dot = spmv_fp32<Tacc>(j, rowptr, colidx, val64, p4, ap);
   pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
@@ -390,17 +357,21 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
 // update, a grid barrier, the SpMV with p.Ap and alpha, a grid barrier, the
 // x/r update with r.r and the gate.  Saves two kernel boundaries per
 // iteration; the barriers are bounded (grid_barrier).
-template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, bool kCoarse>
-__global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, const int* __restrict__ rowptr,
-                                                          const int* __restrict__ colidx, const Tm* __restrict__ val,
-                                                          const double* __restrict__ val64, int n64,
+template <typename Tm, typename Tv, typename Tacc, int LPR, bool kCoarse>
+__global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, JdsArgs j, const int* __restrict__ rowptr,
+                                                          const int* __restrict__ colidx,
+                                                          const double* __restrict__ val64,
                                                           const Tv* __restrict__ z, Tv* p4, Tv* ap, Tv* x, Tv* r,
                                                           int nrows, int mixed, Tacc* partial, PcgScalars* s, int* err)
 {
   if (!running(s)) return;  // uniform: no CTA of this launch has written the status yet
   update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
   if (!grid_barrier(s, err)) return;
-  const Tacc dot = spmv_all<Tm, Tv, Tacc, kTiled, LPR>(rowptr, colidx, val, val64, n64, p4, ap, nrows);
+  Tacc dot;
+  if constexpr (std::is_same<Tm, float>::value)
+    dot = spmv_fp32<Tacc>(j, rowptr, colidx, val64, p4, ap);
+  else
+    dot = spmv_rows<double, double, double, false, LPR>(rowptr, colidx, val64, p4, ap, 0, nrows);
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0)
@@ -656,17 +627,16 @@ struct Engine {
   template <bool kCoarse>
   void fused_head_t(PcgScalars* s, const ApplyArgs& a)
   {
-    constexpr bool kTiled = std::is_same<Tm, float>::value;
-    auto kern = k_iteration_head<Tm, Tv, Tacc, kTiled, kSpmvLanes, kCoarse>;
+    auto kern = k_iteration_head<Tm, Tv, Tacc, kSpmvLanes, kCoarse>;
     static int per_sm = 0;
     if (!per_sm) {
       MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
       MREQ(per_sm > 0, MASPCG_ERR_CUDA, "fused iteration kernel cannot be resident");
     }
     const int grid = std::max(1, std::min(ceil_div(h->nb_int, kTpb / kSpmvLanes), per_sm * h->sm_count));
-    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, h->rowptr.get(), h->colidx.get(), matrix(),
-                       h->val64.get(), exact_rows(), V(h->vz), V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0, partial(), s,
-                       h->failed.get() + 4);
+    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, jds_args(h), h->rowptr.get(), h->colidx.get(),
+                       h->val64.get(), V(h->vz), V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0,
+                       partial(), s, h->failed.get() + 4);
   }
 
   void fused_head(PcgScalars* s)
@@ -677,29 +647,39 @@ struct Engine {
       fused_head_t<false>(s, ApplyArgs{});
   }
 
-  const Tm* matrix();
-  // block rows the FP32-tile SpMV takes from the FP64 matrix (the affine bodies)
-  int exact_rows() const { return std::is_same<Tm, float>::value ? 4 * h->abd_bodies : 0; }
-
-  // SpMV rows per CTA step: kTpb / kSpmvLanes.
+  // FP64 SpMV: lanes per block row.
   static constexpr int kSpmvLanes = 8;
 
+  // The SpMV of the iteration: one wave of resident CTAs (the kernel strides
+  // over the rest).  FP32: the sliced layout, sized so every warp takes the
+  // same number of slice groups where one wave allows it.
   void spmv(PcgScalars* s)
   {
-    constexpr bool kTiled = std::is_same<Tm, float>::value;
-    constexpr int rows = kTpb / kSpmvLanes;
-    // one wave of resident CTAs; the kernel strides over the rest
-    static int per_sm = 0;
-    if (!per_sm) {
-      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv<Tm, Tv, Tacc, kTiled, kSpmvLanes>, kTpb, 0));
-      per_sm = std::max(per_sm, 1);
+    if constexpr (std::is_same<Tm, float>::value) {
+      auto kern = k_spmv_jds<Tacc>;
+      static int per_sm = 0;
+      if (!per_sm) {
+        MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
+        per_sm = std::max(per_sm, 1);
+      }
+      constexpr int groups_per_cta = (kTpb / 32) * kJdsSlicesPerWarp;
+      const int resident = per_sm * h->sm_count;
+      const int need = std::max(1, ceil_div(h->jds_slices, groups_per_cta));
+      const int grid = need <= resident ? need : ceil_div(need, ceil_div(need, resident));
+      launch_pdl(h, kern, dim3(grid), dim3(kTpb), 0, jds_args(h), h->rowptr.get(), h->colidx.get(), h->val64.get(),
+                 V(h->vp4), V(h->vap), partial(), s);
+    } else {
+      constexpr int rows = kTpb / kSpmvLanes;
+      static int per_sm = 0;
+      if (!per_sm) {
+        MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv<kSpmvLanes>, kTpb, 0));
+        per_sm = std::max(per_sm, 1);
+      }
+      const int grid = std::max(1, std::min(ceil_div(h->nb_int, rows), per_sm * h->sm_count));
+      launch_pdl(h, k_spmv<kSpmvLanes>, dim3(grid), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(),
+                 V(h->vp4), V(h->vap), h->nb_int, partial(), s);
     }
-    const int grid = std::max(1, std::min(ceil_div(h->nb_int, rows), per_sm * h->sm_count));
-    launch_pdl(h, k_spmv<Tm, Tv, Tacc, kTiled, kSpmvLanes>, dim3(grid), dim3(kTpb), 0, h->rowptr.get(),
-               h->colidx.get(), matrix(), h->val64.get(), exact_rows(), V(h->vp4), V(h->vap), h->nb_int, partial(), s);
   }
-
-
 
   void true_residual(PcgScalars* s)
   {
@@ -914,22 +894,6 @@ struct Engine {
     }
   }
 };
-
-template <>
-const double* Engine<double, double, double>::matrix()
-{
-  return h->val64.get();
-}
-template <>
-const float* Engine<float, float, float>::matrix()
-{
-  return h->val32.get();
-}
-template <>
-const float* Engine<float, float, double>::matrix()
-{
-  return h->val32.get();
-}
 
 }  // namespace
 

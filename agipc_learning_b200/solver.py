@@ -130,8 +130,60 @@ class MasPcg:
         self.nb = int(block_rows)
         self.matrix_version = getattr(self, "matrix_version", 0) + 1
 
+    def set_matrix_indexed(self, vals, rows, cols, indices, offset, block_rows, fem_offset=0, abd_bodies=0):
+        """The subsystem triplets indices[t] of a larger list, indices minus
+        `offset` (maspcg_set_matrix_bcoo_indexed); the gather runs on the
+        device, so CUDA tensors stay on the device."""
+        v, r, c = _Arg(vals, np.float64), _Arg(rows, np.int32), _Arg(cols, np.int32)
+        ix = _Arg(indices, np.uint32)
+        n = len(rows) if indices is None else len(indices)
+        self._ck(self.lib.maspcg_set_matrix_bcoo_indexed(self.h, v.ptr, r.ptr, c.ptr, int(len(rows)), ix.ptr, int(n),
+                                                         int(offset), int(block_rows), int(fem_offset),
+                                                         int(abd_bodies)))
+        self.nb = int(block_rows)
+        self.matrix_version = getattr(self, "matrix_version", 0) + 1
+
     def build(self):
         self._ck(self.lib.maspcg_build_preconditioner(self.h))
+
+    def refresh_values(self, vals):
+        """New values for the blocks of the last set_matrix (same triplets, same
+        order): merged values, domain matrices and inverses recomputed on the
+        kept structure and hierarchy (maspcg_refresh_matrix_values)."""
+        self._ck(self.lib.maspcg_refresh_matrix_values(self.h, _Arg(vals, np.float64).ptr))
+
+    def refresh_values_indexed(self, vals, indices):
+        """refresh_values with the values picked by index on the device
+        (maspcg_refresh_matrix_values_indexed)."""
+        v, ix = _Arg(vals, np.float64), _Arg(indices, np.uint32)
+        self._ck(self.lib.maspcg_refresh_matrix_values_indexed(self.h, v.ptr, int(len(vals)), ix.ptr))
+
+    def local_diagnostics(self, per_domain=False):
+        """Per-domain SPD and inverse-residual checks of the last build
+        (maspcg_local_diagnostics): the summary dict, and with per_domain the
+        list of per-domain checks."""
+        d = self.info()["domains"]
+        arr = (N.DomainCheck * max(d, 1))() if per_domain else None
+        summ = N.Diagnostics()
+        self._ck(self.lib.maspcg_local_diagnostics(self.h, ctypes.cast(arr, ctypes.c_void_p) if arr else None,
+                                                   ctypes.byref(summ)))
+        out = summ.as_dict()
+        if per_domain:
+            out["domains"] = [{k: getattr(c, k) for k, _ in c._fields_} for c in arr[:d]]
+        return out
+
+    def check_local_matrices(self, packed64, inverse32, bank=32):
+        """gpu_local_checks on caller matrices (maspcg_check_local_matrices):
+        returns (summary, per-domain list)."""
+        p = np.ascontiguousarray(packed64, np.float64)
+        q = np.ascontiguousarray(inverse32, np.float32)
+        count = p.shape[0]
+        arr = (N.DomainCheck * max(count, 1))()
+        summ = N.Diagnostics()
+        self._ck(self.lib.maspcg_check_local_matrices(self.h, int(count), int(bank), p.ctypes.data_as(ctypes.c_void_p),
+                                                      q.ctypes.data_as(ctypes.c_void_p),
+                                                      ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(summ)))
+        return summ.as_dict(), [{k: getattr(c, k) for k, _ in c._fields_} for c in arr[:count]]
 
     @classmethod
     def from_system(cls, s, **cfg):
@@ -412,14 +464,36 @@ class TraditionalMAS32Preconditioner:
         self._engine = e
 
     def setPreconditioner_bcoo(self, triplet_values, row_ids, col_ids, indices, offset, triplet_num, cpNum):
-        idx = np.asarray(indices)[:triplet_num]
-        vals = np.asarray(triplet_values).reshape(-1, 9)[idx]
-        rows = np.asarray(row_ids)[idx] - offset
-        cols = np.asarray(col_ids)[idx] - offset
+        """The subsystem's triplets are gathered on the device by index
+        (maspcg_set_matrix_bcoo_indexed), so the reference's device arrays
+        (CUDA tensors here) are used where they are."""
         pairs = None if self._collisonPairs is None else np.asarray(self._collisonPairs).reshape(-1, 4)[:cpNum]
         self._engine.set_contacts(pairs)
-        self._engine.set_matrix(vals, rows, cols, self.totalNodes, 0, 0)
+        idx = indices[:triplet_num] if indices is not None else None
+        vals = triplet_values.reshape(-1, 9) if hasattr(triplet_values, "reshape") else triplet_values
+        self._engine.set_matrix_indexed(vals, row_ids, col_ids, idx, offset, self.totalNodes, 0, 0)
         self._engine.build()
+
+    def refresh_fixed_graph_bcoo(self, values, rows, cols, indices, offset, count):
+        """refresh_fixed_graph_bcoo (TraditionalMAS32Preconditioner.cu:229-234):
+        new values on the unchanged graph, BCOO structure and contacts; the
+        caller guarantees they are unchanged, as in the reference.  The values
+        are gathered by the same indices as setPreconditioner_bcoo's."""
+        vals = values.reshape(-1, 9) if hasattr(values, "reshape") else values
+        if indices is None:
+            self._engine.refresh_values(vals[:count])
+        else:
+            self._engine.refresh_values_indexed(vals, indices[:count])
+
+    def local_diagnostics_gpu(self):
+        """local_diagnostics_gpu (TraditionalMAS32Preconditioner.cu:182-183)."""
+        return self._engine.local_diagnostics()
+
+    def numerical_diagnostics(self, R=None):
+        """The local part of numerical_diagnostics (:2727-2887): the per-domain
+        SPD and inverse-residual summary (the per-level r.z sums of the last
+        apply are not restated)."""
+        return self._engine.local_diagnostics()
 
     def preconditioning(self, R, Z=None):
         return self._engine.apply_preconditioner(R, Z)

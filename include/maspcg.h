@@ -195,12 +195,51 @@ MASPCG_API maspcg_status maspcg_set_matrix_bcoo(maspcg_handle* h, const double* 
                                                 const int* cols, int n_blocks, int block_rows, int fem_offset_blocks,
                                                 int abd_body_count);
 
+/* The same from a sub-range of a larger triplet list, as the reference hands
+ * a subsystem's triplets to the MAS preconditioner: setPreconditioner_bcoo's
+ * (values, rows, cols, indices, offset, triplet_num)
+ * (TraditionalMAS32Preconditioner.cuh:102-108) with the indices of
+ * LocalPreconditioner::calculate_subsystem_bcoo_indices
+ * (linear_system/preconditioner/i_preconditioner.cu:54-89).  Block t < n_blocks
+ * is source triplet s = indices[t] (s = t when indices is NULL) with rows[s] -
+ * offset and cols[s] - offset; source_count is the length of the source
+ * arrays (9 * source_count values).  The gather runs on the device; host or
+ * device pointers.  An index at or past source_count makes the call return
+ * MASPCG_ERR_INVALID_ARGUMENT ("matrix block index out of range"). */
+MASPCG_API maspcg_status maspcg_set_matrix_bcoo_indexed(maspcg_handle* h, const double* values9_colmajor,
+                                                        const int* rows, const int* cols, long long source_count,
+                                                        const uint32_t* indices, int n_blocks, int offset,
+                                                        int block_rows, int fem_offset_blocks, int abd_body_count);
+
 /* Replaces LocalPreconditioner::assemble of TraditionalMAS32_Preconditioner /
  * MAS_Preconditioner (CEMAS16) / ABDPreconditioner / DiagPreconditioner
  * (traditional_mas32_preconditioner.cu:20-32, fem_mas_preconditioner.cu:18-31,
  * abd_preconditioner.cu:33-36, diag_preconditioner.cu:74-80): hierarchy for
  * the current contacts, domain matrices, inverses. */
 MASPCG_API maspcg_status maspcg_build_preconditioner(maspcg_handle* h);
+
+/* Replaces TraditionalMAS32Preconditioner::refresh_fixed_graph_bcoo
+ * (TraditionalMAS32Preconditioner.cuh:118-121, .cu:229-234; caller
+ * agipc/agipc_galerkin.cu:131): new values for the blocks of the last
+ * maspcg_set_matrix_bcoo, i.e. the same n_blocks triplets with the same rows
+ * and cols in the same order (values9 holds 9 * n_blocks doubles, host or
+ * device).  The BCSR structure, the internal row order and the MAS hierarchy
+ * of the last build are kept; the merged values, the domain matrices and
+ * their inverses, and the ABD / block-Jacobi inverses are recomputed, the
+ * same as maspcg_set_matrix_bcoo + maspcg_build_preconditioner would give for
+ * those values (bit for bit).  As in the reference, the caller guarantees
+ * that the structure, the graph and the contact set are unchanged; nothing
+ * checks it. */
+MASPCG_API maspcg_status maspcg_refresh_matrix_values(maspcg_handle* h, const double* values9_colmajor);
+
+/* The same with the values picked by index from a larger list, as the
+ * reference passes them (refresh_fixed_graph_bcoo(values, rows, cols,
+ * indices, offset, count)): block t takes values9[indices[t]] for the
+ * n_blocks triplets of the last set_matrix (the row and column indices are
+ * unchanged and not needed).  source_count bounds the indices; the gather
+ * runs on the device.  Host or device pointers. */
+MASPCG_API maspcg_status maspcg_refresh_matrix_values_indexed(maspcg_handle* h, const double* values9_colmajor,
+                                                             long long source_count, const uint32_t* indices);
 
 /* Replaces IterativeSolver::solve(x, b) -> iterations
  * (i_linear_system_solver.h:43-44, pcg_solver.cu:160-326).  b, x: 3*block_rows
@@ -267,6 +306,54 @@ MASPCG_API maspcg_status maspcg_get_domain_inverses(maspcg_handle* h, float* out
  * of the last build, before the zero-diagonal rule: recomputed on demand.
  * out: domains*P*9 (P as above). */
 MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* out);
+
+/* Per-domain numerical checks of the MAS preconditioner: the fields of
+ * LocalGpuCheck / check_local_matrices (TraditionalMAS32Preconditioner.cu:
+ * 76-147).  A = the assembled FP64 domain matrix with zero diagonal entries
+ * set to 1, M = the stored inverse decoded to FP32. */
+typedef struct {
+  int local_finite;                /* every entry of A finite */
+  int inverse_finite;              /* every entry of M finite */
+  int local_spd;                   /* FP64 Cholesky of A met only positive pivots */
+  int inverse_spd;                 /* M SPD: implied by local_spd and residual <= 1e-3, else its own Cholesky */
+  double minimum_local_diagonal;
+  double minimum_inverse_diagonal;
+  double inverse_residual;         /* ||A M - I||_F / sqrt(n), n = 3 * bank (0 unless both are finite) */
+} maspcg_domain_check;
+
+/* The summary gpu_local_checks builds from them (:149-180); passed = every
+ * domain SPD both ways, finite, and every inverse residual <= 1e-3.  First
+ * failures are domain indices, -1 if none. */
+typedef struct {
+  int matrix_count;
+  int local_spd_count;
+  int inverse_spd_count;
+  int first_local_spd_failure;
+  int first_inverse_spd_failure;
+  int nonfinite_local_count;
+  int nonfinite_inverse_count;
+  int passed;
+  double minimum_local_diagonal;
+  double minimum_inverse_diagonal;
+  double maximum_inverse_residual;
+} maspcg_diagnostics;
+
+/* The checks on the domains of the last build: local_diagnostics_gpu and the
+ * local part of numerical_diagnostics (TraditionalMAS32Preconditioner.cuh:
+ * 116-117, .cu:182-183, :2727-2887).  per_domain (host, one entry per domain,
+ * maspcg_get_info().domains) may be NULL; summary may be NULL.  The domain
+ * matrices are assembled again on the device for the check. */
+MASPCG_API maspcg_status maspcg_local_diagnostics(maspcg_handle* h, maspcg_domain_check* per_domain,
+                                                  maspcg_diagnostics* summary);
+
+/* The same checks on caller matrices: gpu_local_checks(local, inverse, count)
+ * (:149-180).  packed64: count domains of B(B+1)/2 packed upper FP64 3x3
+ * blocks (the layout of maspcg_get_domain_matrices), inverse32: the same in
+ * FP32 (maspcg_get_domain_inverses); bank 32 or 16.  Host or device
+ * pointers; per_domain / summary on the host, may be NULL.  Any handle. */
+MASPCG_API maspcg_status maspcg_check_local_matrices(maspcg_handle* h, int count, int bank, const double* packed64,
+                                                     const float* inverse32, maspcg_domain_check* per_domain,
+                                                     maspcg_diagnostics* summary);
 
 /* Benchmark introspection (no counterpart in the reference): run one stage
  * `repeats` times on the handle's stream, each run after reading a 256 MB
