@@ -38,6 +38,8 @@ FLAG_APPLY_STAGED2 = 2
 FLAG_APPLY_DIRECT = 4
 FLAG_SEQUENTIAL_COARSE = 8
 FLAG_FUSED_HEAD = 16
+FLAG_SPMV_DIRECT = 32
+FLAG_TWO_REDUCTION = 64
 
 INV_FP32 = 0
 INV_BF16 = 1
@@ -57,7 +59,7 @@ EXPORTS = (
     "maspcg_galerkin_restrict", "maspcg_galerkin_prolong", "maspcg_adjust_contact_triplets",
     "maspcg_zero_boundary_triplets", "maspcg_spmv_working", "maspcg_refresh_matrix_values",
     "maspcg_set_matrix_bcoo_indexed", "maspcg_local_diagnostics", "maspcg_check_local_matrices",
-    "maspcg_refresh_matrix_values_indexed",
+    "maspcg_refresh_matrix_values_indexed", "maspcg_set_wait_test_hooks", "maspcg_element_modulus_gradient",
 )
 
 RESIDUAL_MAX_VECTORS = 8
@@ -167,6 +169,8 @@ def load():
         "maspcg_spmv_working": (I, [H, P, P]),
         "maspcg_refresh_matrix_values": (I, [H, P]),
         "maspcg_refresh_matrix_values_indexed": (I, [H, P, ctypes.c_longlong, P]),
+        "maspcg_set_wait_test_hooks": (I, [H, ctypes.c_longlong, I]),
+        "maspcg_element_modulus_gradient": (I, [H, I, I, P, P, P, P, P, P, P]),
         "maspcg_set_matrix_bcoo_indexed": (I, [H, P, P, P, ctypes.c_longlong, P, I, I, I, I, I]),
         "maspcg_local_diagnostics": (I, [H, P, ctypes.POINTER(Diagnostics)]),
         "maspcg_check_local_matrices": (I, [H, I, I, P, P, P, ctypes.POINTER(Diagnostics)]),

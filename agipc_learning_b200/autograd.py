@@ -11,14 +11,20 @@ libmaspcg.  Its backward:
   dL/dval = maspcg_bcoo_gradient(lam, x): -(lam_r x_c^T + x_r lam_c^T) per
             off-diagonal block, -lam_r x_r^T per diagonal block
 
-x is kept from the forward pass (no Krylov history is stored).  The chain to
-per-tet Young's modulus uses the fact that a tet's Hessian blocks scale with
-its modulus (stable Neo-Hookean with the Lame pair linear in E, and the PSD
-projection commutes with a positive scale): dL/dE_t = sum over the tet's
-element blocks k of <dL/dval_k, val_k> / E_t.
+x is kept from the forward pass (no Krylov history is stored).
 
-Torch is plumbing here: device memory and the autograd graph.  All
-arithmetic runs in the library's kernels.
+`newton_solve_modulus(E_tet, vals, b, solver, rows, cols, nb)` is the same
+solve differentiable in the per-tet Young's modulus: a tet's Hessian blocks
+scale with its modulus (stable Neo-Hookean with the Lame pair linear in E,
+and the PSD projection commutes with a positive scale), so dL/dE_t = sum
+over the tet's element blocks k of <dL/dval_k, val_k> / E_t.  Its backward
+runs the adjoint solve and maspcg_element_modulus_gradient, one kernel that
+forms the outer products and chains them to E without storing dL/dval.
+
+The solves, the adjoint outer products and the chain to E run in the
+library's kernels; torch holds the device memory and the autograd graph.
+`scale_element_blocks` and `modulus_gradient` are torch helpers for tests and
+callers that build perturbed systems or already hold dL/dval.
 """
 from __future__ import annotations
 
@@ -69,6 +75,47 @@ class NewtonSolveFunction(torch.autograd.Function):
         return gvals, lam, None, None, None, None, None, None
 
 
+class NewtonSolveModulusFunction(torch.autograd.Function):
+    """x(E, b) = A(E)^-1 b with the first blocks_per_tet * ntet blocks of
+    `vals` the element blocks at the moduli E (tet order)."""
+
+    @staticmethod
+    def forward(ctx, E_tet, b, vals, solver: MasPcg, rows, cols, nb: int, blocks_per_tet: int = 10,
+                fem_offset: int = 0, abd_bodies: int = 0):
+        x = NewtonSolveFunction.forward(ctx, vals, b, solver, rows, cols, nb, fem_offset, abd_bodies)
+        ctx.bpt = blocks_per_tet
+        ctx.E = E_tet
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        vals, rows, cols, x = ctx.saved_tensors
+        solver = ctx.solver
+        if solver.matrix_version != ctx.version:
+            solver.set_matrix(vals, rows, cols, *ctx.dims)
+            solver.build()
+        gx = gx.contiguous().to(torch.float64)
+        lam = torch.empty_like(gx)
+        _, res = solver.solve(gx, lam)
+        if res["status_name"] != "converged":
+            raise RuntimeError(f"adjoint solve did not converge: {res}")
+        E = ctx.E.contiguous().to(torch.float64)
+        gE = torch.empty_like(E)
+        solver._ck(solver.lib.maspcg_element_modulus_gradient(solver.h, int(E.shape[0]), int(ctx.bpt), _ptr(rows),
+                                                               _ptr(cols), _ptr(vals), _ptr(lam), _ptr(x), _ptr(E),
+                                                               _ptr(gE)))
+        return gE, lam, None, None, None, None, None, None, None, None
+
+
+def newton_solve_modulus(E_tet: torch.Tensor, b: torch.Tensor, vals: torch.Tensor, solver: MasPcg,
+                         rows: torch.Tensor, cols: torch.Tensor, nb: int, blocks_per_tet: int = 10,
+                         fem_offset: int = 0, abd_bodies: int = 0) -> torch.Tensor:
+    """x = A(E)^-1 b, differentiable in the per-tet moduli E_tet and in b;
+    `vals` are the triplet values at E_tet (see the module docstring)."""
+    return NewtonSolveModulusFunction.apply(E_tet, b, vals, solver, rows, cols, nb, blocks_per_tet, fem_offset,
+                                            abd_bodies)
+
+
 def newton_solve(vals: torch.Tensor, b: torch.Tensor, solver: MasPcg, rows: torch.Tensor, cols: torch.Tensor,
                  nb: int, fem_offset: int = 0, abd_bodies: int = 0) -> torch.Tensor:
     """x = A^-1 b, differentiable in `vals` and `b` (see the module docstring)."""
@@ -94,4 +141,5 @@ def scale_element_blocks(vals: torch.Tensor, factor: torch.Tensor, blocks_per_te
     return out
 
 
-__all__ = ["NewtonSolveFunction", "newton_solve", "modulus_gradient", "scale_element_blocks", "np"]
+__all__ = ["NewtonSolveFunction", "NewtonSolveModulusFunction", "newton_solve", "newton_solve_modulus",
+           "modulus_gradient", "scale_element_blocks", "np"]

@@ -42,7 +42,52 @@ __global__ void __launch_bounds__(kAdjTpb) k_bcoo_gradient(const int* __restrict
   for (int e = 0; e < 9; ++e) o[e] = g[e];
 }
 
+// The same outer products chained through the element blocks to each tet's
+// Young's modulus: a tet's blocks are linear in its modulus E_t (the Lame pair
+// is linear in E, and the PSD projection commutes with a positive scale), so
+// dL/dE_t = sum over its blocks k of <G_k, V_k> / E_t with G_k as above; the
+// G_k are never stored.  Blocks [bpt t, bpt t + bpt) of the list are tet t's.
+// One warp per tet: lanes take the blocks, a shuffle sum, lane 0 writes.
+__global__ void __launch_bounds__(kAdjTpb) k_modulus_gradient(const int* __restrict__ rows,
+                                                             const int* __restrict__ cols,
+                                                             const double* __restrict__ vals, int ntet, int bpt,
+                                                             const double* __restrict__ lam,
+                                                             const double* __restrict__ x,
+                                                             const double* __restrict__ E, double* gE)
+{
+  const int t = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (t >= ntet) return;  // whole warp
+  double acc = 0.0;
+  for (int q = lane; q < bpt; q += 32) {
+    const size_t k = (size_t)t * bpt + q;
+    const int r = rows[k], c = cols[k];
+    const double* V = vals + 9 * k;  // column-major: element (i, j) at i + 3j
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        double g = lam[3 * (size_t)r + i] * x[3 * (size_t)c + j];
+        if (r != c) g += x[3 * (size_t)r + i] * lam[3 * (size_t)c + j];
+        s -= g * V[i + 3 * j];
+      }
+    acc += s;
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) gE[t] = acc / E[t];
+}
+
 }  // namespace
+
+void modulus_gradient(maspcg_handle* h, const int* rows, const int* cols, const double* vals, int ntet, int bpt,
+                      const double* lam, const double* x, const double* E, double* gE)
+{
+  if (ntet <= 0) return;
+  k_modulus_gradient<<<ceil_div(32LL * ntet, kAdjTpb), kAdjTpb, 0, h->stream>>>(rows, cols, vals, ntet, bpt, lam, x, E,
+                                                                              gE);
+  MLAUNCHED(h);
+  MCK(cudaGetLastError());
+}
 
 void bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n, const double* lam, const double* x,
                    double* grad)

@@ -155,6 +155,12 @@ void alloc_vectors(maspcg_handle* h)
   const int parts = 32 * h->sm_count + 64;
   h->partial.resize(parts);
   h->partial_rz.resize(parts);
+  h->partial_rr.resize(parts);
+  if (h->cfg.precision != MASPCG_PREC_REFERENCE) {
+    for (auto* b : {&h->cg_r2, &h->cg_s0, &h->cg_s1, &h->cg_p}) b->resize(n * 4);
+    h->cg_z0.resize(4 * (size_t)h->nb_int * 4, 32);
+    h->cg_pc.resize(4 * (size_t)h->nb_int * 4, 32);
+  }
 }
 
 }  // namespace
@@ -307,7 +313,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_MAS16 || c.preconditioner == MASPCG_PRECOND_NONE) ||
-      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~31) != 0 ||
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~127) != 0 ||
       ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_DIRECT))) {
     g_create_error = "invalid configuration";
     return MASPCG_ERR_INVALID_ARGUMENT;
@@ -338,6 +344,8 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     // rows after the coarse correction is added to z
     h->overlap_coarse = (c.flags & MASPCG_FLAG_SEQUENTIAL_COARSE) == 0 && c.precision != MASPCG_PREC_REFERENCE;
     h->fused_head = (c.flags & MASPCG_FLAG_FUSED_HEAD) != 0;
+    h->spmv_staged = (c.flags & MASPCG_FLAG_SPMV_DIRECT) == 0;
+    h->use_cg = (c.flags & MASPCG_FLAG_TWO_REDUCTION) == 0;
     MCK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
     MCK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     MCK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
@@ -884,6 +892,16 @@ MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repe
   });
 }
 
+MASPCG_API maspcg_status maspcg_set_wait_test_hooks(maspcg_handle* h, long long barrier_limit, int barrier_extra)
+{
+  return guard(h, [&] {
+    MREQ(barrier_limit >= 1 && barrier_extra >= 0 && barrier_extra <= 1024, MASPCG_ERR_INVALID_ARGUMENT,
+         "barrier_limit >= 1, 0 <= barrier_extra <= 1024");
+    h->barrier_limit = barrier_limit;
+    h->barrier_extra = barrier_extra;
+  });
+}
+
 MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n_blocks,
                                               const double* lam, const double* x, double* grad9)
 {
@@ -912,6 +930,41 @@ MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows,
       MCK(cudaMemcpyAsync(grad9, h->adj_grad.get(), sizeof(double) * 9 * (size_t)n_blocks, cudaMemcpyDeviceToHost,
                           h->stream));
     }
+    MCK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+MASPCG_API maspcg_status maspcg_element_modulus_gradient(maspcg_handle* h, int n_tets, int blocks_per_tet,
+                                                         const int* rows, const int* cols, const double* values9,
+                                                         const double* lam, const double* x, const double* youngs,
+                                                         double* grad_youngs)
+{
+  return guard(h, [&] {
+    MREQ(h->has_matrix, MASPCG_ERR_NOT_READY, "set_matrix_bcoo first");
+    MREQ(n_tets >= 0 && blocks_per_tet >= 1 && blocks_per_tet <= 64, MASPCG_ERR_INVALID_ARGUMENT,
+         "n_tets >= 0, 1 <= blocks_per_tet <= 64");
+    if (n_tets == 0) return;
+    MREQ(rows && cols && values9 && lam && x && youngs && grad_youngs, MASPCG_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t nblk = (size_t)n_tets * blocks_per_tet;
+    MREQ(nblk <= (size_t)0x7fffffff, MASPCG_ERR_CAPACITY, "too many blocks");
+    {
+      const std::vector<int> hr = host_copy(h, rows, nblk), hc = host_copy(h, cols, nblk);
+      for (size_t t = 0; t < nblk; ++t)
+        MREQ(hr[t] >= 0 && hr[t] < h->nb && hc[t] >= 0 && hc[t] < h->nb, MASPCG_ERR_INVALID_ARGUMENT,
+             "block index outside the system");
+    }
+    const size_t n = 3 * (size_t)h->nb;
+    const int* r = device_in(h, rows, nblk, h->adj_rows);
+    const int* c = device_in(h, cols, nblk, h->adj_cols);
+    DBuf<double> vstage, estage;
+    const double* v = device_in(h, values9, 9 * nblk, vstage);
+    const double* l = device_in(h, lam, n, h->adj_lam);
+    const double* xv = device_in(h, x, n, h->adj_x);
+    const double* e = device_in(h, youngs, (size_t)n_tets, estage);
+    DBuf<double> gstage;
+    double* g = device_out(grad_youngs, (size_t)n_tets, gstage);
+    maspcg::modulus_gradient(h, r, c, v, n_tets, blocks_per_tet, l, xv, e, g);
+    copy_back(h, grad_youngs, (const double*)g, (size_t)n_tets);
     MCK(cudaStreamSynchronize(h->stream));
   });
 }

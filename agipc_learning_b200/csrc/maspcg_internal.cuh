@@ -131,8 +131,11 @@ struct PcgScalars {
   int gate;
   double tol;
   double rz_part[2];  // r.z of the level-0 apply (0) and of the coarse levels (1) when they run concurrently
-  unsigned tickets[8];
+  unsigned tickets[10];
   unsigned barrier_gen;  // generation of the grid barrier of the fused iteration kernel
+  int cg_cur;            // single-reduction recurrence: which of the two r / s buffers holds the current vectors
+  long long barrier_limit;  // spins a grid-barrier wait may take before it gives up (maspcg_set_wait_test_hooks)
+  int barrier_extra;        // arrivals a grid barrier expects beyond the grid (test hook: > 0 never completes)
 };
 
 constexpr int kNeedTrue = 16;  // MIXED: recursive gate met or period end; true residual pending
@@ -214,12 +217,11 @@ struct maspcg_handle {
   // FP32 matrix of the iteration (FP32 / MIXED precision) in the sliced
   // jagged-diagonal layout of spmv_jds.cuh, and the rows it leaves to the
   // FP64 row path
-  maspcg::DBuf<int> jds_base, jds_cbase, jds_coff, jds_xrows, jds_xflag, jds_xpos, jds_len;
-  maspcg::DBuf<unsigned char> jds_perm;
-  maspcg::DBuf<float4> jds_a, jds_b;
-  maspcg::DBuf<float2> jds_c;
+  maspcg::DBuf<int> jds_hdr, jds_xrows, jds_xflag, jds_xpos, jds_len;
+  maspcg::DBuf<long long> jds_srec, jds_bytes;
+  maspcg::DBuf<unsigned char> jds_perm, jds_data;
   int jds_slices = 0, jds_nx = 0;
-  long long jds_entries = 0;
+  long long jds_data_bytes = 0;
   maspcg::DBuf<unsigned long long> keys, keys_sorted;
   maspcg::DBuf<int> kv, kv_sorted, seg_head, seg_start, row_count;
   maspcg::DBuf<double> in_vals;
@@ -245,7 +247,11 @@ struct maspcg_handle {
   maspcg::DBuf<unsigned char> vx, vr, vz, vap;      // vectors in the working precision, 3 per block row
   maspcg::DBuf<unsigned char> vp4;                  // search direction, padded to 4 per block row
   maspcg::DBuf<double> b64, x64, r64;               // FP64: rhs, x (hi), residual scratch
-  maspcg::DBuf<double> partial, partial_rz;
+  maspcg::DBuf<double> partial, partial_rz, partial_rr;
+  // single-reduction recurrence (FP32 / MIXED with MAS32): the second r
+  // buffer, the two s buffers, p, and the padded level-0 (z0) and coarse (pc)
+  // parts of z; vz holds z, vap holds w = A z
+  maspcg::DBuf<unsigned char> cg_r2, cg_s0, cg_s1, cg_p, cg_z0, cg_pc;
   maspcg::DBuf<maspcg::PcgScalars> scal;
   maspcg::PcgScalars* h_scal = nullptr;  // pinned mirror
   maspcg::DBuf<double> io_a, io_b;       // staging for host pointers / permutations
@@ -276,6 +282,10 @@ struct maspcg_handle {
   bool vals_pending = false;      // set_matrix_bcoo: host values still copying on side_stream (ev_join)
   bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
   int apply_variant = 2;          // 16-bit level-0 apply: 0 direct loads, 1 TMA-staged x2 buffers, 2 TMA-staged x1
+  bool spmv_staged = true;        // FP32 SpMV records staged by bulk copies (off: MASPCG_FLAG_SPMV_DIRECT)
+  bool use_cg = true;             // single-reduction recurrence where it applies (off: MASPCG_FLAG_TWO_REDUCTION)
+  long long barrier_limit = 1ll << 24;  // grid-barrier wait bound (spins of 64 ns sleeps)
+  int barrier_extra = 0;                // test hook: extra arrivals a grid barrier waits for
 };
 
 namespace maspcg {
@@ -311,6 +321,8 @@ void spmv_working(maspcg_handle* h, const double* x_int, double* y_int);  // int
 // adjoint.cu (device pointers, caller's row order)
 void bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n, const double* lam, const double* x,
                    double* grad);
+void modulus_gradient(maspcg_handle* h, const int* rows, const int* cols, const double* vals, int ntet, int bpt,
+                      const double* lam, const double* x, const double* E, double* gE);
 
 // assemble.cu (device pointers; returns the unique count / the type counts)
 int convert_bcoo(maspcg_handle* h, const int* rows, const int* cols, const double* vals, int n, int* rows_out,

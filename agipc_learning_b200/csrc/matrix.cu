@@ -7,6 +7,8 @@
 // differs in what it produces: both triangles (the symmetric SpMV of
 // spmv.cu:28-53 scatters B^T with atomics; a row-owned BCSR needs none) and
 // rows renumbered into the MAS partition order.
+#include <algorithm>
+
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -255,9 +257,11 @@ __device__ __forceinline__ int jds_row_len(const int* __restrict__ rowptr, const
 }
 
 // One warp per slice: rank the rows by length (longest first, ties by row),
-// the rank -> row map, and the slice's entry count and width + 1.
+// the rank -> row map, the slice's header (entries rounded up to even, the
+// width, and the column offsets coff[k] = sum over its rows of min(length,
+// k)), and the record's size in bytes.
 __global__ void k_jds_slices(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows, int slices,
-                             unsigned char* perm, int* entries, int* ncols)
+                             unsigned char* perm, int* hdr, long long* bytes)
 {
   const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (s >= slices) return;  // whole warp
@@ -272,33 +276,25 @@ __global__ void k_jds_slices(const int* __restrict__ rowptr, const int* __restri
   perm[32 * (size_t)s + rank] = (unsigned char)(lane | (skip ? 0x80 : 0));
   const int width = (int)__reduce_max_sync(kFull, (unsigned)len);
   const int total = (int)__reduce_add_sync(kFull, (unsigned)len);
-  if (lane == 0) {
-    entries[s] = total;
-    ncols[s] = width + 1;
-  }
-}
-
-// Column offsets of a slice: entries in the columns before column k =
-// sum over its rows of min(length, k).
-__global__ void k_jds_coff(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows, int slices,
-                           const int* __restrict__ cbase, int* coff)
-{
-  const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (s >= slices) return;
-  const int len = jds_row_len(rowptr, xflag, nrows, s, lane);
-  const int c0 = cbase[s], width = cbase[s + 1] - c0 - 1;
-  for (int k = 0; k <= width; ++k) {
+  const int ep = total + (total & 1);
+  int* hd = hdr + (size_t)kJdsHeader * s;
+  for (int k = 0; k < kJdsHeader - 2; ++k) {
     const int v = (int)__reduce_add_sync(kFull, (unsigned)min(len, k));
-    if (lane == 0) coff[c0 + k] = v;
+    if (lane == 0) hd[2 + k] = k <= width ? v : total;
+  }
+  if (lane == 0) {
+    hd[0] = ep;
+    hd[1] = width;
+    bytes[s] = 40LL * ep;
   }
 }
 
 // One warp per slice, lane = rank: the row's blocks in column order into the
-// three planes, rounded to FP32.
+// slice record, rounded to FP32.
 __global__ void k_jds_fill(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                           const double* __restrict__ val64, const int* __restrict__ xflag, int nrows, int slices,
-                           const int* __restrict__ base, const int* __restrict__ cbase, const int* __restrict__ coff,
-                           const unsigned char* __restrict__ perm, float4* pa, float4* pb, float2* pc)
+                           const double* __restrict__ val64, int slices, const int* __restrict__ hdr,
+                           const long long* __restrict__ srec, const unsigned char* __restrict__ perm,
+                           unsigned char* data)
 {
   const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (s >= slices) return;
@@ -306,10 +302,15 @@ __global__ void k_jds_fill(const int* __restrict__ rowptr, const int* __restrict
   if (pm & 0x80u) return;
   const int r = 32 * s + (int)(pm & 31u);
   const int rs = rowptr[r], len = rowptr[r + 1] - rs;
-  const int b0 = base[s], c0 = cbase[s];
+  const int* hd = hdr + (size_t)kJdsHeader * s;
+  const int ep = hd[0];
+  unsigned char* rec = data + srec[s];
+  float4* pa = reinterpret_cast<float4*>(rec);
+  float4* pb = reinterpret_cast<float4*>(rec + 16 * (size_t)ep);
+  float2* pc = reinterpret_cast<float2*>(rec + 32 * (size_t)ep);
   for (int k = 0; k < len; ++k) {
     const int t = rs + k;
-    const size_t e = (size_t)b0 + coff[c0 + k] + lane;
+    const int e = hd[2 + k] + lane;
     const double* m = val64 + 9 * (size_t)t;
     pa[e] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
     pb[e] = make_float4((float)m[4], (float)m[5], (float)m[6], (float)m[7]);
@@ -429,57 +430,46 @@ void build_jds(maspcg_handle* h)
   h->jds_xflag.resize(nrows + 1);
   h->jds_xpos.resize(nrows + 1);
   h->jds_perm.resize(32 * (size_t)slices);
-  h->jds_base.resize(slices + 1);
-  h->jds_cbase.resize(slices + 1);
-  h->jds_len.resize(2 * (size_t)slices + 2);  // entries and width + 1 per slice
-  int* entries = h->jds_len.get();
-  int* ncols = h->jds_len.get() + slices + 1;
+  h->jds_hdr.resize((size_t)kJdsHeader * slices);
+  h->jds_srec.resize(slices + 1);
+  h->jds_bytes.resize(slices + 1);
   MCK(cudaMemsetAsync(h->jds_xflag.get() + nrows, 0, sizeof(int), st));
-  MCK(cudaMemsetAsync(entries + slices, 0, sizeof(int), st));
-  MCK(cudaMemsetAsync(ncols + slices, 0, sizeof(int), st));
+  MCK(cudaMemsetAsync(h->jds_bytes.get() + slices, 0, sizeof(long long), st));
   k_jds_flags<<<ceil_div(nrows, kTpb), kTpb, 0, st>>>(h->rowptr.get(), nrows, n64, h->jds_xflag.get());
   MLAUNCHED(h);
   const int wgrid = ceil_div(32LL * slices, kTpb);
-  k_jds_slices<<<wgrid, kTpb, 0, st>>>(h->rowptr.get(), h->jds_xflag.get(), nrows, slices, h->jds_perm.get(), entries,
-                                       ncols);
+  k_jds_slices<<<wgrid, kTpb, 0, st>>>(h->rowptr.get(), h->jds_xflag.get(), nrows, slices, h->jds_perm.get(),
+                                       h->jds_hdr.get(), h->jds_bytes.get());
   MLAUNCHED(h);
-  size_t need = 0, b = 0;
-  MCK(cub::DeviceScan::ExclusiveSum(nullptr, b, (const int*)nullptr, (int*)nullptr, std::max(nrows, slices) + 1));
-  need = b;
-  h->cub_tmp.resize(std::max(need, h->cub_tmp.n));
-  b = h->cub_tmp.cap;
+  size_t b1 = 0, b2 = 0;
+  MCK(cub::DeviceScan::ExclusiveSum(nullptr, b1, (const int*)nullptr, (int*)nullptr, nrows + 1));
+  MCK(cub::DeviceScan::ExclusiveSum(nullptr, b2, (const long long*)nullptr, (long long*)nullptr, slices + 1));
+  h->cub_tmp.resize(std::max({b1, b2, h->cub_tmp.n}));
+  size_t b = h->cub_tmp.cap;
   MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, h->jds_xflag.get(), h->jds_xpos.get(), nrows + 1, st));
   b = h->cub_tmp.cap;
-  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, entries, h->jds_base.get(), slices + 1, st));
-  b = h->cub_tmp.cap;
-  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, ncols, h->jds_cbase.get(), slices + 1, st));
-  int tail[3] = {0, 0, 0};
-  MCK(cudaMemcpyAsync(&tail[0], h->jds_xpos.get() + nrows, sizeof(int), cudaMemcpyDeviceToHost, st));
-  MCK(cudaMemcpyAsync(&tail[1], h->jds_base.get() + slices, sizeof(int), cudaMemcpyDeviceToHost, st));
-  MCK(cudaMemcpyAsync(&tail[2], h->jds_cbase.get() + slices, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, h->jds_bytes.get(), h->jds_srec.get(), slices + 1, st));
+  int nx = 0;
+  long long total = 0;
+  MCK(cudaMemcpyAsync(&nx, h->jds_xpos.get() + nrows, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaMemcpyAsync(&total, h->jds_srec.get() + slices, sizeof(long long), cudaMemcpyDeviceToHost, st));
   MCK(cudaStreamSynchronize(st));
-  h->jds_nx = tail[0];
-  h->jds_entries = tail[1];
-  h->jds_xrows.resize(std::max(tail[0], 1));
-  h->jds_coff.resize(std::max(tail[2], 1));
-  h->jds_a.resize(std::max<size_t>(tail[1], 1));
-  h->jds_b.resize(std::max<size_t>(tail[1], 1));
-  h->jds_c.resize(std::max<size_t>(tail[1], 1));
+  h->jds_nx = nx;
+  h->jds_data_bytes = total;
+  h->jds_xrows.resize(std::max(nx, 1));
+  h->jds_data.resize(std::max<long long>(total, 16));
   k_jds_xrows<<<ceil_div(nrows, kTpb), kTpb, 0, st>>>(h->jds_xflag.get(), h->jds_xpos.get(), nrows,
                                                       h->jds_xrows.get());
-  MLAUNCHED(h);
-  k_jds_coff<<<wgrid, kTpb, 0, st>>>(h->rowptr.get(), h->jds_xflag.get(), nrows, slices, h->jds_cbase.get(),
-                                     h->jds_coff.get());
   MLAUNCHED(h);
   fill_jds(h);
 }
 
 void fill_jds(maspcg_handle* h)
 {
-  const int nrows = h->nb_int, slices = h->jds_slices;
-  k_jds_fill<<<ceil_div(32LL * slices, kTpb), kTpb, 0, h->stream>>>(
-      h->rowptr.get(), h->colidx.get(), h->val64.get(), h->jds_xflag.get(), nrows, slices, h->jds_base.get(),
-      h->jds_cbase.get(), h->jds_coff.get(), h->jds_perm.get(), h->jds_a.get(), h->jds_b.get(), h->jds_c.get());
+  const int slices = h->jds_slices;
+  k_jds_fill<<<ceil_div(32LL * slices, kTpb), kTpb, 0, h->stream>>>(h->rowptr.get(), h->colidx.get(), h->val64.get(),
+                                                                    slices, h->jds_hdr.get(), h->jds_srec.get(),
+                                                                    h->jds_perm.get(), h->jds_data.get());
   MLAUNCHED(h);
   MCK(cudaGetLastError());
 }

@@ -32,6 +32,9 @@ void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_bas
 
 template <typename Tv, typename Tacc>
 void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant);
+template <typename Tacc>
+void mas_apply_cg(maspcg_handle* h, const CgArgs& cg, float* pc, Tacc* partial, double* partial_rr, int part_base,
+                  int total_parts, int mode, int grid0, PcgScalars* s, bool overlap);
 void launch_factor(maspcg_handle* h, double* assembled_out);
 int mas_level0_grid(maspcg_handle* h);
 template <typename Tv, typename Tacc>
@@ -251,31 +254,68 @@ __global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, c
 }
 
 // FP32 matrix (FP32 / MIXED precision): the sliced jagged-diagonal layout,
-// with the affine-body and long rows from the FP64 BCSR.
-template <typename Tacc>
+// with the affine-body and long rows from the FP64 BCSR.  Direct form: the
+// records are read from global memory.  kCg: the single-reduction
+// recurrence's SpMV w = A z with z gathered as z0 + pc (level-0 and coarse
+// parts of the apply), z written out, and alpha from delta = z.w.
+template <typename Tacc, bool kCg>
 __device__ __forceinline__ Tacc spmv_fp32(const JdsArgs& j, const int* __restrict__ rowptr,
                                           const int* __restrict__ colidx, const double* __restrict__ val64,
-                                          const float* __restrict__ p4, float* ap)
+                                          const SpmvVec& v)
 {
   Tacc dot = 0;
-  if (j.nx > 0) dot = spmv_rows_listed<Tacc, 8>(rowptr, colidx, val64, j.xrows, j.nx, p4, ap);
-  return dot + spmv_jds<Tacc, kJdsSlicesPerWarp, kJdsColumnsPerStep>(j, p4, ap);
+  if (j.nx > 0) dot = spmv_rows_listed<Tacc, 8, kCg>(rowptr, colidx, val64, j.xrows, j.nx, v);
+  return dot + spmv_jds_direct<Tacc, kJdsColumnsPerStep, kCg>(j, v);
 }
 
-template <typename Tacc>
+__device__ __forceinline__ void spmv_end(PcgScalars* s, double total, bool cg)
+{
+  if (cg)
+    cg_alpha(s, total);
+  else
+    spmv_finish(s, total);
+}
+
+template <typename Tacc, bool kCg>
 __global__ void __launch_bounds__(kTpb) k_spmv_jds(JdsArgs j, const int* __restrict__ rowptr,
                                                     const int* __restrict__ colidx, const double* __restrict__ val64,
-                                                    const float* __restrict__ p4, float* ap, Tacc* partial,
-                                                    PcgScalars* s)
+                                                    SpmvVec v, Tacc* partial, PcgScalars* s)
 {
   pdl_wait();
   if (!running(s)) return;
-  const Tacc dot = spmv_fp32<Tacc>(j, rowptr, colidx, val64, p4, ap);
+  const Tacc dot = spmv_fp32<Tacc, kCg>(j, rowptr, colidx, val64, v);
   pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0)
-    spmv_finish(s, (double)total);
+    spmv_end(s, (double)total, kCg);
+}
+
+// Staged form: slice records bulk-copied into two shared-memory slots per
+// warp ahead of the arithmetic (spmv_jds_staged).  A wait that expires
+// records the error, stops the solve (status non-finite) and the whole CTA
+// leaves.
+template <typename Tacc, bool kCg>
+__global__ void __launch_bounds__(kJdsWarps * 32, 1) k_spmv_jds_staged(JdsArgs j, const int* __restrict__ rowptr,
+                                                                       const int* __restrict__ colidx,
+                                                                       const double* __restrict__ val64, SpmvVec v,
+                                                                       Tacc* partial, PcgScalars* s, int* err)
+{
+  extern __shared__ __align__(128) unsigned char jds_slots[];
+  __shared__ __align__(8) uint64_t jds_bars[2 * kJdsWarps];
+  pdl_wait();
+  if (!running(s)) return;
+  Tacc dot = 0;
+  if (j.nx > 0) dot = spmv_rows_listed<Tacc, 8, kCg>(rowptr, colidx, val64, j.xrows, j.nx, v);
+  const bool ok = spmv_jds_staged<Tacc, kJdsColumnsPerStep, kCg>(j, v, jds_slots, jds_bars, err, dot);
+  if (!ok && (threadIdx.x & 31) == 0) s->status = MASPCG_SOLVE_NONFINITE;
+  if (__syncthreads_or(!ok)) return;  // the whole CTA leaves together
+  pdl_trigger();
+  Tacc total = 0;
+  if (grid_finish<Tacc, kJdsWarps * 32>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x,
+                                        total) &&
+      threadIdx.x == 0)
+    spmv_end(s, (double)total, kCg);
 }
 
 // x += alpha p, r -= alpha Ap for the entries this thread strides over;
@@ -317,28 +357,6 @@ __device__ __forceinline__ Tacc update_xr_rows(Tv* x, Tv* r, const Tv* __restric
   return acc;
 }
 
-// Last block of the x/r update: r.r and the stopping gate.  MIXED: x is the
-// FP32 correction since the last replacement and a met gate asks for the
-// FP64 true residual instead of stopping.
-__device__ __forceinline__ void xr_finish(PcgScalars* s, double rr, int mixed)
-{
-  s->rr = rr;
-  if (!isfinite(rr)) {
-    s->status = MASPCG_SOLVE_NONFINITE;
-    s->iterations = s->k;
-    return;
-  }
-  const bool conv = (s->gate == MASPCG_GATE_RZ) ? (fabs(s->rz) <= s->tol * s->rz0) : (rr <= s->tol * s->tol * s->bb);
-  if (conv) {
-    if (mixed) {
-      s->status = kNeedTrue;
-    } else {
-      s->status = MASPCG_SOLVE_CONVERGED;
-      s->iterations = s->k;
-    }
-  }
-}
-
 template <typename Tv, typename Tacc>
 __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __restrict__ p4, const Tv* __restrict__ ap,
                                                      int nrows, int mixed, Tacc* partial, PcgScalars* s)
@@ -350,7 +368,7 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
   Tacc total = 0;
   if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
       threadIdx.x == 0)
-    xr_finish(s, (double)total, mixed);
+    gate_check(s, (double)total, mixed);
 }
 
 // The iteration head as one cooperative kernel (every CTA resident): the p
@@ -369,7 +387,7 @@ __global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, JdsArgs j,
   if (!grid_barrier(s, err)) return;
   Tacc dot;
   if constexpr (std::is_same<Tm, float>::value)
-    dot = spmv_fp32<Tacc>(j, rowptr, colidx, val64, p4, ap);
+    dot = spmv_fp32<Tacc, false>(j, rowptr, colidx, val64, SpmvVec{p4, nullptr, ap, nullptr});
   else
     dot = spmv_rows<double, double, double, false, LPR>(rowptr, colidx, val64, p4, ap, 0, nrows);
   Tacc total = 0;
@@ -384,7 +402,7 @@ __global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, JdsArgs j,
   total = 0;
   if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
       threadIdx.x == 0)
-    xr_finish(s, (double)total, mixed);
+    gate_check(s, (double)total, mixed);
 }
 
 // MIXED: fold the FP32 correction into the FP64 iterate.
@@ -403,11 +421,12 @@ __global__ void __launch_bounds__(kTpb) k_fold_x(double* xhi, float* xlo, int n,
 template <int LPR>
 __global__ void __launch_bounds__(kTpb) k_true_residual(const int* __restrict__ rowptr, const int* __restrict__ colidx,
                                                          const double* __restrict__ val, const double* __restrict__ xhi,
-                                                         const double* __restrict__ b, float* r32, int nrows,
-                                                         double* partial, PcgScalars* s)
+                                                         const double* __restrict__ b, float* r32, float* r32b,
+                                                         int nrows, double* partial, PcgScalars* s)
 {
   pdl_wait();
   if (!(s->status == MASPCG_SOLVE_RUNNING || s->status == kNeedTrue)) return;
+  if (r32b && s->cg_cur) r32 = r32b;  // single-reduction recurrence: the buffer holding the current r
   const int groups_per_block = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
   double acc2 = 0.0;
@@ -552,6 +571,100 @@ __global__ void __launch_bounds__(kTpb) k_l2_evict(const uint4* __restrict__ p, 
   if (acc == 0xffffffffu) *sink = acc;
 }
 
+// Single-reduction recurrence, rows outside the MAS range: the iteration's
+// update of the row (cg.update), then its preconditioner (affine bodies:
+// 12x12 inverse; block-Jacobi rows: 3x3 inverse; else identity) into z0;
+// per-CTA r.z and r.r partials (the level-0 apply completes both).
+template <typename Tacc, typename Tinv>
+__global__ void __launch_bounds__(kTpb) k_other_apply_cg(CgArgs c, int nb_int, int mas_lo, int mas_hi, int bodies,
+                                                          const Tinv* __restrict__ abd_inv,
+                                                          const Tinv* __restrict__ diag_inv, Tacc* partial,
+                                                          double* partial_rr, int part_base, PcgScalars* s)
+{
+  pdl_wait();
+  if (s->status != MASPCG_SOLVE_RUNNING) return;
+  const CgScal cs = cg_scalars(s);
+  Tacc dot = 0;
+  double rr = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int bdy = blockIdx.x * blockDim.x + threadIdx.x; bdy < bodies; bdy += stride) {
+    const Tinv* P = abd_inv + 144 * (size_t)bdy;
+    float in[12];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cg_input_row(c, cs, 4 * bdy + q, true, in + 3 * q);
+    float zb[12];
+#pragma unroll 1
+    for (int a = 0; a < 12; ++a) {
+      Tinv acc = 0;
+#pragma unroll
+      for (int col = 0; col < 12; ++col) acc += P[12 * a + col] * (Tinv)in[col];
+      zb[a] = (float)acc;
+      dot += (Tacc)in[a] * (Tacc)zb[a];
+      rr += (double)in[a] * in[a];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) st_p4(c.z0, 4 * bdy + q, zb[3 * q], zb[3 * q + 1], zb[3 * q + 2]);
+  }
+  for (int row = 4 * bodies + blockIdx.x * blockDim.x + threadIdx.x; row < nb_int; row += stride) {
+    if (row >= mas_lo && row < mas_hi) continue;
+    float r3[3];
+    cg_input_row(c, cs, row, true, r3);
+    float z3[3] = {r3[0], r3[1], r3[2]};
+    if (diag_inv) {
+      const Tinv* D = diag_inv + 9 * (size_t)row;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        z3[i] = (float)(D[3 * i] * (Tinv)r3[0] + D[3 * i + 1] * (Tinv)r3[1] + D[3 * i + 2] * (Tinv)r3[2]);
+    }
+    st_p4(c.z0, row, z3[0], z3[1], z3[2]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      dot += (Tacc)r3[i] * (Tacc)z3[i];
+      rr += (double)r3[i] * r3[i];
+    }
+  }
+  __shared__ Tacc red[kTpb / 32];
+  __shared__ double red2[kTpb / 32];
+  const Tacc bsum = block_sum<Tacc, kTpb>(dot, red);
+  const double bsum2 = block_sum<double, kTpb>(rr, red2);
+  if (threadIdx.x == 0) {
+    partial[part_base + blockIdx.x] = bsum;
+    if (c.update) partial_rr[part_base + blockIdx.x] = bsum2;
+  }
+}
+
+// Single-reduction recurrence, the iteration's update alone (the last
+// iteration of a MIXED batch, whose FP64 residual replacement comes between
+// the update and the apply): every row, r.r, then the stopping gate, and the
+// r / s buffers swap.
+template <typename Tacc>
+__global__ void __launch_bounds__(kTpb) k_cg_update(CgArgs c, int nrows, int mixed, Tacc* partial, PcgScalars* s)
+{
+  pdl_wait();
+  if (s->status != MASPCG_SOLVE_RUNNING) return;
+  const CgScal cs = cg_scalars(s);
+  Tacc acc = 0;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += gridDim.x * blockDim.x) {
+    float rn[3];
+    cg_update_row(c, cs.cur, row, cs.first, cs.alpha, cs.beta, rn);
+    acc += (Tacc)rn[0] * (Tacc)rn[0] + (Tacc)rn[1] * (Tacc)rn[1] + (Tacc)rn[2] * (Tacc)rn[2];
+  }
+  pdl_trigger();
+  Tacc total = 0;
+  if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
+      threadIdx.x == 0) {
+    s->cg_cur ^= 1;
+    gate_check(s, (double)total, mixed);
+  }
+}
+
+// Every entry of a padded vector's three components set to v (the fourth 0).
+__global__ void k_fill_p4(float* p4, int nrows, float v)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nrows) st_p4(p4, r, v, v, v);
+}
+
 // ----------------------------------------------------------------- engine --
 
 template <typename Tm, typename Tv, typename Tacc>
@@ -559,6 +672,7 @@ struct Engine {
   maspcg_handle* h;
   int n, gstream, gspmv, grows, gl0, gother, parts_other, parts_total;
   bool mas, mas16, mixed, ovl;
+  bool cg;  // single-reduction recurrence (FP32 matrix, MAS32)
 
   explicit Engine(maspcg_handle* hh) : h(hh)
   {
@@ -575,8 +689,48 @@ struct Engine {
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;
     parts_other = gother;
     parts_total = gother + gl0;
+    cg = std::is_same<Tm, float>::value && mas && h->use_cg && !h->fused_head;
   }
   Tv* V(maspcg::DBuf<unsigned char>& b) { return reinterpret_cast<Tv*>(b.get()); }
+  static float* Vf(maspcg::DBuf<unsigned char>& b) { return reinterpret_cast<float*>(b.get()); }
+
+  CgArgs cg_args(int update)
+  {
+    CgArgs c{};
+    c.z = Vf(h->vz);
+    c.w = Vf(h->vap);
+    c.p = Vf(h->cg_p);
+    c.x = Vf(h->vx);
+    c.r[0] = Vf(h->vr);
+    c.r[1] = Vf(h->cg_r2);
+    c.s[0] = Vf(h->cg_s0);
+    c.s[1] = Vf(h->cg_s1);
+    c.z0 = Vf(h->cg_z0);
+    c.update = update;
+    return c;
+  }
+
+  // The preconditioner apply of the single-reduction recurrence (update: the
+  // iteration's vector update runs in the same kernels first; mode: RzMode).
+  void cg_precondition(int update, int mode, PcgScalars* s)
+  {
+    const CgArgs c = cg_args(update);
+    if (gother) {
+      const int bodies = h->abd_bodies;
+      const int mas_lo = h->fem_off, mas_hi = h->fem_off + h->c0;
+      if (bodies > 0)
+        launch_pdl(h, k_other_apply_cg<Tacc, double>, dim3(gother), dim3(kTpb), 0, c, h->nb_int, mas_lo, mas_hi,
+                   bodies, (const double*)h->abd_inv64.get(), (const double*)nullptr, partial_rz(),
+                   h->partial_rr.get(), 0, s);
+      else
+        launch_pdl(h, k_other_apply_cg<Tacc, float>, dim3(gother), dim3(kTpb), 0, c, h->nb_int, mas_lo, mas_hi,
+                   bodies, (const float*)h->abd_inv32.get(), (const float*)nullptr, partial_rz(), h->partial_rr.get(),
+                   0, s);
+    }
+    mas_apply_cg<Tacc>(h, c, Vf(h->cg_pc), partial_rz(), h->partial_rr.get(), parts_other, parts_total, mode, gl0, s,
+                       h->overlap_coarse);
+    MCK(cudaGetLastError());
+  }
   Tacc* partial() { return reinterpret_cast<Tacc*>(h->partial.get()); }
   Tacc* partial_rz() { return reinterpret_cast<Tacc*>(h->partial_rz.get()); }
 
@@ -651,23 +805,43 @@ struct Engine {
   static constexpr int kSpmvLanes = 8;
 
   // The SpMV of the iteration: one wave of resident CTAs (the kernel strides
-  // over the rest).  FP32: the sliced layout, sized so every warp takes the
-  // same number of slice groups where one wave allows it.
+  // over the rest).  FP32: the sliced layout, staged through shared memory
+  // (one CTA of kJdsWarps warps per SM) unless MASPCG_FLAG_SPMV_DIRECT.
+  // cg: the single-reduction recurrence's w = A (z0 + pc) (else Ap = A p).
+  template <bool kCg>
+  void spmv_fp32_launch(PcgScalars* s, const SpmvVec& v)
+  {
+    if (h->spmv_staged) {
+      auto kern = k_spmv_jds_staged<Tacc, kCg>;
+      static bool configured = false;
+      if (!configured) {
+        MCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kJdsSmem));
+        configured = true;
+      }
+      const int grid = std::max(1, std::min(h->sm_count, ceil_div(h->jds_slices, kJdsWarps)));
+      launch_pdl(h, kern, dim3(grid), dim3(kJdsWarps * 32), kJdsSmem, jds_args(h), h->rowptr.get(), h->colidx.get(),
+                 h->val64.get(), v, partial(), s, h->failed.get() + 4);
+      return;
+    }
+    auto kern = k_spmv_jds<Tacc, kCg>;
+    static int per_sm = 0;
+    if (!per_sm) {
+      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
+      per_sm = std::max(per_sm, 1);
+    }
+    const int grid = std::max(1, std::min(per_sm * h->sm_count, ceil_div(h->jds_slices, kTpb / 32)));
+    launch_pdl(h, kern, dim3(grid), dim3(kTpb), 0, jds_args(h), h->rowptr.get(), h->colidx.get(), h->val64.get(), v,
+               partial(), s);
+  }
+
   void spmv(PcgScalars* s)
   {
     if constexpr (std::is_same<Tm, float>::value) {
-      auto kern = k_spmv_jds<Tacc>;
-      static int per_sm = 0;
-      if (!per_sm) {
-        MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
-        per_sm = std::max(per_sm, 1);
+      if (cg) {
+        spmv_fp32_launch<true>(s, SpmvVec{Vf(h->cg_z0), Vf(h->cg_pc), Vf(h->vap), Vf(h->vz)});
+        return;
       }
-      constexpr int groups_per_cta = (kTpb / 32) * kJdsSlicesPerWarp;
-      const int resident = per_sm * h->sm_count;
-      const int need = std::max(1, ceil_div(h->jds_slices, groups_per_cta));
-      const int grid = need <= resident ? need : ceil_div(need, ceil_div(need, resident));
-      launch_pdl(h, kern, dim3(grid), dim3(kTpb), 0, jds_args(h), h->rowptr.get(), h->colidx.get(), h->val64.get(),
-                 V(h->vp4), V(h->vap), partial(), s);
+      spmv_fp32_launch<false>(s, SpmvVec{Vf(h->vp4), nullptr, Vf(h->vap), nullptr});
     } else {
       constexpr int rows = kTpb / kSpmvLanes;
       static int per_sm = 0;
@@ -684,9 +858,9 @@ struct Engine {
   void true_residual(PcgScalars* s)
   {
     launch_pdl(h, k_fold_x, dim3(gstream), dim3(kTpb), 0, h->x64.get(), reinterpret_cast<float*>(h->vx.get()), n, 0, s);
-    launch_pdl(h, k_true_residual<16>, dim3(gspmv), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(), h->x64.get(),
-                                               h->b64.get(), reinterpret_cast<float*>(h->vr.get()), h->nb_int,
-                                               h->partial.get(), s);
+    launch_pdl(h, k_true_residual<16>, dim3(gspmv), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(),
+               h->x64.get(), h->b64.get(), reinterpret_cast<float*>(h->vr.get()),
+               cg ? reinterpret_cast<float*>(h->cg_r2.get()) : (float*)nullptr, h->nb_int, h->partial.get(), s);
   }
 
   // y = A x through the iteration's own SpMV kernel: x (internal order, FP64)
@@ -702,7 +876,15 @@ struct Engine {
     init.rz = 1.0;
     init.max_iter = 1 << 30;
     MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-    k_to_p4<Tv><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, V(h->vp4), h->nb_int);
+    if (cg) {
+      // the recurrence's SpMV gathers z0 + pc: x into z0, pc zero
+      init.k = 1;
+      MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+      MCK(cudaMemsetAsync(h->cg_pc.get(), 0, h->cg_pc.bytes(), st));
+      k_to_p4<float><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, Vf(h->cg_z0), h->nb_int);
+    } else {
+      k_to_p4<Tv><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, V(h->vp4), h->nb_int);
+    }
     MLAUNCHED(h);
     const bool pdl = h->use_pdl;
     h->use_pdl = false;
@@ -717,6 +899,18 @@ struct Engine {
   void record_batch(int batch, PcgScalars* s)
   {
     for (int it = 0; it < batch; ++it) {
+      if (cg) {
+        if (mixed && it == batch - 1) {
+          // update, FP64 residual replacement, then the apply of the new r
+          launch_pdl(h, k_cg_update<Tacc>, dim3(grows), dim3(kTpb), 0, cg_args(1), h->nb_int, 1, partial(), s);
+          true_residual(s);
+          cg_precondition(0, kRzLoop, s);
+        } else {
+          cg_precondition(1, mixed ? kRzFusedMix : kRzFusedStd, s);
+        }
+        spmv(s);
+        continue;
+      }
       iteration_head(s);
       if (mixed && it == batch - 1) true_residual(s);
       precondition(V(h->vr), V(h->vz), 2, s, ovl);
@@ -751,6 +945,13 @@ struct Engine {
     if (h->l2_flush.n < kFlushBytes) {
       h->l2_flush.resize(kFlushBytes);
       MCK(cudaMemsetAsync(h->l2_flush.get(), 0, kFlushBytes, st));
+    }
+    if (cg && stage == 0) {
+      // the recurrence's SpMV w = A (z0 + pc) with z0 = 1, pc = 0: delta > 0
+      init.k = 1;
+      MCK(cudaMemsetAsync(h->cg_pc.get(), 0, h->cg_pc.bytes(), st));
+      k_fill_p4<<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(Vf(h->cg_z0), h->nb_int, 1.f);
+      MLAUNCHED(h);
     }
     MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     auto once = [&]() {
@@ -815,12 +1016,22 @@ struct Engine {
     init.max_iter = max_iter;
     init.gate = mixed ? MASPCG_GATE_EUCLID : h->cfg.gate;
     init.tol = h->cfg.tolerance;
+    init.barrier_limit = h->barrier_limit;
+    init.barrier_extra = h->barrier_extra;
     MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     MCK(cudaMemsetAsync(h->failed.get() + 4, 0, sizeof(int), st));
     MCK(cudaEventRecord(h->ev0, st));
     k_init<Tv><<<gstream, kTpb, 0, st>>>(b_int, V(h->vx), V(h->vr), mixed ? h->x64.get() : nullptr, n,
                                          h->partial_rz.get(), s); MLAUNCHED(h);
-    precondition(V(h->vr), V(h->vz), 1, s, ovl);
+    if (cg) {
+      // single-reduction recurrence: z0 = M r0 (pc: its coarse part), then
+      // w = A z, delta = z.w and the first alpha
+      MCK(cudaMemsetAsync(h->cg_pc.get(), 0, h->cg_pc.bytes(), st));
+      cg_precondition(0, kRzInitial, s);
+      spmv(s);
+    } else {
+      precondition(V(h->vr), V(h->vz), 1, s, ovl);
+    }
     // graph of one batch
     const int batch = mixed ? std::max(1, h->cfg.refinement_period) : std::max(1, h->cfg.iterations_per_launch);
     if (h->graph_dirty || h->graph_batch != batch) {

@@ -39,12 +39,50 @@ __device__ __forceinline__ bool grid_finish(Tacc v, Tacc* partial, int slot, int
   return true;
 }
 
-// End of the preconditioner apply: r^T z of this iteration.
-// mode 1: initial apply (rz0); mode 2: inside the loop (beta, k++).
+// The stopping gate after the x / r update of iteration k (PCGSolver::pcg,
+// pcg_solver.cu:277-282: tested with the r.z of before the update): the rz
+// gate |r.z| <= tol r0.z0, or the Euclidean ||r|| <= tol ||b|| on rr.  MIXED:
+// a met gate asks for the FP64 true residual instead of stopping.  Returns
+// true when the loop stops here (gate met or rr not finite).
+__device__ __forceinline__ bool gate_check(PcgScalars* s, double rr, int mixed)
+{
+  s->rr = rr;
+  if (!isfinite(rr)) {
+    s->status = MASPCG_SOLVE_NONFINITE;
+    s->iterations = s->k;
+    return true;
+  }
+  const bool conv = (s->gate == MASPCG_GATE_RZ) ? (fabs(s->rz) <= s->tol * s->rz0) : (rr <= s->tol * s->tol * s->bb);
+  if (!conv) return false;
+  if (mixed) {
+    s->status = kNeedTrue;
+  } else {
+    s->status = MASPCG_SOLVE_CONVERGED;
+    s->iterations = s->k;
+  }
+  return true;
+}
+
+// Modes of the r.z completion (the end of a preconditioner apply).
+enum RzMode {
+  kRzNone = 0,      // standalone apply: no scalar update
+  kRzInitial = 1,   // initial apply: rz0, k = 1
+  kRzLoop = 2,      // in the loop: beta = r.z / previous r.z, k++
+  kRzFusedStd = 4,  // single-reduction recurrence, plain precision: the apply ran behind the iteration's x / r
+                    // update (so the gate on s->rr comes first, and the r / s buffers swap), then as kRzLoop
+  kRzFusedMix = 5   // the same in MIXED precision (a met gate asks for the FP64 true residual)
+};
+
+// End of the preconditioner apply: r^T z of this iteration (mode: RzMode).
 __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode)
 {
+  if (mode == kRzFusedStd || mode == kRzFusedMix) {
+    s->cg_cur ^= 1;
+    if (gate_check(s, s->rr, mode == kRzFusedMix)) return;
+    mode = kRzLoop;
+  }
   s->rz_new = rz_new;
-  if (mode == 1 && rz_new == 0.0 && s->bb == 0.0) {  // b = 0: x = 0 is exact
+  if (mode == kRzInitial && rz_new == 0.0 && s->bb == 0.0) {  // b = 0: x = 0 is exact
     s->rz = s->rz0 = 0.0;
     s->k = 0;
     s->status = MASPCG_SOLVE_CONVERGED;
@@ -61,7 +99,7 @@ __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode
     s->iterations = s->k;
     return;
   }
-  if (mode == 1) {
+  if (mode == kRzInitial) {
     s->rz = rz_new;
     s->rz0 = rz_new;
     s->k = 1;
@@ -77,13 +115,112 @@ __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode
   }
 }
 
+// Single-reduction recurrence (Chronopoulos-Gear): the last block of the
+// SpMV w = A z has delta = z.w; alpha = r.z / (delta - beta r.z / alpha_prev)
+// (delta alone right after the initial apply, k == 1), which equals r.z /
+// p.Ap of the two-reduction form in exact arithmetic.
+__device__ __forceinline__ void cg_alpha(PcgScalars* s, double delta)
+{
+  const double denom = (s->k == 1) ? delta : delta - s->beta * s->rz / s->alpha;
+  s->pap = denom;
+  if (!isfinite(denom)) {
+    s->status = MASPCG_SOLVE_NONFINITE;
+    s->iterations = s->k;
+  } else if (!(denom > 0.0)) {
+    s->status = MASPCG_SOLVE_NONPOSITIVE_CURVATURE;
+    s->iterations = s->k;
+  } else {
+    s->alpha = s->rz / denom;
+  }
+}
+
+// The vectors of the single-reduction recurrence (FP32, internal order).  An
+// iteration's update and its preconditioner apply run in one kernel: with z
+// = M r, w = A z of the previous apply and SpMV,
+//   p = z + beta p,  s = w + beta s  (p = z, s = w at k == 1),
+//   x += alpha p,    r' = r - alpha s,
+// then z' = M r'.  r and s are double-buffered (cur = s->cg_cur): the coarse
+// levels, beside the level-0 apply, form r' again from r, w, s (the same FMAs,
+// so the same bits) while the apply writes it.
+struct CgArgs {
+  const float* z;  // 3 per row: z of this iteration (written by the SpMV)
+  const float* w;  // 3 per row: A z
+  float* p;
+  float* x;
+  float* r[2];
+  float* s[2];
+  float* z0;       // 4 per row (padded): the next z's level-0 / non-MAS part (the SpMV gathers it)
+  int update;      // 1: the iteration's update first; 0: r[cur] is already the residual to precondition
+};
+
+// The update of one row; r' into rn.
+__device__ __forceinline__ void cg_update_row(const CgArgs& c, int cur, int row, bool first, float alpha, float beta,
+                                              float rn[3])
+{
+  const size_t b = 3 * (size_t)row;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float zq = c.z[b + q], wq = c.w[b + q];
+    const float pq = first ? zq : fmaf(beta, c.p[b + q], zq);
+    const float sq = first ? wq : fmaf(beta, c.s[cur][b + q], wq);
+    c.p[b + q] = pq;
+    c.s[cur ^ 1][b + q] = sq;
+    c.x[b + q] = fmaf(alpha, pq, c.x[b + q]);
+    const float rq = fmaf(-alpha, sq, c.r[cur][b + q]);
+    c.r[cur ^ 1][b + q] = rq;
+    rn[q] = rq;
+  }
+}
+
+// r' of one row without writing anything (the coarse levels' restriction):
+// the same operations as cg_update_row.
+__device__ __forceinline__ void cg_residual_row(const CgArgs& c, int cur, int row, bool first, float alpha, float beta,
+                                                float rn[3])
+{
+  const size_t b = 3 * (size_t)row;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float wq = c.w[b + q];
+    const float sq = first ? wq : fmaf(beta, c.s[cur][b + q], wq);
+    rn[q] = fmaf(-alpha, sq, c.r[cur][b + q]);
+  }
+}
+
+// The scalars a fused kernel reads once at entry (nothing changes them until
+// every kernel of the iteration has passed its rows).
+struct CgScal {
+  int cur;
+  bool first;
+  float alpha, beta;
+};
+__device__ __forceinline__ CgScal cg_scalars(const PcgScalars* s)
+{
+  return CgScal{s->cg_cur, s->k == 1, (float)s->alpha, (float)s->beta};
+}
+
+// The residual the apply of one row starts from: r' of the fused update, or
+// r[cur] when the update ran before (update == 0).  Writes the update when
+// `write` (the kernel that owns the row), else only recomputes r'.
+__device__ __forceinline__ void cg_input_row(const CgArgs& c, const CgScal& cs, int row, bool write, float rn[3])
+{
+  if (!c.update) {
+    const size_t b = 3 * (size_t)row;
+    rn[0] = c.r[cs.cur][b];
+    rn[1] = c.r[cs.cur][b + 1];
+    rn[2] = c.r[cs.cur][b + 2];
+    return;
+  }
+  if (write)
+    cg_update_row(c, cs.cur, row, cs.first, cs.alpha, cs.beta, rn);
+  else
+    cg_residual_row(c, cs.cur, row, cs.first, cs.alpha, cs.beta, rn);
+}
+
 // Grid-wide barrier of a cooperative launch (every CTA resident).  The last
 // CTA to arrive resets the count and advances the generation word the
-// others wait on.  The wait is bounded: on expiry the CTA records error 3
-// and the barrier returns false (the caller then leaves; the host reports
-// the error after the graph).
-constexpr long long kBarrierLimit = 1ll << 24;
-
+// others wait on.  The wait is bounded (s->barrier_limit spins): on expiry
+// the CTA records error 3, stops the solve and the barrier returns false
+// (the caller then leaves; the host reports the error after the graph).
 __device__ __forceinline__ bool grid_barrier(PcgScalars* s, int* err)
 {
   __shared__ int ok_s;
@@ -91,18 +228,24 @@ __device__ __forceinline__ bool grid_barrier(PcgScalars* s, int* err)
   if (threadIdx.x == 0) {
     volatile unsigned* gen = &s->barrier_gen;
     const unsigned g0 = *gen;
+    const long long limit = s->barrier_limit;
+    const unsigned expected = gridDim.x + (unsigned)s->barrier_extra;
     __threadfence();
     int ok = 1;
-    if (atomicAdd(&s->tickets[kTicketBarrier], 1u) == gridDim.x - 1) {
+    if (atomicAdd(&s->tickets[kTicketBarrier], 1u) == expected - 1) {
       s->tickets[kTicketBarrier] = 0u;
       __threadfence();
       atomicAdd(&s->barrier_gen, 1u);
     } else {
       long long it = 0;
       while (*gen == g0) {
-        if (++it > kBarrierLimit) {
+        if (++it > limit) {
+          // give up: record the error and stop the solve, so every later
+          // kernel returns at entry and the host reads the error after this
+          // graph launch
           ok = 0;
           atomicExch(err, 3);
+          atomicExch(&s->status, (int)MASPCG_SOLVE_NONFINITE);
           break;
         }
         __nanosleep(64);

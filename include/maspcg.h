@@ -101,7 +101,13 @@ typedef enum {
   MASPCG_FLAG_SEQUENTIAL_COARSE = 8,   /* run the MAS coarse levels before the level-0 apply, not beside it
                                           (always so in MASPCG_PREC_REFERENCE, whose r.z is then summed over
                                           the fine rows as the reference sums it) */
-  MASPCG_FLAG_FUSED_HEAD = 16          /* p update, SpMV and x/r update as one cooperative kernel with grid barriers */
+  MASPCG_FLAG_FUSED_HEAD = 16,         /* p update, SpMV and x/r update as one cooperative kernel with grid barriers */
+  MASPCG_FLAG_SPMV_DIRECT = 32,        /* FP32 SpMV reads its slice records from global memory instead of staging
+                                          them in shared memory with bulk copies */
+  MASPCG_FLAG_TWO_REDUCTION = 64       /* FP32 / MIXED with MAS32: the two-reduction PCG recurrence of the reference
+                                          (p update, SpMV with p.Ap, x / r update, apply with r.z) instead of the
+                                          single-reduction one (the update fused into the apply, one SpMV w = A z
+                                          with z.w; Chronopoulos-Gear), which is the default there */
 } maspcg_flags;
 
 typedef struct {
@@ -493,6 +499,30 @@ MASPCG_API maspcg_status maspcg_galerkin_prolong(maspcg_handle* h, const maspcg_
  * the caller's order.  Host or device pointers. */
 MASPCG_API maspcg_status maspcg_bcoo_gradient(maspcg_handle* h, const int* rows, const int* cols, int n_blocks,
                                               const double* lam, const double* x, double* grad9_colmajor);
+
+/* The matrix adjoint chained to per-tet Young's modulus (no counterpart in
+ * the reference; the backward of the differentiable solve): the first
+ * n_tets * blocks_per_tet blocks of an upper BCOO list are the element blocks
+ * of the tets in tet order (blocks_per_tet each, 10 for a tetrahedron's upper
+ * blocks), each linear in its tet's modulus youngs[t].  With lam and x as in
+ * maspcg_bcoo_gradient, grad_youngs[t] = sum over tet t's blocks k of
+ * <G_k, values9_k> / youngs[t], G_k the block gradient of
+ * maspcg_bcoo_gradient, computed without storing G.  Host or device pointers. */
+MASPCG_API maspcg_status maspcg_element_modulus_gradient(maspcg_handle* h, int n_tets, int blocks_per_tet,
+                                                         const int* rows, const int* cols,
+                                                         const double* values9_colmajor, const double* lam,
+                                                         const double* x, const double* youngs,
+                                                         double* grad_youngs);
+
+/* Test hook for the bounded waits (no counterpart in the reference): the
+ * grid barriers of the MASPCG_FLAG_FUSED_HEAD kernel give up after
+ * barrier_limit spins (default 2^24, each a 64 ns sleep) and then stop the
+ * solve, which returns MASPCG_ERR_CUDA ("a grid barrier of the fused
+ * iteration kernel timed out"); barrier_extra > 0 makes every barrier wait
+ * for arrivals that never come, so a test can drive that path without a GPU
+ * fault.  (0, default) restores normal barriers.  Applies from the next
+ * maspcg_solve. */
+MASPCG_API maspcg_status maspcg_set_wait_test_hooks(maspcg_handle* h, long long barrier_limit, int barrier_extra);
 
 /* Most vectors one maspcg_residual_norms_noalloc call accepts. */
 #define MASPCG_RESIDUAL_MAX_VECTORS 8

@@ -241,7 +241,7 @@ def test_mixed_solve_with_several_domains_per_warp(inverse):
 
 
 @pytest.mark.parametrize("flag", ["FLAG_FUSED_HEAD", "FLAG_PDL", "FLAG_SEQUENTIAL_COARSE", "FLAG_APPLY_STAGED2",
-                                  "FLAG_APPLY_DIRECT"])
+                                  "FLAG_APPLY_DIRECT", "FLAG_SPMV_DIRECT", "FLAG_TWO_REDUCTION"])
 def test_schedule_flags_solve_the_same_system(flag):
     """Every kernel-schedule choice reaches the FP64-verified tolerance on a
     system with several domains per warp, in about the same iterations
@@ -339,3 +339,21 @@ def test_device_pointer_inputs(cfg0):
         torch.cuda.synchronize()
     assert rh["iterations"] == rd["iterations"]
     assert np.array_equal(xh, xd.cpu().numpy())
+
+
+def test_fused_head_barrier_expiry_returns_error_and_handle_recovers(cfg0):
+    """The bounded grid barrier of the cooperative iteration kernel: with a
+    barrier that waits for one arrival too many (nothing ever completes it)
+    and a short spin limit, the solve returns MASPCG_ERR_CUDA with the
+    timeout message instead of hanging; with the normal barrier the next
+    solve on the same handle converges."""
+    from agipc_learning_b200 import _native as N
+    s = cfg0
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16", flags=N.FLAG_FUSED_HEAD) as m:
+        m._ck(m.lib.maspcg_set_wait_test_hooks(m.h, 2000, 1))
+        with pytest.raises(N.MaspcgError) as e:
+            m.solve(s.b)
+        assert e.value.status == N.ERR_CUDA and "grid barrier" in str(e.value)
+        m._ck(m.lib.maspcg_set_wait_test_hooks(m.h, 1 << 24, 0))
+        x, res = m.solve(s.b)
+    assert res["status_name"] == "converged" and res["fp64_gate_met"]

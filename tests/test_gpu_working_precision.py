@@ -44,18 +44,24 @@ def _abd_rows_mask(s):
     return mask
 
 
-@pytest.mark.parametrize("which,precision", [("cfg1_small", "mixed"), ("cfg1_small", "fp32"),
-                                             ("hybrid", "mixed"), ("cfg1_small", "reference")])
-def test_working_spmv_against_oracle(which, precision, request):
+@pytest.mark.parametrize("which,precision,flags", [("cfg1_small", "mixed", 0), ("cfg1_small", "fp32", 0),
+                                                   ("hybrid", "mixed", 0), ("cfg1_small", "reference", 0),
+                                                   ("cfg1_small", "mixed", N.FLAG_SPMV_DIRECT),
+                                                   ("cfg1_small", "mixed", N.FLAG_TWO_REDUCTION),
+                                                   ("hybrid", "mixed", N.FLAG_TWO_REDUCTION | N.FLAG_SPMV_DIRECT)])
+def test_working_spmv_against_oracle(which, precision, flags, request):
     """|y_gpu - A32 x32| <= 48 eps32 (|A32| |x32|) elementwise, where A32 and
     x32 are the FP32-rounded matrix and vector the kernel reads (rows of the
     affine bodies, taken from the FP64 matrix in FP64, within 1e-12 of the
-    FP64 product); reference precision within 1e-12 of the FP64 product."""
+    FP64 product); reference precision within 1e-12 of the FP64 product.
+    Every form the solve can run: the slice records staged in shared memory
+    or read directly, the single-reduction recurrence's SpMV (gathering
+    z0 + pc) or the two-reduction one's (gathering p)."""
     s = synth.config_system(2, scale=16) if which == "hybrid" else request.getfixturevalue(which)
     rng = np.random.default_rng(5)
     x = rng.standard_normal(3 * s.nb)
     with MasPcg.from_system(s, precision=precision, inverse="bf16" if precision == "mixed" else "fp32",
-                            gate="euclid") as m:
+                            gate="euclid", flags=flags) as m:
         y = m.spmv_working(x)
     if precision == "reference":
         ref = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
