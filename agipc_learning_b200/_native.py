@@ -38,12 +38,16 @@ FLAG_APPLY_STAGED2 = 2
 FLAG_APPLY_DIRECT = 4
 FLAG_SEQUENTIAL_COARSE = 8
 FLAG_FUSED_HEAD = 16
-FLAG_SPMV_DIRECT = 32
-FLAG_TWO_REDUCTION = 64
+FLAG_FUSED_UPDATE = 32
 
 INV_FP32 = 0
 INV_BF16 = 1
 INV_FP16 = 2
+MATRIX_F32 = 0
+MATRIX_F32_SUM64 = 1
+MATRIX_F32_SPLIT = 2
+REPLACE_RELIABLE = 0
+REPLACE_PERIODIC = 1
 
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "iteration_cap", 3: "nonpositive_curvature", 4: "nonfinite",
                 5: "invalid_rz"}
@@ -77,7 +81,8 @@ class Config(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("max_iter_ratio", ctypes.c_double), ("max_iterations", ctypes.c_int),
                 ("gate", ctypes.c_int), ("precision", ctypes.c_int), ("inverse_storage", ctypes.c_int),
                 ("preconditioner", ctypes.c_int), ("refinement_period", ctypes.c_int), ("bank_size", ctypes.c_int),
-                ("iterations_per_launch", ctypes.c_int), ("flags", ctypes.c_int)]
+                ("iterations_per_launch", ctypes.c_int), ("flags", ctypes.c_int), ("matrix_form", ctypes.c_int),
+                ("residual_replacement", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):

@@ -156,11 +156,7 @@ void alloc_vectors(maspcg_handle* h)
   h->partial.resize(parts);
   h->partial_rz.resize(parts);
   h->partial_rr.resize(parts);
-  if (h->cfg.precision != MASPCG_PREC_REFERENCE) {
-    for (auto* b : {&h->cg_r2, &h->cg_s0, &h->cg_s1, &h->cg_p}) b->resize(n * 4);
-    h->cg_z0.resize(4 * (size_t)h->nb_int * 4, 32);
-    h->cg_pc.resize(4 * (size_t)h->nb_int * 4, 32);
-  }
+  if (h->cfg.precision != MASPCG_PREC_REFERENCE) h->vr2.resize(n * 4);
 }
 
 }  // namespace
@@ -262,6 +258,8 @@ MASPCG_API void maspcg_config_default(maspcg_config* c)
   c->bank_size = 32;
   c->iterations_per_launch = 8;
   c->flags = 0;
+  c->matrix_form = MASPCG_MATRIX_F32;
+  c->residual_replacement = MASPCG_REPLACE_RELIABLE;
 }
 
 MASPCG_API const char* maspcg_status_string(int s)
@@ -313,7 +311,8 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_MAS16 || c.preconditioner == MASPCG_PRECOND_NONE) ||
-      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~127) != 0 ||
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~63) != 0 || c.matrix_form < 0 ||
+      c.matrix_form > 2 || c.residual_replacement < 0 || c.residual_replacement > 1 ||
       ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_DIRECT))) {
     g_create_error = "invalid configuration";
     return MASPCG_ERR_INVALID_ARGUMENT;
@@ -344,8 +343,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     // rows after the coarse correction is added to z
     h->overlap_coarse = (c.flags & MASPCG_FLAG_SEQUENTIAL_COARSE) == 0 && c.precision != MASPCG_PREC_REFERENCE;
     h->fused_head = (c.flags & MASPCG_FLAG_FUSED_HEAD) != 0;
-    h->spmv_staged = (c.flags & MASPCG_FLAG_SPMV_DIRECT) == 0;
-    h->use_cg = (c.flags & MASPCG_FLAG_TWO_REDUCTION) == 0;
+    h->fuse_update = (c.flags & MASPCG_FLAG_FUSED_UPDATE) != 0;
     MCK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
     MCK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     MCK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));

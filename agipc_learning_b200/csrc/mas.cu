@@ -835,9 +835,9 @@ __device__ __forceinline__ int domain_level(const LevelInfo& lv, int g)
 // to the p update; this kernel then also sums r.z of the coarse levels,
 // sum over domains of R.Z (= r . P Z), and completes r.z with the level-0
 // part (rz_part_done, mode as in rz_update).
-template <typename TI, typename Tv, bool kCg>
+template <typename TI, typename Tv, bool kFused>
 __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, const Tv* __restrict__ r,
-                                                                  PcgScalars* s, int mode, int pair, CgArgs cg)
+                                                                  PcgScalars* s, int mode, int pair, FusedArgs fa)
 {
   __shared__ int queue[kChainQueue];
   __shared__ int tail_s, lo_s, hi_s;
@@ -850,8 +850,8 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
     hi_s = -1;
   }
   __syncthreads();
-  CgScal cs{};
-  if constexpr (kCg) cs = cg_scalars(s);
+  FusedScal fs{};
+  if constexpr (kFused) fs = fused_scalars(s);
   // level 0 -> level 1 (RestrictR of the fine residual); a level-1 node's
   // children all lie in one bank, so its sum is written, not accumulated
 #pragma unroll
@@ -861,9 +861,9 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_coarse_chain(ApplyArgs a, 
       const int slot = bank * kBank + lane;
       const int key = a.cmap1[slot];
       float v[3];
-      if constexpr (kCg) {
+      if constexpr (kFused) {
         // r' of the iteration's update, formed as the level-0 apply forms it
-        cg_input_row(cg, cs, a.fem_off + slot, false, v);
+        fused_input_row(fa, fs, a.fem_off + slot, false, v);
       } else {
         const Tv* rp = r + 3 * (size_t)(a.fem_off + slot);
         v[0] = (float)rp[0];
@@ -1281,10 +1281,10 @@ Mas16Args make_mas16_args(maspcg_handle* h)
 // Level-0 apply + prolongation + r.z; with `partial` set, the last block
 // completes the r.z reduction over [0, total_parts) and, for mode > 0,
 // updates the PCG scalars (rz0 / beta / k).
-template <typename TI, typename Tv, typename Tacc, bool kCg>
+template <typename TI, typename Tv, typename Tacc, bool kFused>
 __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial,
                                                       int part_base, int total_parts, int mode, PcgScalars* s,
-                                                      int coarse_add, int pair, CgArgs cg, double* partial_rr)
+                                                      int coarse_add, int pair, FusedArgs fa, double* partial_rr)
 {
   pdl_wait();
   if (s && s->status != MASPCG_SOLVE_RUNNING) return;
@@ -1292,17 +1292,17 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
   const int warps_total = gridDim.x * (blockDim.x >> 5);
   Tacc dot = 0;
   double rr = 0.0;
-  CgScal cs{};
-  if constexpr (kCg) cs = cg_scalars(s);
+  FusedScal fs{};
+  if constexpr (kFused) fs = fused_scalars(s);
   for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < a.lv.dom_begin[1]; g += warps_total) {
     const int slot = kBank * g + lane;
     const size_t row3 = 3 * (size_t)(a.fem_off + slot);
     Tv r0, r1, r2;
-    if constexpr (kCg) {
+    if constexpr (kFused) {
       float rn[3];
-      cg_input_row(cg, cs, a.fem_off + slot, true, rn);
+      fused_input_row(fa, fs, a.fem_off + slot, true, rn);
       r0 = rn[0], r1 = rn[1], r2 = rn[2];
-      if (cg.update) rr += (double)rn[0] * rn[0] + (double)rn[1] * rn[1] + (double)rn[2] * rn[2];
+      if (fa.update) rr += (double)rn[0] * rn[0] + (double)rn[1] * rn[1] + (double)rn[2] * rn[2];
     } else {
       r0 = r[row3], r1 = r[row3 + 1], r2 = r[row3 + 2];
     }
@@ -1327,17 +1327,13 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
       y[1] += cc[1];
       y[2] += cc[2];
     }
-    if constexpr (kCg) {
-      st_p4(cg.z0, a.fem_off + slot, y[0], y[1], y[2]);
-    } else {
-      z[row3] = (Tv)y[0];
-      z[row3 + 1] = (Tv)y[1];
-      z[row3 + 2] = (Tv)y[2];
-    }
+    z[row3] = (Tv)y[0];
+    z[row3 + 1] = (Tv)y[1];
+    z[row3 + 2] = (Tv)y[2];
     dot += (Tacc)r0 * (Tacc)(Tv)y[0] + (Tacc)r1 * (Tacc)(Tv)y[1] + (Tacc)r2 * (Tacc)(Tv)y[2];
   }
   pdl_trigger();
-  if (kCg && cg.update) {
+  if (kFused && fa.update) {
     double rt = 0.0;
     if (grid_finish<double, kApplyTpb>(rr, partial_rr, part_base + blockIdx.x, total_parts, &s->tickets[kTicketXr],
                                        gridDim.x, rt) &&
@@ -1368,10 +1364,10 @@ __global__ void MAS_APPLY_BOUNDS(TI) k_level0_apply(ApplyArgs a, const Tv* __res
 // records the error and the whole CTA leaves.
 constexpr int kApplyWarps = 4;
 
-template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf, bool kCg>
+template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf, bool kFused>
 __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     k_apply_tma(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
-                PcgScalars* s, int g_begin, int g_end, int* err, int coarse_add, int pair, CgArgs cg,
+                PcgScalars* s, int g_begin, int g_end, int* err, int coarse_add, int pair, FusedArgs fa,
                 double* partial_rr)
 {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1404,8 +1400,8 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
   for (int j = 0; j < kBuf; ++j) ph[j] = 0;
   Tacc dot = 0;
   double rr = 0.0;
-  CgScal cs{};
-  if constexpr (kCg) cs = cg_scalars(s);
+  FusedScal fs{};
+  if constexpr (kFused) fs = fused_scalars(s);
   int i = 0;
   bool ok = true;
   for (int g = g_begin + gw; g < g_end; g += warps_total, ++i) {
@@ -1418,13 +1414,13 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     size_t base;
     if (kLevel0) {
       base = 3 * (size_t)(a.fem_off + kBank * g + lane);
-      if constexpr (kCg) {
+      if constexpr (kFused) {
         float rn[3];
-        cg_input_row(cg, cs, a.fem_off + kBank * g + lane, true, rn);
+        fused_input_row(fa, fs, a.fem_off + kBank * g + lane, true, rn);
         rv[0] = rn[0];
         rv[1] = rn[1];
         rv[2] = rn[2];
-        if (cg.update) rr += (double)rn[0] * rn[0] + (double)rn[1] * rn[1] + (double)rn[2] * rn[2];
+        if (fa.update) rr += (double)rn[0] * rn[0] + (double)rn[1] * rn[1] + (double)rn[2] * rn[2];
       } else {
         rv[0] = r[base];
         rv[1] = r[base + 1];
@@ -1467,18 +1463,11 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
         y[1] += cc[1];
         y[2] += cc[2];
       }
-      if constexpr (kCg) {
-        const int row = a.fem_off + kBank * g + lane;
-        st_p4(cg.z0, row, y[0], y[1], y[2]);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) dot += (Tacc)rv[q] * (Tacc)y[q];
-      } else {
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const Tv zv = (Tv)y[q];
-          z[base + q] = zv;
-          dot += (Tacc)rv[q] * (Tacc)zv;
-        }
+      for (int q = 0; q < 3; ++q) {
+        const Tv zv = (Tv)y[q];
+        z[base + q] = zv;
+        dot += (Tacc)rv[q] * (Tacc)zv;
       }
     } else {
       a.coarse_z[base] = y[0];
@@ -1499,7 +1488,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     if (s) s->status = MASPCG_SOLVE_NONFINITE;
   }
   if (__syncthreads_or(!ok)) return;  // the whole CTA leaves together
-  if (kCg && kLevel0 && cg.update) {
+  if (kFused && kLevel0 && fa.update) {
     // r.r of the updated residual first: its last block stores it before its
     // arrival on the r.z ticket, so the r.z completion below sees it
     double rt = 0.0;
@@ -1724,20 +1713,20 @@ ApplyArgs make_apply_args(maspcg_handle* h)
 // Level-0 domain apply variants (the solve uses h->apply_variant).
 enum ApplyVariant { kApplyDirect = 0, kApplyStaged2 = 1, kApplyStaged1 = 2 };
 
-template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf, bool kCg = false>
+template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf, bool kFused = false>
 void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, Tacc* partial, int part_base,
                       int total_parts, int mode, PcgScalars* s, int g_begin, int g_end, int grid, int coarse_add,
-                      int pair, const CgArgs& cg = CgArgs{}, double* partial_rr = nullptr)
+                      int pair, const FusedArgs& fa = FusedArgs{}, double* partial_rr = nullptr)
 {
   constexpr int bytes = kApplyWarps * (kBuf * kRecBytes16 + kApplyScratch);
-  auto kern = k_apply_tma<TI, Tv, Tacc, kLevel0, kBuf, kCg>;
+  auto kern = k_apply_tma<TI, Tv, Tacc, kLevel0, kBuf, kFused>;
   static bool configured = false;
   if (!configured) {
     MCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     configured = true;
   }
   launch_pdl(h, kern, dim3(grid), dim3(kApplyWarps * 32), bytes, a, r, z, partial, part_base, total_parts, mode, s,
-             g_begin, g_end, h->failed.get() + 4, coarse_add, pair, cg, partial_rr);
+             g_begin, g_end, h->failed.get() + 4, coarse_add, pair, fa, partial_rr);
 }
 
 // CTAs of a staged apply over `domains` domains: one wave of resident CTAs.
@@ -1764,10 +1753,10 @@ inline int level0_grid(const maspcg_handle* h, int variant)
 // Level-0 apply (with r.z) in the given variant; coarse_add: z includes the
 // coarse correction (else the p update adds it); pair: r.z is completed
 // together with the concurrently running coarse levels.
-template <typename TI, typename Tv, typename Tacc, bool kCg = false>
+template <typename TI, typename Tv, typename Tacc, bool kFused = false>
 void level0_apply(maspcg_handle* h, const ApplyArgs& a, int variant, const Tv* r, Tv* z, Tacc* partial, int part_base,
                   int total_parts, int mode, PcgScalars* s, int grid0, int coarse_add = 1, int pair = 0,
-                  const CgArgs& cg = CgArgs{}, double* partial_rr = nullptr)
+                  const FusedArgs& fa = FusedArgs{}, double* partial_rr = nullptr)
 {
   const int d0 = h->lv.dom_begin[1];
   if (std::is_same<TI, float>::value) variant = kApplyDirect;
@@ -1775,48 +1764,35 @@ void level0_apply(maspcg_handle* h, const ApplyArgs& a, int variant, const Tv* r
   switch (variant) {
     case kApplyStaged2:
       if constexpr (sizeof(TI) == 2)
-        launch_apply_tma<TI, Tv, Tacc, true, 2, kCg>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
-                                                     coarse_add, pair, cg, partial_rr);
+        launch_apply_tma<TI, Tv, Tacc, true, 2, kFused>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0,
+                                                        grid0, coarse_add, pair, fa, partial_rr);
       break;
     case kApplyStaged1:
       if constexpr (sizeof(TI) == 2)
-        launch_apply_tma<TI, Tv, Tacc, true, 1, kCg>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0, grid0,
-                                                     coarse_add, pair, cg, partial_rr);
+        launch_apply_tma<TI, Tv, Tacc, true, 1, kFused>(h, a, r, z, partial, part_base, total_parts, mode, s, 0, d0,
+                                                        grid0, coarse_add, pair, fa, partial_rr);
       break;
+
     default:
-      launch_pdl(h, k_level0_apply<TI, Tv, Tacc, kCg>, dim3(grid0), dim3(kApplyTpb),
+      launch_pdl(h, k_level0_apply<TI, Tv, Tacc, kFused>, dim3(grid0), dim3(kApplyTpb),
                  sizeof(TI) == 2 ? kDirectSmem16 : 0, a, r, z, partial, part_base, total_parts, mode, s, coarse_add,
-                 pair, cg, partial_rr);
+                 pair, fa, partial_rr);
       break;
   }
 }
 
-template <typename TI, typename Tv, bool kCg = false>
+template <typename TI, typename Tv, bool kFused = false>
 void launch_chain(maspcg_handle* h, cudaStream_t st, const ApplyArgs& a, const Tv* r, PcgScalars* s, int mode, int pair,
-                  const CgArgs& cg = CgArgs{})
+                  const FusedArgs& fa = FusedArgs{})
 {
   constexpr int bytes = chain_smem_bytes<TI>();
-  auto kern = k_coarse_chain<TI, Tv, kCg>;
+  auto kern = k_coarse_chain<TI, Tv, kFused>;
   static bool configured = false;
   if (!configured && bytes > 48 * 1024)
     MCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   configured = true;
   launch_pdl_on(h, st, kern, dim3(ceil_div(h->c0 / kBank, kChainUnitBanks)), dim3(kChainWarps * 32), bytes, a, r, s,
-                mode, pair, cg);
-}
-
-// The coarse correction of z for every level-0 slot (CollectFinalZ of the
-// coarse levels): pc = sum over levels of the level's z at the slot's
-// ancestor, padded 4 per row; padding slots get zero.
-__global__ void __launch_bounds__(256) k_prolong(ApplyArgs a, float* pc, const PcgScalars* s)
-{
-  pdl_wait();
-  if (s && s->status != MASPCG_SOLVE_RUNNING) return;
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < a.c0; slot += gridDim.x * blockDim.x) {
-    float cc[3];
-    coarse_correction(a, slot, cc);
-    st_p4(pc, a.fem_off + slot, cc[0], cc[1], cc[2]);
-  }
+                mode, pair, fa);
 }
 
 // The MAS apply.  Sequential form: the coarse levels, then the level-0 apply
@@ -1847,34 +1823,38 @@ void mas_apply_t(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_b
   MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
 }
 
-// The MAS apply of the single-reduction recurrence: the level-0 apply
-// writes z0 (padded) behind the iteration's update (cg.update), the coarse
-// levels restrict the same updated residual and the prolongation writes the
-// coarse part pc; r.z is completed from the two parts (R.Z of the coarse
-// levels and r.z0), r.r of the update comes from the level-0 apply.  The
-// coarse levels run on the side stream (overlap) or before the level-0 apply.
+// The MAS apply behind the iteration's fused x / r update (fa.update; else
+// fa.r[cur] is the residual): the level-0 apply updates its rows and
+// preconditions r', the coarse levels restrict the same r' formed again.
+// Overlapped (inside the solve, outside the reference precision): the coarse
+// levels run on the side stream, r.z is completed from the two parts and the
+// next p update adds the coarse correction; else they run first and the
+// level-0 apply adds it.  r.r of the update comes from the level-0 apply.
 template <typename TI, typename Tacc>
-void mas_apply_cg_t(maspcg_handle* h, const CgArgs& cg, float* pc, Tacc* partial, double* partial_rr, int part_base,
-                    int total_parts, int mode, int grid0, PcgScalars* s, bool overlap)
+void mas_apply_fused_t(maspcg_handle* h, const FusedArgs& fa, float* z, Tacc* partial, double* partial_rr,
+                       int part_base, int total_parts, int mode, int grid0, PcgScalars* s, bool overlap)
 {
   ApplyArgs a = make_apply_args(h);
   const LevelInfo& lv = h->lv;
   const int variant = std::is_same<TI, float>::value ? (int)kApplyDirect : h->apply_variant;
-  const bool coarse = lv.levelnum > 1;
-  cudaStream_t side = overlap ? h->side_stream : h->stream;
-  if (coarse) {
-    if (overlap) {
-      MCK(cudaEventRecord(h->ev_fork, h->stream));
-      MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
-    }
-    launch_chain<TI, float, true>(h, side, a, nullptr, s, mode, 1, cg);
-    launch_pdl_on(h, side, k_prolong, dim3(std::max(1, std::min(ceil_div(h->c0, 256), 4 * h->sm_count))), dim3(256), 0,
-                  a, pc, (const PcgScalars*)s);
-    if (overlap) MCK(cudaEventRecord(h->ev_join, h->side_stream));
+  if (lv.levelnum <= 1) {
+    level0_apply<TI, float, Tacc, true>(h, a, variant, nullptr, z, partial, part_base, total_parts, mode, s, grid0, 1,
+                                        0, fa, partial_rr);
+    return;
   }
-  level0_apply<TI, float, Tacc, true>(h, a, variant, nullptr, nullptr, partial, part_base, total_parts, mode, s, grid0,
-                                      0, coarse ? 1 : 0, cg, partial_rr);
-  if (coarse && overlap) MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+  if (!overlap) {
+    launch_chain<TI, float, true>(h, h->stream, a, nullptr, s, mode, 0, fa);
+    level0_apply<TI, float, Tacc, true>(h, a, variant, nullptr, z, partial, part_base, total_parts, mode, s, grid0, 1,
+                                        0, fa, partial_rr);
+    return;
+  }
+  MCK(cudaEventRecord(h->ev_fork, h->stream));
+  MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+  launch_chain<TI, float, true>(h, h->side_stream, a, nullptr, s, mode, 1, fa);
+  MCK(cudaEventRecord(h->ev_join, h->side_stream));
+  level0_apply<TI, float, Tacc, true>(h, a, variant, nullptr, z, partial, part_base, total_parts, mode, s, grid0, 0, 1,
+                                      fa, partial_rr);
+  MCK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
 }
 
 }  // namespace
@@ -1901,27 +1881,27 @@ void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_bas
 }
 
 template <typename Tacc>
-void mas_apply_cg(maspcg_handle* h, const CgArgs& cg, float* pc, Tacc* partial, double* partial_rr, int part_base,
-                  int total_parts, int mode, int grid0, PcgScalars* s, bool overlap)
+void mas_apply_fused(maspcg_handle* h, const FusedArgs& fa, float* z, Tacc* partial, double* partial_rr, int part_base,
+                     int total_parts, int mode, int grid0, PcgScalars* s, bool overlap)
 {
   switch (h->cfg.inverse_storage) {
     case MASPCG_INV_BF16:
-      mas_apply_cg_t<__nv_bfloat16, Tacc>(h, cg, pc, partial, partial_rr, part_base, total_parts, mode, grid0, s,
-                                          overlap);
+      mas_apply_fused_t<__nv_bfloat16, Tacc>(h, fa, z, partial, partial_rr, part_base, total_parts, mode, grid0, s,
+                                             overlap);
       break;
     case MASPCG_INV_FP16:
-      mas_apply_cg_t<__half, Tacc>(h, cg, pc, partial, partial_rr, part_base, total_parts, mode, grid0, s, overlap);
+      mas_apply_fused_t<__half, Tacc>(h, fa, z, partial, partial_rr, part_base, total_parts, mode, grid0, s, overlap);
       break;
     default:
-      mas_apply_cg_t<float, Tacc>(h, cg, pc, partial, partial_rr, part_base, total_parts, mode, grid0, s, overlap);
+      mas_apply_fused_t<float, Tacc>(h, fa, z, partial, partial_rr, part_base, total_parts, mode, grid0, s, overlap);
       break;
   }
   MCK(cudaGetLastError());
 }
-template void mas_apply_cg<float>(maspcg_handle*, const CgArgs&, float*, float*, double*, int, int, int, int,
-                                  PcgScalars*, bool);
-template void mas_apply_cg<double>(maspcg_handle*, const CgArgs&, float*, double*, double*, int, int, int, int,
-                                   PcgScalars*, bool);
+template void mas_apply_fused<float>(maspcg_handle*, const FusedArgs&, float*, float*, double*, int, int, int, int,
+                                     PcgScalars*, bool);
+template void mas_apply_fused<double>(maspcg_handle*, const FusedArgs&, float*, double*, double*, int, int, int, int,
+                                      PcgScalars*, bool);
 
 // Stage timing helpers: the level-0 domain apply alone, and the domain
 // assembly + inversion alone (member lists from the last build).

@@ -25,16 +25,24 @@ struct ApplyArgs {
 
 // Coarse correction of a level-0 slot: the sum over the coarse levels of the
 // level's z at the slot's ancestor (the prolongation, CollectFinalZ).  Returns
-// false for a padding slot, whose z is zero.
+// false for a padding slot, whose z is zero.  The ancestors are loaded
+// together with the padding mark (none depends on another), so the
+// correction costs two dependent loads, not three.
 __device__ __forceinline__ bool coarse_correction(const ApplyArgs& a, int slot, float c[3])
 {
   c[0] = c[1] = c[2] = 0.f;
+  int node[kMaxLevels];
+#pragma unroll
+  for (int l = 1; l < kMaxLevels; ++l) node[l] = l < a.lv.levelnum ? __ldg(a.cmap[l] + slot) : -1;
   if (a.pmr[slot] < 0) return false;
-  for (int l = 1; l < a.lv.levelnum; ++l) {
-    const float* q = a.coarse_z + 3 * (size_t)(a.lv.begin[l] - a.c0 + a.cmap[l][slot]);
-    c[0] += q[0];
-    c[1] += q[1];
-    c[2] += q[2];
+#pragma unroll
+  for (int l = 1; l < kMaxLevels; ++l) {
+    if (l < a.lv.levelnum) {
+      const float* q = a.coarse_z + 3 * (size_t)(a.lv.begin[l] - a.c0 + node[l]);
+      c[0] += q[0];
+      c[1] += q[1];
+      c[2] += q[2];
+    }
   }
   return true;
 }

@@ -133,9 +133,11 @@ struct PcgScalars {
   double rz_part[2];  // r.z of the level-0 apply (0) and of the coarse levels (1) when they run concurrently
   unsigned tickets[10];
   unsigned barrier_gen;  // generation of the grid barrier of the fused iteration kernel
-  int cg_cur;            // single-reduction recurrence: which of the two r / s buffers holds the current vectors
+  int rbuf;              // fused x / r update: which of the two r buffers holds the current residual
   long long barrier_limit;  // spins a grid-barrier wait may take before it gives up (maspcg_set_wait_test_hooks)
   int barrier_extra;        // arrivals a grid barrier expects beyond the grid (test hook: > 0 never completes)
+  double rr_peak;           // MIXED: largest r.r since the last residual replacement (b.b at the start)
+  int replace_mode;         // MIXED: maspcg_replacement
 };
 
 constexpr int kNeedTrue = 16;  // MIXED: recursive gate met or period end; true residual pending
@@ -214,14 +216,8 @@ struct maspcg_handle {
   maspcg::DBuf<int> int_of_row, row_of_int;
   maspcg::DBuf<int> rowptr, colidx;
   maspcg::DBuf<double> val64;     // row-major 3x3 blocks
-  // FP32 matrix of the iteration (FP32 / MIXED precision) in the sliced
-  // jagged-diagonal layout of spmv_jds.cuh, and the rows it leaves to the
-  // FP64 row path
-  maspcg::DBuf<int> jds_hdr, jds_xrows, jds_xflag, jds_xpos, jds_len;
-  maspcg::DBuf<long long> jds_srec, jds_bytes;
-  maspcg::DBuf<unsigned char> jds_perm, jds_data;
-  int jds_slices = 0, jds_nx = 0;
-  long long jds_data_bytes = 0;
+  maspcg::DBuf<float> val32;      // tiles of 32 blocks, element-major: (t/32)*288 + 32e + t%32
+  maspcg::DBuf<unsigned short> val_lo;  // MASPCG_MATRIX_F32_SPLIT: BF16 of A - A32, laid out as val32
   maspcg::DBuf<unsigned long long> keys, keys_sorted;
   maspcg::DBuf<int> kv, kv_sorted, seg_head, seg_start, row_count;
   maspcg::DBuf<double> in_vals;
@@ -248,10 +244,7 @@ struct maspcg_handle {
   maspcg::DBuf<unsigned char> vp4;                  // search direction, padded to 4 per block row
   maspcg::DBuf<double> b64, x64, r64;               // FP64: rhs, x (hi), residual scratch
   maspcg::DBuf<double> partial, partial_rz, partial_rr;
-  // single-reduction recurrence (FP32 / MIXED with MAS32): the second r
-  // buffer, the two s buffers, p, and the padded level-0 (z0) and coarse (pc)
-  // parts of z; vz holds z, vap holds w = A z
-  maspcg::DBuf<unsigned char> cg_r2, cg_s0, cg_s1, cg_p, cg_z0, cg_pc;
+  maspcg::DBuf<unsigned char> vr2;  // second residual buffer of the fused x / r update (FP32 / MIXED)
   maspcg::DBuf<maspcg::PcgScalars> scal;
   maspcg::PcgScalars* h_scal = nullptr;  // pinned mirror
   maspcg::DBuf<double> io_a, io_b;       // staging for host pointers / permutations
@@ -282,8 +275,7 @@ struct maspcg_handle {
   bool vals_pending = false;      // set_matrix_bcoo: host values still copying on side_stream (ev_join)
   bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
   int apply_variant = 2;          // 16-bit level-0 apply: 0 direct loads, 1 TMA-staged x2 buffers, 2 TMA-staged x1
-  bool spmv_staged = true;        // FP32 SpMV records staged by bulk copies (off: MASPCG_FLAG_SPMV_DIRECT)
-  bool use_cg = true;             // single-reduction recurrence where it applies (off: MASPCG_FLAG_TWO_REDUCTION)
+  bool fuse_update = false;       // x / r update inside the apply kernels (MASPCG_FLAG_FUSED_UPDATE)
   long long barrier_limit = 1ll << 24;  // grid-barrier wait bound (spins of 64 ns sleeps)
   int barrier_extra = 0;                // test hook: extra arrivals a grid barrier waits for
 };
@@ -295,8 +287,6 @@ void build_hierarchy(maspcg_handle* h);
 
 // matrix.cu
 void build_internal_matrix(maspcg_handle* h, const double* vals_dev, const int* rows_dev, const int* cols_dev, int n);
-void build_jds(maspcg_handle* h);  // FP32 sliced layout from the FP64 BCSR (FP32 / MIXED precision)
-void fill_jds(maspcg_handle* h);   // its values only (structure unchanged)
 // New values for the structure of the last build_internal_matrix (same
 // triplets in the same order): the FP64 BCSR values and the FP32 layout.
 void refresh_internal_values(maspcg_handle* h, const double* vals_dev);

@@ -14,7 +14,6 @@
 
 #include "maspcg_internal.cuh"
 #include "spmv_row.cuh"
-#include "spmv_jds.cuh"
 
 namespace maspcg {
 namespace {
@@ -74,7 +73,8 @@ __global__ void k_fill_structure(const unsigned long long* __restrict__ keys, co
 // One thread per stored block: sum its input blocks in sorted (= input) order.
 __global__ void k_fill_values(const unsigned long long* __restrict__ keys, const int* __restrict__ vals_sorted,
                               const int* __restrict__ seg_start, int nnzb, int m_valid,
-                              const double* __restrict__ in_vals, double* val64)
+                              const double* __restrict__ in_vals, double* val64, float* val32,
+                              unsigned short* val_lo)
 {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nnzb) return;
@@ -98,7 +98,15 @@ __global__ void k_fill_values(const unsigned long long* __restrict__ keys, const
     }
   }
 #pragma unroll
-  for (int q = 0; q < 9; ++q) val64[9 * (size_t)u + q] = a[q];
+  for (int q = 0; q < 9; ++q) {
+    val64[9 * (size_t)u + q] = a[q];
+    const size_t at = (size_t)(u >> 5) * 288 + 32 * q + (u & 31);  // tiles of 32 blocks, element-major
+    const float hi = (float)a[q];
+    val32[at] = hi;
+    // the remainder a - hi is exact in FP64; its BF16 rounding carries A to
+    // about 2^-32 relative
+    if (val_lo) val_lo[at] = __bfloat16_as_ushort(__float2bfloat16_rn((float)(a[q] - (double)hi)));
+  }
 }
 
 // y = a*A*x + b*y, FP64, half-warp per block row.
@@ -230,94 +238,6 @@ __global__ void k_abd_inverse(const int* __restrict__ rowptr, const int* __restr
     }
 }
 
-// ---- the FP32 sliced jagged-diagonal matrix (spmv_jds.cuh) ---------------
-
-// Rows on the FP64 row path: the affine bodies [0, n64) and rows longer than
-// kJdsMaxLen blocks.
-__global__ void k_jds_flags(const int* __restrict__ rowptr, int nrows, int n64, int* xflag)
-{
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nrows) return;
-  xflag[r] = (r < n64 || rowptr[r + 1] - rowptr[r] > kJdsMaxLen) ? 1 : 0;
-}
-
-__global__ void k_jds_xrows(const int* __restrict__ xflag, const int* __restrict__ xpos, int nrows, int* xrows)
-{
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nrows && xflag[r]) xrows[xpos[r]] = r;
-}
-
-// Length of the slice row of lane `lane` in slice s (0 past the end and on
-// the FP64 row path).
-__device__ __forceinline__ int jds_row_len(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows,
-                                           int s, int lane)
-{
-  const int r = 32 * s + lane;
-  return (r < nrows && !xflag[r]) ? rowptr[r + 1] - rowptr[r] : 0;
-}
-
-// One warp per slice: rank the rows by length (longest first, ties by row),
-// the rank -> row map, the slice's header (entries rounded up to even, the
-// width, and the column offsets coff[k] = sum over its rows of min(length,
-// k)), and the record's size in bytes.
-__global__ void k_jds_slices(const int* __restrict__ rowptr, const int* __restrict__ xflag, int nrows, int slices,
-                             unsigned char* perm, int* hdr, long long* bytes)
-{
-  const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (s >= slices) return;  // whole warp
-  const int r = 32 * s + lane;
-  const int len = jds_row_len(rowptr, xflag, nrows, s, lane);
-  int rank = 0;
-  for (int j = 0; j < 32; ++j) {
-    const int lj = __shfl_sync(kFull, len, j);
-    rank += (lj > len || (lj == len && j < lane)) ? 1 : 0;
-  }
-  const bool skip = r >= nrows || xflag[r];
-  perm[32 * (size_t)s + rank] = (unsigned char)(lane | (skip ? 0x80 : 0));
-  const int width = (int)__reduce_max_sync(kFull, (unsigned)len);
-  const int total = (int)__reduce_add_sync(kFull, (unsigned)len);
-  const int ep = total + (total & 1);
-  int* hd = hdr + (size_t)kJdsHeader * s;
-  for (int k = 0; k < kJdsHeader - 2; ++k) {
-    const int v = (int)__reduce_add_sync(kFull, (unsigned)min(len, k));
-    if (lane == 0) hd[2 + k] = k <= width ? v : total;
-  }
-  if (lane == 0) {
-    hd[0] = ep;
-    hd[1] = width;
-    bytes[s] = 40LL * ep;
-  }
-}
-
-// One warp per slice, lane = rank: the row's blocks in column order into the
-// slice record, rounded to FP32.
-__global__ void k_jds_fill(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                           const double* __restrict__ val64, int slices, const int* __restrict__ hdr,
-                           const long long* __restrict__ srec, const unsigned char* __restrict__ perm,
-                           unsigned char* data)
-{
-  const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (s >= slices) return;
-  const unsigned pm = perm[32 * (size_t)s + lane];
-  if (pm & 0x80u) return;
-  const int r = 32 * s + (int)(pm & 31u);
-  const int rs = rowptr[r], len = rowptr[r + 1] - rs;
-  const int* hd = hdr + (size_t)kJdsHeader * s;
-  const int ep = hd[0];
-  unsigned char* rec = data + srec[s];
-  float4* pa = reinterpret_cast<float4*>(rec);
-  float4* pb = reinterpret_cast<float4*>(rec + 16 * (size_t)ep);
-  float2* pc = reinterpret_cast<float2*>(rec + 32 * (size_t)ep);
-  for (int k = 0; k < len; ++k) {
-    const int t = rs + k;
-    const int e = hd[2 + k] + lane;
-    const double* m = val64 + 9 * (size_t)t;
-    pa[e] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
-    pb[e] = make_float4((float)m[4], (float)m[5], (float)m[6], (float)m[7]);
-    pc[e] = make_float2((float)m[8], __int_as_float(colidx[t]));
-  }
-}
-
 size_t cub_bytes_sort(int m, int end_bit)
 {
   size_t b = 0;
@@ -401,6 +321,8 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
   h->nnzb = nnzb;
   h->colidx.resize(nnzb, 4);  // 16-byte tail for TMA bulk copies
   h->val64.resize((size_t)9 * nnzb, 2);
+  h->val32.resize((size_t)9 * (((size_t)nnzb + 31) / 32 * 32));
+  if (h->cfg.matrix_form == MASPCG_MATRIX_F32_SPLIT) h->val_lo.resize(h->val32.n);
   h->row_count.resize(nb_int + 1);
   h->rowptr.resize(nb_int + 1);
   MCK(cudaMemsetAsync(h->row_count.get(), 0, sizeof(int) * (nb_int + 1), st));
@@ -414,62 +336,9 @@ void build_internal_matrix(maspcg_handle* h, const double* vals, const int* rows
     h->vals_pending = false;
   }
   k_fill_values<<<ceil_div(nnzb, kTpb), kTpb, 0, st>>>(h->keys_sorted.get(), h->kv_sorted.get(), h->seg_start.get(),
-                                                      nnzb, m_valid, vals, h->val64.get());
-  MLAUNCHED(h);
-  MCK(cudaGetLastError());
-  if (h->cfg.precision != MASPCG_PREC_REFERENCE) build_jds(h);
-}
-
-void build_jds(maspcg_handle* h)
-{
-  cudaStream_t st = h->stream;
-  const int nrows = h->nb_int;
-  const int slices = ceil_div(nrows, 32);
-  const int n64 = 4 * h->abd_bodies;
-  h->jds_slices = slices;
-  h->jds_xflag.resize(nrows + 1);
-  h->jds_xpos.resize(nrows + 1);
-  h->jds_perm.resize(32 * (size_t)slices);
-  h->jds_hdr.resize((size_t)kJdsHeader * slices);
-  h->jds_srec.resize(slices + 1);
-  h->jds_bytes.resize(slices + 1);
-  MCK(cudaMemsetAsync(h->jds_xflag.get() + nrows, 0, sizeof(int), st));
-  MCK(cudaMemsetAsync(h->jds_bytes.get() + slices, 0, sizeof(long long), st));
-  k_jds_flags<<<ceil_div(nrows, kTpb), kTpb, 0, st>>>(h->rowptr.get(), nrows, n64, h->jds_xflag.get());
-  MLAUNCHED(h);
-  const int wgrid = ceil_div(32LL * slices, kTpb);
-  k_jds_slices<<<wgrid, kTpb, 0, st>>>(h->rowptr.get(), h->jds_xflag.get(), nrows, slices, h->jds_perm.get(),
-                                       h->jds_hdr.get(), h->jds_bytes.get());
-  MLAUNCHED(h);
-  size_t b1 = 0, b2 = 0;
-  MCK(cub::DeviceScan::ExclusiveSum(nullptr, b1, (const int*)nullptr, (int*)nullptr, nrows + 1));
-  MCK(cub::DeviceScan::ExclusiveSum(nullptr, b2, (const long long*)nullptr, (long long*)nullptr, slices + 1));
-  h->cub_tmp.resize(std::max({b1, b2, h->cub_tmp.n}));
-  size_t b = h->cub_tmp.cap;
-  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, h->jds_xflag.get(), h->jds_xpos.get(), nrows + 1, st));
-  b = h->cub_tmp.cap;
-  MCK(cub::DeviceScan::ExclusiveSum(h->cub_tmp.get(), b, h->jds_bytes.get(), h->jds_srec.get(), slices + 1, st));
-  int nx = 0;
-  long long total = 0;
-  MCK(cudaMemcpyAsync(&nx, h->jds_xpos.get() + nrows, sizeof(int), cudaMemcpyDeviceToHost, st));
-  MCK(cudaMemcpyAsync(&total, h->jds_srec.get() + slices, sizeof(long long), cudaMemcpyDeviceToHost, st));
-  MCK(cudaStreamSynchronize(st));
-  h->jds_nx = nx;
-  h->jds_data_bytes = total;
-  h->jds_xrows.resize(std::max(nx, 1));
-  h->jds_data.resize(std::max<long long>(total, 16));
-  k_jds_xrows<<<ceil_div(nrows, kTpb), kTpb, 0, st>>>(h->jds_xflag.get(), h->jds_xpos.get(), nrows,
-                                                      h->jds_xrows.get());
-  MLAUNCHED(h);
-  fill_jds(h);
-}
-
-void fill_jds(maspcg_handle* h)
-{
-  const int slices = h->jds_slices;
-  k_jds_fill<<<ceil_div(32LL * slices, kTpb), kTpb, 0, h->stream>>>(h->rowptr.get(), h->colidx.get(), h->val64.get(),
-                                                                    slices, h->jds_hdr.get(), h->jds_srec.get(),
-                                                                    h->jds_perm.get(), h->jds_data.get());
+                                                      nnzb, m_valid, vals, h->val64.get(), h->val32.get(),
+                                                      h->cfg.matrix_form == MASPCG_MATRIX_F32_SPLIT ? h->val_lo.get()
+                                                                                                    : nullptr);
   MLAUNCHED(h);
   MCK(cudaGetLastError());
 }
@@ -483,10 +352,12 @@ void refresh_internal_values(maspcg_handle* h, const double* vals)
   }
   k_fill_values<<<ceil_div(h->nnzb, kTpb), kTpb, 0, st>>>(h->keys_sorted.get(), h->kv_sorted.get(),
                                                           h->seg_start.get(), h->nnzb, h->m_valid, vals,
-                                                          h->val64.get());
+                                                          h->val64.get(), h->val32.get(),
+                                                          h->cfg.matrix_form == MASPCG_MATRIX_F32_SPLIT
+                                                              ? h->val_lo.get()
+                                                              : nullptr);
   MLAUNCHED(h);
   MCK(cudaGetLastError());
-  if (h->cfg.precision != MASPCG_PREC_REFERENCE) fill_jds(h);
 }
 
 void launch_spmv64(maspcg_handle* h, const double* x, double* y, double a, double b)

@@ -22,7 +22,6 @@
 #include "pcg_device.cuh"
 #include "mas_args.cuh"
 #include "spmv_row.cuh"
-#include "spmv_jds.cuh"
 
 namespace maspcg {
 
@@ -33,8 +32,8 @@ void mas_apply(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int part_bas
 template <typename Tv, typename Tacc>
 void mas_level0_only(maspcg_handle* h, const Tv* r, Tv* z, Tacc* partial, int grid0, PcgScalars* s, int variant);
 template <typename Tacc>
-void mas_apply_cg(maspcg_handle* h, const CgArgs& cg, float* pc, Tacc* partial, double* partial_rr, int part_base,
-                  int total_parts, int mode, int grid0, PcgScalars* s, bool overlap);
+void mas_apply_fused(maspcg_handle* h, const FusedArgs& fa, float* z, Tacc* partial, double* partial_rr, int part_base,
+                     int total_parts, int mode, int grid0, PcgScalars* s, bool overlap);
 void launch_factor(maspcg_handle* h, double* assembled_out);
 int mas_level0_grid(maspcg_handle* h);
 template <typename Tv, typename Tacc>
@@ -63,8 +62,10 @@ __global__ void __launch_bounds__(kTpb) k_init(const double* __restrict__ b, Tv*
   }
   double total = 0.0;
   if (grid_finish<double>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketAux], gridDim.x, total) &&
-      threadIdx.x == 0)
+      threadIdx.x == 0) {
     s->bb = total;
+    s->rr_peak = total;
+  }
 }
 
 // Entries [4q, 4q + 4) of a vector as 16-byte (FP32) / 2 x 16-byte (FP64)
@@ -132,26 +133,53 @@ __global__ void __launch_bounds__(kTpb) k_update_p(ApplyArgs a, const Tv* __rest
   update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
 }
 
-// One row-major 3x3 block of the FP64 matrix.
+// One 3x3 block of the matrix.  FP32: tiles of 32 blocks stored element-major
+// (element e of block t at (t/32)*288 + 32e + t%32), so a warp's element loads
+// are coalesced and a tile is one contiguous 1152-byte run.  FP64: row-major
+// blocks.
 template <bool kTiled, typename Tm>
 __device__ __forceinline__ void load_block(const Tm* __restrict__ val, int t, Tm m[9])
 {
-  static_assert(!kTiled, "the FP32 matrix uses the sliced layout of spmv_jds.cuh");
+  if (kTiled) {
+    const Tm* b = val + (size_t)(t >> 5) * 288 + (t & 31);
 #pragma unroll
-  for (int e = 0; e < 9; ++e) m[e] = __ldcs(val + 9 * (size_t)t + e);
+    for (int e = 0; e < 9; ++e) m[e] = __ldcs(b + 32 * e);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = __ldcs(val + 9 * (size_t)t + e);
+  }
 }
 
-// Ap = A p for block rows [lo, nrows) in the matrix's own precision;
-// returns this thread's share of p.Ap.  LPR lanes per block row and two row
-// groups per thread in flight at once (rows r and r + stride); each lane
-// takes two blocks of each row per step and issues all four blocks' loads
-// before the arithmetic.
-template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR>
-__device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                          const Tm* __restrict__ val, const Tv* __restrict__ p4, Tv* ap, int lo,
-                                          int nrows)
+// The BF16 remainder of an FP32 tile block (MASPCG_MATRIX_F32_SPLIT), at the
+// same positions as load_block's tiles.
+__device__ __forceinline__ void load_block_lo(const unsigned short* __restrict__ lo, int t, float m[9])
 {
-  using A = typename AccOf<Tm>::type;
+  const unsigned short* b = lo + (size_t)(t >> 5) * 288 + (t & 31);
+#pragma unroll
+  for (int e = 0; e < 9; ++e) m[e] = __uint_as_float((uint32_t)__ldcs(b + 32 * e) << 16);
+}
+
+// Accumulator of the SpMV rows: FP64 for the FP64 matrix and for the FP32
+// forms with FP64 sums (each FP32 x FP32 product is exact in FP64).
+template <typename Tm, int kForm>
+using SpmvAcc = typename std::conditional<std::is_same<Tm, float>::value && kForm == MASPCG_MATRIX_F32, float,
+                                          double>::type;
+
+// Ap = A p for block rows [lo, nrows); returns this thread's share of p.Ap.
+// LPR lanes per block row and two row groups per thread in flight at once
+// (rows r and r + stride); each lane takes kPer blocks of each row per step
+// and issues all their loads before the arithmetic (kPer = 2 with FP32 sums;
+// 1 with FP64 sums, whose accumulators and converted operands take the
+// registers of the second pair).  kForm (FP32 tiles): the
+// maspcg_matrix_form, i.e. FP32 or FP64 sums, and with the split form the
+// BF16 remainder's products summed beside them in FP32.
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, int kForm>
+__device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                          const Tm* __restrict__ val, const unsigned short* __restrict__ val_lo,
+                                          const Tv* __restrict__ p4, Tv* ap, int lo, int nrows)
+{
+  using A = SpmvAcc<Tm, kForm>;
+  constexpr bool kSplit = kTiled && kForm == MASPCG_MATRIX_F32_SPLIT;
   constexpr int kRows = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
   const int step = gridDim.x * kRows;
@@ -165,22 +193,31 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
   int nsa, nea, nsb, neb;
   extent(lo + blockIdx.x * kRows + threadIdx.x / LPR, nsa, nea);
   extent(lo + blockIdx.x * kRows + threadIdx.x / LPR + step, nsb, neb);
+  constexpr int kPer = std::is_same<A, double>::value && kTiled ? 1 : 2;
+  constexpr int kIn = 2 * kPer;  // blocks in flight per step
   for (int row0 = lo + blockIdx.x * kRows; row0 < nrows; row0 += 2 * step) {
     const int ra = row0 + threadIdx.x / LPR, rb = ra + step;
     const int sa = nsa, ea = nea, sb = nsb, eb = neb;
     extent(ra + 2 * step, nsa, nea);
     extent(rb + 2 * step, nsb, neb);
     A a[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    const int na = (ea - sa + 2 * LPR - 1) / (2 * LPR), nbk = (eb - sb + 2 * LPR - 1) / (2 * LPR);
+    float al[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};  // kSplit: the remainder's products
+    const int na = (ea - sa + kPer * LPR - 1) / (kPer * LPR), nbk = (eb - sb + kPer * LPR - 1) / (kPer * LPR);
     const int steps = max(__reduce_max_sync(kFull, (unsigned)na), __reduce_max_sync(kFull, (unsigned)nbk));
     for (int k = 0; k < steps; ++k) {
-      int tt[4] = {sa + sub + 2 * LPR * k, sa + sub + 2 * LPR * k + LPR, sb + sub + 2 * LPR * k,
-                   sb + sub + 2 * LPR * k + LPR};
-      const bool in[4] = {tt[0] < ea, tt[1] < ea, tt[2] < eb, tt[3] < eb};
-      Tm m[4][9];
-      int c[4];
+      // blocks j < kPer of row a, the rest of row b
+      int tt[kIn];
+      bool in[kIn];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kIn; ++j) {
+        const int half = j / kPer, i = j % kPer;
+        tt[j] = (half ? sb : sa) + sub + kPer * LPR * k + i * LPR;
+        in[j] = tt[j] < (half ? eb : ea);
+      }
+      Tm m[kIn][9];
+      int c[kIn];
+#pragma unroll
+      for (int j = 0; j < kIn; ++j) {
         c[j] = in[j] ? __ldcs(colidx + tt[j]) : 0;
         if (in[j]) {
           load_block<kTiled>(val, tt[j], m[j]);
@@ -190,13 +227,32 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
         }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kIn; ++j) {
         const P4<Tv> x = ld_p4(p4, c[j]);
-        A* o = a[j >> 1];
+        A* o = a[j / kPer];
         o[0] += (A)m[j][0] * (A)x.x + (A)m[j][1] * (A)x.y + (A)m[j][2] * (A)x.z;
         o[1] += (A)m[j][3] * (A)x.x + (A)m[j][4] * (A)x.y + (A)m[j][5] * (A)x.z;
         o[2] += (A)m[j][6] * (A)x.x + (A)m[j][7] * (A)x.y + (A)m[j][8] * (A)x.z;
+        if constexpr (kSplit) {
+          float w[9];
+          if (in[j]) {
+            load_block_lo(val_lo, tt[j], w);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 9; ++e) w[e] = 0.f;
+          }
+          float* ol = al[j / kPer];
+          ol[0] += w[0] * (float)x.x + w[1] * (float)x.y + w[2] * (float)x.z;
+          ol[1] += w[3] * (float)x.x + w[4] * (float)x.y + w[5] * (float)x.z;
+          ol[2] += w[6] * (float)x.x + w[7] * (float)x.y + w[8] * (float)x.z;
+        }
       }
+    }
+    if constexpr (kSplit) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) a[h][q] += (A)al[h][q];
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h)
@@ -236,86 +292,82 @@ __device__ __forceinline__ void spmv_finish(PcgScalars* s, double pap)
   }
 }
 
-// The SpMV of the iteration with p.Ap; the last block computes alpha.
-// FP64 matrix (reference precision): full BCSR, LPR lanes per block row.
-template <int LPR>
-__global__ void __launch_bounds__(kTpb) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                                const double* __restrict__ val, const double* __restrict__ p4,
-                                                double* ap, int nrows, double* partial, PcgScalars* s)
+// Ap for block rows [0, n64) from the FP64 matrix with FP64 sums, used when
+// the iteration runs on the FP32 tiles: these are the affine-body rows, whose
+// 12x12 blocks carry the orthogonality stiffness (~1e7 on the diagonal)
+// beside rotation modes held only by the mass (~1e-4), a spread FP32 values
+// or sums cannot keep positive definite.
+template <typename Tv, typename Tacc, int LPR>
+__device__ __forceinline__ Tacc spmv_rows_exact(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                                const double* __restrict__ val64, const Tv* __restrict__ p4, Tv* ap,
+                                                int n64)
 {
-  pdl_wait();
-  if (!running(s)) return;
-  const double dot = spmv_rows<double, double, double, false, LPR>(rowptr, colidx, val, p4, ap, 0, nrows);
-  pdl_trigger();
-  double total = 0;
-  if (grid_finish<double>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
-      threadIdx.x == 0)
-    spmv_finish(s, total);
+  constexpr int kRows = kTpb / LPR;
+  const int sub = threadIdx.x % LPR;
+  double dot = 0.0;
+  for (int row0 = blockIdx.x * kRows; row0 < n64; row0 += gridDim.x * kRows) {
+    const int row = row0 + threadIdx.x / LPR;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (row < n64) {
+      const int re = __ldg(rowptr + row + 1);
+      for (int t = __ldg(rowptr + row) + sub; t < re; t += LPR) {
+        double m[9];
+        load_block<false>(val64, t, m);
+        const P4<Tv> x = ld_p4(p4, __ldcs(colidx + t));
+        a0 += m[0] * (double)x.x + m[1] * (double)x.y + m[2] * (double)x.z;
+        a1 += m[3] * (double)x.x + m[4] * (double)x.y + m[5] * (double)x.z;
+        a2 += m[6] * (double)x.x + m[7] * (double)x.y + m[8] * (double)x.z;
+      }
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(kFull, a0, o, LPR);
+      a1 += __shfl_xor_sync(kFull, a1, o, LPR);
+      a2 += __shfl_xor_sync(kFull, a2, o, LPR);
+    }
+    if (row < n64 && sub < 3) {
+      const Tv y = (Tv)(sub == 0 ? a0 : (sub == 1 ? a1 : a2));
+      ap[3 * (size_t)row + sub] = y;
+      const P4<Tv> pr = ld_p4(p4, row);
+      dot += (double)(sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z)) * (double)y;
+    }
+  }
+  return (Tacc)dot;
 }
 
-// FP32 matrix (FP32 / MIXED precision): the sliced jagged-diagonal layout,
-// with the affine-body and long rows from the FP64 BCSR.  Direct form: the
-// records are read from global memory.  kCg: the single-reduction
-// recurrence's SpMV w = A z with z gathered as z0 + pc (level-0 and coarse
-// parts of the apply), z written out, and alpha from delta = z.w.
-template <typename Tacc, bool kCg>
-__device__ __forceinline__ Tacc spmv_fp32(const JdsArgs& j, const int* __restrict__ rowptr,
-                                          const int* __restrict__ colidx, const double* __restrict__ val64,
-                                          const SpmvVec& v)
+// Both parts of the product: rows [0, n64) exact (n64 is 0 for the FP64
+// matrix), the rest from `val`.
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, int kForm>
+__device__ __forceinline__ Tacc spmv_all(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                         const Tm* __restrict__ val, const unsigned short* __restrict__ val_lo,
+                                         const double* __restrict__ val64, int n64, const Tv* __restrict__ p4,
+                                         Tv* ap, int nrows)
 {
   Tacc dot = 0;
-  if (j.nx > 0) dot = spmv_rows_listed<Tacc, 8, kCg>(rowptr, colidx, val64, j.xrows, j.nx, v);
-  return dot + spmv_jds_direct<Tacc, kJdsColumnsPerStep, kCg>(j, v);
+  if (n64 > 0) dot = spmv_rows_exact<Tv, Tacc, LPR>(rowptr, colidx, val64, p4, ap, n64);
+  return dot + spmv_rows<Tm, Tv, Tacc, kTiled, LPR, kForm>(rowptr, colidx, val, val_lo, p4, ap, n64, nrows);
 }
 
-__device__ __forceinline__ void spmv_end(PcgScalars* s, double total, bool cg)
-{
-  if (cg)
-    cg_alpha(s, total);
-  else
-    spmv_finish(s, total);
-}
+// Resident CTAs per SM the SpMV asks of the register allocator: three (80
+// registers) for the FP32 tiles in every form, two for the FP64 matrix.
+template <typename Tm, int kForm>
+constexpr int spmv_min_ctas() { return std::is_same<Tm, float>::value ? 3 : 2; }
 
-template <typename Tacc, bool kCg>
-__global__ void __launch_bounds__(kTpb) k_spmv_jds(JdsArgs j, const int* __restrict__ rowptr,
-                                                    const int* __restrict__ colidx, const double* __restrict__ val64,
-                                                    SpmvVec v, Tacc* partial, PcgScalars* s)
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, int kForm>
+__global__ void __launch_bounds__(kTpb, spmv_min_ctas<Tm, kForm>()) k_spmv(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                                const Tm* __restrict__ val, const unsigned short* __restrict__ val_lo,
+                                                const double* __restrict__ val64, int n64,
+                                                const Tv* __restrict__ p4, Tv* ap, int nrows, Tacc* partial,
+                                                PcgScalars* s)
 {
   pdl_wait();
   if (!running(s)) return;
-  const Tacc dot = spmv_fp32<Tacc, kCg>(j, rowptr, colidx, val64, v);
+  const Tacc dot = spmv_all<Tm, Tv, Tacc, kTiled, LPR, kForm>(rowptr, colidx, val, val_lo, val64, n64, p4, ap, nrows);
   pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0)
-    spmv_end(s, (double)total, kCg);
-}
-
-// Staged form: slice records bulk-copied into two shared-memory slots per
-// warp ahead of the arithmetic (spmv_jds_staged).  A wait that expires
-// records the error, stops the solve (status non-finite) and the whole CTA
-// leaves.
-template <typename Tacc, bool kCg>
-__global__ void __launch_bounds__(kJdsWarps * 32, 1) k_spmv_jds_staged(JdsArgs j, const int* __restrict__ rowptr,
-                                                                       const int* __restrict__ colidx,
-                                                                       const double* __restrict__ val64, SpmvVec v,
-                                                                       Tacc* partial, PcgScalars* s, int* err)
-{
-  extern __shared__ __align__(128) unsigned char jds_slots[];
-  __shared__ __align__(8) uint64_t jds_bars[2 * kJdsWarps];
-  pdl_wait();
-  if (!running(s)) return;
-  Tacc dot = 0;
-  if (j.nx > 0) dot = spmv_rows_listed<Tacc, 8, kCg>(rowptr, colidx, val64, j.xrows, j.nx, v);
-  const bool ok = spmv_jds_staged<Tacc, kJdsColumnsPerStep, kCg>(j, v, jds_slots, jds_bars, err, dot);
-  if (!ok && (threadIdx.x & 31) == 0) s->status = MASPCG_SOLVE_NONFINITE;
-  if (__syncthreads_or(!ok)) return;  // the whole CTA leaves together
-  pdl_trigger();
-  Tacc total = 0;
-  if (grid_finish<Tacc, kJdsWarps * 32>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x,
-                                        total) &&
-      threadIdx.x == 0)
-    spmv_end(s, (double)total, kCg);
+    spmv_finish(s, (double)total);
 }
 
 // x += alpha p, r -= alpha Ap for the entries this thread strides over;
@@ -375,21 +427,18 @@ __global__ void __launch_bounds__(kTpb) k_update_xr(Tv* x, Tv* r, const Tv* __re
 // update, a grid barrier, the SpMV with p.Ap and alpha, a grid barrier, the
 // x/r update with r.r and the gate.  Saves two kernel boundaries per
 // iteration; the barriers are bounded (grid_barrier).
-template <typename Tm, typename Tv, typename Tacc, int LPR, bool kCoarse>
-__global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, JdsArgs j, const int* __restrict__ rowptr,
-                                                          const int* __restrict__ colidx,
-                                                          const double* __restrict__ val64,
+template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, bool kCoarse, int kForm>
+__global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, const int* __restrict__ rowptr,
+                                                          const int* __restrict__ colidx, const Tm* __restrict__ val,
+                                                          const unsigned short* __restrict__ val_lo,
+                                                          const double* __restrict__ val64, int n64,
                                                           const Tv* __restrict__ z, Tv* p4, Tv* ap, Tv* x, Tv* r,
                                                           int nrows, int mixed, Tacc* partial, PcgScalars* s, int* err)
 {
   if (!running(s)) return;  // uniform: no CTA of this launch has written the status yet
   update_p_rows<Tv, kCoarse>(a, z, p4, nrows, s->k == 1, (Tv)s->beta);
   if (!grid_barrier(s, err)) return;
-  Tacc dot;
-  if constexpr (std::is_same<Tm, float>::value)
-    dot = spmv_fp32<Tacc, false>(j, rowptr, colidx, val64, SpmvVec{p4, nullptr, ap, nullptr});
-  else
-    dot = spmv_rows<double, double, double, false, LPR>(rowptr, colidx, val64, p4, ap, 0, nrows);
+  const Tacc dot = spmv_all<Tm, Tv, Tacc, kTiled, LPR, kForm>(rowptr, colidx, val, val_lo, val64, n64, p4, ap, nrows);
   Tacc total = 0;
   if (grid_finish<Tacc>(dot, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketSpmv], gridDim.x, total) &&
       threadIdx.x == 0)
@@ -416,6 +465,25 @@ __global__ void __launch_bounds__(kTpb) k_fold_x(double* xhi, float* xlo, int n,
   }
 }
 
+// MIXED, at the end of each graph of refinement_period iterations: is the
+// recursive residual replaced by the FP64 true residual now?  Always when the
+// recursive gate was met (kNeedTrue: the true residual decides the stop).
+// MASPCG_REPLACE_PERIODIC: at every graph end.  MASPCG_REPLACE_RELIABLE: once
+// ||r|| has fallen to kReliableDrop of the largest ||r|| since the last
+// replacement (a reliable update in the sense of Sleijpen and van der Vorst,
+// 1996): each replacement perturbs the Krylov recurrence by the gap between
+// the recursive and the true residual, so it is made where the residual has
+// shrunk enough that the gap is worth closing, a few times per decade of
+// reduction rather than every period.  Read at entry by both kernels of the
+// step; neither writes the scalars before its last block.
+constexpr double kReliableDrop = 0.1;
+__device__ __forceinline__ bool replace_due(const PcgScalars* s)
+{
+  if (s->status == kNeedTrue) return true;
+  if (s->status != MASPCG_SOLVE_RUNNING) return false;
+  return s->replace_mode == MASPCG_REPLACE_PERIODIC || s->rr <= kReliableDrop * kReliableDrop * s->rr_peak;
+}
+
 // MIXED: r = b - A x_hi in FP64 with the FP64 matrix; FP32 copy for the
 // iteration; last block: stop on the true residual or resume.
 template <int LPR>
@@ -425,8 +493,8 @@ __global__ void __launch_bounds__(kTpb) k_true_residual(const int* __restrict__ 
                                                          int nrows, double* partial, PcgScalars* s)
 {
   pdl_wait();
-  if (!(s->status == MASPCG_SOLVE_RUNNING || s->status == kNeedTrue)) return;
-  if (r32b && s->cg_cur) r32 = r32b;  // single-reduction recurrence: the buffer holding the current r
+  if (!replace_due(s)) return;
+  (void)r32b;
   const int groups_per_block = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
   double acc2 = 0.0;
@@ -449,7 +517,9 @@ __global__ void __launch_bounds__(kTpb) k_true_residual(const int* __restrict__ 
       threadIdx.x == 0) {
     s->rr_true = total;
     s->rr = total;
+    s->rr_peak = total;
     s->refinements += 1;
+    s->rbuf = 0;  // the replaced residual lives in the first r buffer
     if (!isfinite(total)) {
       s->status = MASPCG_SOLVE_NONFINITE;
       s->iterations = s->k;
@@ -571,19 +641,18 @@ __global__ void __launch_bounds__(kTpb) k_l2_evict(const uint4* __restrict__ p, 
   if (acc == 0xffffffffu) *sink = acc;
 }
 
-// Single-reduction recurrence, rows outside the MAS range: the iteration's
-// update of the row (cg.update), then its preconditioner (affine bodies:
-// 12x12 inverse; block-Jacobi rows: 3x3 inverse; else identity) into z0;
-// per-CTA r.z and r.r partials (the level-0 apply completes both).
+// Rows outside the MAS range behind the iteration's fused x / r update
+// (fa.update): the update of the row, then its preconditioner (affine bodies:
+// 12x12 inverse; other rows: identity, as in the reference) into z; per-CTA
+// r.z and r.r partials (the level-0 apply completes both).
 template <typename Tacc, typename Tinv>
-__global__ void __launch_bounds__(kTpb) k_other_apply_cg(CgArgs c, int nb_int, int mas_lo, int mas_hi, int bodies,
-                                                          const Tinv* __restrict__ abd_inv,
-                                                          const Tinv* __restrict__ diag_inv, Tacc* partial,
-                                                          double* partial_rr, int part_base, PcgScalars* s)
+__global__ void __launch_bounds__(kTpb) k_other_apply_fused(FusedArgs fa, float* z, int nb_int, int mas_lo,
+                                                             int mas_hi, int bodies, const Tinv* __restrict__ abd_inv,
+                                                             Tacc* partial, double* partial_rr, PcgScalars* s)
 {
   pdl_wait();
   if (s->status != MASPCG_SOLVE_RUNNING) return;
-  const CgScal cs = cg_scalars(s);
+  const FusedScal fs = fused_scalars(s);
   Tacc dot = 0;
   double rr = 0.0;
   const int stride = gridDim.x * blockDim.x;
@@ -591,35 +660,26 @@ __global__ void __launch_bounds__(kTpb) k_other_apply_cg(CgArgs c, int nb_int, i
     const Tinv* P = abd_inv + 144 * (size_t)bdy;
     float in[12];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) cg_input_row(c, cs, 4 * bdy + q, true, in + 3 * q);
-    float zb[12];
+    for (int q = 0; q < 4; ++q) fused_input_row(fa, fs, 4 * bdy + q, true, in + 3 * q);
 #pragma unroll 1
     for (int a = 0; a < 12; ++a) {
       Tinv acc = 0;
 #pragma unroll
       for (int col = 0; col < 12; ++col) acc += P[12 * a + col] * (Tinv)in[col];
-      zb[a] = (float)acc;
-      dot += (Tacc)in[a] * (Tacc)zb[a];
+      const float zv = (float)acc;
+      z[12 * (size_t)bdy + a] = zv;
+      dot += (Tacc)in[a] * (Tacc)zv;
       rr += (double)in[a] * in[a];
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) st_p4(c.z0, 4 * bdy + q, zb[3 * q], zb[3 * q + 1], zb[3 * q + 2]);
   }
   for (int row = 4 * bodies + blockIdx.x * blockDim.x + threadIdx.x; row < nb_int; row += stride) {
     if (row >= mas_lo && row < mas_hi) continue;
     float r3[3];
-    cg_input_row(c, cs, row, true, r3);
-    float z3[3] = {r3[0], r3[1], r3[2]};
-    if (diag_inv) {
-      const Tinv* D = diag_inv + 9 * (size_t)row;
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-        z3[i] = (float)(D[3 * i] * (Tinv)r3[0] + D[3 * i + 1] * (Tinv)r3[1] + D[3 * i + 2] * (Tinv)r3[2]);
-    }
-    st_p4(c.z0, row, z3[0], z3[1], z3[2]);
+    fused_input_row(fa, fs, row, true, r3);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      dot += (Tacc)r3[i] * (Tacc)z3[i];
+      z[3 * (size_t)row + i] = r3[i];
+      dot += (Tacc)r3[i] * (Tacc)r3[i];
       rr += (double)r3[i] * r3[i];
     }
   }
@@ -628,41 +688,39 @@ __global__ void __launch_bounds__(kTpb) k_other_apply_cg(CgArgs c, int nb_int, i
   const Tacc bsum = block_sum<Tacc, kTpb>(dot, red);
   const double bsum2 = block_sum<double, kTpb>(rr, red2);
   if (threadIdx.x == 0) {
-    partial[part_base + blockIdx.x] = bsum;
-    if (c.update) partial_rr[part_base + blockIdx.x] = bsum2;
+    partial[blockIdx.x] = bsum;
+    if (fa.update) partial_rr[blockIdx.x] = bsum2;
   }
 }
 
-// Single-reduction recurrence, the iteration's update alone (the last
-// iteration of a MIXED batch, whose FP64 residual replacement comes between
-// the update and the apply): every row, r.r, then the stopping gate, and the
-// r / s buffers swap.
+// The x / r update of the last iteration of a MIXED batch, whose FP64
+// residual replacement comes between the update and the apply: r' of the
+// current buffer into the first one, x, r.r and the stopping gate.
 template <typename Tacc>
-__global__ void __launch_bounds__(kTpb) k_cg_update(CgArgs c, int nrows, int mixed, Tacc* partial, PcgScalars* s)
+__global__ void __launch_bounds__(kTpb) k_update_xr_fused(FusedArgs fa, int nrows, int mixed, Tacc* partial,
+                                                           PcgScalars* s)
 {
   pdl_wait();
   if (s->status != MASPCG_SOLVE_RUNNING) return;
-  const CgScal cs = cg_scalars(s);
+  const FusedScal fs = fused_scalars(s);
   Tacc acc = 0;
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += gridDim.x * blockDim.x) {
-    float rn[3];
-    cg_update_row(c, cs.cur, row, cs.first, cs.alpha, cs.beta, rn);
-    acc += (Tacc)rn[0] * (Tacc)rn[0] + (Tacc)rn[1] * (Tacc)rn[1] + (Tacc)rn[2] * (Tacc)rn[2];
+    const size_t b = 3 * (size_t)row;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float rq = fmaf(-fs.alpha, fa.ap[b + q], fa.r[fs.cur][b + q]);
+      fa.x[b + q] = fmaf(fs.alpha, fa.p4[4 * (size_t)row + q], fa.x[b + q]);
+      fa.r[0][b + q] = rq;
+      acc += (Tacc)rq * (Tacc)rq;
+    }
   }
   pdl_trigger();
   Tacc total = 0;
   if (grid_finish<Tacc>(acc, partial, blockIdx.x, gridDim.x, &s->tickets[kTicketXr], gridDim.x, total) &&
       threadIdx.x == 0) {
-    s->cg_cur ^= 1;
+    s->rbuf = 0;
     gate_check(s, (double)total, mixed);
   }
-}
-
-// Every entry of a padded vector's three components set to v (the fourth 0).
-__global__ void k_fill_p4(float* p4, int nrows, float v)
-{
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nrows) st_p4(p4, r, v, v, v);
 }
 
 // ----------------------------------------------------------------- engine --
@@ -672,7 +730,7 @@ struct Engine {
   maspcg_handle* h;
   int n, gstream, gspmv, grows, gl0, gother, parts_other, parts_total;
   bool mas, mas16, mixed, ovl;
-  bool cg;  // single-reduction recurrence (FP32 matrix, MAS32)
+  bool fused;  // the x / r update runs inside the apply kernels (FP32 matrix, MAS32)
 
   explicit Engine(maspcg_handle* hh) : h(hh)
   {
@@ -689,50 +747,44 @@ struct Engine {
     gother = other ? std::max(1, std::min(ceil_div(std::max(h->nb_int, 1), kTpb), 2 * h->sm_count)) : 0;
     parts_other = gother;
     parts_total = gother + gl0;
-    cg = std::is_same<Tm, float>::value && mas && h->use_cg && !h->fused_head;
+    fused = std::is_same<Tm, float>::value && mas && h->fuse_update && !h->fused_head;
   }
   Tv* V(maspcg::DBuf<unsigned char>& b) { return reinterpret_cast<Tv*>(b.get()); }
   static float* Vf(maspcg::DBuf<unsigned char>& b) { return reinterpret_cast<float*>(b.get()); }
+  Tacc* partial() { return reinterpret_cast<Tacc*>(h->partial.get()); }
+  Tacc* partial_rz() { return reinterpret_cast<Tacc*>(h->partial_rz.get()); }
 
-  CgArgs cg_args(int update)
+  FusedArgs fused_args(int update)
   {
-    CgArgs c{};
-    c.z = Vf(h->vz);
-    c.w = Vf(h->vap);
-    c.p = Vf(h->cg_p);
-    c.x = Vf(h->vx);
-    c.r[0] = Vf(h->vr);
-    c.r[1] = Vf(h->cg_r2);
-    c.s[0] = Vf(h->cg_s0);
-    c.s[1] = Vf(h->cg_s1);
-    c.z0 = Vf(h->cg_z0);
-    c.update = update;
-    return c;
+    FusedArgs f{};
+    f.p4 = Vf(h->vp4);
+    f.ap = Vf(h->vap);
+    f.x = Vf(h->vx);
+    f.r[0] = Vf(h->vr);
+    f.r[1] = Vf(h->vr2);
+    f.update = update;
+    return f;
   }
 
-  // The preconditioner apply of the single-reduction recurrence (update: the
-  // iteration's vector update runs in the same kernels first; mode: RzMode).
-  void cg_precondition(int update, int mode, PcgScalars* s)
+  // The preconditioner apply behind the iteration's fused x / r update
+  // (mode: RzMode).
+  void fused_precondition(int mode, PcgScalars* s)
   {
-    const CgArgs c = cg_args(update);
+    const FusedArgs f = fused_args(1);
     if (gother) {
       const int bodies = h->abd_bodies;
       const int mas_lo = h->fem_off, mas_hi = h->fem_off + h->c0;
       if (bodies > 0)
-        launch_pdl(h, k_other_apply_cg<Tacc, double>, dim3(gother), dim3(kTpb), 0, c, h->nb_int, mas_lo, mas_hi,
-                   bodies, (const double*)h->abd_inv64.get(), (const double*)nullptr, partial_rz(),
-                   h->partial_rr.get(), 0, s);
+        launch_pdl(h, k_other_apply_fused<Tacc, double>, dim3(gother), dim3(kTpb), 0, f, Vf(h->vz), h->nb_int, mas_lo,
+                   mas_hi, bodies, (const double*)h->abd_inv64.get(), partial_rz(), h->partial_rr.get(), s);
       else
-        launch_pdl(h, k_other_apply_cg<Tacc, float>, dim3(gother), dim3(kTpb), 0, c, h->nb_int, mas_lo, mas_hi,
-                   bodies, (const float*)h->abd_inv32.get(), (const float*)nullptr, partial_rz(), h->partial_rr.get(),
-                   0, s);
+        launch_pdl(h, k_other_apply_fused<Tacc, float>, dim3(gother), dim3(kTpb), 0, f, Vf(h->vz), h->nb_int, mas_lo,
+                   mas_hi, bodies, (const float*)h->abd_inv32.get(), partial_rz(), h->partial_rr.get(), s);
     }
-    mas_apply_cg<Tacc>(h, c, Vf(h->cg_pc), partial_rz(), h->partial_rr.get(), parts_other, parts_total, mode, gl0, s,
-                       h->overlap_coarse);
+    mas_apply_fused<Tacc>(h, f, Vf(h->vz), partial_rz(), h->partial_rr.get(), parts_other, parts_total, mode, gl0, s,
+                          ovl);
     MCK(cudaGetLastError());
   }
-  Tacc* partial() { return reinterpret_cast<Tacc*>(h->partial.get()); }
-  Tacc* partial_rz() { return reinterpret_cast<Tacc*>(h->partial_rz.get()); }
 
   // overlap: the coarse levels run beside the level-0 apply and z leaves the
   // coarse correction to the next p update (inside the solve only).
@@ -778,89 +830,88 @@ struct Engine {
   }
 
   // The iteration head as one cooperative launch: one resident wave of CTAs.
-  template <bool kCoarse>
+  template <bool kCoarse, int kForm>
   void fused_head_t(PcgScalars* s, const ApplyArgs& a)
   {
-    auto kern = k_iteration_head<Tm, Tv, Tacc, kSpmvLanes, kCoarse>;
+    constexpr bool kTiled = std::is_same<Tm, float>::value;
+    auto kern = k_iteration_head<Tm, Tv, Tacc, kTiled, kSpmvLanes, kCoarse, kForm>;
     static int per_sm = 0;
     if (!per_sm) {
       MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
       MREQ(per_sm > 0, MASPCG_ERR_CUDA, "fused iteration kernel cannot be resident");
     }
     const int grid = std::max(1, std::min(ceil_div(h->nb_int, kTpb / kSpmvLanes), per_sm * h->sm_count));
-    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, jds_args(h), h->rowptr.get(), h->colidx.get(),
-                       h->val64.get(), V(h->vz), V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0,
-                       partial(), s, h->failed.get() + 4);
+    launch_cooperative(h, kern, dim3(grid), dim3(kTpb), 0, a, h->rowptr.get(), h->colidx.get(), matrix(),
+                       matrix_lo(), h->val64.get(), exact_rows(), V(h->vz), V(h->vp4), V(h->vap), V(h->vx), V(h->vr), h->nb_int, mixed ? 1 : 0, partial(), s,
+                       h->failed.get() + 4);
+  }
+
+  template <int kForm>
+  void fused_head_f(PcgScalars* s)
+  {
+    if (ovl)
+      fused_head_t<true, kForm>(s, mas_apply_args(h));
+    else
+      fused_head_t<false, kForm>(s, ApplyArgs{});
   }
 
   void fused_head(PcgScalars* s)
   {
-    if (ovl)
-      fused_head_t<true>(s, mas_apply_args(h));
-    else
-      fused_head_t<false>(s, ApplyArgs{});
+    switch (form()) {
+      case MASPCG_MATRIX_F32_SUM64: fused_head_f<MASPCG_MATRIX_F32_SUM64>(s); break;
+      case MASPCG_MATRIX_F32_SPLIT: fused_head_f<MASPCG_MATRIX_F32_SPLIT>(s); break;
+      default: fused_head_f<MASPCG_MATRIX_F32>(s); break;
+    }
   }
 
-  // FP64 SpMV: lanes per block row.
+  const Tm* matrix();
+  // the BF16 remainder of the split form (else unused)
+  const unsigned short* matrix_lo() const { return h->val_lo.get(); }
+  // the matrix form the FP32 tiles run in; the FP64 matrix has one form
+  int form() const { return std::is_same<Tm, float>::value ? h->cfg.matrix_form : (int)MASPCG_MATRIX_F32; }
+  // block rows the FP32-tile SpMV takes from the FP64 matrix (the affine bodies)
+  int exact_rows() const { return std::is_same<Tm, float>::value ? 4 * h->abd_bodies : 0; }
+
+  // SpMV rows per CTA step: kTpb / kSpmvLanes.
   static constexpr int kSpmvLanes = 8;
 
-  // The SpMV of the iteration: one wave of resident CTAs (the kernel strides
-  // over the rest).  FP32: the sliced layout, staged through shared memory
-  // (one CTA of kJdsWarps warps per SM) unless MASPCG_FLAG_SPMV_DIRECT.
-  // cg: the single-reduction recurrence's w = A (z0 + pc) (else Ap = A p).
-  template <bool kCg>
-  void spmv_fp32_launch(PcgScalars* s, const SpmvVec& v)
+  template <int kForm>
+  void spmv_t(PcgScalars* s)
   {
-    if (h->spmv_staged) {
-      auto kern = k_spmv_jds_staged<Tacc, kCg>;
-      static bool configured = false;
-      if (!configured) {
-        MCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kJdsSmem));
-        configured = true;
-      }
-      const int grid = std::max(1, std::min(h->sm_count, ceil_div(h->jds_slices, kJdsWarps)));
-      launch_pdl(h, kern, dim3(grid), dim3(kJdsWarps * 32), kJdsSmem, jds_args(h), h->rowptr.get(), h->colidx.get(),
-                 h->val64.get(), v, partial(), s, h->failed.get() + 4);
-      return;
-    }
-    auto kern = k_spmv_jds<Tacc, kCg>;
+    constexpr bool kTiled = std::is_same<Tm, float>::value;
+    constexpr int rows = kTpb / kSpmvLanes;
+    auto kern = k_spmv<Tm, Tv, Tacc, kTiled, kSpmvLanes, kForm>;
+    // one wave of resident CTAs; the kernel strides over the rest
     static int per_sm = 0;
     if (!per_sm) {
       MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTpb, 0));
       per_sm = std::max(per_sm, 1);
     }
-    const int grid = std::max(1, std::min(per_sm * h->sm_count, ceil_div(h->jds_slices, kTpb / 32)));
-    launch_pdl(h, kern, dim3(grid), dim3(kTpb), 0, jds_args(h), h->rowptr.get(), h->colidx.get(), h->val64.get(), v,
-               partial(), s);
+    const int grid = std::max(1, std::min(ceil_div(h->nb_int, rows), per_sm * h->sm_count));
+    launch_pdl(h, kern, dim3(grid), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), matrix(), matrix_lo(),
+               h->val64.get(), exact_rows(), V(h->vp4), V(h->vap), h->nb_int, partial(), s);
   }
 
   void spmv(PcgScalars* s)
   {
     if constexpr (std::is_same<Tm, float>::value) {
-      if (cg) {
-        spmv_fp32_launch<true>(s, SpmvVec{Vf(h->cg_z0), Vf(h->cg_pc), Vf(h->vap), Vf(h->vz)});
-        return;
+      switch (form()) {
+        case MASPCG_MATRIX_F32_SUM64: spmv_t<MASPCG_MATRIX_F32_SUM64>(s); return;
+        case MASPCG_MATRIX_F32_SPLIT: spmv_t<MASPCG_MATRIX_F32_SPLIT>(s); return;
+        default: break;
       }
-      spmv_fp32_launch<false>(s, SpmvVec{Vf(h->vp4), nullptr, Vf(h->vap), nullptr});
-    } else {
-      constexpr int rows = kTpb / kSpmvLanes;
-      static int per_sm = 0;
-      if (!per_sm) {
-        MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv<kSpmvLanes>, kTpb, 0));
-        per_sm = std::max(per_sm, 1);
-      }
-      const int grid = std::max(1, std::min(ceil_div(h->nb_int, rows), per_sm * h->sm_count));
-      launch_pdl(h, k_spmv<kSpmvLanes>, dim3(grid), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(),
-                 V(h->vp4), V(h->vap), h->nb_int, partial(), s);
     }
+    spmv_t<MASPCG_MATRIX_F32>(s);
   }
+
+
 
   void true_residual(PcgScalars* s)
   {
     launch_pdl(h, k_fold_x, dim3(gstream), dim3(kTpb), 0, h->x64.get(), reinterpret_cast<float*>(h->vx.get()), n, 0, s);
     launch_pdl(h, k_true_residual<16>, dim3(gspmv), dim3(kTpb), 0, h->rowptr.get(), h->colidx.get(), h->val64.get(),
                h->x64.get(), h->b64.get(), reinterpret_cast<float*>(h->vr.get()),
-               cg ? reinterpret_cast<float*>(h->cg_r2.get()) : (float*)nullptr, h->nb_int, h->partial.get(), s);
+               (float*)nullptr, h->nb_int, h->partial.get(), s);
   }
 
   // y = A x through the iteration's own SpMV kernel: x (internal order, FP64)
@@ -876,15 +927,7 @@ struct Engine {
     init.rz = 1.0;
     init.max_iter = 1 << 30;
     MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-    if (cg) {
-      // the recurrence's SpMV gathers z0 + pc: x into z0, pc zero
-      init.k = 1;
-      MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-      MCK(cudaMemsetAsync(h->cg_pc.get(), 0, h->cg_pc.bytes(), st));
-      k_to_p4<float><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, Vf(h->cg_z0), h->nb_int);
-    } else {
-      k_to_p4<Tv><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, V(h->vp4), h->nb_int);
-    }
+    k_to_p4<Tv><<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(x_int, V(h->vp4), h->nb_int);
     MLAUNCHED(h);
     const bool pdl = h->use_pdl;
     h->use_pdl = false;
@@ -899,16 +942,22 @@ struct Engine {
   void record_batch(int batch, PcgScalars* s)
   {
     for (int it = 0; it < batch; ++it) {
-      if (cg) {
-        if (mixed && it == batch - 1) {
-          // update, FP64 residual replacement, then the apply of the new r
-          launch_pdl(h, k_cg_update<Tacc>, dim3(grows), dim3(kTpb), 0, cg_args(1), h->nb_int, 1, partial(), s);
-          true_residual(s);
-          cg_precondition(0, kRzLoop, s);
-        } else {
-          cg_precondition(1, mixed ? kRzFusedMix : kRzFusedStd, s);
-        }
+      if (fused) {
+        const ApplyArgs a = ovl ? mas_apply_args(h) : ApplyArgs{};
+        if (ovl)
+          launch_pdl(h, k_update_p<Tv, true>, dim3(grows), dim3(kTpb), 0, a, V(h->vz), V(h->vp4), h->nb_int, s);
+        else
+          launch_pdl(h, k_update_p<Tv, false>, dim3(grows), dim3(kTpb), 0, a, V(h->vz), V(h->vp4), h->nb_int, s);
         spmv(s);
+        if (mixed && it == batch - 1) {
+          // x / r update, FP64 residual replacement, then the apply of the new r
+          launch_pdl(h, k_update_xr_fused<Tacc>, dim3(grows), dim3(kTpb), 0, fused_args(1), h->nb_int, 1, partial(),
+                     s);
+          true_residual(s);
+          precondition(V(h->vr), V(h->vz), 2, s, ovl);
+        } else {
+          fused_precondition(mixed ? kRzFusedMix : kRzFusedStd, s);
+        }
         continue;
       }
       iteration_head(s);
@@ -945,13 +994,6 @@ struct Engine {
     if (h->l2_flush.n < kFlushBytes) {
       h->l2_flush.resize(kFlushBytes);
       MCK(cudaMemsetAsync(h->l2_flush.get(), 0, kFlushBytes, st));
-    }
-    if (cg && stage == 0) {
-      // the recurrence's SpMV w = A (z0 + pc) with z0 = 1, pc = 0: delta > 0
-      init.k = 1;
-      MCK(cudaMemsetAsync(h->cg_pc.get(), 0, h->cg_pc.bytes(), st));
-      k_fill_p4<<<ceil_div(h->nb_int, kTpb), kTpb, 0, st>>>(Vf(h->cg_z0), h->nb_int, 1.f);
-      MLAUNCHED(h);
     }
     MCK(cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     auto once = [&]() {
@@ -1014,6 +1056,7 @@ struct Engine {
     PcgScalars init{};
     init.status = MASPCG_SOLVE_RUNNING;
     init.max_iter = max_iter;
+    init.replace_mode = h->cfg.residual_replacement;
     init.gate = mixed ? MASPCG_GATE_EUCLID : h->cfg.gate;
     init.tol = h->cfg.tolerance;
     init.barrier_limit = h->barrier_limit;
@@ -1023,15 +1066,7 @@ struct Engine {
     MCK(cudaEventRecord(h->ev0, st));
     k_init<Tv><<<gstream, kTpb, 0, st>>>(b_int, V(h->vx), V(h->vr), mixed ? h->x64.get() : nullptr, n,
                                          h->partial_rz.get(), s); MLAUNCHED(h);
-    if (cg) {
-      // single-reduction recurrence: z0 = M r0 (pc: its coarse part), then
-      // w = A z, delta = z.w and the first alpha
-      MCK(cudaMemsetAsync(h->cg_pc.get(), 0, h->cg_pc.bytes(), st));
-      cg_precondition(0, kRzInitial, s);
-      spmv(s);
-    } else {
-      precondition(V(h->vr), V(h->vz), 1, s, ovl);
-    }
+    precondition(V(h->vr), V(h->vz), 1, s, ovl);
     // graph of one batch
     const int batch = mixed ? std::max(1, h->cfg.refinement_period) : std::max(1, h->cfg.iterations_per_launch);
     if (h->graph_dirty || h->graph_batch != batch) {
@@ -1105,6 +1140,22 @@ struct Engine {
     }
   }
 };
+
+template <>
+const double* Engine<double, double, double>::matrix()
+{
+  return h->val64.get();
+}
+template <>
+const float* Engine<float, float, float>::matrix()
+{
+  return h->val32.get();
+}
+template <>
+const float* Engine<float, float, double>::matrix()
+{
+  return h->val32.get();
+}
 
 }  // namespace
 

@@ -47,6 +47,7 @@ __device__ __forceinline__ bool grid_finish(Tacc v, Tacc* partial, int slot, int
 __device__ __forceinline__ bool gate_check(PcgScalars* s, double rr, int mixed)
 {
   s->rr = rr;
+  s->rr_peak = fmax(s->rr_peak, rr);
   if (!isfinite(rr)) {
     s->status = MASPCG_SOLVE_NONFINITE;
     s->iterations = s->k;
@@ -68,8 +69,8 @@ enum RzMode {
   kRzNone = 0,      // standalone apply: no scalar update
   kRzInitial = 1,   // initial apply: rz0, k = 1
   kRzLoop = 2,      // in the loop: beta = r.z / previous r.z, k++
-  kRzFusedStd = 4,  // single-reduction recurrence, plain precision: the apply ran behind the iteration's x / r
-                    // update (so the gate on s->rr comes first, and the r / s buffers swap), then as kRzLoop
+  kRzFusedStd = 4,  // the apply ran behind the iteration's x / r update: the r buffers swap and the gate on s->rr
+                    // comes first, then as kRzLoop
   kRzFusedMix = 5   // the same in MIXED precision (a met gate asks for the FP64 true residual)
 };
 
@@ -77,7 +78,7 @@ enum RzMode {
 __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode)
 {
   if (mode == kRzFusedStd || mode == kRzFusedMix) {
-    s->cg_cur ^= 1;
+    s->rbuf ^= 1;
     if (gate_check(s, s->rr, mode == kRzFusedMix)) return;
     mode = kRzLoop;
   }
@@ -115,105 +116,49 @@ __device__ __forceinline__ void rz_update(PcgScalars* s, double rz_new, int mode
   }
 }
 
-// Single-reduction recurrence (Chronopoulos-Gear): the last block of the
-// SpMV w = A z has delta = z.w; alpha = r.z / (delta - beta r.z / alpha_prev)
-// (delta alone right after the initial apply, k == 1), which equals r.z /
-// p.Ap of the two-reduction form in exact arithmetic.
-__device__ __forceinline__ void cg_alpha(PcgScalars* s, double delta)
-{
-  const double denom = (s->k == 1) ? delta : delta - s->beta * s->rz / s->alpha;
-  s->pap = denom;
-  if (!isfinite(denom)) {
-    s->status = MASPCG_SOLVE_NONFINITE;
-    s->iterations = s->k;
-  } else if (!(denom > 0.0)) {
-    s->status = MASPCG_SOLVE_NONPOSITIVE_CURVATURE;
-    s->iterations = s->k;
-  } else {
-    s->alpha = s->rz / denom;
-  }
-}
-
-// The vectors of the single-reduction recurrence (FP32, internal order).  An
-// iteration's update and its preconditioner apply run in one kernel: with z
-// = M r, w = A z of the previous apply and SpMV,
-//   p = z + beta p,  s = w + beta s  (p = z, s = w at k == 1),
-//   x += alpha p,    r' = r - alpha s,
-// then z' = M r'.  r and s are double-buffered (cur = s->cg_cur): the coarse
-// levels, beside the level-0 apply, form r' again from r, w, s (the same FMAs,
-// so the same bits) while the apply writes it.
-struct CgArgs {
-  const float* z;  // 3 per row: z of this iteration (written by the SpMV)
-  const float* w;  // 3 per row: A z
-  float* p;
+// The x / r update of a PCG iteration fused into the preconditioner apply
+// that follows it (the kernels that read r to precondition it update their
+// own rows first):
+//   x += alpha p,   r' = r - alpha Ap
+// r is double-buffered (cur = s->rbuf): the coarse levels, beside the level-0
+// apply, restrict r' formed again from r and Ap (the same FMA, so the same
+// bits) while the apply writes it; the r.z completion swaps the buffers.
+struct FusedArgs {
+  const float* p4;  // search direction, padded 4 per row
+  const float* ap;  // A p, 3 per row
   float* x;
   float* r[2];
-  float* s[2];
-  float* z0;       // 4 per row (padded): the next z's level-0 / non-MAS part (the SpMV gathers it)
-  int update;      // 1: the iteration's update first; 0: r[cur] is already the residual to precondition
+  int update;       // 1: the update first; 0: r[cur] is already the residual to precondition
 };
-
-// The update of one row; r' into rn.
-__device__ __forceinline__ void cg_update_row(const CgArgs& c, int cur, int row, bool first, float alpha, float beta,
-                                              float rn[3])
-{
-  const size_t b = 3 * (size_t)row;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const float zq = c.z[b + q], wq = c.w[b + q];
-    const float pq = first ? zq : fmaf(beta, c.p[b + q], zq);
-    const float sq = first ? wq : fmaf(beta, c.s[cur][b + q], wq);
-    c.p[b + q] = pq;
-    c.s[cur ^ 1][b + q] = sq;
-    c.x[b + q] = fmaf(alpha, pq, c.x[b + q]);
-    const float rq = fmaf(-alpha, sq, c.r[cur][b + q]);
-    c.r[cur ^ 1][b + q] = rq;
-    rn[q] = rq;
-  }
-}
-
-// r' of one row without writing anything (the coarse levels' restriction):
-// the same operations as cg_update_row.
-__device__ __forceinline__ void cg_residual_row(const CgArgs& c, int cur, int row, bool first, float alpha, float beta,
-                                                float rn[3])
-{
-  const size_t b = 3 * (size_t)row;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const float wq = c.w[b + q];
-    const float sq = first ? wq : fmaf(beta, c.s[cur][b + q], wq);
-    rn[q] = fmaf(-alpha, sq, c.r[cur][b + q]);
-  }
-}
 
 // The scalars a fused kernel reads once at entry (nothing changes them until
 // every kernel of the iteration has passed its rows).
-struct CgScal {
+struct FusedScal {
   int cur;
-  bool first;
-  float alpha, beta;
+  float alpha;
 };
-__device__ __forceinline__ CgScal cg_scalars(const PcgScalars* s)
-{
-  return CgScal{s->cg_cur, s->k == 1, (float)s->alpha, (float)s->beta};
-}
+__device__ __forceinline__ FusedScal fused_scalars(const PcgScalars* s) { return FusedScal{s->rbuf, (float)s->alpha}; }
 
-// The residual the apply of one row starts from: r' of the fused update, or
-// r[cur] when the update ran before (update == 0).  Writes the update when
-// `write` (the kernel that owns the row), else only recomputes r'.
-__device__ __forceinline__ void cg_input_row(const CgArgs& c, const CgScal& cs, int row, bool write, float rn[3])
+// The residual the apply of one row starts from: r' of the update (written,
+// with x, when `write`: the kernel that owns the row), or r[cur] when the
+// update ran before (update == 0).
+__device__ __forceinline__ void fused_input_row(const FusedArgs& f, const FusedScal& fs, int row, bool write,
+                                                float rn[3])
 {
-  if (!c.update) {
-    const size_t b = 3 * (size_t)row;
-    rn[0] = c.r[cs.cur][b];
-    rn[1] = c.r[cs.cur][b + 1];
-    rn[2] = c.r[cs.cur][b + 2];
+  const size_t b = 3 * (size_t)row;
+  if (!f.update) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) rn[q] = f.r[fs.cur][b + q];
     return;
   }
-  if (write)
-    cg_update_row(c, cs.cur, row, cs.first, cs.alpha, cs.beta, rn);
-  else
-    cg_residual_row(c, cs.cur, row, cs.first, cs.alpha, cs.beta, rn);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    rn[q] = fmaf(-fs.alpha, f.ap[b + q], f.r[fs.cur][b + q]);
+    if (write) {
+      f.x[b + q] = fmaf(fs.alpha, f.p4[4 * (size_t)row + q], f.x[b + q]);
+      f.r[fs.cur ^ 1][b + q] = rn[q];
+    }
+  }
 }
 
 // Grid-wide barrier of a cooperative launch (every CTA resident).  The last

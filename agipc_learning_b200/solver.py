@@ -20,6 +20,8 @@ from . import _native as N
 _PREC = {"reference": N.PREC_REFERENCE, "fp32": N.PREC_FP32, "mixed": N.PREC_MIXED}
 _GATE = {"rz": N.GATE_RZ, "euclid": N.GATE_EUCLID}
 _INV = {"fp32": N.INV_FP32, "bf16": N.INV_BF16, "fp16": N.INV_FP16}
+_MATRIX = {"f32": N.MATRIX_F32, "f32_sum64": N.MATRIX_F32_SUM64, "f32_split": N.MATRIX_F32_SPLIT}
+_REPLACE = {"reliable": N.REPLACE_RELIABLE, "periodic": N.REPLACE_PERIODIC}
 _PC = {"mas32": N.PRECOND_MAS32, "cemas16": N.PRECOND_MAS16, "block_jacobi": N.PRECOND_BLOCK_JACOBI,
        "none": N.PRECOND_NONE}
 
@@ -60,7 +62,8 @@ class MasPcg:
     """One linear system on one GPU: graph -> contacts -> matrix -> build -> solve."""
 
     def __init__(self, *, tolerance=1e-4, max_iter_ratio=0.3, max_iterations=0, gate="rz", precision="reference",
-                 inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8, flags=0):
+                 inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8, flags=0,
+                 matrix="f32", replacement="reliable"):
         lib = N.load()
         cfg = N.Config()
         lib.maspcg_config_default(ctypes.byref(cfg))
@@ -75,6 +78,8 @@ class MasPcg:
         cfg.refinement_period = refinement_period
         cfg.iterations_per_launch = iterations_per_launch
         cfg.flags = flags
+        cfg.matrix_form = _MATRIX[matrix]
+        cfg.residual_replacement = _REPLACE[replacement]
         self.cfg = cfg
         h = ctypes.c_void_p()
         N.check(lib.maspcg_create(ctypes.byref(cfg), ctypes.byref(h)), None)

@@ -587,9 +587,7 @@ def run_ours(args, world, rank, local):
                       "mas_level0_variants": ms_l0_variants, "domain_factor": ms_factor,
                       "solve_device_ms": res_mixed["solve_ms"]},
         "stage_errors": stage_errors or None,
-        "roofline": {"kernel": "k_spmv_jds_staged (FP32 sliced jagged-diagonal SpMV, records bulk-copied to shared "
-                               "memory; single-reduction recurrence w = A z with z.w)", "bound": "hbm",
-                     "achieved": ach,
+        "roofline": {"kernel": "k_spmv (BCSR SpMV + p.Ap, FP32 32-block tiles)", "bound": "hbm", "achieved": ach,
                      "peak": peak,
                      "unit": "GB/s", "frac": ach / peak if ach else None, "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes": spmv_bytes,

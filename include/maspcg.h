@@ -66,8 +66,9 @@ typedef enum {
   /* everything FP32 (matrix, vectors, dots, FP32 domain inverses) */
   MASPCG_PREC_FP32 = 1,
   /* FP32 matrix and vectors, 16-bit domain inverses with FP32 accumulation,
-   * FP64 dots, FP64 true residual every refinement_period iterations with
-   * residual replacement (reliable updates); stops on the FP64 true residual */
+   * FP64 dots, the FP32 x folded into an FP64 x every refinement_period
+   * iterations and the recursive residual replaced by the FP64 true residual
+   * as residual_replacement says; stops on the FP64 true residual */
   MASPCG_PREC_MIXED = 2
 } maspcg_precision;
 
@@ -86,11 +87,39 @@ typedef struct {
   int precision;         /* maspcg_precision */
   int inverse_storage;   /* maspcg_inverse_storage (FP32 unless MIXED; always FP32 for CEMAS16) */
   int preconditioner;    /* maspcg_preconditioner */
-  int refinement_period; /* MIXED: iterations between FP64 true residuals (default 16) */
+  int refinement_period; /* MIXED: iterations between checks for an FP64 true residual (default 16) */
   int bank_size;         /* MAS bank: 32 (GPU_MAS_BANKSIZE) for MAS32, 16 (BANKSIZE) for CEMAS16 */
   int iterations_per_launch; /* PCG iterations per CUDA-graph launch (default 8) */
   int flags;             /* maspcg_flags: kernel-schedule choices, 0 = defaults */
+  int matrix_form;       /* maspcg_matrix_form: the iteration matrix of FP32 / MIXED precision */
+  int residual_replacement; /* maspcg_replacement: when MIXED replaces the recursive residual */
 } maspcg_config;
+
+/* When MIXED precision replaces the recursive residual r by the FP64 true
+ * residual b - A x (checked at the end of every graph of refinement_period
+ * iterations; always when the recursive gate is met, where the true residual
+ * decides the stop).  x_hi += x_lo is folded at every check either way. */
+typedef enum {
+  MASPCG_REPLACE_RELIABLE = 0, /* once ||r|| has fallen to 0.1 of its largest value since the last replacement
+                                  (the default: a few replacements per decade of reduction) */
+  MASPCG_REPLACE_PERIODIC = 1  /* at every check */
+} maspcg_replacement;
+
+/* How FP32 and MIXED precision store the iteration's matrix and sum its
+ * products (maspcg_config.matrix_form).  The reference precision always runs
+ * the FP64 matrix with FP64 sums, and the affine-body rows always take the
+ * FP64 matrix.  A product of two FP32 numbers is exact in FP64, so
+ * MASPCG_MATRIX_F32_SUM64 computes the FP32-valued operator A32 p to FP64
+ * accuracy before the single rounding of the result: on stiff contact rows
+ * (barrier blocks beside a soft mass term) FP32 sums lose more than the FP32
+ * values themselves do. */
+typedef enum {
+  MASPCG_MATRIX_F32 = 0,       /* FP32 values, products and sums (the default: the fewest instructions) */
+  MASPCG_MATRIX_F32_SUM64 = 1, /* FP32 values; exact products summed in FP64 */
+  MASPCG_MATRIX_F32_SPLIT = 2  /* FP32 values plus BF16 values of the remainder A - A32, so the operator is A to
+                                  about 2^-32 relative: for systems whose stiffness spread FP32 values cannot
+                                  carry (18 more bytes per block); sums as MASPCG_MATRIX_F32_SUM64 */
+} maspcg_matrix_form;
 
 /* Kernel-schedule choices (bits of maspcg_config.flags); results do not depend
  * on them beyond floating-point summation order. */
@@ -102,12 +131,9 @@ typedef enum {
                                           (always so in MASPCG_PREC_REFERENCE, whose r.z is then summed over
                                           the fine rows as the reference sums it) */
   MASPCG_FLAG_FUSED_HEAD = 16,         /* p update, SpMV and x/r update as one cooperative kernel with grid barriers */
-  MASPCG_FLAG_SPMV_DIRECT = 32,        /* FP32 SpMV reads its slice records from global memory instead of staging
-                                          them in shared memory with bulk copies */
-  MASPCG_FLAG_TWO_REDUCTION = 64       /* FP32 / MIXED with MAS32: the two-reduction PCG recurrence of the reference
-                                          (p update, SpMV with p.Ap, x / r update, apply with r.z) instead of the
-                                          single-reduction one (the update fused into the apply, one SpMV w = A z
-                                          with z.w; Chronopoulos-Gear), which is the default there */
+  MASPCG_FLAG_FUSED_UPDATE = 32        /* FP32 / MIXED with MAS32: the x / r update run by the preconditioner's apply
+                                          kernels on their own rows instead of a kernel of its own (measured slower:
+                                          the latency-bound apply kernels take longer than the update they absorb) */
 } maspcg_flags;
 
 typedef struct {

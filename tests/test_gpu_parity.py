@@ -241,7 +241,7 @@ def test_mixed_solve_with_several_domains_per_warp(inverse):
 
 
 @pytest.mark.parametrize("flag", ["FLAG_FUSED_HEAD", "FLAG_PDL", "FLAG_SEQUENTIAL_COARSE", "FLAG_APPLY_STAGED2",
-                                  "FLAG_APPLY_DIRECT", "FLAG_SPMV_DIRECT", "FLAG_TWO_REDUCTION"])
+                                  "FLAG_APPLY_DIRECT", "FLAG_FUSED_UPDATE"])
 def test_schedule_flags_solve_the_same_system(flag):
     """Every kernel-schedule choice reaches the FP64-verified tolerance on a
     system with several domains per warp, in about the same iterations

@@ -4,6 +4,8 @@ against the oracle, through the C ABI (needs a B200):
 * the iteration's SpMV in its working precision (FP32 32-block tiles with
   FP32 sums; FP64 affine-body rows) against the FP64 product of the same
   FP32-rounded operands, elementwise within a rounding bound;
+* the solve with the x / r update as a kernel of its own against the same
+  solve with the update fused into the apply kernels;
 * the tensor-core level-0 apply of 16-bit factored domain records (every
   staging variant) plus the coarse levels, against the oracle's apply run
   with the GPU's own decoded inverses;
@@ -44,24 +46,28 @@ def _abd_rows_mask(s):
     return mask
 
 
-@pytest.mark.parametrize("which,precision,flags", [("cfg1_small", "mixed", 0), ("cfg1_small", "fp32", 0),
-                                                   ("hybrid", "mixed", 0), ("cfg1_small", "reference", 0),
-                                                   ("cfg1_small", "mixed", N.FLAG_SPMV_DIRECT),
-                                                   ("cfg1_small", "mixed", N.FLAG_TWO_REDUCTION),
-                                                   ("hybrid", "mixed", N.FLAG_TWO_REDUCTION | N.FLAG_SPMV_DIRECT)])
-def test_working_spmv_against_oracle(which, precision, flags, request):
-    """|y_gpu - A32 x32| <= 48 eps32 (|A32| |x32|) elementwise, where A32 and
-    x32 are the FP32-rounded matrix and vector the kernel reads (rows of the
-    affine bodies, taken from the FP64 matrix in FP64, within 1e-12 of the
-    FP64 product); reference precision within 1e-12 of the FP64 product.
-    Every form the solve can run: the slice records staged in shared memory
-    or read directly, the single-reduction recurrence's SpMV (gathering
-    z0 + pc) or the two-reduction one's (gathering p)."""
+@pytest.mark.parametrize("which,precision,matrix", [("cfg1_small", "mixed", "f32"), ("cfg1_small", "fp32", "f32"),
+                                                    ("hybrid", "mixed", "f32"), ("cfg1_small", "reference", "f32"),
+                                                    ("cfg1_small", "mixed", "f32_sum64"),
+                                                    ("hybrid", "mixed", "f32_sum64"),
+                                                    ("cfg1_small", "mixed", "f32_split"),
+                                                    ("hybrid", "fp32", "f32_split")])
+def test_working_spmv_against_oracle(which, precision, matrix, request):
+    """The iteration's own product y = A p against the oracle, elementwise,
+    with A32 and x32 the FP32-rounded matrix and vector the kernel reads:
+    * f32 (FP32 sums): within 48 eps32 (|A32| |x32|);
+    * f32_sum64 (exact FP32 x FP32 products, FP64 sums, one rounding at the
+      end): |y - A32 x32| <= eps32 |A32 x32| + 1e-12 (|A32| |x32|);
+    * f32_split (A32 plus the BF16 remainder, so the operator is A to about
+      2^-32): |y - A x32| <= eps32 |A x32| + 2^-30 (|A| |x32|);
+    rows of the affine bodies always from the FP64 matrix in FP64, one
+    rounding at the end; reference precision within 1e-12 of the FP64
+    product."""
     s = synth.config_system(2, scale=16) if which == "hybrid" else request.getfixturevalue(which)
     rng = np.random.default_rng(5)
     x = rng.standard_normal(3 * s.nb)
     with MasPcg.from_system(s, precision=precision, inverse="bf16" if precision == "mixed" else "fp32",
-                            gate="euclid", flags=flags) as m:
+                            gate="euclid", matrix=matrix) as m:
         y = m.spmv_working(x)
     if precision == "reference":
         ref = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
@@ -73,9 +79,16 @@ def test_working_spmv_against_oracle(which, precision, flags, request):
     mag = oracle.sym_spmv(1.0, np.abs(_round32(s.vals)), s.rows, s.cols, np.abs(x32))
     abd = _abd_rows_mask(s)
     fem = ~abd
-    # the kernel's FP32 output: the FP64 product of the rounded operands, plus
-    # the FP32 summation error and the final rounding
-    assert np.all(np.abs(y[fem] - ref[fem]) <= 48 * EPS32 * mag[fem] + 1e-300)
+    if matrix == "f32":
+        # the FP64 product of the rounded operands, plus the FP32 summation
+        # error and the final rounding
+        assert np.all(np.abs(y[fem] - ref[fem]) <= 48 * EPS32 * mag[fem] + 1e-300)
+    elif matrix == "f32_sum64":
+        assert np.all(np.abs(y[fem] - ref[fem]) <= EPS32 * np.abs(ref[fem]) + 1e-12 * mag[fem] + 1e-300)
+    else:
+        r64 = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x32)
+        m64 = oracle.sym_spmv(1.0, np.abs(s.vals), s.rows, s.cols, np.abs(x32))
+        assert np.all(np.abs(y[fem] - r64[fem]) <= EPS32 * np.abs(r64[fem]) + 2.0 ** -30 * m64[fem] + 1e-300)
     if abd.any():
         ref64 = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x32)
         mag64 = oracle.sym_spmv(1.0, np.abs(s.vals), s.rows, s.cols, np.abs(x32))
@@ -130,6 +143,25 @@ def test_mixed_apply_inside_the_solve_schedule(cfg1_40):
     assert r1["fp64_gate_met"] and r2["fp64_gate_met"]
     assert abs(r1["iterations"] - r2["iterations"]) <= max(4, int(0.05 * r2["iterations"]))
     assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) <= 1e-3
+
+
+@pytest.mark.parametrize("name", ["cfg1_40", "hybrid"])
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_fused_update_matches_separate_update(name, precision):
+    """The x / r update run by the apply kernels on their own rows
+    (MASPCG_FLAG_FUSED_UPDATE) and as a kernel of its own take the same
+    iterations (to summation order: the update arithmetic is the same FMA)
+    and give the same solution."""
+    s = _solution_case(name)
+    cfg = dict(gate="euclid", precision=precision, inverse="bf16" if precision == "mixed" else "fp32")
+    with MasPcg.from_system(s, **cfg) as m:
+        x1, r1 = m.solve(s.b)
+    with MasPcg.from_system(s, flags=N.FLAG_FUSED_UPDATE, **cfg) as m:
+        x2, r2 = m.solve(s.b)
+    assert r1["status_name"] == r2["status_name"]
+    assert abs(r1["iterations"] - r2["iterations"]) <= max(3, int(0.03 * r2["iterations"])), (r1, r2)
+    if r1["fp64_gate_met"] and r2["fp64_gate_met"]:
+        assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) <= 1e-4
 
 
 def _solution_case(name):
