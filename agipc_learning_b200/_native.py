@@ -46,8 +46,8 @@ INV_FP16 = 2
 MATRIX_F32 = 0
 MATRIX_F32_SUM64 = 1
 MATRIX_F32_SPLIT = 2
-REPLACE_RELIABLE = 0
-REPLACE_PERIODIC = 1
+REPLACE_PERIODIC = 0
+REPLACE_RELIABLE = 1
 
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "iteration_cap", 3: "nonpositive_curvature", 4: "nonfinite",
                 5: "invalid_rz"}

@@ -259,7 +259,7 @@ MASPCG_API void maspcg_config_default(maspcg_config* c)
   c->iterations_per_launch = 8;
   c->flags = 0;
   c->matrix_form = MASPCG_MATRIX_F32;
-  c->residual_replacement = MASPCG_REPLACE_RELIABLE;
+  c->residual_replacement = MASPCG_REPLACE_PERIODIC;
 }
 
 MASPCG_API const char* maspcg_status_string(int s)
@@ -791,7 +791,7 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
     DBuf<double> tmp;
     tmp.resize(n);
     MCK(cudaMemsetAsync(tmp.get(), 0, n * sizeof(double), h->stream));
-    maspcg::build_mas_domains(h, tmp.get());
+    maspcg::gather_mas_domains(h, tmp.get());
     MCK(cudaMemcpyAsync(out, tmp.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     MCK(cudaStreamSynchronize(h->stream));
     h->graph_dirty = true;
@@ -869,7 +869,7 @@ MASPCG_API maspcg_status maspcg_local_diagnostics(maspcg_handle* h, maspcg_domai
     DBuf<double> a;
     a.resize(per * std::max(D, 1));
     MCK(cudaMemsetAsync(a.get(), 0, per * D * sizeof(double), h->stream));
-    maspcg::build_mas_domains(h, a.get());
+    maspcg::gather_mas_domains(h, a.get());
     std::vector<float> inv(per * D);
     maspcg::decode_inverses(h, inv.data());
     DBuf<float> b;

@@ -237,6 +237,7 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
 #pragma unroll
       for (int j = 0; j < 3; ++j) o[i + 3 * j] = acc[3 * i + j];
   }
+  if (kAssembled && a.gather_only) return;  // uniform: no barrier has run yet
   if (lane == w) {
     if (acc[0] == 0.0) acc[0] = 1.0;
     if (acc[4] == 0.0) acc[4] = 1.0;
@@ -1586,7 +1587,7 @@ void build_mas_domains(maspcg_handle* h, double* assembled_out)
 }
 
 template <int kB>
-void launch_factor_t(maspcg_handle* h, double* assembled_out)
+void launch_factor_t(maspcg_handle* h, double* assembled_out, bool gather_only = false)
 {
   cudaStream_t st = h->stream;
   const LevelInfo& lv = h->lv;
@@ -1594,9 +1595,11 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out)
   const int storage = kB == 16 ? (int)MASPCG_INV_FP32 : h->cfg.inverse_storage;
   const int d0 = lv.dom_begin[1];
   const int coarse_domains = lv.domains - d0;
-  // coarse-level Galerkin sums
-  h->coarse64.resize((size_t)std::max(coarse_domains, 1) * kB * kB * 9);
-  MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * kB * kB * 9 * sizeof(double), st));
+  // coarse-level Galerkin sums (kept from the build when only gathering)
+  if (!gather_only) {
+    h->coarse64.resize((size_t)std::max(coarse_domains, 1) * kB * kB * 9);
+    MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * kB * kB * 9 * sizeof(double), st));
+  }
   CoarseArgs ca{};
   ca.pmr = h->pmr.get();
   ca.prefix_orig = h->prefix_orig.get();
@@ -1618,7 +1621,7 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out)
   ca.fem_off = h->fem_off;
   ca.c0 = c0;
   ca.coarse64 = h->coarse64.get();
-  if (items > 0) {
+  if (items > 0 && !gather_only) {
     k_coarse_assemble<kB><<<ceil_div((long long)items * 32, 256), 256, 0, st>>>(ca);
     MLAUNCHED(h);
   }
@@ -1640,7 +1643,8 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out)
   fa.failed = h->failed.get() + 3;
   fa.assembled = assembled_out;
   fa.coarse64 = h->coarse64.get();
-  if (kB == 32 && storage != MASPCG_INV_FP32) {
+  fa.gather_only = gather_only ? 1 : 0;
+  if (kB == 32 && storage != MASPCG_INV_FP32 && !gather_only) {
     h->dom64.resize((size_t)lv.domains * kPacked * 9);
     fa.dom64 = h->dom64.get();
   }
@@ -1668,6 +1672,10 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out)
   }
 #undef MAS_FACTOR
   MLAUNCHED(h);
+  if (gather_only) {
+    MCK(cudaGetLastError());
+    return;
+  }
   if constexpr (kB == 32) {
     if (storage == MASPCG_INV_BF16) {
       k_domain_chol16<__nv_bfloat16><<<grid, kCholThreads, 0, st>>>(fa);
@@ -1686,6 +1694,14 @@ void launch_factor(maspcg_handle* h, double* assembled_out)
     launch_factor_t<16>(h, assembled_out);
   else
     launch_factor_t<32>(h, assembled_out);
+}
+
+void gather_mas_domains(maspcg_handle* h, double* assembled_out)
+{
+  if (h->bank == 16)
+    launch_factor_t<16>(h, assembled_out, true);
+  else
+    launch_factor_t<32>(h, assembled_out, true);
 }
 
 namespace {

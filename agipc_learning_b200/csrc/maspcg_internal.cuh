@@ -173,6 +173,7 @@ struct FactorArgs {
   double* assembled;             // optional: packed FP64 domain matrices (reference layout)
   const double* coarse64;        // coarse-level domain matrices (32x32 blocks, row-major 3x3)
   double* dom64;                 // 16-bit storage: lower FP64 blocks per domain (kPacked x 9, row-major)
+  int gather_only;               // write `assembled` and stop: the stored inverses are left as they are
 };
 
 }  // namespace maspcg
@@ -297,6 +298,10 @@ void build_block_jacobi(maspcg_handle* h);
 
 // mas.cu
 void build_mas_domains(maspcg_handle* h, double* assembled_out);
+// The packed FP64 domain matrices the stored inverses were built from: level
+// 0 gathered again (a fixed order), the coarse levels from the build's own
+// Galerkin sums; neither the sums nor the inverses are recomputed.
+void gather_mas_domains(maspcg_handle* h, double* assembled_out);
 void mas_apply_launch(maspcg_handle* h, const void* r, void* z, bool finalize_rz);
 void decode_inverses(maspcg_handle* h, float* out_host);
 

@@ -63,7 +63,7 @@ class MasPcg:
 
     def __init__(self, *, tolerance=1e-4, max_iter_ratio=0.3, max_iterations=0, gate="rz", precision="reference",
                  inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8, flags=0,
-                 matrix="f32", replacement="reliable"):
+                 matrix="f32", replacement="periodic"):
         lib = N.load()
         cfg = N.Config()
         lib.maspcg_config_default(ctypes.byref(cfg))

@@ -464,8 +464,8 @@ def run_ours(args, world, rank, local):
     x_d = torch.zeros_like(b_d)
     stream = torch.cuda.Stream(device=dev)
 
-    def make(precision, inverse, gate="euclid", tol=1e-4):
-        m = MasPcg(gate=gate, precision=precision, inverse=inverse, tolerance=tol)
+    def make(precision, inverse, gate="euclid", tol=1e-4, **opts):
+        m = MasPcg(gate=gate, precision=precision, inverse=inverse, tolerance=tol, **opts)
         m.set_stream(stream.cuda_stream)
         m.set_graph(s.fem_count, s.node_offset, s.neighbor_start, s.neighbor_num, s.neighbor_list,
                     s.part_map_real, s.real_map_part)
@@ -511,6 +511,19 @@ def run_ours(args, world, rank, local):
 
     step_refresh(mixed)
     t_refresh, res_refresh = timed(mixed, step_refresh, args.steps)
+    # the opt-in forms of the mixed solve on the same step: exact FP64 sums in
+    # the SpMV, the BF16 remainder of the matrix, reliable-update replacement
+    variants = {}
+    for key, opts in (("reliable_replacement", {"replacement": "reliable"}),
+                      ("matrix_f32_sum64", {"matrix": "f32_sum64"}),
+                      ("matrix_f32_split", {"matrix": "f32_split"})):
+        mv = make("mixed", "bf16", **opts)
+        step(mv)
+        t_v, res_v = timed(mv, step, max(1, min(args.steps, 3)))
+        variants[key] = {"ms_per_solve": t_v / max(1, min(args.steps, 3)), "iterations": res_v["iterations"],
+                         "refinements": res_v["refinements"], "rel_res_true": res_v["rel_res_true"],
+                         "fp64_gate_met": bool(res_v["fp64_gate_met"]), "options": opts}
+        mv.close()
     # the reference's own stopping rule (rz gate) in the reference precision
     refp = make("reference", "fp32", gate="rz")
     step(refp)
@@ -572,10 +585,12 @@ def run_ours(args, world, rank, local):
         "dtype": "fp32 (matrix, vectors) + bf16 (MAS inverses) + fp64 (dots, residual)", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas": world, "gate": "FP64-verified ||b-Ax||/||b|| <= 1e-4",
                    "l2": "inputs larger than L2: FP64 BCOO %.0f MB uploaded per step" % (72 * len(s.rows) / 1e6),
-                   "precision": "mixed", "inverse": "bf16", "refinement_period": 16},
+                   "precision": "mixed", "inverse": "bf16", "refinement_period": 16, "matrix_form": "f32",
+                   "residual_replacement": "periodic"},
         "iterations": res_mixed["iterations"], "rel_res_true": res_mixed["rel_res_true"],
         "refinements": res_mixed["refinements"],
         "fp32_plain": fp32_report,
+        "mixed_variants": variants,
         "refresh_step": {"ms_per_solve": t_refresh / args.steps, "iterations": res_refresh["iterations"],
                          "rel_res_true": res_refresh["rel_res_true"],
                          "what": "maspcg_refresh_matrix_values (values only: merge values, domain factors) + solve"},

@@ -100,9 +100,11 @@ typedef struct {
  * iterations; always when the recursive gate is met, where the true residual
  * decides the stop).  x_hi += x_lo is folded at every check either way. */
 typedef enum {
-  MASPCG_REPLACE_RELIABLE = 0, /* once ||r|| has fallen to 0.1 of its largest value since the last replacement
-                                  (the default: a few replacements per decade of reduction) */
-  MASPCG_REPLACE_PERIODIC = 1  /* at every check */
+  MASPCG_REPLACE_PERIODIC = 0, /* at every check (the default: the fewest iterations on every system measured) */
+  MASPCG_REPLACE_RELIABLE = 1  /* once ||r|| has fallen to 0.1 of its largest value since the last replacement: a
+                                  few FP64 residuals per decade of reduction instead of one per period, but with
+                                  FP32 sums the recursive residual can drift between them (more iterations on
+                                  contact-dense systems) */
 } maspcg_replacement;
 
 /* How FP32 and MIXED precision store the iteration's matrix and sum its

@@ -172,12 +172,21 @@ def test_local_checks_reference_self_test_cases():
 @pytest.mark.parametrize("precision,inverse", [("reference", "fp32"), ("mixed", "bf16")])
 def test_local_diagnostics_match_oracle(cfg1_small, precision, inverse):
     """The checks on the handle's own domains against the oracle's
-    restatement of check_local_matrices on the same matrices."""
+    restatement of check_local_matrices on the same matrices: the matrices
+    the stored inverses were built from (level 0 gathered again, the coarse
+    levels from the build's own Galerkin sums), which neither the checks nor
+    the matrix read-back rebuild, so the preconditioner is unchanged."""
     s = cfg1_small
+    rng = np.random.default_rng(2)
+    r = rng.standard_normal(3 * s.nb)
     with MasPcg.from_system(s, precision=precision, inverse=inverse) as m:
+        inv0 = m.domain_inverses()
+        z0 = m.apply_preconditioner(r)
         d = m.local_diagnostics(per_domain=True)
         p64 = m.domain_matrices()
         inv = m.domain_inverses()
+        z1 = m.apply_preconditioner(r)
+    assert np.array_equal(inv0, inv) and np.array_equal(z0, z1)
     o = oracle.local_checks(p64, inv)
     assert d["matrix_count"] == len(o)
     for g, c in zip(d["domains"], o):
