@@ -316,6 +316,26 @@ def test_hybrid_full_scale_mixed_precision_converges(cfg2_full, inverse):
     assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) <= 1e-4
 
 
+def test_iteration_cap_and_nonpositive_curvature_statuses(cfg0):
+    """PCGSolver::pcg's other exits: the iteration cap (max_iterations
+    counts the initial apply, as max_iter does) and p.Ap <= 0 on a negative
+    definite system (no preconditioner, so r.z stays positive and the first
+    curvature test fires).  The handle stays usable after both."""
+    s = cfg0
+    with MasPcg.from_system(s, gate="euclid", max_iterations=5) as m:
+        _, res = m.solve(s.b)
+        assert res["status_name"] == "iteration_cap" and res["iterations"] == 5, res
+    with MasPcg(preconditioner="none", gate="euclid") as m:
+        m.set_matrix(-s.vals, s.rows, s.cols, s.nb, s.fem_offset, s.abd_bodies)
+        m.build()
+        _, res = m.solve(s.b)
+        assert res["status_name"] == "nonpositive_curvature" and res["iterations"] <= 2, res
+        m.set_matrix(s.vals, s.rows, s.cols, s.nb, s.fem_offset, s.abd_bodies)
+        m.build()
+        _, res = m.solve(s.b)
+        assert res["status_name"] in ("converged", "iteration_cap"), res
+
+
 def test_nonfinite_rhs_reports_status_without_fault(cfg0):
     s = cfg0
     b = s.b.copy()
