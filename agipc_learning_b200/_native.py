@@ -39,7 +39,6 @@ FLAG_APPLY_DIRECT = 4
 FLAG_SEQUENTIAL_COARSE = 8
 FLAG_FUSED_HEAD = 16
 FLAG_FUSED_UPDATE = 32
-FLAG_RECORDS_IN_L2 = 64
 
 INV_FP32 = 0
 INV_BF16 = 1

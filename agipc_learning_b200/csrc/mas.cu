@@ -1369,7 +1369,7 @@ template <typename TI, typename Tv, typename Tacc, bool kLevel0, int kBuf, bool 
 __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     k_apply_tma(ApplyArgs a, const Tv* __restrict__ r, Tv* z, Tacc* partial, int part_base, int total_parts, int mode,
                 PcgScalars* s, int g_begin, int g_end, int* err, int coarse_add, int pair, FusedArgs fa,
-                double* partial_rr, int keep_in_l2)
+                double* partial_rr)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kApplyWarps][kBuf];
@@ -1382,16 +1382,6 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
   const int gw = blockIdx.x * kApplyWarps + lw;
   unsigned char* buf = smem + (size_t)lw * (kBuf * kBytes + kApplyScratch);
   const TI* inv = reinterpret_cast<const TI*>(a.inv);
-  // keep_in_l2 (MASPCG_FLAG_RECORDS_IN_L2): the records are copied with the
-  // evict_last policy, so between two applies they can stay in L2 while the
-  // SpMV streams the matrix past them with evict_first loads
-  const uint64_t policy = keep_in_l2 ? l2_evict_last_policy() : 0;
-  auto copy_record = [&](unsigned char* dst, const TI* src, uint64_t* b) {
-    if (keep_in_l2)
-      tma_bulk_g2s_policy(dst, src, kBytes, b, policy);
-    else
-      tma_bulk_g2s(dst, src, kBytes, b);
-  };
   if (lane == 0) {
 #pragma unroll
     for (int j = 0; j < kBuf; ++j) mbar_init(&bar[lw][j], 1);
@@ -1401,7 +1391,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
       const int gj = g_begin + gw + j * warps_total;
       if (gj < g_end) {
         mbar_expect_tx(&bar[lw][j], kBytes);
-        copy_record(buf + j * kBytes, inv + (size_t)gj * inv_elems<TI>(), &bar[lw][j]);
+        tma_bulk_g2s(buf + j * kBytes, inv + (size_t)gj * inv_elems<TI>(), kBytes, &bar[lw][j]);
       }
     }
   }
@@ -1461,7 +1451,7 @@ __global__ void __launch_bounds__(kApplyWarps * 32, kBuf == 1 ? 4 : 2)
     if (lane == 0 && gn < g_end) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&bar[lw][st], kBytes);
-      copy_record(buf + st * kBytes, inv + (size_t)gn * inv_elems<TI>(), &bar[lw][st]);
+      tma_bulk_g2s(buf + st * kBytes, inv + (size_t)gn * inv_elems<TI>(), kBytes, &bar[lw][st]);
     }
     if (kLevel0) {
       const int slot = kBank * g + lane;
@@ -1752,7 +1742,7 @@ void launch_apply_tma(maspcg_handle* h, const ApplyArgs& a, const Tv* r, Tv* z, 
     configured = true;
   }
   launch_pdl(h, kern, dim3(grid), dim3(kApplyWarps * 32), bytes, a, r, z, partial, part_base, total_parts, mode, s,
-             g_begin, g_end, h->failed.get() + 4, coarse_add, pair, fa, partial_rr, h->records_in_l2 ? 1 : 0);
+             g_begin, g_end, h->failed.get() + 4, coarse_add, pair, fa, partial_rr);
 }
 
 // CTAs of a staged apply over `domains` domains: one wave of resident CTAs.

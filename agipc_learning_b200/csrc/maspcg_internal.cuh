@@ -277,7 +277,6 @@ struct maspcg_handle {
   bool overlap_coarse = true;     // coarse levels beside the level-0 apply (off: MASPCG_FLAG_SEQUENTIAL_COARSE)
   int apply_variant = 2;          // 16-bit level-0 apply: 0 direct loads, 1 TMA-staged x2 buffers, 2 TMA-staged x1
   bool fuse_update = false;       // x / r update inside the apply kernels (MASPCG_FLAG_FUSED_UPDATE)
-  bool records_in_l2 = false;     // MASPCG_FLAG_RECORDS_IN_L2
   long long barrier_limit = 1ll << 24;  // grid-barrier wait bound (spins of 64 ns sleeps)
   int barrier_extra = 0;                // test hook: extra arrivals a grid barrier waits for
 };

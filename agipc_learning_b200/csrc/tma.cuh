@@ -33,26 +33,6 @@ __device__ __forceinline__ void tma_bulk_g2s(void* dst, const void* src, unsigne
       : "memory");
 }
 
-// L2 policy that marks the lines a copy brings in as last to evict
-// (createpolicy, applied to the whole copy).
-__device__ __forceinline__ uint64_t l2_evict_last_policy()
-{
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-
-// tma_bulk_g2s with an L2 cache policy.
-__device__ __forceinline__ void tma_bulk_g2s_policy(void* dst, const void* src, unsigned bytes, uint64_t* bar,
-                                                    uint64_t policy)
-{
-  asm volatile(
-      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
-      : "memory");
-}
-
 // Bounded wait for the phase `parity` of the barrier; false on expiry.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
 {

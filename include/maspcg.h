@@ -133,11 +133,9 @@ typedef enum {
                                           (always so in MASPCG_PREC_REFERENCE, whose r.z is then summed over
                                           the fine rows as the reference sums it) */
   MASPCG_FLAG_FUSED_HEAD = 16,         /* p update, SpMV and x/r update as one cooperative kernel with grid barriers */
-  MASPCG_FLAG_FUSED_UPDATE = 32,       /* FP32 / MIXED with MAS32: the x / r update run by the preconditioner's apply
+  MASPCG_FLAG_FUSED_UPDATE = 32        /* FP32 / MIXED with MAS32: the x / r update run by the preconditioner's apply
                                           kernels on their own rows instead of a kernel of its own (measured slower:
                                           the latency-bound apply kernels take longer than the update they absorb) */
-  MASPCG_FLAG_RECORDS_IN_L2 = 64       /* the 16-bit level-0 domain records are copied with an L2 evict_last policy,
-                                          so they can stay in L2 from one apply to the next */
 } maspcg_flags;
 
 typedef struct {
