@@ -44,7 +44,7 @@ INV_FP32 = 0
 INV_BF16 = 1
 INV_FP16 = 2
 MATRIX_F32 = 0
-MATRIX_F32_SUM64 = 1
+MATRIX_F32_ACCURATE = 1
 MATRIX_F32_SPLIT = 2
 REPLACE_PERIODIC = 0
 REPLACE_RELIABLE = 1

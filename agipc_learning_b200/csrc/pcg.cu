@@ -159,20 +159,35 @@ __device__ __forceinline__ void load_block_lo(const unsigned short* __restrict__
   for (int e = 0; e < 9; ++e) m[e] = __uint_as_float((uint32_t)__ldcs(b + 32 * e) << 16);
 }
 
-// Accumulator of the SpMV rows: FP64 for the FP64 matrix and for the FP32
-// forms with FP64 sums (each FP32 x FP32 product is exact in FP64).
+// Accumulator of the SpMV rows: the matrix's own type (FP32 tiles, FP64
+// matrix).  The FP32 forms with accurate sums add a low part beside it.
 template <typename Tm, int kForm>
-using SpmvAcc = typename std::conditional<std::is_same<Tm, float>::value && kForm == MASPCG_MATRIX_F32, float,
-                                          double>::type;
+using SpmvAcc = typename AccOf<Tm>::type;
+
+// hi + lo += a b with the product exact and the sum compensated: the
+// product's rounding error from one FMA, the sum's from TwoSum (Ogita, Rump
+// and Oishi's Dot2), so a row accumulates its products to about 2^-48 of the
+// sum of their magnitudes without leaving FP32.  The round-to-nearest
+// intrinsics keep the compiler from contracting the steps into FMAs, which
+// would change the error terms.
+__device__ __forceinline__ void dot2_add(float& hi, float& lo, float a, float b)
+{
+  const float p = __fmul_rn(a, b);
+  const float e = fmaf(a, b, -p);
+  const float s = __fadd_rn(hi, p);
+  const float bp = __fsub_rn(s, hi);
+  const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(p, bp));
+  hi = s;
+  lo = __fadd_rn(lo, __fadd_rn(err, e));
+}
 
 // Ap = A p for block rows [lo, nrows); returns this thread's share of p.Ap.
 // LPR lanes per block row and two row groups per thread in flight at once
 // (rows r and r + stride); each lane takes kPer blocks of each row per step
-// and issues all their loads before the arithmetic (kPer = 2 with FP32 sums;
-// 1 with FP64 sums, whose accumulators and converted operands take the
-// registers of the second pair).  kForm (FP32 tiles): the
-// maspcg_matrix_form, i.e. FP32 or FP64 sums, and with the split form the
-// BF16 remainder's products summed beside them in FP32.
+// and issues all their loads before the arithmetic.  kForm (FP32 tiles): the
+// maspcg_matrix_form, i.e. FP32 sums or compensated sums of exact products
+// (dot2_add), and with the split form the BF16 remainder's products added to
+// the low parts.
 template <typename Tm, typename Tv, typename Tacc, bool kTiled, int LPR, int kForm>
 __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const int* __restrict__ colidx,
                                           const Tm* __restrict__ val, const unsigned short* __restrict__ val_lo,
@@ -180,6 +195,7 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
 {
   using A = SpmvAcc<Tm, kForm>;
   constexpr bool kSplit = kTiled && kForm == MASPCG_MATRIX_F32_SPLIT;
+  constexpr bool kDot2 = kTiled && kForm != MASPCG_MATRIX_F32;  // compensated sums of exact products
   constexpr int kRows = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
   const int step = gridDim.x * kRows;
@@ -193,7 +209,7 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
   int nsa, nea, nsb, neb;
   extent(lo + blockIdx.x * kRows + threadIdx.x / LPR, nsa, nea);
   extent(lo + blockIdx.x * kRows + threadIdx.x / LPR + step, nsb, neb);
-  constexpr int kPer = std::is_same<A, double>::value && kTiled ? 1 : 2;
+  constexpr int kPer = 2;
   constexpr int kIn = 2 * kPer;  // blocks in flight per step
   for (int row0 = lo + blockIdx.x * kRows; row0 < nrows; row0 += 2 * step) {
     const int ra = row0 + threadIdx.x / LPR, rb = ra + step;
@@ -201,7 +217,7 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
     extent(ra + 2 * step, nsa, nea);
     extent(rb + 2 * step, nsb, neb);
     A a[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    float al[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};  // kSplit: the remainder's products
+    float al[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};  // kDot2: the low parts (and the remainder's products)
     const int na = (ea - sa + kPer * LPR - 1) / (kPer * LPR), nbk = (eb - sb + kPer * LPR - 1) / (kPer * LPR);
     const int steps = max(__reduce_max_sync(kFull, (unsigned)na), __reduce_max_sync(kFull, (unsigned)nbk));
     for (int k = 0; k < steps; ++k) {
@@ -230,9 +246,18 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
       for (int j = 0; j < kIn; ++j) {
         const P4<Tv> x = ld_p4(p4, c[j]);
         A* o = a[j / kPer];
-        o[0] += (A)m[j][0] * (A)x.x + (A)m[j][1] * (A)x.y + (A)m[j][2] * (A)x.z;
-        o[1] += (A)m[j][3] * (A)x.x + (A)m[j][4] * (A)x.y + (A)m[j][5] * (A)x.z;
-        o[2] += (A)m[j][6] * (A)x.x + (A)m[j][7] * (A)x.y + (A)m[j][8] * (A)x.z;
+        if constexpr (kDot2) {
+          float* ol = al[j / kPer];
+          const float xv[3] = {(float)x.x, (float)x.y, (float)x.z};
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int t = 0; t < 3; ++t) dot2_add(o[i], ol[i], m[j][3 * i + t], xv[t]);
+        } else {
+          o[0] += (A)m[j][0] * (A)x.x + (A)m[j][1] * (A)x.y + (A)m[j][2] * (A)x.z;
+          o[1] += (A)m[j][3] * (A)x.x + (A)m[j][4] * (A)x.y + (A)m[j][5] * (A)x.z;
+          o[2] += (A)m[j][6] * (A)x.x + (A)m[j][7] * (A)x.y + (A)m[j][8] * (A)x.z;
+        }
         if constexpr (kSplit) {
           float w[9];
           if (in[j]) {
@@ -248,25 +273,27 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
         }
       }
     }
-    if constexpr (kSplit) {
+    // lane partial sums of each row component, added across the row's LPR
+    // lanes (in FP64 when the sums are compensated: hi + lo, then exact adds)
+    using R = typename std::conditional<kDot2, double, A>::type;
+    R u[2][3];
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
+    for (int h = 0; h < 2; ++h)
 #pragma unroll
-        for (int q = 0; q < 3; ++q) a[h][q] += (A)al[h][q];
-    }
+      for (int q = 0; q < 3; ++q) u[h][q] = kDot2 ? (R)a[h][q] + (R)al[h][q] : (R)a[h][q];
 #pragma unroll
     for (int h = 0; h < 2; ++h)
 #pragma unroll
       for (int o = LPR / 2; o > 0; o >>= 1) {
-        a[h][0] += __shfl_xor_sync(kFull, a[h][0], o, LPR);
-        a[h][1] += __shfl_xor_sync(kFull, a[h][1], o, LPR);
-        a[h][2] += __shfl_xor_sync(kFull, a[h][2], o, LPR);
+        u[h][0] += __shfl_xor_sync(kFull, u[h][0], o, LPR);
+        u[h][1] += __shfl_xor_sync(kFull, u[h][1], o, LPR);
+        u[h][2] += __shfl_xor_sync(kFull, u[h][2], o, LPR);
       }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int row = h ? rb : ra;
       if (row < nrows && sub < 3) {
-        const Tv y = (Tv)(sub == 0 ? a[h][0] : (sub == 1 ? a[h][1] : a[h][2]));
+        const Tv y = (Tv)(sub == 0 ? u[h][0] : (sub == 1 ? u[h][1] : u[h][2]));
         ap[3 * (size_t)row + sub] = y;
         const P4<Tv> pr = ld_p4(p4, row);
         const Tv pv = sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z);
@@ -858,7 +885,7 @@ struct Engine {
   void fused_head(PcgScalars* s)
   {
     switch (form()) {
-      case MASPCG_MATRIX_F32_SUM64: fused_head_f<MASPCG_MATRIX_F32_SUM64>(s); break;
+      case MASPCG_MATRIX_F32_ACCURATE: fused_head_f<MASPCG_MATRIX_F32_ACCURATE>(s); break;
       case MASPCG_MATRIX_F32_SPLIT: fused_head_f<MASPCG_MATRIX_F32_SPLIT>(s); break;
       default: fused_head_f<MASPCG_MATRIX_F32>(s); break;
     }
@@ -896,7 +923,7 @@ struct Engine {
   {
     if constexpr (std::is_same<Tm, float>::value) {
       switch (form()) {
-        case MASPCG_MATRIX_F32_SUM64: spmv_t<MASPCG_MATRIX_F32_SUM64>(s); return;
+        case MASPCG_MATRIX_F32_ACCURATE: spmv_t<MASPCG_MATRIX_F32_ACCURATE>(s); return;
         case MASPCG_MATRIX_F32_SPLIT: spmv_t<MASPCG_MATRIX_F32_SPLIT>(s); return;
         default: break;
       }

@@ -515,7 +515,7 @@ def run_ours(args, world, rank, local):
     # the SpMV, the BF16 remainder of the matrix, reliable-update replacement
     variants = {}
     for key, opts in (("reliable_replacement", {"replacement": "reliable"}),
-                      ("matrix_f32_sum64", {"matrix": "f32_sum64"}),
+                      ("matrix_f32_accurate", {"matrix": "f32_accurate", "replacement": "reliable"}),
                       ("matrix_f32_split", {"matrix": "f32_split"})):
         mv = make("mixed", "bf16", **opts)
         step(mv)

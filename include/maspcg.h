@@ -110,17 +110,19 @@ typedef enum {
 /* How FP32 and MIXED precision store the iteration's matrix and sum its
  * products (maspcg_config.matrix_form).  The reference precision always runs
  * the FP64 matrix with FP64 sums, and the affine-body rows always take the
- * FP64 matrix.  A product of two FP32 numbers is exact in FP64, so
- * MASPCG_MATRIX_F32_SUM64 computes the FP32-valued operator A32 p to FP64
- * accuracy before the single rounding of the result: on stiff contact rows
+ * FP64 matrix.  MASPCG_MATRIX_F32_ACCURATE forms each FP32 x FP32 product
+ * exactly (its rounding error from one FMA) and sums them compensated in
+ * pairs of FP32 numbers (Ogita, Rump and Oishi's Dot2), so the FP32-valued
+ * operator A32 p is computed to about 2^-48 of the sum of the terms'
+ * magnitudes before the single rounding of the result: on stiff contact rows
  * (barrier blocks beside a soft mass term) FP32 sums lose more than the FP32
  * values themselves do. */
 typedef enum {
   MASPCG_MATRIX_F32 = 0,       /* FP32 values, products and sums (the default: the fewest instructions) */
-  MASPCG_MATRIX_F32_SUM64 = 1, /* FP32 values; exact products summed in FP64 */
+  MASPCG_MATRIX_F32_ACCURATE = 1, /* FP32 values; exact products, compensated sums */
   MASPCG_MATRIX_F32_SPLIT = 2  /* FP32 values plus BF16 values of the remainder A - A32, so the operator is A to
                                   about 2^-32 relative: for systems whose stiffness spread FP32 values cannot
-                                  carry (18 more bytes per block); sums as MASPCG_MATRIX_F32_SUM64 */
+                                  carry (18 more bytes per block); sums as MASPCG_MATRIX_F32_ACCURATE */
 } maspcg_matrix_form;
 
 /* Kernel-schedule choices (bits of maspcg_config.flags); results do not depend

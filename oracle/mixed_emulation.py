@@ -18,7 +18,7 @@ switched on or off:
   `period` iterations), or "none";
 * `beta`: "fr" (r.z ratio, the reference's) or "flexible" (Polak-Ribiere);
 * `sums` (with matrix="f32"): "f64" (exact products summed in FP64, the
-  library's MASPCG_MATRIX_F32_SUM64), "block32" (each 3x3 block's three row
+  library's MASPCG_MATRIX_F32_ACCURATE), "block32" (each 3x3 block's three row
   sums in FP32, products rounded, then FP64 across blocks) or "f32"
   (the same, and the blocks of a row added in FP32 in column order).  The
   FP32 forms round every product, where the GPU's fused multiply-adds round

@@ -48,15 +48,15 @@ def _abd_rows_mask(s):
 
 @pytest.mark.parametrize("which,precision,matrix", [("cfg1_small", "mixed", "f32"), ("cfg1_small", "fp32", "f32"),
                                                     ("hybrid", "mixed", "f32"), ("cfg1_small", "reference", "f32"),
-                                                    ("cfg1_small", "mixed", "f32_sum64"),
-                                                    ("hybrid", "mixed", "f32_sum64"),
+                                                    ("cfg1_small", "mixed", "f32_accurate"),
+                                                    ("hybrid", "mixed", "f32_accurate"),
                                                     ("cfg1_small", "mixed", "f32_split"),
                                                     ("hybrid", "fp32", "f32_split")])
 def test_working_spmv_against_oracle(which, precision, matrix, request):
     """The iteration's own product y = A p against the oracle, elementwise,
     with A32 and x32 the FP32-rounded matrix and vector the kernel reads:
     * f32 (FP32 sums): within 48 eps32 (|A32| |x32|);
-    * f32_sum64 (exact FP32 x FP32 products, FP64 sums, one rounding at the
+    * f32_accurate (exact FP32 x FP32 products, FP64 sums, one rounding at the
       end): |y - A32 x32| <= eps32 |A32 x32| + 1e-12 (|A32| |x32|);
     * f32_split (A32 plus the BF16 remainder, so the operator is A to about
       2^-32): |y - A x32| <= eps32 |A x32| + 2^-30 (|A| |x32|);
@@ -83,7 +83,7 @@ def test_working_spmv_against_oracle(which, precision, matrix, request):
         # the FP64 product of the rounded operands, plus the FP32 summation
         # error and the final rounding
         assert np.all(np.abs(y[fem] - ref[fem]) <= 48 * EPS32 * mag[fem] + 1e-300)
-    elif matrix == "f32_sum64":
+    elif matrix == "f32_accurate":
         assert np.all(np.abs(y[fem] - ref[fem]) <= EPS32 * np.abs(ref[fem]) + 1e-12 * mag[fem] + 1e-300)
     else:
         r64 = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x32)
@@ -177,7 +177,7 @@ def _solution_case(name):
 # replacement): the default FP32 sums take 740 iterations on the 24^3 contact
 # system (oracle 577; exact products with FP64 sums: 567) and 360 on the
 # 16-scale hybrid system (oracle 231; FP32 values plus the BF16 remainder: 240).
-_FORM = {"cfg0": "f32", "cfg1_24": "f32_sum64", "cfg1_40": "f32", "hybrid": "f32_split"}
+_FORM = {"cfg0": "f32", "cfg1_24": "f32_accurate", "cfg1_40": "f32", "hybrid": "f32_split"}
 
 
 @pytest.mark.parametrize("name", ["cfg0", "cfg1_24", "cfg1_40", "hybrid"])
@@ -211,7 +211,7 @@ def test_reliable_replacement(cfg1_40):
     true residual is formed a few times per decade of reduction instead of
     once every 16 iterations."""
     s = cfg1_40
-    cfg = dict(gate="euclid", precision="mixed", inverse="bf16", matrix="f32_sum64")
+    cfg = dict(gate="euclid", precision="mixed", inverse="bf16", matrix="f32_accurate")
     with MasPcg.from_system(s, replacement="reliable", **cfg) as m:
         _, rel = m.solve(s.b)
     with MasPcg.from_system(s, replacement="periodic", **cfg) as m:
