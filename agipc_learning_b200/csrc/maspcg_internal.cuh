@@ -138,6 +138,8 @@ struct PcgScalars {
   int barrier_extra;        // arrivals a grid barrier expects beyond the grid (test hook: > 0 never completes)
   double rr_peak;           // MIXED: largest r.r since the last residual replacement (b.b at the start)
   int replace_mode;         // MIXED: maspcg_replacement
+  int graph_launches;       // batches run by the device-side solve loop
+  int max_launches;         // ... and the most it may run
 };
 
 constexpr int kNeedTrue = 16;  // MIXED: recursive gate met or period end; true residual pending
@@ -267,6 +269,7 @@ struct maspcg_handle {
   cudaGraphExec_t graph_exec = nullptr;
   int graph_batch = 0;
   bool graph_dirty = true;
+  bool graph_loop = false;        // graph_exec runs the whole solve loop (a conditional WHILE node)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int grid_stream = 0;  // CTAs for grid-stride kernels
   long long kernel_launches = 0;  // this library's kernels launched on the handle

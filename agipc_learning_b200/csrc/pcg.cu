@@ -481,6 +481,14 @@ __global__ void __launch_bounds__(kTpb) k_iteration_head(ApplyArgs a, const int*
     gate_check(s, (double)total, mixed);
 }
 
+// The end of one batch inside the device-side solve loop: run the next batch
+// while the solve is running and the batch cap is not reached.
+__global__ void k_loop_condition(cudaGraphConditionalHandle handle, PcgScalars* s)
+{
+  const int n = ++s->graph_launches;
+  cudaGraphSetConditional(handle, (s->status == MASPCG_SOLVE_RUNNING && n < s->max_launches) ? 1u : 0u);
+}
+
 // MIXED: fold the FP32 correction into the FP64 iterate.
 __global__ void __launch_bounds__(kTpb) k_fold_x(double* xhi, float* xlo, int n, int force, const PcgScalars* s)
 {
@@ -965,6 +973,73 @@ struct Engine {
     MCK(cudaGetLastError());
   }
 
+  // The solve loop as one graph: a conditional WHILE node whose body is one
+  // batch followed by k_loop_condition, so the batches repeat on the device
+  // with no host round trip between them.  Where the driver does not take a
+  // conditional node, the graph is the batch alone and the host relaunches
+  // it after each status read.
+  void build_graph(int batch, PcgScalars* s)
+  {
+    cudaStream_t st = h->stream;
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+    h->graph_loop = false;
+    const long long launches_before = h->kernel_launches;
+    auto capture = [&](cudaGraph_t into, cudaGraphConditionalHandle handle, bool loop) -> cudaGraph_t {
+      cudaGraph_t g = nullptr;
+      if (loop)
+        MCK(cudaStreamBeginCaptureToGraph(st, into, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      else
+        MCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        record_batch(batch, s);
+        if (loop) {
+          k_loop_condition<<<1, 1, 0, st>>>(handle, s);
+          MLAUNCHED(h);
+          MCK(cudaGetLastError());
+        }
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g && !loop) cudaGraphDestroy(g);
+        h->kernel_launches = launches_before;
+        throw;
+      }
+      MCK(cudaStreamEndCapture(st, &g));
+      return g;
+    };
+    cudaGraph_t parent = nullptr;
+    bool loop = cudaGraphCreate(&parent, 0) == cudaSuccess;
+    cudaGraphConditionalHandle handle{};
+    cudaGraph_t body = nullptr;
+    if (loop) {
+      cudaGraphNodeParams p{};
+      p.type = cudaGraphNodeTypeConditional;
+      cudaGraphNode_t node;
+      loop = cudaGraphConditionalHandleCreate(&handle, parent, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+      if (loop) {
+        p.conditional.handle = handle;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        loop = cudaGraphAddNode(&node, parent, nullptr, 0, &p) == cudaSuccess;
+        if (loop) body = p.conditional.phGraph_out[0];
+      }
+      if (!loop) {
+        cudaGetLastError();  // the driver does not take conditional nodes: the host loop it is
+        cudaGraphDestroy(parent);
+        parent = nullptr;
+      }
+    }
+    cudaGraph_t g = loop ? (capture(body, handle, true), parent) : capture(nullptr, handle, false);
+    h->graph_kernels = h->kernel_launches - launches_before;
+    h->kernel_launches = launches_before;
+    const cudaError_t e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    MCK(e);
+    h->graph_loop = loop;
+    h->graph_batch = batch;
+    h->graph_dirty = false;
+  }
+
   // One graph = `batch` iterations.
   void record_batch(int batch, PcgScalars* s)
   {
@@ -1084,6 +1159,9 @@ struct Engine {
     init.status = MASPCG_SOLVE_RUNNING;
     init.max_iter = max_iter;
     init.replace_mode = h->cfg.residual_replacement;
+    init.graph_launches = 0;
+    init.max_launches = max_iter / (mixed ? std::max(1, h->cfg.refinement_period)
+                                          : std::max(1, h->cfg.iterations_per_launch)) + 4;
     init.gate = mixed ? MASPCG_GATE_EUCLID : h->cfg.gate;
     init.tol = h->cfg.tolerance;
     init.barrier_limit = h->barrier_limit;
@@ -1096,39 +1174,30 @@ struct Engine {
     precondition(V(h->vr), V(h->vz), 1, s, ovl);
     // graph of one batch
     const int batch = mixed ? std::max(1, h->cfg.refinement_period) : std::max(1, h->cfg.iterations_per_launch);
-    if (h->graph_dirty || h->graph_batch != batch) {
-      if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-      h->graph_exec = nullptr;
-      cudaGraph_t g = nullptr;
-      const long long launches_before = h->kernel_launches;
-      MCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      try {
-        record_batch(batch, s);
-      } catch (...) {
-        cudaStreamEndCapture(st, &g);
-        if (g) cudaGraphDestroy(g);
-        h->kernel_launches = launches_before;
-        throw;
-      }
-      MCK(cudaStreamEndCapture(st, &g));
-      h->graph_kernels = h->kernel_launches - launches_before;
-      h->kernel_launches = launches_before;
-      MCK(cudaGraphInstantiate(&h->graph_exec, g, 0));
-      cudaGraphDestroy(g);
-      h->graph_batch = batch;
-      h->graph_dirty = false;
-    }
+    if (h->graph_dirty || h->graph_batch != batch) build_graph(batch, s);
     int launches = 0;
     // The first status read also covers the initial apply.
     MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
     MCK(cudaStreamSynchronize(st));
     const int max_launches = max_iter / batch + 4;
-    while (h->h_scal->status == MASPCG_SOLVE_RUNNING && launches < max_launches) {
-      MCK(cudaGraphLaunch(h->graph_exec, st));
-      h->kernel_launches += h->graph_kernels;
-      ++launches;
-      MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
-      MCK(cudaStreamSynchronize(st));
+    if (h->graph_loop) {
+      // one launch: the batches repeat on the device until the status
+      // leaves RUNNING (or the cap), then one status read
+      if (h->h_scal->status == MASPCG_SOLVE_RUNNING) {
+        MCK(cudaGraphLaunch(h->graph_exec, st));
+        MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        MCK(cudaStreamSynchronize(st));
+        launches = h->h_scal->graph_launches;
+        h->kernel_launches += h->graph_kernels * launches;
+      }
+    } else {
+      while (h->h_scal->status == MASPCG_SOLVE_RUNNING && launches < max_launches) {
+        MCK(cudaGraphLaunch(h->graph_exec, st));
+        h->kernel_launches += h->graph_kernels;
+        ++launches;
+        MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        MCK(cudaStreamSynchronize(st));
+      }
     }
     {
       int terr = 0;
