@@ -46,6 +46,7 @@ INV_FP16 = 2
 MATRIX_F32 = 0
 MATRIX_F32_ACCURATE = 1
 MATRIX_F32_SPLIT = 2
+MATRIX_F32_COMPENSATED = 3
 REPLACE_PERIODIC = 0
 REPLACE_RELIABLE = 1
 

@@ -164,6 +164,16 @@ __device__ __forceinline__ void load_block_lo(const unsigned short* __restrict__
 template <typename Tm, int kForm>
 using SpmvAcc = typename AccOf<Tm>::type;
 
+// hi + lo += t, the sum's rounding error kept by TwoSum (round-to-nearest
+// intrinsics, so the compiler cannot contract the steps).
+__device__ __forceinline__ void two_sum_add(float& hi, float& lo, float t)
+{
+  const float s = __fadd_rn(hi, t);
+  const float bp = __fsub_rn(s, hi);
+  lo = __fadd_rn(lo, __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(t, bp)));
+  hi = s;
+}
+
 // hi + lo += a b with the product exact and the sum compensated: the
 // product's rounding error from one FMA, the sum's from TwoSum (Ogita, Rump
 // and Oishi's Dot2), so a row accumulates its products to about 2^-48 of the
@@ -195,7 +205,10 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
 {
   using A = SpmvAcc<Tm, kForm>;
   constexpr bool kSplit = kTiled && kForm == MASPCG_MATRIX_F32_SPLIT;
-  constexpr bool kDot2 = kTiled && kForm != MASPCG_MATRIX_F32;  // compensated sums of exact products
+  constexpr bool kDot2 = kTiled && kForm != MASPCG_MATRIX_F32;  // compensated sums (below)
+  // COMPENSATED: each block row's three products by an FP32 FMA chain, only
+  // the sum across blocks compensated; the other forms: every product exact
+  constexpr bool kBlockFma = kForm == MASPCG_MATRIX_F32_COMPENSATED;
   constexpr int kRows = kTpb / LPR;
   const int sub = threadIdx.x % LPR;
   const int step = gridDim.x * kRows;
@@ -250,9 +263,15 @@ __device__ __forceinline__ Tacc spmv_rows(const int* __restrict__ rowptr, const 
           float* ol = al[j / kPer];
           const float xv[3] = {(float)x.x, (float)x.y, (float)x.z};
 #pragma unroll
-          for (int i = 0; i < 3; ++i)
+          for (int i = 0; i < 3; ++i) {
+            if constexpr (kBlockFma) {
+              two_sum_add(o[i], ol[i], fmaf(m[j][3 * i], xv[0], fmaf(m[j][3 * i + 1], xv[1],
+                                                                     __fmul_rn(m[j][3 * i + 2], xv[2]))));
+            } else {
 #pragma unroll
-            for (int t = 0; t < 3; ++t) dot2_add(o[i], ol[i], m[j][3 * i + t], xv[t]);
+              for (int t = 0; t < 3; ++t) dot2_add(o[i], ol[i], m[j][3 * i + t], xv[t]);
+            }
+          }
         } else {
           o[0] += (A)m[j][0] * (A)x.x + (A)m[j][1] * (A)x.y + (A)m[j][2] * (A)x.z;
           o[1] += (A)m[j][3] * (A)x.x + (A)m[j][4] * (A)x.y + (A)m[j][5] * (A)x.z;
@@ -894,6 +913,7 @@ struct Engine {
   {
     switch (form()) {
       case MASPCG_MATRIX_F32_ACCURATE: fused_head_f<MASPCG_MATRIX_F32_ACCURATE>(s); break;
+      case MASPCG_MATRIX_F32_COMPENSATED: fused_head_f<MASPCG_MATRIX_F32_COMPENSATED>(s); break;
       case MASPCG_MATRIX_F32_SPLIT: fused_head_f<MASPCG_MATRIX_F32_SPLIT>(s); break;
       default: fused_head_f<MASPCG_MATRIX_F32>(s); break;
     }
@@ -933,6 +953,7 @@ struct Engine {
       switch (form()) {
         case MASPCG_MATRIX_F32_ACCURATE: spmv_t<MASPCG_MATRIX_F32_ACCURATE>(s); return;
         case MASPCG_MATRIX_F32_SPLIT: spmv_t<MASPCG_MATRIX_F32_SPLIT>(s); return;
+        case MASPCG_MATRIX_F32_COMPENSATED: spmv_t<MASPCG_MATRIX_F32_COMPENSATED>(s); return;
         default: break;
       }
     }

@@ -20,7 +20,8 @@ from . import _native as N
 _PREC = {"reference": N.PREC_REFERENCE, "fp32": N.PREC_FP32, "mixed": N.PREC_MIXED}
 _GATE = {"rz": N.GATE_RZ, "euclid": N.GATE_EUCLID}
 _INV = {"fp32": N.INV_FP32, "bf16": N.INV_BF16, "fp16": N.INV_FP16}
-_MATRIX = {"f32": N.MATRIX_F32, "f32_accurate": N.MATRIX_F32_ACCURATE, "f32_split": N.MATRIX_F32_SPLIT}
+_MATRIX = {"f32": N.MATRIX_F32, "f32_accurate": N.MATRIX_F32_ACCURATE, "f32_split": N.MATRIX_F32_SPLIT,
+           "f32_compensated": N.MATRIX_F32_COMPENSATED}
 _REPLACE = {"reliable": N.REPLACE_RELIABLE, "periodic": N.REPLACE_PERIODIC}
 _PC = {"mas32": N.PRECOND_MAS32, "cemas16": N.PRECOND_MAS16, "block_jacobi": N.PRECOND_BLOCK_JACOBI,
        "none": N.PRECOND_NONE}

@@ -516,6 +516,7 @@ def run_ours(args, world, rank, local):
     variants = {}
     for key, opts in (("reliable_replacement", {"replacement": "reliable"}),
                       ("matrix_f32_accurate", {"matrix": "f32_accurate", "replacement": "reliable"}),
+                      ("matrix_f32_compensated", {"matrix": "f32_compensated"}),
                       ("matrix_f32_split", {"matrix": "f32_split"})):
         mv = make("mixed", "bf16", **opts)
         step(mv)

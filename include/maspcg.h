@@ -120,9 +120,12 @@ typedef enum {
 typedef enum {
   MASPCG_MATRIX_F32 = 0,       /* FP32 values, products and sums (the default: the fewest instructions) */
   MASPCG_MATRIX_F32_ACCURATE = 1, /* FP32 values; exact products, compensated sums */
-  MASPCG_MATRIX_F32_SPLIT = 2  /* FP32 values plus BF16 values of the remainder A - A32, so the operator is A to
+  MASPCG_MATRIX_F32_SPLIT = 2, /* FP32 values plus BF16 values of the remainder A - A32, so the operator is A to
                                   about 2^-32 relative: for systems whose stiffness spread FP32 values cannot
                                   carry (18 more bytes per block); sums as MASPCG_MATRIX_F32_ACCURATE */
+  MASPCG_MATRIX_F32_COMPENSATED = 3 /* FP32 values; each block row's three products by FMA in FP32, the blocks of a
+                                       row summed compensated (TwoSum): cheaper than ACCURATE, enough for contact-
+                                       dense systems with periodic replacement */
 } maspcg_matrix_form;
 
 /* Kernel-schedule choices (bits of maspcg_config.flags); results do not depend
