@@ -1112,7 +1112,8 @@ struct Engine {
     MREQ(stage != 3 || mas || mas16, MASPCG_ERR_NOT_READY, "stage 3 needs a MAS preconditioner");
     MREQ(stage != 2 || mas, MASPCG_ERR_NOT_READY, "stage 2 needs a MAS32 preconditioner");
     MREQ(stage < 4 || stage > 6 || mas, MASPCG_ERR_NOT_READY, "stages 4-6 need a MAS32 preconditioner");
-    MREQ(stage >= 0 && stage <= 6, MASPCG_ERR_INVALID_ARGUMENT, "unknown stage");
+    MREQ(stage != 7 || mixed, MASPCG_ERR_NOT_READY, "stage 7 needs the mixed precision");
+    MREQ(stage >= 0 && stage <= 7, MASPCG_ERR_INVALID_ARGUMENT, "unknown stage");
     constexpr size_t kFlushBytes = 256u << 20;
     if (h->l2_flush.n < kFlushBytes) {
       h->l2_flush.resize(kFlushBytes);
@@ -1125,6 +1126,7 @@ struct Engine {
         case 1: precondition(V(h->vr), V(h->vz), 0, s); break;
         case 2: mas_level0_only<Tv, Tacc>(h, V(h->vr), V(h->vz), partial_rz(), gl0, s, -1); break;
         case 3: launch_factor(h, nullptr); break;
+        case 7: true_residual(s); break;
         default: mas_level0_only<Tv, Tacc>(h, V(h->vr), V(h->vz), partial_rz(), gl0, s, stage == 6 ? 0 : stage - 3);
       }
     };

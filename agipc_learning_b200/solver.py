@@ -383,7 +383,9 @@ class MasPcg:
 
     def time_stage(self, stage: int, repeats: int = 20) -> float:
         """Mean device ms of one stage (0 SpMV, 1 preconditioner, 2 MAS level-0
-        apply, 3 domain assembly + inversion) over `repeats` back-to-back runs."""
+        apply, 3 domain assembly + inversion, 4-6 level-0 apply variants, 7 the
+        mixed solve's FP64 residual replacement) over `repeats` runs, each
+        after an L2 eviction."""
         ms = ctypes.c_double()
         self._ck(self.lib.maspcg_time_stage(self.h, int(stage), int(repeats), ctypes.byref(ms)))
         return ms.value

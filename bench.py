@@ -563,6 +563,7 @@ def run_ours(args, world, rank, local):
     ms_prec = stage(1, 20)
     ms_l0 = stage(2, 20)
     ms_factor = stage(3, 3)
+    ms_replace = stage(7, 10)
     ms_l0_variants = {"tma_staged_x2": stage(4, 20), "tma_staged_x1": stage(5, 20), "direct_loads": stage(6, 20)}
     nbi, bf = info["internal_block_rows"], info["bcsr_blocks"]
     d0 = s.fem_count // 32 if s.fem_count % 32 == 0 else (s.fem_count + 31) // 32
@@ -601,6 +602,7 @@ def run_ours(args, world, rank, local):
                                         "gate": "reference rz gate |r.z| <= 1e-4 r0.z0, FP64 PCG + FP32 MAS"},
         "stages_ms": {"spmv": ms_spmv, "precondition": ms_prec, "mas_level0": ms_l0,
                       "mas_level0_variants": ms_l0_variants, "domain_factor": ms_factor,
+                      "residual_replacement": ms_replace,
                       "solve_device_ms": res_mixed["solve_ms"]},
         "stage_errors": stage_errors or None,
         "roofline": {"kernel": "k_spmv (BCSR SpMV + p.Ap, FP32 32-block tiles)", "bound": "hbm", "achieved": ach,

@@ -408,6 +408,8 @@ MASPCG_API maspcg_status maspcg_check_local_matrices(maspcg_handle* h, int count
  *      in shared memory by TMA bulk copies), two slots per warp
  *   5  the same with one slot per warp (more warps per SM; the solve's choice)
  *   6  the same apply with each record staged by per-lane 16-byte loads (no TMA)
+ *   7  MASPCG_PREC_MIXED only: the residual replacement, x_hi += x_lo and
+ *      r = b - A x_hi with the FP64 matrix (FP64 sums, FP32 copy of r)
  *   (stage 2 times the variant the solve uses; 4-6 exist to compare them)
  * Vector contents are left unspecified afterwards. */
 MASPCG_API maspcg_status maspcg_time_stage(maspcg_handle* h, int stage, int repeats, double* mean_ms);

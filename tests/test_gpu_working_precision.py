@@ -306,3 +306,21 @@ def test_full_size_mixed_solve_against_oracle():
     assert res["status_name"] == "converged" and res["fp64_gate_met"]
     assert abs(res["iterations"] - ro["iterations"]) <= max(2, int(0.1 * ro["iterations"]))
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-4
+
+
+def test_time_stage_residual_replacement(cfg1_small):
+    """maspcg_time_stage stage 7 runs the mixed solve's FP64 residual
+    replacement alone (x_hi fold + r = b - A x_hi), returns its device time
+    and leaves the handle usable: the next solve repeats the first one
+    exactly.  Other precisions have no replacement step and refuse it."""
+    s = cfg1_small
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16") as m:
+        x0, r0 = m.solve(s.b)
+        assert m.time_stage(7, 3) > 0.0
+        x1, r1 = m.solve(s.b)
+    assert r1["iterations"] == r0["iterations"]
+    assert np.array_equal(x0, x1)
+    with MasPcg.from_system(s, gate="euclid", precision="reference") as m:
+        m.solve(s.b)
+        with pytest.raises(N.MaspcgError):
+            m.time_stage(7, 1)
