@@ -332,3 +332,34 @@ def compare_hierarchy(g, o):
     assert np.array_equal(g["coarse_table"][:, :L - 1], o["coarse_table"][:, :L - 1])
     assert np.array_equal(g["prefix_original"], o["prefix_original"])
     assert g["total_clusters"] == o["total_clusters"]
+
+
+def load_cfg0_replay():
+    """The reference's CPU block-Jacobi replay of config 0 (tests/golden/cfg0_replay,
+    made by tests/golden/make_golden.py): (its report for the sample, the
+    SHA-256 of the exported snapshot arrays)."""
+    d = os.path.join(GOLDEN, "cfg0_replay")
+    report = json.load(open(os.path.join(d, "reference_cpu_replay.json")))["samples"][0]
+    return report, json.load(open(os.path.join(d, "manifest.json")))["sha256"]
+
+
+def cfg0_snapshot_sums():
+    """Config 0 regenerated and written as the golden generator writes it;
+    the SHA-256 of each array file."""
+    import importlib.util
+    import tempfile
+
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    with tempfile.TemporaryDirectory() as tmp:
+        return mg.cfg0_snapshot(os.path.join(tmp, "cfg0"))
+
+
+def direct_solution(s):
+    """x = A^-1 b by SciPy's sparse LU (the replay's --direct-reference)."""
+    from scipy.sparse.linalg import spsolve
+
+    from oracle.mixed_emulation import full_matrix
+
+    return spsolve(full_matrix(s).tocsc(), s.b)

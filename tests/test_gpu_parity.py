@@ -268,6 +268,24 @@ def test_block_jacobi_matches_oracle(cfg0):
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-5
 
 
+def test_block_jacobi_on_config0_against_the_reference_replay(cfg0):
+    """The GPU's block-Jacobi PCG (reference precision, Euclidean 1e-4) on
+    config 0 against the reference's own CPU replay of the same system
+    (replay_frozen_coarse.py:70-111, committed report): the replay's 300
+    iterations within one, the FP64 gate met, and the same direction error
+    against the sparse direct solution to 1%."""
+    report, _ = H.load_cfg0_replay()
+    with MasPcg.from_system(cfg0, preconditioner="block_jacobi", gate="euclid", precision="reference",
+                            tolerance=1e-4) as m:
+        x, res = m.solve(cfg0.b)
+    cpu = report["cpu_block_jacobi"]
+    assert abs(res["iterations"] - cpu["iterations"]) <= 1
+    assert res["rel_res_true"] <= 1e-4
+    xd = H.direct_solution(cfg0)
+    direction = np.linalg.norm(x - xd) / np.linalg.norm(xd)
+    assert direction == pytest.approx(report["direct_reference"]["cpu_relative_direction_error"], rel=1e-2)
+
+
 def test_hybrid_abd_fem_matches_oracle():
     s = synth.config_system(2, scale=16)
     xo, ro, _ = oracle.solve_system(s, gate=oracle.GATE_EUCLID)

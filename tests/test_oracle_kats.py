@@ -4,7 +4,9 @@ Pins: spmv self-test (spmv.cu:301-459), MAS32 hierarchy self-test
 (TraditionalMAS32Preconditioner.cu:257-427), local-diagnostics cases
 (:182-215), hierarchy_capacity asserts (tests/runtime_options_tests.cpp:33-36)
 and the 257-block coarse replay fixture with its published results
-(reports/agipc_reproduction/AGIPC_COARSE_MAS32_REPLAY.md:35-52).
+(reports/agipc_reproduction/AGIPC_COARSE_MAS32_REPLAY.md:35-52); config 0
+replayed by the reference's own CPU block-Jacobi PCG
+(reports/agipc_reproduction/replay_frozen_coarse.py:70-111).
 """
 import numpy as np
 import pytest
@@ -130,3 +132,25 @@ def test_full_bcsr_matches_symmetric_spmv():
     y = oracle.bcsr_spmv(rp, ci, fv, x)
     ref = oracle.sym_spmv(1.0, vals, rows, cols, x)
     assert np.max(np.abs(y - ref)) <= 1e-12
+
+
+def test_block_jacobi_on_config0_against_the_reference_replay():
+    """Config 0 written as a coarse snapshot and solved by the reference's own
+    CPU block-Jacobi PCG at the 1e-4 Euclidean gate (replay_frozen_coarse.py:
+    70-111; report committed by tests/golden/make_golden.py).  The regenerated
+    system hashes to the one the reference read, and the oracle's block-Jacobi
+    PCG takes the replay's iteration count, with its true residual and its
+    direction error against the sparse direct solution."""
+    from agipc_learning_b200 import synth
+
+    report, sums = H.load_cfg0_replay()
+    assert H.cfg0_snapshot_sums() == sums
+    s = synth.config_system(0)
+    x, res, _ = oracle.solve_system(s, precond=oracle.PRECOND_DIAG3, gate=oracle.GATE_EUCLID, tol=1e-4)
+    cpu = report["cpu_block_jacobi"]
+    assert cpu["converged"] and res["iterations"] == cpu["iterations"] == 300
+    # 300 iterations in another summation order: the residuals agree to 1e-3
+    assert res["rel_res_true"] == pytest.approx(cpu["relative_residual"], rel=1e-3)
+    xd = H.direct_solution(s)
+    direction = np.linalg.norm(x - xd) / np.linalg.norm(xd)
+    assert direction == pytest.approx(report["direct_reference"]["cpu_relative_direction_error"], rel=1e-3)
