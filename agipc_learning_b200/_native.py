@@ -56,7 +56,7 @@ SOLVE_STATUS = {0: "running", 1: "converged", 2: "iteration_cap", 3: "nonpositiv
 # every function declared in include/maspcg.h
 EXPORTS = (
     "maspcg_config_default", "maspcg_status_string", "maspcg_last_error", "maspcg_create", "maspcg_destroy",
-    "maspcg_set_stream", "maspcg_set_graph", "maspcg_set_contacts", "maspcg_set_matrix_bcoo",
+    "maspcg_set_stream", "maspcg_get_stream", "maspcg_set_graph", "maspcg_set_contacts", "maspcg_set_matrix_bcoo",
     "maspcg_build_preconditioner", "maspcg_solve", "maspcg_apply_preconditioner", "maspcg_spmv", "maspcg_get_info",
     "maspcg_get_hierarchy", "maspcg_get_bcsr", "maspcg_get_domain_inverses", "maspcg_get_domain_matrices",
     "maspcg_time_stage", "maspcg_residual_norms_noalloc", "maspcg_bcoo_gradient", "maspcg_convert_bcoo",
@@ -149,6 +149,7 @@ def load():
         "maspcg_create": (I, [ctypes.POINTER(Config), ctypes.POINTER(H)]),
         "maspcg_destroy": (I, [H]),
         "maspcg_set_stream": (I, [H, P]),
+        "maspcg_get_stream": (I, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "maspcg_set_graph": (I, [H, I, I, P, P, P, I, P, I, P]),
         "maspcg_set_contacts": (I, [H, P, I]),
         "maspcg_set_matrix_bcoo": (I, [H, P, P, P, I, I, I, I]),

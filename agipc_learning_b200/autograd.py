@@ -28,16 +28,10 @@ callers that build perturbed systems or already hold dL/dval.
 """
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 import torch
 
 from .solver import MasPcg
-
-
-def _ptr(t: torch.Tensor):
-    return ctypes.c_void_p(t.data_ptr())
 
 
 class NewtonSolveFunction(torch.autograd.Function):
@@ -101,9 +95,11 @@ class NewtonSolveModulusFunction(torch.autograd.Function):
             raise RuntimeError(f"adjoint solve did not converge: {res}")
         E = ctx.E.contiguous().to(torch.float64)
         gE = torch.empty_like(E)
-        solver._ck(solver.lib.maspcg_element_modulus_gradient(solver.h, int(E.shape[0]), int(ctx.bpt), _ptr(rows),
-                                                               _ptr(cols), _ptr(vals), _ptr(lam), _ptr(x), _ptr(E),
-                                                               _ptr(gE)))
+        a = [solver._arg(rows, np.int32), solver._arg(cols, np.int32), solver._arg(vals, np.float64),
+             solver._arg(lam, np.float64), solver._arg(x, np.float64), solver._arg(E, np.float64),
+             solver._arg(gE, np.float64, writable=True)]
+        solver._ck(solver.lib.maspcg_element_modulus_gradient(solver.h, int(E.shape[0]), int(ctx.bpt),
+                                                               *[q.ptr for q in a]))
         return gE, lam, None, None, None, None, None, None, None, None
 
 

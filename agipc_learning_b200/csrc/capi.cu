@@ -385,6 +385,13 @@ MASPCG_API maspcg_status maspcg_set_stream(maspcg_handle* h, void* stream)
   });
 }
 
+MASPCG_API maspcg_status maspcg_get_stream(const maspcg_handle* h, void** stream)
+{
+  if (!h || !stream) return MASPCG_ERR_INVALID_ARGUMENT;
+  *stream = static_cast<void*>(h->stream);
+  return MASPCG_OK;
+}
+
 MASPCG_API maspcg_status maspcg_set_graph(maspcg_handle* h, int vert_num, int collision_node_offset,
                                           const uint32_t* neighbor_start, const uint32_t* neighbor_num,
                                           const uint32_t* neighbor_list, int neighbor_list_size,

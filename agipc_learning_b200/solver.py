@@ -36,6 +36,7 @@ class _Arg:
 
     def __init__(self, a, np_dtype, writable=False):
         self.keep = None
+        self.device = None  # CUDA tensors: the device of the torch stream that produces / consumes them
         if a is None:
             self.ptr = None
             return
@@ -49,6 +50,7 @@ class _Arg:
                 a = a.to(want).contiguous()
             self.keep = a
             self.ptr = ctypes.c_void_p(a.data_ptr())
+            self.device = a.device if a.is_cuda else None
         else:
             arr = np.asarray(a)
             if arr.dtype != np_dtype or not arr.flags["C_CONTIGUOUS"]:
@@ -65,6 +67,7 @@ class MasPcg:
     def __init__(self, *, tolerance=1e-4, max_iter_ratio=0.3, max_iterations=0, gate="rz", precision="reference",
                  inverse="fp32", preconditioner="mas32", refinement_period=16, iterations_per_launch=8, flags=0,
                  matrix="f32", replacement="periodic"):
+        self._torch_args = []
         lib = N.load()
         cfg = N.Config()
         lib.maspcg_config_default(ctypes.byref(cfg))
@@ -108,7 +111,36 @@ class MasPcg:
         self.close()
 
     def _ck(self, status):
+        """Checks a call's status.  If the call took CUDA tensors, torch's
+        current stream first waits for the handle's stream (an event, no host
+        sync): torch work after the call sees the outputs, and tensors the call
+        read are not recycled by torch's allocator before the reads are done."""
+        pending, self._torch_args = self._torch_args, []
+        if pending:
+            import torch
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.ExternalStream(self._stream_ptr(), device=pending[0]))
+            torch.cuda.current_stream(pending[0]).wait_event(ev)
         N.check(status, self.h)
+
+    def _stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        N.check(self.lib.maspcg_get_stream(self.h, ctypes.byref(s)), self.h)
+        return s.value or 0
+
+    def _arg(self, a, np_dtype, writable=False) -> "_Arg":
+        """An argument for the next call.  A CUDA tensor may still be being
+        written by torch's current stream, and the library runs on its own
+        stream (non-blocking unless set_stream chose another): the handle's
+        stream waits for torch's first (an event, no host sync)."""
+        arg = _Arg(a, np_dtype, writable)
+        if arg.device is not None:
+            import torch
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream(arg.device))
+            torch.cuda.ExternalStream(self._stream_ptr(), device=arg.device).wait_event(ev)
+            self._torch_args.append(arg.device)
+        return arg
 
     # -- inputs
     def set_stream(self, stream_ptr: int | None):
@@ -116,9 +148,9 @@ class MasPcg:
 
     def set_graph(self, vert_num, node_offset, neighbor_start, neighbor_num, neighbor_list, part_map_real,
                   real_map_part):
-        a = [_Arg(neighbor_start, np.uint32), _Arg(neighbor_num, np.uint32),
-             _Arg(neighbor_list if len(neighbor_list) else np.zeros(1, np.uint32), np.uint32),
-             _Arg(part_map_real, np.int32), _Arg(real_map_part, np.int32)]
+        a = [self._arg(neighbor_start, np.uint32), self._arg(neighbor_num, np.uint32),
+             self._arg(neighbor_list if len(neighbor_list) else np.zeros(1, np.uint32), np.uint32),
+             self._arg(part_map_real, np.int32), self._arg(real_map_part, np.int32)]
         self._ck(self.lib.maspcg_set_graph(self.h, int(vert_num), int(node_offset), a[0].ptr, a[1].ptr, a[2].ptr,
                                            int(len(neighbor_list)), a[3].ptr, int(len(part_map_real)), a[4].ptr))
         self.nv = int(vert_num)
@@ -126,11 +158,11 @@ class MasPcg:
     def set_contacts(self, pairs):
         p = np.zeros((0, 4), np.int32) if pairs is None else pairs
         n = len(p)
-        arg = _Arg(p if n else np.zeros(4, np.int32), np.int32)
+        arg = self._arg(p if n else np.zeros(4, np.int32), np.int32)
         self._ck(self.lib.maspcg_set_contacts(self.h, arg.ptr, int(n)))
 
     def set_matrix(self, vals, rows, cols, block_rows, fem_offset=0, abd_bodies=0):
-        v, r, c = _Arg(vals, np.float64), _Arg(rows, np.int32), _Arg(cols, np.int32)
+        v, r, c = self._arg(vals, np.float64), self._arg(rows, np.int32), self._arg(cols, np.int32)
         self._ck(self.lib.maspcg_set_matrix_bcoo(self.h, v.ptr, r.ptr, c.ptr, int(len(rows)), int(block_rows),
                                                  int(fem_offset), int(abd_bodies)))
         self.nb = int(block_rows)
@@ -140,8 +172,8 @@ class MasPcg:
         """The subsystem triplets indices[t] of a larger list, indices minus
         `offset` (maspcg_set_matrix_bcoo_indexed); the gather runs on the
         device, so CUDA tensors stay on the device."""
-        v, r, c = _Arg(vals, np.float64), _Arg(rows, np.int32), _Arg(cols, np.int32)
-        ix = _Arg(indices, np.uint32)
+        v, r, c = self._arg(vals, np.float64), self._arg(rows, np.int32), self._arg(cols, np.int32)
+        ix = self._arg(indices, np.uint32)
         n = len(rows) if indices is None else len(indices)
         self._ck(self.lib.maspcg_set_matrix_bcoo_indexed(self.h, v.ptr, r.ptr, c.ptr, int(len(rows)), ix.ptr, int(n),
                                                          int(offset), int(block_rows), int(fem_offset),
@@ -156,12 +188,12 @@ class MasPcg:
         """New values for the blocks of the last set_matrix (same triplets, same
         order): merged values, domain matrices and inverses recomputed on the
         kept structure and hierarchy (maspcg_refresh_matrix_values)."""
-        self._ck(self.lib.maspcg_refresh_matrix_values(self.h, _Arg(vals, np.float64).ptr))
+        self._ck(self.lib.maspcg_refresh_matrix_values(self.h, self._arg(vals, np.float64).ptr))
 
     def refresh_values_indexed(self, vals, indices):
         """refresh_values with the values picked by index on the device
         (maspcg_refresh_matrix_values_indexed)."""
-        v, ix = _Arg(vals, np.float64), _Arg(indices, np.uint32)
+        v, ix = self._arg(vals, np.float64), self._arg(indices, np.uint32)
         self._ck(self.lib.maspcg_refresh_matrix_values_indexed(self.h, v.ptr, int(len(vals)), ix.ptr))
 
     def local_diagnostics(self, per_domain=False):
@@ -207,33 +239,33 @@ class MasPcg:
     def _out(self, out, n):
         if out is None:
             out = np.zeros(n, np.float64)
-        return out, _Arg(out, np.float64, writable=True)
+        return out, self._arg(out, np.float64, writable=True)
 
     def solve(self, b, x=None):
-        bx = _Arg(b, np.float64)
+        bx = self._arg(b, np.float64)
         x, xa = self._out(x, 3 * self.nb)
         res = N.Result()
         self._ck(self.lib.maspcg_solve(self.h, bx.ptr, xa.ptr, ctypes.byref(res)))
         return x, res.as_dict()
 
     def apply_preconditioner(self, r, z=None):
-        ra = _Arg(r, np.float64)
+        ra = self._arg(r, np.float64)
         z, za = self._out(z, 3 * self.nb)
         self._ck(self.lib.maspcg_apply_preconditioner(self.h, ra.ptr, za.ptr))
         return z
 
     def spmv(self, x, a=1.0, b=0.0, y=None):
-        xa = _Arg(x, np.float64)
+        xa = self._arg(x, np.float64)
         if y is None:
             y = np.zeros(3 * self.nb, np.float64)
-        ya = _Arg(y, np.float64, writable=True)
+        ya = self._arg(y, np.float64, writable=True)
         self._ck(self.lib.maspcg_spmv(self.h, float(a), xa.ptr, float(b), ya.ptr))
         return y
 
     def spmv_working(self, x, y=None):
         """y = A x as the PCG iteration's own SpMV kernel forms it, in the
         working precision (maspcg_spmv_working)."""
-        xa = _Arg(x, np.float64)
+        xa = self._arg(x, np.float64)
         y, ya = self._out(y, 3 * self.nb)
         self._ck(self.lib.maspcg_spmv_working(self.h, xa.ptr, ya.ptr))
         return y
@@ -242,8 +274,8 @@ class MasPcg:
         """Contact-pair dedup in place (maspcg_adjust_contact_triplets;
         adjust_fem_fem_contact_indices_kernel).  numpy arrays are adjusted in
         place and returned; CUDA tensors likewise."""
-        r, c, v = _Arg(rows, np.int32, True), _Arg(cols, np.int32, True), _Arg(values9, np.float64, True)
-        bd = _Arg(bd_type, np.int32)
+        r, c, v = self._arg(rows, np.int32, True), self._arg(cols, np.int32, True), self._arg(values9, np.float64, True)
+        bd = self._arg(bd_type, np.int32)
         self._ck(self.lib.maspcg_adjust_contact_triplets(self.h, int(len(rows)), r.ptr, c.ptr, v.ptr, bd.ptr,
                                                          int(len(bd_type)), int(fem_offset)))
         return rows, cols, values9
@@ -251,8 +283,8 @@ class MasPcg:
     def zero_boundary_triplets(self, rows, cols, values9, bd_type, index_offset):
         """Boundary blocks cleared in place (maspcg_zero_boundary_triplets;
         zero_fem_boundary_hessian_kernel)."""
-        r, c, v = _Arg(rows, np.int32), _Arg(cols, np.int32), _Arg(values9, np.float64, True)
-        bd = _Arg(bd_type, np.int32)
+        r, c, v = self._arg(rows, np.int32), self._arg(cols, np.int32), self._arg(values9, np.float64, True)
+        bd = self._arg(bd_type, np.int32)
         self._ck(self.lib.maspcg_zero_boundary_triplets(self.h, int(len(rows)), r.ptr, c.ptr, v.ptr, bd.ptr,
                                                         int(len(bd_type)), int(index_offset)))
         return values9
@@ -272,8 +304,8 @@ class MasPcg:
         order.  Returns (rows, cols, values9) trimmed to the unique count."""
         n = int(len(rows))
         ro, co, vo = self._outs(rows, n)
-        r, c, v = _Arg(rows, np.int32), _Arg(cols, np.int32), _Arg(values9, np.float64)
-        ra, ca, va = _Arg(ro, np.int32, True), _Arg(co, np.int32, True), _Arg(vo, np.float64, True)
+        r, c, v = self._arg(rows, np.int32), self._arg(cols, np.int32), self._arg(values9, np.float64)
+        ra, ca, va = self._arg(ro, np.int32, True), self._arg(co, np.int32, True), self._arg(vo, np.float64, True)
         cnt = ctypes.c_int()
         self._ck(self.lib.maspcg_convert_bcoo(self.h, v.ptr, r.ptr, c.ptr, n, va.ptr, ra.ptr, ca.ptr, ctypes.byref(cnt)))
         u = cnt.value
@@ -284,9 +316,9 @@ class MasPcg:
         GIPC::partitionContactHessian).  Returns (rows, cols, values9, counts[4])."""
         n = int(len(rows))
         ro, co, vo = self._outs(rows, n)
-        r, c, v = _Arg(rows, np.int32), _Arg(cols, np.int32), _Arg(values9, np.float64)
-        t = _Arg(type_hash, np.uint64)
-        ra, ca, va = _Arg(ro, np.int32, True), _Arg(co, np.int32, True), _Arg(vo, np.float64, True)
+        r, c, v = self._arg(rows, np.int32), self._arg(cols, np.int32), self._arg(values9, np.float64)
+        t = self._arg(type_hash, np.uint64)
+        ra, ca, va = self._arg(ro, np.int32, True), self._arg(co, np.int32, True), self._arg(vo, np.float64, True)
         counts = (ctypes.c_int * 4)()
         self._ck(self.lib.maspcg_partition_contact_triplets(self.h, v.ptr, r.ptr, c.ptr, t.ptr, n, va.ptr, ra.ptr,
                                                             ca.ptr, counts))
@@ -301,10 +333,10 @@ class MasPcg:
         nt, nv = len(tets), len(x) // 3
         grad = np.zeros(3 * nv) if gradient is None else np.ascontiguousarray(gradient, np.float64).copy()
         rows, cols, vals = np.zeros(10 * nt, np.int32), np.zeros(10 * nt, np.int32), np.zeros((10 * nt, 9))
-        a = [_Arg(tets, np.uint32), _Arg(x, np.float64), _Arg(dm_inverse, np.float64), _Arg(volume, np.float64),
-             _Arg(len_rate, np.float64), _Arg(vol_rate, np.float64)]
-        o = [_Arg(grad, np.float64, True), _Arg(rows, np.int32, True), _Arg(cols, np.int32, True),
-             _Arg(vals, np.float64, True)]
+        a = [self._arg(tets, np.uint32), self._arg(x, np.float64), self._arg(dm_inverse, np.float64), self._arg(volume, np.float64),
+             self._arg(len_rate, np.float64), self._arg(vol_rate, np.float64)]
+        o = [self._arg(grad, np.float64, True), self._arg(rows, np.int32, True), self._arg(cols, np.int32, True),
+             self._arg(vals, np.float64, True)]
         self._ck(self.lib.maspcg_fem_snk1_gradient_hessian(self.h, nt, a[0].ptr, nv, a[1].ptr, a[2].ptr, a[3].ptr,
                                                            a[4].ptr, a[5].ptr, float(dt), int(hessian_offset),
                                                            o[0].ptr, o[1].ptr, o[2].ptr, o[3].ptr))
@@ -313,11 +345,11 @@ class MasPcg:
     def bcoo_gradient(self, rows, cols, lam, x, out=None):
         """dL/d(values) of upper BCOO blocks for lam = A^-1 dL/dx (maspcg_bcoo_gradient)."""
         n = int(len(rows))
-        r, c = _Arg(rows, np.int32), _Arg(cols, np.int32)
-        la, xa = _Arg(lam, np.float64), _Arg(x, np.float64)
+        r, c = self._arg(rows, np.int32), self._arg(cols, np.int32)
+        la, xa = self._arg(lam, np.float64), self._arg(x, np.float64)
         if out is None:
             out = np.zeros((n, 9), np.float64)
-        oa = _Arg(out, np.float64, writable=True)
+        oa = self._arg(out, np.float64, writable=True)
         self._ck(self.lib.maspcg_bcoo_gradient(self.h, r.ptr, c.ptr, n, la.ptr, xa.ptr, oa.ptr))
         return out
 
@@ -337,8 +369,8 @@ class MasPcg:
         count = x2.shape[0]
         res = np.zeros(max(count, 1), np.float64)
         rhs = np.zeros(max(count, 1), np.float64)
-        self._ck(self.lib.maspcg_residual_norms_noalloc(self.h, int(count), ctypes.c_void_p(x2.data_ptr()),
-                                                        ctypes.c_void_p(b2.data_ptr()),
+        xa, ba = self._arg(x2, np.float64), self._arg(b2, np.float64)
+        self._ck(self.lib.maspcg_residual_norms_noalloc(self.h, int(count), xa.ptr, ba.ptr,
                                                         res.ctypes.data_as(ctypes.c_void_p),
                                                         rhs.ctypes.data_as(ctypes.c_void_p)))
         return res[:count], rhs[:count]

@@ -187,8 +187,14 @@ MASPCG_API const char* maspcg_last_error(const maspcg_handle* h);
  * linear_system/solver/pcg_solver.h:7-24).  Uses the current CUDA device. */
 MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle** out);
 MASPCG_API maspcg_status maspcg_destroy(maspcg_handle* h);
-/* cudaStream_t; NULL selects the handle's own stream. */
+/* cudaStream_t; NULL selects the handle's own stream (created non-blocking:
+ * it does not wait for work on the legacy default stream, so a caller that
+ * produces inputs on another stream orders them before the call). */
 MASPCG_API maspcg_status maspcg_set_stream(maspcg_handle* h, void* stream);
+/* The cudaStream_t the handle's work runs on (no counterpart in the
+ * reference, which runs on the caller's stream): the one set by
+ * maspcg_set_stream, else the handle's own. */
+MASPCG_API maspcg_status maspcg_get_stream(const maspcg_handle* h, void** stream);
 
 /* Replaces TraditionalMAS32Preconditioner::initPreconditioner_Neighbor +
  * the caller's cudaMemcpy of d_neighborListInit / d_neighborStart /

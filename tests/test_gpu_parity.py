@@ -395,3 +395,30 @@ def test_fused_head_barrier_expiry_returns_error_and_handle_recovers(cfg0):
         m._ck(m.lib.maspcg_set_wait_test_hooks(m.h, 1 << 24, 0))
         x, res = m.solve(s.b)
     assert res["status_name"] == "converged" and res["fp64_gate_met"]
+
+
+def test_torch_inputs_are_ordered_before_the_library_reads_them(cfg0):
+    """CUDA tensors produced by torch work still queued on torch's stream: the
+    mirror makes the handle's stream wait for it (the handle's own stream is
+    non-blocking).  torch's stream is held ~25 ms by a spinning kernel, the
+    inputs are written by kernels queued behind it, and the library is called
+    at once: the refreshed values and the right-hand side it reads are the
+    finished ones (the solution is the one from host inputs)."""
+    import torch
+    s = cfg0
+    dev = torch.device("cuda")
+    with MasPcg.from_system(s, gate="euclid") as m:
+        x_host, r_host = m.solve(s.b)
+        vals_d = torch.from_numpy(np.ascontiguousarray(s.vals)).to(dev)
+        b_d = torch.from_numpy(s.b).to(dev)
+        torch.cuda.synchronize()
+        torch.cuda._sleep(50_000_000)
+        vals_late = vals_d * 1.0
+        b_late = b_d * 1.0
+        m.refresh_values(vals_late)
+        x = torch.empty_like(b_d)
+        _, res = m.solve(b_late, x)
+        # the refresh re-sums the coarse domain matrices (FP64 atomics): the
+        # same solve up to rounding
+        assert res["status_name"] == "converged" and abs(res["iterations"] - r_host["iterations"]) <= 1
+        assert np.linalg.norm(x.cpu().numpy() - x_host) <= 1e-6 * np.linalg.norm(x_host)
