@@ -336,6 +336,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
     MCK(cudaEventCreate(&h->ev0));
     MCK(cudaEventCreate(&h->ev1));
     MCK(cudaMallocHost(reinterpret_cast<void**>(&h->h_scal), sizeof(maspcg::PcgScalars)));
+    MCK(cudaMallocHost(reinterpret_cast<void**>(&h->h_err), sizeof(int)));
     h->scal.resize(1);
     h->grid_stream = 4 * h->sm_count;
     h->use_pdl = (c.flags & MASPCG_FLAG_PDL) != 0;
@@ -370,6 +371,7 @@ MASPCG_API maspcg_status maspcg_destroy(maspcg_handle* h)
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   if (h->h_scal) cudaFreeHost(h->h_scal);
+  if (h->h_err) cudaFreeHost(h->h_err);
   if (h->side_stream) cudaStreamDestroy(h->side_stream);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;

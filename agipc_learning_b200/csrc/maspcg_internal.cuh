@@ -250,6 +250,7 @@ struct maspcg_handle {
   maspcg::DBuf<unsigned char> vr2;  // second residual buffer of the fused x / r update (FP32 / MIXED)
   maspcg::DBuf<maspcg::PcgScalars> scal;
   maspcg::PcgScalars* h_scal = nullptr;  // pinned mirror
+  int* h_err = nullptr;                  // pinned mirror of the solve's kernel error word
   maspcg::DBuf<double> io_a, io_b;       // staging for host pointers / permutations
   maspcg::DBuf<unsigned char> l2_flush;  // maspcg_time_stage only: written between timed launches
   maspcg::DBuf<int> adj_rows, adj_cols;   // maspcg_bcoo_gradient staging for host arguments

@@ -1199,21 +1199,19 @@ struct Engine {
     const int batch = mixed ? std::max(1, h->cfg.refinement_period) : std::max(1, h->cfg.iterations_per_launch);
     if (h->graph_dirty || h->graph_batch != batch) build_graph(batch, s);
     int launches = 0;
-    // The first status read also covers the initial apply.
-    MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
-    MCK(cudaStreamSynchronize(st));
     const int max_launches = max_iter / batch + 4;
     if (h->graph_loop) {
-      // one launch: the batches repeat on the device until the status
-      // leaves RUNNING (or the cap), then one status read
-      if (h->h_scal->status == MASPCG_SOLVE_RUNNING) {
-        MCK(cudaGraphLaunch(h->graph_exec, st));
-        MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
-        MCK(cudaStreamSynchronize(st));
-        launches = h->h_scal->graph_launches;
-        h->kernel_launches += h->graph_kernels * launches;
-      }
+      // one launch: the batches repeat on the device until the status leaves
+      // RUNNING (or the cap).  Nothing waits on the host between the start
+      // and the end of the solve: a solve already stopped at entry runs one
+      // batch whose kernels return at once, and the status, the batch count
+      // and the error word are read once at the end.
+      MCK(cudaGraphLaunch(h->graph_exec, st));
     } else {
+      // the host loop: a status read before each launch (the first also
+      // covers the initial apply)
+      MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+      MCK(cudaStreamSynchronize(st));
       while (h->h_scal->status == MASPCG_SOLVE_RUNNING && launches < max_launches) {
         MCK(cudaGraphLaunch(h->graph_exec, st));
         h->kernel_launches += h->graph_kernels;
@@ -1221,14 +1219,6 @@ struct Engine {
         MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
         MCK(cudaStreamSynchronize(st));
       }
-    }
-    {
-      int terr = 0;
-      MCK(cudaMemcpy(&terr, h->failed.get() + 4, sizeof(int), cudaMemcpyDeviceToHost));
-      MREQ(terr == 0, MASPCG_ERR_CUDA,
-           terr == 2   ? "coarse-level dataflow queue overflow in the preconditioner apply"
-           : terr == 3 ? "a grid barrier of the fused iteration kernel timed out"
-                       : "a TMA mbarrier wait expired in the preconditioner apply");
     }
     // final FP64 iterate
     if (mixed) {
@@ -1241,7 +1231,19 @@ struct Engine {
     launch_spmv64(h, h->x64.get(), h->r64.get(), 1.0, 0.0);
     k_residual_norm<<<gstream, kTpb, 0, st>>>(h->b64.get(), h->r64.get(), n, h->partial_rz.get(), s); MLAUNCHED(h);
     MCK(cudaMemcpyAsync(h->h_scal, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    MCK(cudaMemcpyAsync(h->h_err, h->failed.get() + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
     MCK(cudaStreamSynchronize(st));
+    if (h->graph_loop) {
+      launches = h->h_scal->graph_launches;
+      h->kernel_launches += h->graph_kernels * launches;
+    }
+    {
+      const int terr = *h->h_err;
+      MREQ(terr == 0, MASPCG_ERR_CUDA,
+           terr == 2   ? "coarse-level dataflow queue overflow in the preconditioner apply"
+           : terr == 3 ? "a grid barrier of the fused iteration kernel timed out"
+                       : "a TMA mbarrier wait expired in the preconditioner apply");
+    }
     float ms = 0.f;
     MCK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (res) {
