@@ -342,27 +342,45 @@ __device__ __forceinline__ void spmv_finish(PcgScalars* s, double pap)
 // the iteration runs on the FP32 tiles: these are the affine-body rows, whose
 // 12x12 blocks carry the orthogonality stiffness (~1e7 on the diagonal)
 // beside rotation modes held only by the mass (~1e-4), a spread FP32 values
-// or sums cannot keep positive definite.
-template <typename Tv, typename Tacc, int LPR>
+// or sums cannot keep positive definite.  A body row also holds the coupling
+// blocks of every FEM vertex in contact with the body (tens of blocks), so
+// each row takes a whole warp, two blocks per lane per step with all their
+// loads issued before the arithmetic.
+template <typename Tv, typename Tacc>
 __device__ __forceinline__ Tacc spmv_rows_exact(const int* __restrict__ rowptr, const int* __restrict__ colidx,
                                                 const double* __restrict__ val64, const Tv* __restrict__ p4, Tv* ap,
                                                 int n64)
 {
+  constexpr int LPR = 32, kPer = 2;
   constexpr int kRows = kTpb / LPR;
-  const int sub = threadIdx.x % LPR;
+  const int lane = threadIdx.x % LPR;
   double dot = 0.0;
   for (int row0 = blockIdx.x * kRows; row0 < n64; row0 += gridDim.x * kRows) {
-    const int row = row0 + threadIdx.x / LPR;
+    const int row = row0 + threadIdx.x / LPR;  // warp-uniform
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     if (row < n64) {
-      const int re = __ldg(rowptr + row + 1);
-      for (int t = __ldg(rowptr + row) + sub; t < re; t += LPR) {
-        double m[9];
-        load_block<false>(val64, t, m);
-        const P4<Tv> x = ld_p4(p4, __ldcs(colidx + t));
-        a0 += m[0] * (double)x.x + m[1] * (double)x.y + m[2] * (double)x.z;
-        a1 += m[3] * (double)x.x + m[4] * (double)x.y + m[5] * (double)x.z;
-        a2 += m[6] * (double)x.x + m[7] * (double)x.y + m[8] * (double)x.z;
+      const int rs = __ldg(rowptr + row), re = __ldg(rowptr + row + 1);
+      for (int t0 = rs + lane; t0 < re; t0 += kPer * LPR) {
+        double m[kPer][9];
+        int c[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+          const int t = t0 + j * LPR;
+          c[j] = t < re ? __ldcs(colidx + t) : 0;
+          if (t < re) {
+            load_block<false>(val64, t, m[j]);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 9; ++e) m[j][e] = 0.0;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+          const P4<Tv> x = ld_p4(p4, c[j]);
+          a0 += m[j][0] * (double)x.x + m[j][1] * (double)x.y + m[j][2] * (double)x.z;
+          a1 += m[j][3] * (double)x.x + m[j][4] * (double)x.y + m[j][5] * (double)x.z;
+          a2 += m[j][6] * (double)x.x + m[j][7] * (double)x.y + m[j][8] * (double)x.z;
+        }
       }
     }
 #pragma unroll
@@ -371,11 +389,11 @@ __device__ __forceinline__ Tacc spmv_rows_exact(const int* __restrict__ rowptr, 
       a1 += __shfl_xor_sync(kFull, a1, o, LPR);
       a2 += __shfl_xor_sync(kFull, a2, o, LPR);
     }
-    if (row < n64 && sub < 3) {
-      const Tv y = (Tv)(sub == 0 ? a0 : (sub == 1 ? a1 : a2));
-      ap[3 * (size_t)row + sub] = y;
+    if (row < n64 && lane < 3) {
+      const Tv y = (Tv)(lane == 0 ? a0 : (lane == 1 ? a1 : a2));
+      ap[3 * (size_t)row + lane] = y;
       const P4<Tv> pr = ld_p4(p4, row);
-      dot += (double)(sub == 0 ? pr.x : (sub == 1 ? pr.y : pr.z)) * (double)y;
+      dot += (double)(lane == 0 ? pr.x : (lane == 1 ? pr.y : pr.z)) * (double)y;
     }
   }
   return (Tacc)dot;
@@ -390,7 +408,7 @@ __device__ __forceinline__ Tacc spmv_all(const int* __restrict__ rowptr, const i
                                          Tv* ap, int nrows)
 {
   Tacc dot = 0;
-  if (n64 > 0) dot = spmv_rows_exact<Tv, Tacc, LPR>(rowptr, colidx, val64, p4, ap, n64);
+  if (n64 > 0) dot = spmv_rows_exact<Tv, Tacc>(rowptr, colidx, val64, p4, ap, n64);
   return dot + spmv_rows<Tm, Tv, Tacc, kTiled, LPR, kForm>(rowptr, colidx, val, val_lo, p4, ap, n64, nrows);
 }
 
