@@ -392,7 +392,7 @@ def other_configs(args, stream, dev, peak):
     events, mean after a warm-up), iterations and FP64 residual in mixed
     precision (BF16 inverses) and in the reference precision, and the SpMV's
     HBM rate (the L2-resident small systems are latency-bound: their rate is
-    reported, not judged against the HBM peak)."""
+    reported, not compared with the HBM peak)."""
     import torch
     from agipc_learning_b200 import synth
     from agipc_learning_b200.solver import MasPcg

@@ -40,7 +40,7 @@ def test_emulation_sum_modes_agree_on_a_benign_system():
 def test_config2_iteration_count_is_bimodal_in_the_oracle():
     """The reference's FP64 PCG on config 2 (2,000 affine bodies + slab) takes
     490 iterations on its b and about 546 when b is perturbed by 1e-12
-    relative: the count the iteration bar is judged against depends on
+    relative: the count the iteration bar is measured against depends on
     rounding at the 1e-16 level on this system (and only on this one)."""
     import numpy as np
     s = synth.config_system(2)
