@@ -400,10 +400,11 @@ def test_fused_head_barrier_expiry_returns_error_and_handle_recovers(cfg0):
 def test_torch_inputs_are_ordered_before_the_library_reads_them(cfg0):
     """CUDA tensors produced by torch work still queued on torch's stream: the
     mirror makes the handle's stream wait for it (the handle's own stream is
-    non-blocking).  torch's stream is held ~25 ms by a spinning kernel, the
-    inputs are written by kernels queued behind it, and the library is called
-    at once: the refreshed values and the right-hand side it reads are the
-    finished ones (the solution is the one from host inputs)."""
+    non-blocking).  The inputs hold NaN, torch's stream is held ~25 ms by a
+    spinning kernel, the values are copied in by kernels queued behind it, and
+    the library is called at once: the refreshed values and the right-hand
+    side it reads are the finished ones (the solution is the one from host
+    inputs; unordered reads would see NaN)."""
     import torch
     s = cfg0
     dev = torch.device("cuda")
@@ -411,10 +412,13 @@ def test_torch_inputs_are_ordered_before_the_library_reads_them(cfg0):
         x_host, r_host = m.solve(s.b)
         vals_d = torch.from_numpy(np.ascontiguousarray(s.vals)).to(dev)
         b_d = torch.from_numpy(s.b).to(dev)
+        # the inputs hold NaN until the copies queued behind the held stream
+        vals_late = torch.full_like(vals_d, float("nan"))
+        b_late = torch.full_like(b_d, float("nan"))
         torch.cuda.synchronize()
         torch.cuda._sleep(50_000_000)
-        vals_late = vals_d * 1.0
-        b_late = b_d * 1.0
+        vals_late.copy_(vals_d)
+        b_late.copy_(b_d)
         m.refresh_values(vals_late)
         x = torch.empty_like(b_d)
         _, res = m.solve(b_late, x)
