@@ -125,7 +125,7 @@ class Info(ctypes.Structure):
                 ("vert_num", ctypes.c_int), ("part_map_size", ctypes.c_int),
                 ("going_next_capacity", ctypes.c_longlong), ("internal_block_rows", ctypes.c_int),
                 ("bcsr_blocks", ctypes.c_int), ("failed_domains", ctypes.c_int),
-                ("kernel_launches", ctypes.c_longlong)]
+                ("kernel_launches", ctypes.c_longlong), ("graph_captures", ctypes.c_longlong)]
 
 
 _LIB = None

@@ -536,7 +536,8 @@ void finish_set_matrix(maspcg_handle* h, const double* v, const int* r, const in
   MCK(cudaStreamSynchronize(h->stream));
   h->has_matrix = true;
   h->has_precond = false;
-  h->graph_dirty = true;
+  // no graph_dirty: the solve re-captures when the sizes or any buffer
+  // changed (graph_signature)
 }
 }  // namespace
 
@@ -580,7 +581,7 @@ MASPCG_API maspcg_status maspcg_set_matrix_bcoo_indexed(maspcg_handle* h, const 
     const double* sv = device_in(h, values9, 9 * (size_t)source_count, h->asm_vals);
     const int* sr = device_in(h, rows, (size_t)source_count, h->asm_rows);
     const int* sc = device_in(h, cols, (size_t)source_count, h->asm_cols);
-    DBuf<unsigned> idx_stage;
+    DBuf<unsigned> idx_stage{false};
     const unsigned* ix = indices ? device_in(h, (const unsigned*)indices, (size_t)n_blocks, idx_stage) : nullptr;
     h->in_vals.resize((size_t)9 * n_blocks);
     h->in_rows.resize((size_t)n_blocks);
@@ -604,7 +605,6 @@ MASPCG_API maspcg_status maspcg_build_preconditioner(maspcg_handle* h)
     maspcg::build_block_jacobi(h);
     MCK(cudaStreamSynchronize(h->stream));
     h->has_precond = true;
-    h->graph_dirty = true;
   });
 }
 
@@ -618,7 +618,6 @@ MASPCG_API maspcg_status maspcg_refresh_matrix_values(maspcg_handle* h, const do
     if (h->mas_layout) maspcg::build_mas_domains(h, nullptr);
     maspcg::build_block_jacobi(h);
     MCK(cudaStreamSynchronize(h->stream));
-    h->graph_dirty = true;
   });
 }
 
@@ -632,7 +631,7 @@ MASPCG_API maspcg_status maspcg_refresh_matrix_values_indexed(maspcg_handle* h, 
     const std::vector<uint32_t> ix = host_copy(h, indices, (size_t)h->n_in);
     for (uint32_t t : ix) MREQ((long long)t < source_count, MASPCG_ERR_INVALID_ARGUMENT, "index past the source");
     const double* sv = device_in(h, values9, 9 * (size_t)source_count, h->asm_vals);
-    DBuf<unsigned> idx_stage;
+    DBuf<unsigned> idx_stage{false};
     const unsigned* id = device_in(h, (const unsigned*)indices, (size_t)h->n_in, idx_stage);
     h->in_vals.resize((size_t)9 * h->n_in);
     maspcg::gather_triplets(h, h->n_in, id, nullptr, nullptr, sv, source_count, 0, nullptr, nullptr,
@@ -641,7 +640,6 @@ MASPCG_API maspcg_status maspcg_refresh_matrix_values_indexed(maspcg_handle* h, 
     if (h->mas_layout) maspcg::build_mas_domains(h, nullptr);
     maspcg::build_block_jacobi(h);
     MCK(cudaStreamSynchronize(h->stream));
-    h->graph_dirty = true;
   });
 }
 
@@ -741,6 +739,7 @@ MASPCG_API maspcg_status maspcg_get_info(maspcg_handle* h, maspcg_info* info)
     i.bcsr_blocks = h->nnzb;
     i.failed_domains = h->failed_domains;
     i.kernel_launches = h->kernel_launches;
+    i.graph_captures = h->graph_captures;
     *info = i;
   });
 }
@@ -797,7 +796,7 @@ MASPCG_API maspcg_status maspcg_get_domain_matrices(maspcg_handle* h, double* ou
     MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS preconditioner first");
     MREQ(out, MASPCG_ERR_INVALID_ARGUMENT, "null output");
     const size_t n = (size_t)h->lv.domains * (h->bank == 16 ? maspcg::kMas16Packed : maspcg::kPacked) * 9;
-    DBuf<double> tmp;
+    DBuf<double> tmp{false};
     tmp.resize(n);
     MCK(cudaMemsetAsync(tmp.get(), 0, n * sizeof(double), h->stream));
     maspcg::gather_mas_domains(h, tmp.get());
@@ -812,7 +811,7 @@ namespace {
 void run_local_checks(maspcg_handle* h, int count, int bank, const double* p64, const float* i32,
                       maspcg_domain_check* per_domain, maspcg_diagnostics* summary)
 {
-  DBuf<double> res;
+  DBuf<double> res{false};
   res.resize(7 * (size_t)std::max(count, 1));
   maspcg::check_local_matrices(h, count, bank, p64, i32, res.get());
   std::vector<double> r(7 * (size_t)count);
@@ -860,8 +859,8 @@ MASPCG_API maspcg_status maspcg_check_local_matrices(maspcg_handle* h, int count
     MREQ(count >= 0, MASPCG_ERR_INVALID_ARGUMENT, "negative count");
     MREQ(bank == 32 || bank == 16, MASPCG_ERR_INVALID_ARGUMENT, "bank must be 32 or 16");
     const size_t per = (size_t)bank * (bank + 1) / 2 * 9;
-    DBuf<double> a;
-    DBuf<float> b;
+    DBuf<double> a{false};
+    DBuf<float> b{false};
     const double* pa = count ? device_in(h, packed64, per * count, a) : nullptr;
     const float* pb = count ? device_in(h, inverse32, per * count, b) : nullptr;
     run_local_checks(h, count, bank, pa, pb, per_domain, summary);
@@ -875,13 +874,13 @@ MASPCG_API maspcg_status maspcg_local_diagnostics(maspcg_handle* h, maspcg_domai
     MREQ(h->has_precond && h->mas_layout, MASPCG_ERR_NOT_READY, "build a MAS preconditioner first");
     const int D = h->lv.domains;
     const size_t per = (size_t)(h->bank == 16 ? maspcg::kMas16Packed : maspcg::kPacked) * 9;
-    DBuf<double> a;
+    DBuf<double> a{false};
     a.resize(per * std::max(D, 1));
     MCK(cudaMemsetAsync(a.get(), 0, per * D * sizeof(double), h->stream));
     maspcg::gather_mas_domains(h, a.get());
     std::vector<float> inv(per * D);
     maspcg::decode_inverses(h, inv.data());
-    DBuf<float> b;
+    DBuf<float> b{false};
     b.resize(per * std::max(D, 1));
     MCK(cudaMemcpyAsync(b.get(), inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     run_local_checks(h, D, h->bank, a.get(), b.get(), per_domain, summary);
@@ -963,12 +962,12 @@ MASPCG_API maspcg_status maspcg_element_modulus_gradient(maspcg_handle* h, int n
     const size_t n = 3 * (size_t)h->nb;
     const int* r = device_in(h, rows, nblk, h->adj_rows);
     const int* c = device_in(h, cols, nblk, h->adj_cols);
-    DBuf<double> vstage, estage;
+    DBuf<double> vstage{false}, estage{false};
     const double* v = device_in(h, values9, 9 * nblk, vstage);
     const double* l = device_in(h, lam, n, h->adj_lam);
     const double* xv = device_in(h, x, n, h->adj_x);
     const double* e = device_in(h, youngs, (size_t)n_tets, estage);
-    DBuf<double> gstage;
+    DBuf<double> gstage{false};
     double* g = device_out(grad_youngs, (size_t)n_tets, gstage);
     maspcg::modulus_gradient(h, r, c, v, n_tets, blocks_per_tet, l, xv, e, g);
     copy_back(h, grad_youngs, (const double*)g, (size_t)n_tets);

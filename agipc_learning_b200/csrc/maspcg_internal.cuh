@@ -20,6 +20,7 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstring>
 #include <utility>
 #include <stdexcept>
@@ -84,19 +85,30 @@ struct Error : std::runtime_error {
     if (!(cond)) throw ::maspcg::Error((status), (msg)); \
   } while (0)
 
-// Grow-only device buffer.
+// Counts device-buffer (re)allocations and releases in the process: a
+// captured solve graph holds buffer addresses, so a graph captured at one
+// count is reused only while the count is unchanged.
+inline std::atomic<unsigned long long> g_buf_epoch{0};
+
+// Grow-only device buffer.  A function-local temporary, which no solve graph
+// can hold, is made uncounted (DBuf<T> b{false}).
 template <typename T>
 struct DBuf {
   T* p = nullptr;
   size_t cap = 0;
   size_t n = 0;
+  bool counted = true;  // (re)allocations advance g_buf_epoch
   DBuf() = default;
+  explicit DBuf(bool count) : counted(count) {}
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   void release()
   {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      if (counted) ++g_buf_epoch;
+    }
     p = nullptr;
     cap = n = 0;
   }
@@ -108,6 +120,7 @@ struct DBuf {
       if (p) cudaFree(p);
       p = nullptr;
       cap = 0;
+      if (counted) ++g_buf_epoch;
       if (need) {
         MCK(cudaMalloc(reinterpret_cast<void**>(&p), need * sizeof(T)));
         cap = need;
@@ -269,6 +282,8 @@ struct maspcg_handle {
   maspcg::DBuf<double> fem_x, fem_dminv, fem_vol, fem_len, fem_volr, fem_grad;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_batch = 0;
+  std::vector<unsigned long long> graph_sig;  // what graph_exec was captured against (graph_signature)
+  long long graph_captures = 0;               // solve graphs captured and instantiated
   bool graph_dirty = true;
   bool graph_loop = false;        // graph_exec runs the whole solve loop (a conditional WHILE node)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -797,6 +797,36 @@ __global__ void __launch_bounds__(kTpb) k_update_xr_fused(FusedArgs fa, int nrow
 
 // ----------------------------------------------------------------- engine --
 
+// Everything a captured solve graph depends on besides device data: the
+// buffer allocation count (addresses), the stream, the sizes, the level table
+// of the hierarchy, the configuration and the launch options.  A graph is
+// re-captured only when this changes (or graph_dirty is set), so a Newton
+// step that refreshes values or rebuilds the preconditioner on the same
+// structure reuses it.
+std::vector<unsigned long long> graph_signature(const maspcg_handle* h)
+{
+  std::vector<unsigned long long> s = {g_buf_epoch.load(), (unsigned long long)(uintptr_t)h->stream,
+                                       (unsigned long long)h->nb, (unsigned long long)h->nb_int,
+                                       (unsigned long long)h->n_in, (unsigned long long)h->nnzb,
+                                       (unsigned long long)h->fem_off, (unsigned long long)h->abd_bodies,
+                                       (unsigned long long)h->c0, (unsigned long long)h->mas_layout,
+                                       (unsigned long long)h->has_precond, (unsigned long long)h->use_pdl,
+                                       (unsigned long long)h->fused_head, (unsigned long long)h->overlap_coarse,
+                                       (unsigned long long)h->apply_variant, (unsigned long long)h->fuse_update,
+                                       (unsigned long long)h->nv, (unsigned long long)h->bank};
+  auto bytes = [&s](const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; i += 8) {
+      unsigned long long w = 0;
+      std::memcpy(&w, c + i, std::min<size_t>(8, n - i));
+      s.push_back(w);
+    }
+  };
+  bytes(&h->cfg, sizeof(h->cfg));
+  bytes(&h->lv, sizeof(h->lv));
+  return s;
+}
+
 template <typename Tm, typename Tv, typename Tacc>
 struct Engine {
   maspcg_handle* h;
@@ -1077,6 +1107,8 @@ struct Engine {
     h->graph_loop = loop;
     h->graph_batch = batch;
     h->graph_dirty = false;
+    h->graph_sig = graph_signature(h);
+    ++h->graph_captures;
   }
 
   // One graph = `batch` iterations.
@@ -1215,7 +1247,7 @@ struct Engine {
     precondition(V(h->vr), V(h->vz), 1, s, ovl);
     // graph of one batch
     const int batch = mixed ? std::max(1, h->cfg.refinement_period) : std::max(1, h->cfg.iterations_per_launch);
-    if (h->graph_dirty || h->graph_batch != batch) build_graph(batch, s);
+    if (h->graph_dirty || h->graph_batch != batch || graph_signature(h) != h->graph_sig) build_graph(batch, s);
     int launches = 0;
     const int max_launches = max_iter / batch + 4;
     if (h->graph_loop) {

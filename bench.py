@@ -487,18 +487,22 @@ def run_ours(args, world, rank, local):
         _, res = m.solve(b_d, x_d)
         return res
 
-    def timed(m, fn, k):
+    def timed(m, fn, k, steps_ms=None):
+        """k steps between two events on the library's stream; with a list,
+        also each step's own time (an event after every step)."""
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(k + 1)]
+        ev[0].record(stream)
         res = None
-        for _ in range(k):
+        for i in range(k):
             res = fn(m)
-        e1.record(stream)
+            ev[i + 1].record(stream)
         torch.cuda.synchronize()
-        return max_over_ranks(e0.elapsed_time(e1), dist, dev), res
+        if steps_ms is not None:
+            steps_ms.extend(round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(k))
+        return max_over_ranks(ev[0].elapsed_time(ev[k]), dist, dev), res
 
     mixed = make("mixed", "bf16")
     plain = make("fp32", "fp32")
@@ -506,8 +510,9 @@ def run_ours(args, world, rank, local):
         step(mixed)
         step(plain)
     launches0 = mixed.info()["kernel_launches"]
+    step_ms = []
     with ClockSampler(local) as clk:
-        t_mixed, res_mixed = timed(mixed, step, args.steps)
+        t_mixed, res_mixed = timed(mixed, step, args.steps, step_ms)
     launches = mixed.info()["kernel_launches"] - launches0
     t_plain, res_plain = timed(plain, step, args.steps)
     fp32_report = fp32_comparison(make, step, timed, t_mixed, res_mixed, t_plain, res_plain, args.steps)
@@ -592,7 +597,7 @@ def run_ours(args, world, rank, local):
     value = job_ms_per_solve(t_mixed, world, args.steps)
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_mixed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": t_mixed / args.steps, "step_ms": step_ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 (matrix, vectors) + bf16 (MAS inverses) + fp64 (dots, residual)", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas": world, "gate": "FP64-verified ||b-Ax||/||b|| <= 1e-4",
                    "l2": "inputs larger than L2: FP64 BCOO %.0f MB uploaded per step" % (72 * len(s.rows) / 1e6),

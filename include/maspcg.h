@@ -322,6 +322,9 @@ typedef struct {
   int failed_domains;    /* domains whose elimination met a pivot <= 0 */
   long long kernel_launches; /* kernels of this library launched on the handle so far
                                 (graph launches count every kernel node) */
+  long long graph_captures;  /* solve graphs captured and instantiated so far: a solve
+                                re-captures only when buffers, sizes, the hierarchy's
+                                level table, the configuration or the stream changed */
 } maspcg_info;
 
 MASPCG_API maspcg_status maspcg_get_info(maspcg_handle* h, maspcg_info* info);

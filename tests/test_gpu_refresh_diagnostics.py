@@ -195,3 +195,33 @@ def test_local_diagnostics_match_oracle(cfg1_small, precision, inverse):
         assert g["minimum_local_diagonal"] == pytest.approx(c["minimum_local_diagonal"], rel=1e-12)
         assert g["inverse_residual"] == pytest.approx(c["inverse_residual"], rel=1e-6, abs=1e-12)
     assert d["passed"] == all(c["local_spd"] and c["inverse_spd"] and c["inverse_residual"] <= 1e-3 for c in o)
+
+
+def test_solve_graph_is_reused_across_newton_steps(cfg1_small):
+    """A Newton step on the same structure (set_matrix + build, or a values
+    refresh) reuses the captured solve graph: maspcg_info.graph_captures stays
+    at one, and every solve gives the first one's answer.  A new stream is
+    captured anew."""
+    s = cfg1_small
+    with MasPcg.from_system(s, gate="euclid", precision="mixed", inverse="bf16") as m:
+        x0, r0 = m.solve(s.b)
+        assert m.info()["graph_captures"] == 1
+        for _ in range(2):
+            m.set_matrix(s.vals, s.rows, s.cols, s.nb, s.fem_offset, s.abd_bodies)
+            m.build()
+            x1, r1 = m.solve(s.b)
+            # the rebuild re-sums the coarse domain matrices (FP64 atomics):
+            # the same solve up to rounding
+            assert r1["status_name"] == "converged" and abs(r1["iterations"] - r0["iterations"]) <= 1
+            assert np.linalg.norm(x1 - x0) <= 1e-6 * np.linalg.norm(x0)
+        m.refresh_values(s.vals)
+        x2, r2 = m.solve(s.b)
+        assert r2["status_name"] == "converged" and np.linalg.norm(x2 - x0) <= 1e-6 * np.linalg.norm(x0)
+        assert m.info()["graph_captures"] == 1
+        import torch
+        st = torch.cuda.Stream()
+        m.set_stream(st.cuda_stream)
+        x3, r3 = m.solve(s.b)
+        assert m.info()["graph_captures"] == 2
+        assert np.linalg.norm(x3 - x0) <= 1e-6 * np.linalg.norm(x0)
+        m.set_stream(None)
