@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(1024, 1) k_domain_factor(FactorArgs a, int dom
 // shared memory only, so the thread layout is free.
 constexpr int kCholThreads = 544;  // 528 lower blocks in 17 warps
 template <typename TI>
-__global__ void __launch_bounds__(kCholThreads, 2) k_domain_chol16(FactorArgs a)
+__global__ void __launch_bounds__(kCholThreads, 2) k_domain_chol16(FactorArgs a, int dom_offset)
 {
   __shared__ double dinv[kBank][9];      // L_qq^-1 (lower, row-major), kept for W below
   __shared__ double panel[2][kBank][9];  // L_wq
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(kCholThreads, 2) k_domain_chol16(FactorArgs a)
   __shared__ float sscale[96];
   __shared__ unsigned smax[96];
   __shared__ int fail;
-  const int g = blockIdx.x;
+  const int g = blockIdx.x + dom_offset;
   const bool act = threadIdx.x < kPacked;
   int w = -1, lane = -1;
   if (act) {
@@ -1596,10 +1596,7 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out, bool gather_only =
   const int d0 = lv.dom_begin[1];
   const int coarse_domains = lv.domains - d0;
   // coarse-level Galerkin sums (kept from the build when only gathering)
-  if (!gather_only) {
-    h->coarse64.resize((size_t)std::max(coarse_domains, 1) * kB * kB * 9);
-    MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * kB * kB * 9 * sizeof(double), st));
-  }
+  if (!gather_only) h->coarse64.resize((size_t)std::max(coarse_domains, 1) * kB * kB * 9);
   CoarseArgs ca{};
   ca.pmr = h->pmr.get();
   ca.prefix_orig = h->prefix_orig.get();
@@ -1621,9 +1618,23 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out, bool gather_only =
   ca.fem_off = h->fem_off;
   ca.c0 = c0;
   ca.coarse64 = h->coarse64.get();
-  if (items > 0 && !gather_only) {
-    k_coarse_assemble<kB><<<ceil_div((long long)items * 32, 256), 256, 0, st>>>(ca);
-    MLAUNCHED(h);
+  // The coarse sums feed only the coarse domains: with level-0 domains to
+  // factor they are assembled on the side stream meanwhile, and the coarse
+  // domains are factored after the join.
+  const bool split = !gather_only && items > 0 && d0 > 0 && coarse_domains > 0;
+  if (!gather_only) {
+    cudaStream_t cs = st;
+    if (split) {
+      MCK(cudaEventRecord(h->ev_fork, st));
+      MCK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+      cs = h->side_stream;
+    }
+    MCK(cudaMemsetAsync(h->coarse64.get(), 0, (size_t)coarse_domains * kB * kB * 9 * sizeof(double), cs));
+    if (items > 0) {
+      k_coarse_assemble<kB><<<ceil_div((long long)items * 32, 256), 256, 0, cs>>>(ca);
+      MLAUNCHED(h);
+    }
+    if (split) MCK(cudaEventRecord(h->ev_join, cs));
   }
   FactorArgs fa{};
   fa.lv = lv;
@@ -1648,42 +1659,49 @@ void launch_factor_t(maspcg_handle* h, double* assembled_out, bool gather_only =
     h->dom64.resize((size_t)lv.domains * kPacked * 9);
     fa.dom64 = h->dom64.get();
   }
-  const int grid = lv.domains;
-#define MAS_FACTOR(TI, ASM) k_domain_factor<TI, ASM, kB><<<grid, 32 * kB, 0, st>>>(fa, 0)
-  if constexpr (kB == 16) {
-    if (assembled_out)
-      MAS_FACTOR(float, true);
-    else
-      MAS_FACTOR(float, false);
-  } else if (assembled_out) {
-    if (storage == MASPCG_INV_FP32)
-      MAS_FACTOR(float, true);
-    else if (storage == MASPCG_INV_BF16)
-      MAS_FACTOR(__nv_bfloat16, true);
-    else
-      MAS_FACTOR(__half, true);
-  } else {
-    if (storage == MASPCG_INV_FP32)
-      MAS_FACTOR(float, false);
-    else if (storage == MASPCG_INV_BF16)
-      MAS_FACTOR(__nv_bfloat16, false);
-    else
-      MAS_FACTOR(__half, false);
-  }
-#undef MAS_FACTOR
-  MLAUNCHED(h);
-  if (gather_only) {
-    MCK(cudaGetLastError());
-    return;
-  }
-  if constexpr (kB == 32) {
-    if (storage == MASPCG_INV_BF16) {
-      k_domain_chol16<__nv_bfloat16><<<grid, kCholThreads, 0, st>>>(fa);
-      MLAUNCHED(h);
-    } else if (storage == MASPCG_INV_FP16) {
-      k_domain_chol16<__half><<<grid, kCholThreads, 0, st>>>(fa);
-      MLAUNCHED(h);
+  // domains [g0, g0 + n): gather / Gauss-Jordan, then the 16-bit Cholesky
+  auto factor = [&](int g0, int n) {
+    if (n <= 0) return;
+#define MAS_FACTOR(TI, ASM) k_domain_factor<TI, ASM, kB><<<n, 32 * kB, 0, st>>>(fa, g0)
+    if constexpr (kB == 16) {
+      if (assembled_out)
+        MAS_FACTOR(float, true);
+      else
+        MAS_FACTOR(float, false);
+    } else if (assembled_out) {
+      if (storage == MASPCG_INV_FP32)
+        MAS_FACTOR(float, true);
+      else if (storage == MASPCG_INV_BF16)
+        MAS_FACTOR(__nv_bfloat16, true);
+      else
+        MAS_FACTOR(__half, true);
+    } else {
+      if (storage == MASPCG_INV_FP32)
+        MAS_FACTOR(float, false);
+      else if (storage == MASPCG_INV_BF16)
+        MAS_FACTOR(__nv_bfloat16, false);
+      else
+        MAS_FACTOR(__half, false);
     }
+#undef MAS_FACTOR
+    MLAUNCHED(h);
+    if (gather_only) return;
+    if constexpr (kB == 32) {
+      if (storage == MASPCG_INV_BF16) {
+        k_domain_chol16<__nv_bfloat16><<<n, kCholThreads, 0, st>>>(fa, g0);
+        MLAUNCHED(h);
+      } else if (storage == MASPCG_INV_FP16) {
+        k_domain_chol16<__half><<<n, kCholThreads, 0, st>>>(fa, g0);
+        MLAUNCHED(h);
+      }
+    }
+  };
+  if (split) {
+    factor(0, d0);
+    MCK(cudaStreamWaitEvent(st, h->ev_join, 0));
+    factor(d0, lv.domains - d0);
+  } else {
+    factor(0, lv.domains);
   }
   MCK(cudaGetLastError());
 }
