@@ -39,6 +39,7 @@ FLAG_APPLY_DIRECT = 4
 FLAG_SEQUENTIAL_COARSE = 8
 FLAG_FUSED_HEAD = 16
 FLAG_FUSED_UPDATE = 32
+FLAG_HOST_LOOP = 64
 
 INV_FP32 = 0
 INV_BF16 = 1

@@ -311,7 +311,7 @@ MASPCG_API maspcg_status maspcg_create(const maspcg_config* cfg, maspcg_handle**
       c.inverse_storage < 0 || c.inverse_storage > 2 ||
       !(c.preconditioner == MASPCG_PRECOND_BLOCK_JACOBI || c.preconditioner == MASPCG_PRECOND_MAS32 ||
         c.preconditioner == MASPCG_PRECOND_MAS16 || c.preconditioner == MASPCG_PRECOND_NONE) ||
-      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~63) != 0 || c.matrix_form < 0 ||
+      c.max_iterations < 0 || !(c.max_iter_ratio >= 0) || (c.flags & ~127) != 0 || c.matrix_form < 0 ||
       c.matrix_form > 3 || c.residual_replacement < 0 || c.residual_replacement > 1 ||
       ((c.flags & MASPCG_FLAG_APPLY_STAGED2) && (c.flags & MASPCG_FLAG_APPLY_DIRECT))) {
     g_create_error = "invalid configuration";

@@ -1077,7 +1077,7 @@ struct Engine {
       return g;
     };
     cudaGraph_t parent = nullptr;
-    bool loop = cudaGraphCreate(&parent, 0) == cudaSuccess;
+    bool loop = (h->cfg.flags & MASPCG_FLAG_HOST_LOOP) == 0 && cudaGraphCreate(&parent, 0) == cudaSuccess;
     cudaGraphConditionalHandle handle{};
     cudaGraph_t body = nullptr;
     if (loop) {

@@ -138,9 +138,13 @@ typedef enum {
                                           (always so in MASPCG_PREC_REFERENCE, whose r.z is then summed over
                                           the fine rows as the reference sums it) */
   MASPCG_FLAG_FUSED_HEAD = 16,         /* p update, SpMV and x/r update as one cooperative kernel with grid barriers */
-  MASPCG_FLAG_FUSED_UPDATE = 32        /* FP32 / MIXED with MAS32: the x / r update run by the preconditioner's apply
+  MASPCG_FLAG_FUSED_UPDATE = 32,       /* FP32 / MIXED with MAS32: the x / r update run by the preconditioner's apply
                                           kernels on their own rows instead of a kernel of its own (measured slower:
                                           the latency-bound apply kernels take longer than the update they absorb) */
+  MASPCG_FLAG_HOST_LOOP = 64           /* the solve loop as a graph of one batch relaunched by the host after each
+                                          status read, instead of one graph with a conditional WHILE node (the path
+                                          drivers without conditional nodes take; per-kernel profilers cannot see
+                                          inside a graph with conditional nodes) */
 } maspcg_flags;
 
 typedef struct {

@@ -241,7 +241,7 @@ def test_mixed_solve_with_several_domains_per_warp(inverse):
 
 
 @pytest.mark.parametrize("flag", ["FLAG_FUSED_HEAD", "FLAG_PDL", "FLAG_SEQUENTIAL_COARSE", "FLAG_APPLY_STAGED2",
-                                  "FLAG_APPLY_DIRECT", "FLAG_FUSED_UPDATE"])
+                                  "FLAG_APPLY_DIRECT", "FLAG_FUSED_UPDATE", "FLAG_HOST_LOOP"])
 def test_schedule_flags_solve_the_same_system(flag):
     """Every kernel-schedule choice reaches the FP64-verified tolerance on a
     system with several domains per warp, in about the same iterations
@@ -255,6 +255,8 @@ def test_schedule_flags_solve_the_same_system(flag):
     assert res["status_name"] == "converged", res
     assert res["rel_res_true"] <= 1e-4
     assert abs(res["iterations"] - base["iterations"]) <= max(8, int(0.05 * base["iterations"]))
+    if flag == "FLAG_HOST_LOOP":  # the same kernels in the same order, only relaunched from the host
+        assert res["iterations"] == base["iterations"] and res["launches"] > 1
     Ax = oracle.sym_spmv(1.0, s.vals, s.rows, s.cols, x)
     assert np.linalg.norm(s.b - Ax) / np.linalg.norm(s.b) <= 1e-4
 
