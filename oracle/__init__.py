@@ -76,6 +76,7 @@ def lib(bank=32):
             "orc_adjust_contacts": (I, [I, P, P, P, P, I, I]),
             "orc_zero_boundary": (I, [I, P, P, P, P, I, I]),
             "orc_mas_set_inverses": (None, [P, P]),
+            "orc_direct_solve": (I, [I, I, P, P, P, P, P, ctypes.POINTER(LL)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -309,6 +310,23 @@ def bcsr_spmv(rowptr, col, vals, x):
     lib().orc_bcsr_spmv(len(rowptr) - 1, _p(_c(rowptr, np.int32)), _p(_c(col, np.int32)), _p(_c(vals, np.float64)),
                         _p(x), _p(y))
     return y
+
+
+def direct_solve(nb, rows, cols, vals, b, stats=None):
+    """x = A^-1 b in FP64 for the upper BCOO system: reverse Cuthill-McKee
+    ordering and an envelope Cholesky (orc_direct_solve).  Raises ValueError
+    on a non-positive pivot.  `stats` (a dict) receives the envelope size."""
+    x = np.zeros(3 * int(nb))
+    env = ctypes.c_longlong()
+    rc = lib().orc_direct_solve(int(nb), len(rows), _p(_c(rows, np.int32)), _p(_c(cols, np.int32)),
+                                _p(_c(vals, np.float64)), _p(_c(b, np.float64)), _p(x), ctypes.byref(env))
+    if rc == -1:
+        raise ValueError("orc_direct_solve: the matrix is not positive definite")
+    if rc != 0:
+        raise MemoryError("orc_direct_solve: out of memory")
+    if stats is not None:
+        stats["envelope"] = env.value
+    return x
 
 
 def compute_num_levels(n, bank=32):

@@ -1253,3 +1253,261 @@ int orc_pcg(const orc_pcg_opts* o, const double* vals9, const int* rows, const i
   free(pc.diag_inv); free(pc.abd_inv);
   return k;
 }
+
+
+/* ---- FP64 direct solve: reverse Cuthill-McKee + envelope Cholesky ----
+ *
+ * Ordering (Cuthill and McKee, 1969, reversed as George, 1971, recommends):
+ * per connected component of the block graph, a breadth-first search from a
+ * pseudo-peripheral node (George and Liu, 1979: start at a node of minimum
+ * degree, move to a minimum-degree node of the last level while the number
+ * of levels grows), neighbours visited in increasing degree; the whole order
+ * reversed.  The three scalars of a block stay together.
+ *
+ * Factorisation: row i of L is stored from its first nonzero column f(i) to
+ * the diagonal (the envelope of A under the ordering holds all of L's fill),
+ * and L_ij = (A_ij - sum_{k >= max(f(i), f(j))} L_ik L_jk) / L_jj row by row.
+ */
+static int cmp_int(const void* a, const void* b)
+{
+  const int x = *(const int*)a, y = *(const int*)b;
+  return (x > y) - (x < y);
+}
+
+/* Breadth-first levels from s over unvisited (mark == 0) nodes; returns the
+ * number of levels, fills `order` with the visit order and `last` with the
+ * first index of the last level.  Marks are reset before returning. */
+static int bfs_levels(int s, const int* ptr, const int* adj, int* mark, int* order, int* count, int* last)
+{
+  int head = 0, tail = 0, levels = 0;
+  order[tail++] = s;
+  mark[s] = 1;
+  int level_end = tail;
+  *last = 0;
+  while (head < tail) {
+    *last = head;
+    for (; head < level_end; ++head) {
+      const int u = order[head];
+      for (int q = ptr[u]; q < ptr[u + 1]; ++q)
+        if (!mark[adj[q]]) {
+          mark[adj[q]] = 1;
+          order[tail++] = adj[q];
+        }
+    }
+    level_end = tail;
+    ++levels;
+  }
+  for (int q = 0; q < tail; ++q) mark[order[q]] = 0;
+  *count = tail;
+  return levels;
+}
+
+static int rcm_order(int nb, int nblocks, const int* rows, const int* cols, int* perm)
+{
+  int* deg = (int*)calloc((size_t)nb + 1, sizeof(int));
+  int* ptr = (int*)malloc(sizeof(int) * ((size_t)nb + 1));
+  if (!deg || !ptr) return -2;
+  for (int k = 0; k < nblocks; ++k)
+    if (rows[k] != cols[k]) {
+      deg[rows[k]]++;
+      deg[cols[k]]++;
+    }
+  ptr[0] = 0;
+  for (int i = 0; i < nb; ++i) ptr[i + 1] = ptr[i] + deg[i];
+  int* adj = (int*)malloc(sizeof(int) * ((size_t)ptr[nb] + 1));
+  int* fill = (int*)calloc((size_t)nb, sizeof(int));
+  int* mark = (int*)calloc((size_t)nb, sizeof(int));
+  int* order = (int*)malloc(sizeof(int) * ((size_t)nb + 1));
+  int* nbr = (int*)malloc(sizeof(int) * ((size_t)nb + 1));
+  if (!adj || !fill || !mark || !order || !nbr) return -2;
+  for (int k = 0; k < nblocks; ++k)
+    if (rows[k] != cols[k]) {
+      adj[ptr[rows[k]] + fill[rows[k]]++] = cols[k];
+      adj[ptr[cols[k]] + fill[cols[k]]++] = rows[k];
+    }
+  /* sorted, unique neighbour lists; degree = unique neighbours */
+  for (int i = 0; i < nb; ++i) {
+    int* a = adj + ptr[i];
+    const int n = fill[i];
+    qsort(a, (size_t)n, sizeof(int), cmp_int);
+    int m = 0;
+    for (int q = 0; q < n; ++q)
+      if (m == 0 || a[q] != a[m - 1]) a[m++] = a[q];
+    deg[i] = m;
+  }
+  /* compact into ptr/adj with the unique lists */
+  {
+    int w = 0;
+    for (int i = 0; i < nb; ++i) {
+      const int s = ptr[i];
+      ptr[i] = w;
+      for (int q = 0; q < deg[i]; ++q) adj[w++] = adj[s + q];
+    }
+    ptr[nb] = w;
+  }
+  int* visited = (int*)calloc((size_t)nb, sizeof(int));
+  if (!visited) return -2;
+  int out = 0;
+  for (;;) {
+    /* an unvisited node of minimum degree starts the next component */
+    int s = -1;
+    for (int i = 0; i < nb; ++i)
+      if (!visited[i] && (s < 0 || deg[i] < deg[s])) s = i;
+    if (s < 0) break;
+    /* pseudo-peripheral node over the component (visited nodes are masked) */
+    for (int i = 0; i < nb; ++i) mark[i] = visited[i];
+    int count = 0, last = 0;
+    int levels = bfs_levels(s, ptr, adj, mark, order, &count, &last);
+    for (int it = 0; it < 16; ++it) {
+      int best = order[last];
+      for (int q = last; q < count; ++q)
+        if (deg[order[q]] < deg[best]) best = order[q];
+      int c2 = 0, l2 = 0;
+      const int lv2 = bfs_levels(best, ptr, adj, mark, order, &c2, &l2);
+      if (lv2 <= levels) break;
+      s = best;
+      levels = lv2;
+      count = c2;
+      last = l2;
+    }
+    /* Cuthill-McKee from s: neighbours in increasing degree (then index) */
+    int head = out, tail = out;
+    perm[tail++] = s;
+    visited[s] = 1;
+    while (head < tail) {
+      const int u = perm[head++];
+      int n = 0;
+      for (int q = ptr[u]; q < ptr[u + 1]; ++q)
+        if (!visited[adj[q]]) {
+          visited[adj[q]] = 1;
+          nbr[n++] = adj[q];
+        }
+      for (int a = 1; a < n; ++a) { /* insertion sort by (degree, index) */
+        const int v = nbr[a];
+        int b = a - 1;
+        while (b >= 0 && (deg[nbr[b]] > deg[v] || (deg[nbr[b]] == deg[v] && nbr[b] > v))) {
+          nbr[b + 1] = nbr[b];
+          --b;
+        }
+        nbr[b + 1] = v;
+      }
+      for (int a = 0; a < n; ++a) perm[tail++] = nbr[a];
+    }
+    out = tail;
+  }
+  for (int i = 0, j = nb - 1; i < j; ++i, --j) { /* reverse */
+    const int t = perm[i];
+    perm[i] = perm[j];
+    perm[j] = t;
+  }
+  free(deg);
+  free(ptr);
+  free(adj);
+  free(fill);
+  free(mark);
+  free(order);
+  free(nbr);
+  free(visited);
+  return 0;
+}
+
+int orc_direct_solve(int nb, int nblocks, const int* rows, const int* cols, const double* vals9, const double* b,
+                     double* x, long long* envelope_out)
+{
+  const int n = 3 * nb;
+  int* perm = (int*)malloc(sizeof(int) * ((size_t)nb + 1));
+  int* inv = (int*)malloc(sizeof(int) * ((size_t)nb + 1));
+  int* first = (int*)malloc(sizeof(int) * ((size_t)n + 1));
+  long long* off = (long long*)malloc(sizeof(long long) * ((size_t)n + 1));
+  if (!perm || !inv || !first || !off) return -2;
+  if (rcm_order(nb, nblocks, rows, cols, perm) != 0) return -2;
+  for (int k = 0; k < nb; ++k) inv[perm[k]] = k;
+  for (int i = 0; i < n; ++i) first[i] = i;
+  /* the envelope: first column of every row of the reordered lower triangle */
+  for (int k = 0; k < nblocks; ++k) {
+    const int pr = inv[rows[k]], pc = inv[cols[k]];
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) {
+        int i = 3 * pr + a, j = 3 * pc + c;
+        if (i < j) {
+          const int t = i;
+          i = j;
+          j = t;
+        }
+        if (j < first[i]) first[i] = j;
+      }
+  }
+  off[0] = 0;
+  for (int i = 0; i < n; ++i) off[i + 1] = off[i] + (i - first[i] + 1);
+  double* env = (double*)calloc((size_t)off[n], sizeof(double));
+  if (!env) return -2;
+  if (envelope_out) *envelope_out = off[n];
+  /* scatter A's lower triangle: a diagonal block adds each of its entries
+     once at its own position, an off-diagonal block stands for itself and
+     its transpose, which meet at one lower position */
+  for (int k = 0; k < nblocks; ++k) {
+    const int pr = inv[rows[k]], pc = inv[cols[k]];
+    const double* v = vals9 + 9 * (size_t)k;
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) {
+        int i = 3 * pr + a, j = 3 * pc + c;
+        if (rows[k] == cols[k] && i < j) continue; /* upper half of a diagonal block */
+        if (i < j) {
+          const int t = i;
+          i = j;
+          j = t;
+        }
+        env[off[i] + (j - first[i])] += v[a + 3 * c];
+      }
+  }
+  /* L L^T, row by row */
+  int status = 0;
+  for (int i = 0; i < n && status == 0; ++i) {
+    const int fi = first[i];
+    double* Li = env + off[i] - fi; /* Li[j] = L_ij, j in [fi, i] */
+    for (int j = fi; j < i; ++j) {
+      const int fj = first[j];
+      const double* Lj = env + off[j] - fj;
+      const int k0 = fi > fj ? fi : fj;
+      double s = Li[j];
+      for (int k = k0; k < j; ++k) s -= Li[k] * Lj[k];
+      Li[j] = s / Lj[j];
+    }
+    double d = Li[i];
+    for (int k = fi; k < i; ++k) d -= Li[k] * Li[k];
+    if (!(d > 0.0)) {
+      status = -1;
+      break;
+    }
+    Li[i] = sqrt(d);
+  }
+  if (status == 0) {
+    double* z = (double*)malloc(sizeof(double) * (size_t)n);
+    if (!z) {
+      free(env);
+      return -2;
+    }
+    for (int k = 0; k < nb; ++k)
+      for (int a = 0; a < 3; ++a) z[3 * k + a] = b[3 * (size_t)perm[k] + a];
+    for (int i = 0; i < n; ++i) { /* L y = P b */
+      const double* Li = env + off[i] - first[i];
+      double s = z[i];
+      for (int k = first[i]; k < i; ++k) s -= Li[k] * z[k];
+      z[i] = s / Li[i];
+    }
+    for (int i = n - 1; i >= 0; --i) { /* L^T z = y, by columns of L^T = rows of L */
+      const double* Li = env + off[i] - first[i];
+      z[i] /= Li[i];
+      for (int k = first[i]; k < i; ++k) z[k] -= Li[k] * z[i];
+    }
+    for (int k = 0; k < nb; ++k)
+      for (int a = 0; a < 3; ++a) x[3 * (size_t)perm[k] + a] = z[3 * k + a];
+    free(z);
+  }
+  free(env);
+  free(perm);
+  free(inv);
+  free(first);
+  free(off);
+  return status;
+}

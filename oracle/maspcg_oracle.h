@@ -195,6 +195,17 @@ int orc_pcg(const orc_pcg_opts* o, const double* vals9, const int* rows, const i
 
 int orc_num_threads(void);
 
+/* FP64 direct solve of the symmetric positive definite system given by its
+ * upper BCOO blocks (Eigen column-major 3x3 values; repeated blocks add):
+ * reverse Cuthill-McKee ordering of the block graph, envelope (skyline)
+ * Cholesky A = L L^T of the reordered scalar matrix, two triangular solves.
+ * The FP64 direct oracle at small sizes (the reference's own scripts use
+ * SciPy's sparse LU; Eigen's sparse Cholesky is not available here).
+ * Returns 0, -1 if a pivot is not positive, -2 if memory runs out.
+ * envelope_out (may be NULL) receives the number of stored entries of L. */
+int orc_direct_solve(int nb, int nblocks, const int* rows, const int* cols, const double* vals9, const double* b,
+                     double* x, long long* envelope_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,4 +1,5 @@
-"""The GPU solve against an FP64 sparse direct solve (SciPy SuperLU) of the
+"""The GPU solve against an FP64 sparse direct solve (SciPy SuperLU, and on
+the 20^3 system also the oracle's envelope Cholesky) of the
 20^3 system (both precisions, to 1e-12 and 1e-10) and of the hybrid ABD + FEM
 system scaled down (reference precision, 1e-8).  The solution error is
 bounded by the condition number times the residual; the hybrid system's
@@ -10,6 +11,7 @@ system this ill-conditioned."""
 import numpy as np
 import pytest
 
+import oracle
 from agipc_learning_b200 import synth
 from agipc_learning_b200.solver import MasPcg
 from tests.test_direct_cpu import sparse_from_upper
@@ -38,3 +40,7 @@ def test_solution_matches_direct_solve(which, precision, tol, drift, bound):
     assert res["status_name"] == "converged", res
     assert np.linalg.norm(A @ x - s.b) <= drift * tol * np.linalg.norm(s.b)
     assert np.linalg.norm(x - xd) <= bound * np.linalg.norm(xd)
+    if which == "cfg0":
+        # also against the oracle's own FP64 Cholesky (RCM + envelope)
+        xc = oracle.direct_solve(s.nb, s.rows, s.cols, s.vals, s.b)
+        assert np.linalg.norm(x - xc) <= bound * np.linalg.norm(xc)
